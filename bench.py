@@ -1,0 +1,399 @@
+#!/usr/bin/env python3
+"""Newton-step assembly benchmark: IGAP4STANDARD phys/ge at 64^3 quadratic elements.
+
+One step = one residual assembly (volume + Neumann + Dirichlet rows) followed by
+one tangent assembly (volume + Dirichlet row/column elimination) into the CSR
+arrays of the reference's AIJ pattern: the work snesiga_Residual +
+snesiga_Tangent do per Newton iteration (src/snesiga_Residual.c:13,
+src/snesiga_Tangent.c:13).  Synthetic, seeded input: 64^3 elements on the unit
+cube with interior knots perturbed by +-0.1h (seed 1), (lambda, mu, l) =
+(1, 1, 0.1) mapped onto par_mat, x=0 clamped / x=1 u_x = 0.01 X, state
+uniform in +-1e-3 (seed 0).
+
+  value     FP64 path, inputs resident in HBM, ms per assembly (device events)
+  mixed     FP32-built tangent + FP64 residual, same timing
+  e2e       FP64 path through the host-pointer C ABI (U in, R and CSR values out)
+  roofline  tangent volume kernel against the measured FP64 FMA peak
+  cpu_baseline  the reference's own assembly (oracle/_ref) on the host cores
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "Newton-step assembly ms & adjoint grads/s at 64^3, mixed vs FP64, 1xB200"
+
+# Algorithmic flops per element (4^3 Gauss points):
+#  tangent  64 * 2 * (30*81*10 + 81*81*10) = B^T D B with the dof-block-sparse B
+#  residual 64 * 2 * (27*30 + 27*30) + 64 * 270 (interpolation, test contraction, basis)
+TAN_ALG_FLOPS = 64 * 2 * (30 * 81 * 10 + 81 * 81 * 10)
+RES_ALG_FLOPS = 64 * (2 * (27 * 30 + 27 * 30) + 270)
+# flops the tangent kernel executes per element (rank-12 form, upper triangle):
+#  K += X^T Y (3321 x 12), X (972 x 9), Gamma (378 x 9), geometric block (243 x 4)
+TAN_EXEC_FLOPS = 64 * 2 * (3321 * 12 + 972 * 9 + 378 * 9 + 243 * 4)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=64, help="elements per side")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=4, help="elements per side of the CPU sample mesh")
+    return ap.parse_args()
+
+
+def workload(n):
+    from igap4standard_b200 import mesh
+    nelem = (n, n, n)
+    kn = mesh.knots_for(nelem, perturb=0.1, seed=1)
+    pm = mesh.par_mat_from_lame(1.0, 1.0, 0.1)
+    bc, pd = mesh.bc_config0()
+    return nelem, kn, pm, bc, pd
+
+
+def config_dict(n, ndof, nnz):
+    return {"workload": "phys/ge Newton-step assembly (residual+BCs, tangent+BCs into AIJ) %d^3 elements" % n,
+            "nelem": [n, n, n], "dofs": ndof, "nnz": nnz, "gauss_points": "4x4x4",
+            "knots": "open, interior perturbed +-0.1h (seed 1)", "material": "lambda=mu=1, l=0.1 mapped to par_mat",
+            "state": "uniform +-1e-3 (seed 0)",
+            "l2": "inputs larger than L2: every step writes the %.2f GB CSR value array" % (nnz * 8 / 1e9),
+            "parallelism": "replicas (one mesh per GPU)"}
+
+
+# ------------------------------------------------------------------ CPU side
+
+def _ref_sample_worker(args):
+    """One process: the reference's residual + tangent on an m^3 sample mesh."""
+    m, seed = args
+    sys.path.insert(0, REPO)
+    from oracle import ref
+    from igap4standard_b200 import mesh
+    nelem = (m, m, m)
+    kn = mesh.knots_for(nelem, perturb=0.1, seed=1)
+    pm = mesh.par_mat_from_lame(1.0, 1.0, 0.1)
+    bc, pd = mesh.bc_config0()
+    C = ref.case("ge", nelem, kn, pm, bc, np.zeros(9), pd, np.zeros(39))
+    U = np.random.default_rng(seed).uniform(-1e-3, 1e-3, C.ndof)
+    t0 = time.perf_counter()
+    C.residual(U)
+    t1 = time.perf_counter()
+    C.tangent(U)
+    t2 = time.perf_counter()
+    C.close()
+    return (t1 - t0, t2 - t1, m ** 3)
+
+
+class RefPool:
+    """Host-core pool running the reference's CPU assembly (spawned processes)."""
+
+    def __init__(self, procs):
+        import multiprocessing as mp
+        self.procs = procs
+        self.pool = mp.get_context("spawn").Pool(procs)
+
+    def sample(self, m):
+        t0 = time.perf_counter()
+        res = self.pool.map(_ref_sample_worker, [(m, i) for i in range(self.procs)])
+        wall = time.perf_counter() - t0
+        tr = np.mean([r[0] for r in res]) / res[0][2]
+        tt = np.mean([r[1] for r in res]) / res[0][2]
+        return tr, tt, wall
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def cpu_procs():
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    """--impl reference: the reference's own assembly on all host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    try:
+        from oracle import ref
+        if not ref.available():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_iga.so not built here"}))
+            return 0
+    except Exception as e:  # pragma: no cover
+        print(json.dumps({"impl": "reference", "unavailable": "oracle import failed: %s" % e}))
+        return 0
+    from igap4standard_b200 import mesh
+    n = args.n
+    nel = n ** 3
+    P = cpu_procs()
+    pool = RefPool(P)
+    m = args.cpu_sample
+    for _ in range(max(args.warmup, 0)):
+        pool.sample(m)
+    per = []
+    walls = []
+    for _ in range(args.steps):
+        tr, tt, wall = pool.sample(m)
+        per.append((tr, tt))
+        walls.append(wall)
+    pool.close()
+    tr = float(np.mean([p[0] for p in per]))
+    tt = float(np.mean([p[1] for p in per]))
+    ms = (tr + tt) * nel / P * 1e3
+    ndof, nnz = mesh.n_dof((n, n, n)), mesh.nnz_of((n, n, n))
+    sample = ("%d processes x %d^3-element mesh per step (residual+tangent, reference code), per-element time "
+              "extrapolated to %d^3 elements with %d processes in parallel (throughput mode, no MPI)" % (P, m, n, P))
+    line = {"impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(n, ndof, nnz),
+            "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": P, "kind": "reference", "sample": sample,
+                             "residual_us_per_element": tr * 1e6, "tangent_ms_per_element": tt * 1e3},
+            "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "sample_wall_s": float(np.mean(walls))}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ GPU side
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    mx.append(float(p[2]))
+                except ValueError:
+                    continue
+                for k, nm in enumerate(names[1:], start=5):
+                    if p[k].lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    from igap4standard_b200 import Assembly
+    from igap4standard_b200.assembly import fma_peak_tflops
+
+    n = args.n
+    nelem, kn, pm, bc, pd = workload(n)
+    A = Assembly(nelem, kn, pm, bc, pd, device=local)
+    stream = torch.cuda.Stream(device=dev)
+    A.set_stream(stream.cuda_stream)
+    ndof, nnz, nel = A.ndof, A.nnz, A.nelem_total
+    g = torch.Generator(device="cpu").manual_seed(0)
+    U_host = (torch.rand(ndof, dtype=torch.float64, generator=g) * 2e-3 - 1e-3)
+    U = U_host.to(dev)
+    R = torch.empty(ndof, dtype=torch.float64, device=dev)
+    V64 = torch.empty(nnz, dtype=torch.float64, device=dev)
+    V32 = torch.empty(nnz, dtype=torch.float32, device=dev)
+    A.set_profiling(True)
+
+    def step(prec):
+        A.residual_device(U.data_ptr(), R.data_ptr())
+        launches = A.last_launch_count()
+        A.tangent_device(U.data_ptr(), (V64 if prec == "fp64" else V32).data_ptr(), prec)
+        launches += A.last_launch_count()
+        return launches
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(prec, K, W):
+        for _ in range(W):
+            step(prec)
+            A.last_kernel_ms()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        kms = np.zeros(6)
+        launches = 0
+        e0.record(stream)
+        for _ in range(K):
+            launches += step(prec)
+            kms += np.array(A.last_kernel_ms())   # waits for this step's events
+        e1.record(stream)
+        barrier()
+        t = e0.elapsed_time(e1) / K
+        if world > 1:
+            tt = torch.tensor([t], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t, kms / K, launches
+
+    peak64 = fma_peak_tflops("fp64", local)
+    peak32 = fma_peak_tflops("fp32", local)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t64, k64, launches64 = timed("fp64", args.steps, args.warmup)
+    clk = clocks.stop()
+    t32, k32, launches32 = timed("fp32", args.steps, max(1, args.warmup // 2))
+
+    # ---- end to end through the host-pointer C ABI (pinned host buffers)
+    e2e = None
+    if not args.no_e2e:
+        Uh = U_host.pin_memory()
+        Rh = torch.empty(ndof, dtype=torch.float64).pin_memory()
+        Vh = torch.empty(nnz, dtype=torch.float64).pin_memory()
+        uptr, rptr, vptr = Uh.data_ptr(), Rh.data_ptr(), Vh.data_ptr()
+        lib = A.lib
+        from igap4standard_b200.native import vp, check
+
+        def e2e_step():
+            check(lib, "igab_residual", lib.igab_residual(A.h, vp(uptr), vp(rptr)))
+            check(lib, "igab_tangent", lib.igab_tangent(A.h, vp(uptr), vp(vptr), 0))
+
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        barrier()
+        te = (time.perf_counter() - t0) * 1e3 / args.steps
+        if world > 1:
+            tt = torch.tensor([te], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        e2e = {"value": round(te / world, 3), "unit": "ms", "h2d_bytes_per_step": 2 * ndof * 8,
+               "d2h_bytes_per_step": ndof * 8 + nnz * 8, "ms_per_step": round(te, 3),
+               "timing": "host wall clock around igab_residual + igab_tangent (FP64), pinned host buffers"}
+
+    # ---- roofline of the dominant kernel (tangent volume, 8 colour launches per step)
+    tan_ms = k64[2]
+    nlaunch = max(k64[5], 1)
+    achieved = nel * TAN_ALG_FLOPS / (tan_ms * 1e-3) / 1e12
+    executed = nel * TAN_EXEC_FLOPS / (tan_ms * 1e-3) / 1e12
+    traffic = None
+    tp = os.path.join(REPO, "profiles", "tangent_volume_traffic.json")
+    if os.path.exists(tp):
+        try:
+            with open(tp) as f:
+                traffic = json.load(f).get("bytes_per_element")
+            if traffic is not None:
+                traffic = traffic * nel / nlaunch
+        except Exception:
+            traffic = None
+    roofline = {"bound": "tensor", "pipe": "FP64 FMA (SIMT)", "achieved": round(achieved, 3), "peak": round(peak64, 3),
+                "unit": "TFLOP/s", "frac": round(achieved / peak64, 4), "traffic": traffic,
+                "kernel": "k_tan_volume<double,2>", "avg_launch_ms": round(tan_ms / nlaunch, 3),
+                "flops_per_launch": nel * TAN_ALG_FLOPS / nlaunch,
+                "flops_definition": "algorithmic B^T D B per element = 64*2*(30*81*10+81*81*10) (effective: the "
+                                    "kernel executes %d flops per element)" % TAN_EXEC_FLOPS,
+                "executed_tflops": round(executed, 3),
+                "peak_source": "measured FP64 FMA probe (igab_fma_peak), burst; MEASURED_PEAKS.json has no FP64"}
+    res_tf = nel * RES_ALG_FLOPS / (k64[0] * 1e-3) / 1e12 if k64[0] > 0 else None
+
+    line = {"metric": METRIC, "value": round(t64 / world, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(t64, 3), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_dict(n, ndof, nnz),
+            "mixed": {"value": round(t32 / world, 3), "unit": "ms", "ms_per_step": round(t32, 3),
+                      "speedup_vs_fp64": round(t64 / t32, 3), "dtype": "f32 tangent, f64 residual",
+                      "tangent_volume_ms": round(k32[2], 3)},
+            "phases_ms": {"residual_volume": round(k64[0], 3), "residual_bc": round(k64[1], 3),
+                          "tangent_volume": round(k64[2], 3), "tangent_dirichlet": round(k64[3], 3)},
+            "residual_tflops_alg": round(res_tf, 3) if res_tf else None,
+            "adjoint_grads_per_s": None,
+            "clocks": clk, "gpu_launches": int(launches64), "roofline": roofline,
+            "peaks_measured": {"fp64_tflops": round(peak64, 2), "fp32_tflops": round(peak32, 2)},
+            "e2e": e2e}
+
+    if rank == 0 and not args.no_cpu:
+        try:
+            from oracle import ref
+            if ref.available():
+                P = min(cpu_procs(), 64)
+                pool = RefPool(P)
+                tr, tt, wall = pool.sample(args.cpu_sample)
+                pool.close()
+                ms = (tr + tt) * nel / P * 1e3
+                line["cpu_baseline"] = {"value": round(ms, 1), "unit": "ms", "cores": P, "kind": "reference",
+                                        "sample": "%d processes x %d^3 elements (reference residual+tangent), "
+                                                  "per-element time extrapolated to %d^3 (%.1f s wall)"
+                                                  % (P, args.cpu_sample, n, wall)}
+            else:
+                line["cpu_baseline"] = None
+        except Exception as e:
+            line["cpu_baseline"] = {"error": str(e)}
+    if rank == 0:
+        print(json.dumps(line))
+    A.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

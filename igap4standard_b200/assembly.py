@@ -1,0 +1,153 @@
+"""Python face of the plain C ABI (include/igab.h)."""
+import ctypes
+import numpy as np
+
+from . import native
+from .native import IgabMeshDesc, check, vp
+
+PHYS = {"ge": 0, "getime": 1}
+PREC = {"fp64": 0, "fp32": 1}
+
+
+def _ptr(a):
+    return a.ctypes.data_as(vp)
+
+
+class Assembly:
+    """One single-rank mesh on one GPU: residual and tangent assembly.
+
+    Mirrors what snesiga_init + snesiga_Residual/snesiga_Tangent do for one
+    rank (IGAP4STANDARD src/snesiga_init.c:12, src/snesiga_Residual.c:13,
+    src/snesiga_Tangent.c:13), with plain arrays instead of PETSc objects."""
+
+    def __init__(self, nelem, knots, par_mat, bc_type, par_dirichlet=None, par_periodic=None,
+                 phys="ge", device=0):
+        self.lib = native.lib_cuda()
+        d = IgabMeshDesc()
+        d.phys = PHYS[phys]
+        for i in range(3):
+            d.nelem[i] = int(nelem[i])
+        self._knots = np.ascontiguousarray(knots, dtype=np.float64)
+        if self._knots.size != sum(int(n) + 5 for n in nelem):
+            raise ValueError("knots must hold nelem[d]+5 values per direction")
+        d.knots = self._knots.ctypes.data_as(native.c_double_p)
+        for i in range(9):
+            d.par_mat[i] = float(par_mat[i])
+            d.par_dirichlet[i] = float(par_dirichlet[i]) if par_dirichlet is not None else 0.0
+            d.par_periodic[i] = float(par_periodic[i]) if par_periodic is not None else 0.0
+        for i in range(36):
+            d.bc_type[i] = int(bc_type[i])
+        h = vp()
+        check(self.lib, "igab_create", self.lib.igab_create(ctypes.byref(d), int(device), ctypes.byref(h)))
+        self.h = h
+        nd, nz, ne = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()
+        check(self.lib, "igab_sizes", self.lib.igab_sizes(h, ctypes.byref(nd), ctypes.byref(nz), ctypes.byref(ne)))
+        self.ndof, self.nnz, self.nelem_total = nd.value, nz.value, ne.value
+        self.nelem = tuple(int(n) for n in nelem)
+        self.phys = phys
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.igab_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- pattern
+    def pattern(self, with_cols=True):
+        rowptr = np.empty(self.ndof + 1, dtype=np.int32)
+        cols = np.empty(self.nnz, dtype=np.int32) if with_cols else None
+        check(self.lib, "igab_csr_pattern",
+              self.lib.igab_csr_pattern(self.h, _ptr(rowptr), _ptr(cols) if with_cols else None))
+        return rowptr, cols
+
+    def csr_offset(self, row, col):
+        return self.lib.igab_csr_offset(self.h, int(row), int(col))
+
+    # ---- parameters
+    def set_par_mat(self, pm):
+        a = np.ascontiguousarray(pm, dtype=np.float64)
+        check(self.lib, "igab_set_par_mat", self.lib.igab_set_par_mat(self.h, _ptr(a)))
+
+    def set_par_dirichlet(self, pd):
+        a = np.ascontiguousarray(pd, dtype=np.float64)
+        check(self.lib, "igab_set_par_dirichlet", self.lib.igab_set_par_dirichlet(self.h, _ptr(a)))
+
+    def set_par_periodic(self, pp):
+        a = np.ascontiguousarray(pp, dtype=np.float64)
+        check(self.lib, "igab_set_par_periodic", self.lib.igab_set_par_periodic(self.h, _ptr(a)))
+
+    def neumann_points(self):
+        n = ctypes.c_long()
+        check(self.lib, "igab_neumann_points", self.lib.igab_neumann_points(self.h, ctypes.byref(n), None, None))
+        xyz = np.empty((n.value, 3))
+        meta = np.empty((n.value, 3), dtype=np.int32)
+        if n.value:
+            check(self.lib, "igab_neumann_points",
+                  self.lib.igab_neumann_points(self.h, ctypes.byref(n), _ptr(xyz), _ptr(meta)))
+        return xyz, meta
+
+    def set_neumann_values(self, values):
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        check(self.lib, "igab_set_neumann_values", self.lib.igab_set_neumann_values(self.h, _ptr(a)))
+
+    def set_history(self, level, U):
+        a = np.ascontiguousarray(U, dtype=np.float64)
+        check(self.lib, "igab_set_history", self.lib.igab_set_history(self.h, int(level), _ptr(a), 0))
+
+    def set_tile(self, residual_tile=0, tangent_tile=0):
+        check(self.lib, "igab_set_tile", self.lib.igab_set_tile(self.h, residual_tile, tangent_tile))
+
+    # ---- host-pointer assembly
+    def residual(self, U, out=None):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        R = out if out is not None else np.empty(self.ndof)
+        check(self.lib, "igab_residual", self.lib.igab_residual(self.h, _ptr(U), _ptr(R)))
+        return R
+
+    def tangent(self, U, prec="fp64", out=None):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        dt = np.float64 if prec == "fp64" else np.float32
+        v = out if out is not None else np.empty(self.nnz, dtype=dt)
+        check(self.lib, "igab_tangent", self.lib.igab_tangent(self.h, _ptr(U), _ptr(v), PREC[prec]))
+        return v
+
+    # ---- device-pointer assembly (integers from e.g. torch.Tensor.data_ptr())
+    def residual_device(self, U_ptr, R_ptr):
+        check(self.lib, "igab_residual_device", self.lib.igab_residual_device(self.h, vp(U_ptr), vp(R_ptr)))
+
+    def tangent_device(self, U_ptr, vals_ptr, prec="fp64"):
+        check(self.lib, "igab_tangent_device",
+              self.lib.igab_tangent_device(self.h, vp(U_ptr), vp(vals_ptr), PREC[prec]))
+
+    def set_stream(self, stream_ptr):
+        check(self.lib, "igab_set_stream", self.lib.igab_set_stream(self.h, vp(stream_ptr)))
+
+    def sync(self):
+        check(self.lib, "igab_sync", self.lib.igab_sync(self.h))
+
+    def last_launch_count(self):
+        n = ctypes.c_int()
+        check(self.lib, "igab_last_launch_count", self.lib.igab_last_launch_count(self.h, ctypes.byref(n)))
+        return n.value
+
+    # ---- measurement
+    def set_profiling(self, on=True):
+        check(self.lib, "igab_set_profiling", self.lib.igab_set_profiling(self.h, 1 if on else 0))
+
+    def last_kernel_ms(self):
+        """[res volume, res boundary, tan volume, tan Dirichlet] ms and the two volume launch counts."""
+        ms = (ctypes.c_double * 6)()
+        check(self.lib, "igab_last_kernel_ms", self.lib.igab_last_kernel_ms(self.h, ms))
+        return list(ms)
+
+
+def fma_peak_tflops(prec="fp64", device=0):
+    lib = native.lib_cuda()
+    t = ctypes.c_double()
+    check(lib, "igab_fma_peak", lib.igab_fma_peak(int(device), PREC[prec], ctypes.byref(t)))
+    return t.value

@@ -1,0 +1,124 @@
+/*
+ * Internal state of an assembly context (not part of the ABI).
+ */
+#ifndef IGAB_INTERNAL_H
+#define IGAB_INTERNAL_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "igab.h"
+#include "igab_math.cuh"
+
+#define IGAB_NQ 4         /* Gauss points per direction (src/snesiga_Residual.c:99) */
+#define IGAB_NQ3 64
+#define IGAB_TAB1D 36     /* doubles per element per direction: [q 4][l 3][k 3] */
+
+/* Everything a kernel needs about the mesh and physics, passed by value. */
+struct igab_geom {
+    int ne[3];            /* elements per direction */
+    int nb[3];            /* control points per direction = ne + 2 */
+    long ndof;
+    const double *tab[3]; /* 1-D basis tables [e][q][l][k] */
+    const double *wh[3];  /* [e][q] Gauss weight times element length */
+    const double *xq[3];  /* [e][q] Gauss point coordinate */
+    const int *rowptr;    /* CSR row pointer [ndof+1] */
+    igab_ge_coef coef;
+    double pp[9];         /* par_periodic */
+    int periodic;         /* any pp != 0 */
+    /* transient (phys/getime): history pointers and time-integration scalars */
+    const double *hist1;  /* U at t_n     (U_hist level 1) */
+    const double *hist0;  /* U at t_{n-1} (U_hist level 2) */
+    double rho, cii, dt;
+    int phys;
+};
+
+struct igab_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    int phys = IGAB_PHYS_GE;
+    int torder = 0;
+    int ne[3] = {0, 0, 0}, nb[3] = {0, 0, 0};
+    long ncp = 0, ndof = 0, nnz = 0, nel = 0;
+    std::vector<double> knots[3];
+    double par_mat[9], par_dirichlet[9], par_periodic[9];
+    int bc_type[36];
+
+    /* host copies */
+    std::vector<int> rowptr_h;
+    double gauss_x[IGAB_NQ], gauss_w[IGAB_NQ];
+
+    /* device: tables */
+    double *d_tab[3] = {nullptr, nullptr, nullptr};
+    double *d_wh[3] = {nullptr, nullptr, nullptr};
+    double *d_xq[3] = {nullptr, nullptr, nullptr};
+    int *d_rowptr = nullptr;
+
+    /* Dirichlet: unique rows, last-written value (residual) */
+    long nd = 0;
+    int *d_drow = nullptr;
+    double *d_dg = nullptr;
+    bool dirichlet_dirty = true;
+
+    /* Neumann: active (face, order, dof) combos in the reference's loop order */
+    struct combo { int face, order, dof; long offset; int ne0, ne1; };
+    std::vector<combo> combos;
+    long n_neu_points = 0;
+    double *d_hval = nullptr;          /* traction values at surface Gauss points */
+    bool neumann_nonzero = false;
+    long n_neu_rows = 0;               /* rows receiving Neumann terms */
+    int *d_neu_row = nullptr;          /* dof per row */
+    int *d_neu_ptr = nullptr;          /* [n_neu_rows+1] into entries */
+    int4 *d_neu_ent = nullptr;         /* (combo, layer slot, bx, by) */
+    double *d_dnz = nullptr;           /* [6 faces][2 layers] normal derivative of the basis at the face */
+    int *d_combo_info = nullptr;       /* [ncombo][8]: face, order, dof, ne0, ne1, offset_lo, offset_hi, dir map */
+
+    /* history (transient) */
+    double *d_hist = nullptr;          /* [torder][ndof] */
+
+    /* owned scratch for the host-pointer entry points */
+    double *d_U = nullptr, *d_R = nullptr;
+    void *d_vals = nullptr;
+    int vals_prec = -1;
+
+    int tile_res = 2, tile_tan = 2;
+    int last_launches = 0;
+
+    /* profiling events: [0..2] residual (start, after volume, end), [3..5] tangent */
+    bool profiling = false;
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool ev_res = false, ev_tan = false;
+    int nvol_res = 0, nvol_tan = 0;
+
+    igab_geom geom() const;
+};
+
+/* kernels / launchers (igab_kernels.cu) */
+int igab_launch_residual(igab_ctx *c, const double *dU, double *dR);
+int igab_launch_tangent(igab_ctx *c, const double *dU, void *dvals, int prec);
+int igab_launch_csr_cols(igab_ctx *c, int *dcols);
+int igab_launch_check_finite(igab_ctx *c, const void *dev, long n, int prec, int *all_finite);
+int igab_launch_basis_tables(igab_ctx *c, int d, const double *dkv, const double *dgx, const double *dgw);
+int igab_launch_fma_peak(int prec, double *tflops);
+/* record profiling event k on the context stream if profiling is on */
+static inline void igab_mark(igab_ctx *c, int k)
+{
+    if (c->profiling && c->ev[k]) cudaEventRecord(c->ev[k], c->stream);
+}
+
+/* error helpers (igab_capi.cu) */
+void igab_set_error(const char *fmt, ...);
+#define IGAB_CUDA_TRY(call)                                                        \
+    do {                                                                           \
+        cudaError_t _e = (call);                                                   \
+        if (_e != cudaSuccess) {                                                   \
+            igab_set_error("%s:%d %s: %s", __FILE__, __LINE__, #call,             \
+                           cudaGetErrorString(_e));                                \
+            return IGAB_ERR_CUDA;                                                  \
+        }                                                                          \
+    } while (0)
+
+#endif

@@ -1,0 +1,929 @@
+/*
+ * Element-assembly kernels for sm_100a (FP64 residual; FP64 / FP32 tangent).
+ *
+ * Schedule (both operators): the mesh is cut into tiles of TE^3 elements
+ * (TE >= 2).  Tiles are coloured by the parity of their tile coordinates
+ * (8 colours); two tiles of one colour are at least TE elements apart, so
+ * the control points they touch are disjoint and one launch per colour can
+ * read-modify-write the global residual / CSR values without atomics.  Inside
+ * a tile the accumulation order is fixed, so results are bitwise repeatable.
+ *
+ * Residual (src/snesiga_Residual.c:99-174): per element, 64 threads, one per
+ * Gauss point.  The field and its derivatives at the Gauss points come from
+ * a sum-factorised interpolation (z, then y in shared memory, then x in
+ * registers).  The test-function contraction runs the same factorisation
+ * backwards, with the sums over the Gauss points of x, y and z done by warp
+ * shuffles (reduce-scatter across the 4 lanes of a direction) and one
+ * shared-memory step across the two warps.
+ *
+ * Tangent (src/snesiga_Tangent.c:99-190): per element, 256 threads.  With
+ * the energy written as W = Phi(v(u)) over 12 variables (igab_math.cuh),
+ *   K_e = sum_q w_q [ X_q^T Phi''_q X_q + blockdiag(Gamma_q) ],
+ * X_q[v][(a,k)] = sum_m dv/du_{k,m} N_a^{m}(q), a rank-12 update per point
+ * plus a geometric block shared by the three displacement components.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "igab_internal.h"
+
+namespace {
+
+/* derivative multi-index of component alpha (eval_Bspline order):
+ * 0:(0,0,0) 1:(1,0,0) 2:(0,1,0) 3:(0,0,1) 4:(2,0,0) 5:(1,1,0) 6:(1,0,1) 7:(0,2,0) 8:(0,1,1) 9:(0,0,2) */
+__host__ __device__ constexpr int a_kx(int a) { return a == 1 || a == 5 || a == 6 ? 1 : (a == 4 ? 2 : 0); }
+__host__ __device__ constexpr int a_ky(int a) { return a == 2 || a == 5 || a == 8 ? 1 : (a == 7 ? 2 : 0); }
+__host__ __device__ constexpr int a_kz(int a) { return a == 3 || a == 6 || a == 8 ? 1 : (a == 9 ? 2 : 0); }
+/* (ky,kz) pair index: 0:(0,0) 1:(1,0) 2:(0,1) 3:(2,0) 4:(1,1) 5:(0,2) */
+__host__ __device__ constexpr int kk_of(int ky, int kz)
+{
+    return (ky == 0 && kz == 0) ? 0 : (ky == 1 && kz == 0) ? 1 : (ky == 0 && kz == 1) ? 2
+         : (ky == 2 && kz == 0) ? 3 : (ky == 1 && kz == 1) ? 4 : 5;
+}
+__host__ __device__ constexpr int kk_ky(int kk) { return kk == 1 || kk == 4 ? 1 : (kk == 3 ? 2 : 0); }
+__host__ __device__ constexpr int kk_kz(int kk) { return kk == 2 || kk == 4 ? 1 : (kk == 5 ? 2 : 0); }
+__host__ __device__ constexpr int a_kk(int a) { return kk_of(a_ky(a), a_kz(a)); }
+
+__device__ __forceinline__ void group_sync(int group)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(group + 1), "r"(64) : "memory");
+}
+
+__device__ __forceinline__ double shfl_xor(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+
+/* tile bookkeeping for one colour */
+struct tile_t {
+    int t[3];   /* tile coordinates */
+    int e0[3];  /* first element */
+    int nv[3];  /* valid elements per direction */
+};
+
+__device__ __forceinline__ bool decode_tile(const igab_geom &g, int TE, int colour, int bid, tile_t &T)
+{
+    int c[3] = {colour & 1, (colour >> 1) & 1, (colour >> 2) & 1};
+    int nc[3];
+    for (int d = 0; d < 3; d++) {
+        int nt = (g.ne[d] + TE - 1) / TE;
+        nc[d] = nt > c[d] ? (nt - c[d] + 1) / 2 : 0;
+    }
+    int i2 = bid % nc[2];
+    int i1 = (bid / nc[2]) % nc[1];
+    int i0 = bid / (nc[2] * nc[1]);
+    if (i0 >= nc[0]) return false;
+    T.t[0] = 2 * i0 + c[0]; T.t[1] = 2 * i1 + c[1]; T.t[2] = 2 * i2 + c[2];
+    for (int d = 0; d < 3; d++) {
+        T.e0[d] = T.t[d] * TE;
+        int r = g.ne[d] - T.e0[d];
+        T.nv[d] = r < TE ? r : TE;
+    }
+    return true;
+}
+
+__device__ __forceinline__ long cp_index(const igab_geom &g, int x, int y, int z)
+{
+    return ((long)x * g.nb[1] + y) * g.nb[2] + z;
+}
+
+/* position of column (cx,cy,cz,k2) inside the CSR row of control point (x,y,z) */
+__device__ __forceinline__ int csr_pos(const igab_geom &g, int x, int y, int z, int cx, int cy, int cz, int k2)
+{
+    int x0 = x > 2 ? x - 2 : 0;
+    int y0 = y > 2 ? y - 2 : 0, y1 = y + 2 < g.nb[1] - 1 ? y + 2 : g.nb[1] - 1;
+    int z0 = z > 2 ? z - 2 : 0, z1 = z + 2 < g.nb[2] - 1 ? z + 2 : g.nb[2] - 1;
+    int nyb = y1 - y0 + 1, nzb = z1 - z0 + 1;
+    return (((cx - x0) * nyb + (cy - y0)) * nzb + (cz - z0)) * 3 + k2;
+}
+
+/* ============================================================ residual */
+
+template <int TE>
+struct res_smem {
+    static constexpr int TC = TE + 2;
+    static constexpr int NCP = TC * TC * TC;
+    double U[NCP * 3];
+    double Racc[NCP * 3];
+    double tab[3][TE][IGAB_TAB1D];
+    double wh[3][TE][IGAB_NQ];
+    double xq[3][TE][IGAB_NQ];
+    double A[4][972];
+    double C[4][864];
+    double red[4][81];
+    double Re[4][81];
+};
+
+template <int TE>
+__global__ void __launch_bounds__(256) k_res_volume(igab_geom g, const double *__restrict__ U,
+                                                    double *__restrict__ R, int colour)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    res_smem<TE> &S = *reinterpret_cast<res_smem<TE> *>(smem_raw);
+    constexpr int TC = TE + 2;
+    constexpr int NCP = TC * TC * TC;
+    constexpr int NEL = TE * TE * TE;
+    tile_t T;
+    if (!decode_tile(g, TE, colour, blockIdx.x, T)) return;
+    const int tid = threadIdx.x;
+
+    /* ---- stage control-point values and 1-D tables of the tile */
+    for (int idx = tid; idx < NCP * 3; idx += blockDim.x) {
+        int i = idx % 3, cp = idx / 3;
+        int lz = cp % TC, ly = (cp / TC) % TC, lx = cp / (TC * TC);
+        double v = 0.0;
+        if (lx < T.nv[0] + 2 && ly < T.nv[1] + 2 && lz < T.nv[2] + 2)
+            v = U[3 * cp_index(g, T.e0[0] + lx, T.e0[1] + ly, T.e0[2] + lz) + i];
+        S.U[idx] = v;
+        S.Racc[idx] = 0.0;
+    }
+    for (int idx = tid; idx < 3 * TE * IGAB_TAB1D; idx += blockDim.x) {
+        int d = idx / (TE * IGAB_TAB1D), r = idx % (TE * IGAB_TAB1D), le = r / IGAB_TAB1D, o = r % IGAB_TAB1D;
+        S.tab[d][le][o] = le < T.nv[d] ? g.tab[d][(long)(T.e0[d] + le) * IGAB_TAB1D + o] : 0.0;
+    }
+    for (int idx = tid; idx < 3 * TE * IGAB_NQ; idx += blockDim.x) {
+        int d = idx / (TE * IGAB_NQ), r = idx % (TE * IGAB_NQ), le = r / IGAB_NQ, q = r % IGAB_NQ;
+        bool ok = le < T.nv[d];
+        S.wh[d][le][q] = ok ? g.wh[d][(long)(T.e0[d] + le) * IGAB_NQ + q] : 0.0;
+        S.xq[d][le][q] = ok ? g.xq[d][(long)(T.e0[d] + le) * IGAB_NQ + q] : 0.0;
+    }
+    __syncthreads();
+
+    const int group = tid >> 6;
+    const int gt = tid & 63;
+    const int qx = gt & 3, qy = (gt >> 2) & 3, qz = gt >> 4;
+
+    for (int base = 0; base < NEL; base += 4) {
+        const int le = base + group;
+        const int lex = le / (TE * TE), ley = (le / TE) % TE, lez = le % TE;
+        const bool valid = lex < T.nv[0] && ley < T.nv[1] && lez < T.nv[2];
+        if (valid) {
+            const double *Bx = S.tab[0][lex];
+            const double *By = S.tab[1][ley];
+            const double *Bz = S.tab[2][lez];
+            /* stage A: contract z.  A[qz][ax][ay][kz][i] */
+            for (int o = gt; o < 972; o += 64) {
+                int i = o % 3, kz = (o / 3) % 3, ay = (o / 9) % 3, ax = (o / 27) % 3, q = o / 81;
+                const double *u0 = &S.U[(((lex + ax) * TC + (ley + ay)) * TC + lez) * 3 + i];
+                S.A[group][o] = Bz[q * 9 + 0 * 3 + kz] * u0[0] + Bz[q * 9 + 1 * 3 + kz] * u0[3] +
+                                Bz[q * 9 + 2 * 3 + kz] * u0[6];
+            }
+            group_sync(group);
+            /* stage C: contract y.  C[qy + 4 qz][ax][kk][i] */
+            for (int o = gt; o < 864; o += 64) {
+                int i = o % 3, kk = (o / 3) % 6, ax = (o / 18) % 3, qq = o / 54;
+                int qyy = qq & 3, qzz = qq >> 2;
+                int ky = kk_ky(kk), kz = kk_kz(kk);
+                const double *a0 = &S.A[group][((qzz * 3 + ax) * 3) * 9 + kz * 3 + i];
+                S.C[group][o] = By[qyy * 9 + 0 * 3 + ky] * a0[0] + By[qyy * 9 + 1 * 3 + ky] * a0[9] +
+                                By[qyy * 9 + 2 * 3 + ky] * a0[18];
+            }
+            group_sync(group);
+            /* stage X: one Gauss point per thread */
+            double u[30];
+            const int qq = qy + 4 * qz;
+#pragma unroll
+            for (int a = 0; a < 10; a++) {
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int ax = 0; ax < 3; ax++)
+                        s += Bx[qx * 9 + ax * 3 + a_kx(a)] * S.C[group][((qq * 3 + ax) * 6 + a_kk(a)) * 3 + i];
+                    u[10 * i + a] = s;
+                }
+            }
+            if (g.periodic) {
+                double X[3] = {S.xq[0][lex][qx], S.xq[1][ley][qy], S.xq[2][lez][qz]};
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    u[10 * i] += g.pp[3 * i] * X[0] + g.pp[3 * i + 1] * X[1] + g.pp[3 * i + 2] * X[2];
+#pragma unroll
+                    for (int J = 0; J < 3; J++) u[10 * i + 1 + J] += g.pp[3 * i + J];
+                }
+            }
+            /* integrand */
+            double r[30];
+            {
+                igab_ge_point<double> P;
+                igab_ge_eval(u, g.coef, P);
+                igab_ge_residual(P, r);
+            }
+            const double w = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz];
+#pragma unroll
+            for (int k = 0; k < 30; k++) r[k] *= w;
+
+            /* backward step 1: partial sums over x for this point, P1[ax][kk][i] */
+            double P1[3][18];
+#pragma unroll
+            for (int ax = 0; ax < 3; ax++)
+#pragma unroll
+                for (int s = 0; s < 18; s++) P1[ax][s] = 0.0;
+#pragma unroll
+            for (int a = 0; a < 10; a++)
+#pragma unroll
+                for (int ax = 0; ax < 3; ax++) {
+                    double b = Bx[qx * 9 + ax * 3 + a_kx(a)];
+#pragma unroll
+                    for (int i = 0; i < 3; i++) P1[ax][a_kk(a) * 3 + i] += b * r[10 * i + a];
+                }
+            /* reduce-scatter over the 4 x-lanes: lane qx keeps ax = qx (qx < 3) */
+            const int b1 = (qx >> 1) & 1, b0 = qx & 1;
+#pragma unroll
+            for (int s = 0; s < 18; s++) {
+                double x1 = b1 ? P1[0][s] : P1[2][s];
+                double y1 = shfl_xor(x1, 2);
+                double x2 = b1 ? P1[1][s] : 0.0;
+                double y2 = shfl_xor(x2, 2);
+                if (b1) P1[2][s] += y1; else { P1[0][s] += y1; P1[1][s] += y2; }
+            }
+            double Y[18];
+#pragma unroll
+            for (int s = 0; s < 18; s++) {
+                double x = b1 ? P1[2][s] : (b0 ? P1[0][s] : P1[1][s]);
+                double y = shfl_xor(x, 1);
+                double mine = b1 ? P1[2][s] : (b0 ? P1[1][s] : P1[0][s]);
+                Y[s] = mine + y;
+            }
+            /* backward step 2: contract y for ax = qx; P2[ay][kz][i] */
+            double P2[3][9];
+#pragma unroll
+            for (int ay = 0; ay < 3; ay++)
+#pragma unroll
+                for (int s = 0; s < 9; s++) P2[ay][s] = 0.0;
+#pragma unroll
+            for (int kk = 0; kk < 6; kk++)
+#pragma unroll
+                for (int ay = 0; ay < 3; ay++) {
+                    double b = By[qy * 9 + ay * 3 + kk_ky(kk)];
+#pragma unroll
+                    for (int i = 0; i < 3; i++) P2[ay][kk_kz(kk) * 3 + i] += b * Y[kk * 3 + i];
+                }
+            /* reduce-scatter over the 4 y-lanes (lane bits 2,3): lane qy keeps ay = qy */
+            const int c1 = (qy >> 1) & 1, c0 = qy & 1;
+#pragma unroll
+            for (int s = 0; s < 9; s++) {
+                double x1 = c1 ? P2[0][s] : P2[2][s];
+                double y1 = shfl_xor(x1, 8);
+                double x2 = c1 ? P2[1][s] : 0.0;
+                double y2 = shfl_xor(x2, 8);
+                if (c1) P2[2][s] += y1; else { P2[0][s] += y1; P2[1][s] += y2; }
+            }
+            double Z[9];
+#pragma unroll
+            for (int s = 0; s < 9; s++) {
+                double x = c1 ? P2[2][s] : (c0 ? P2[0][s] : P2[1][s]);
+                double y = shfl_xor(x, 4);
+                double mine = c1 ? P2[2][s] : (c0 ? P2[1][s] : P2[0][s]);
+                Z[s] = mine + y;
+            }
+            /* backward step 3: contract z for (ax, ay) = (qx, qy); sum over qz */
+            double P3[9];
+#pragma unroll
+            for (int az = 0; az < 3; az++)
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int kz = 0; kz < 3; kz++) s += Bz[qz * 9 + az * 3 + kz] * Z[kz * 3 + i];
+                    P3[az * 3 + i] = s;
+                }
+#pragma unroll
+            for (int s = 0; s < 9; s++) P3[s] += shfl_xor(P3[s], 16);
+            const bool owner = qx < 3 && qy < 3 && (qz & 1) == 0;
+            if (owner && qz == 2)
+#pragma unroll
+                for (int s = 0; s < 9; s++) S.red[group][(qx * 3 + qy) * 9 + s] = P3[s];
+            group_sync(group);
+            if (owner && qz == 0)
+#pragma unroll
+                for (int s = 0; s < 9; s++) S.Re[group][(qx * 3 + qy) * 9 + s] = P3[s] + S.red[group][(qx * 3 + qy) * 9 + s];
+        }
+        __syncthreads();
+        /* ---- fixed-order accumulation of the (up to) 4 element vectors into the tile */
+        for (int idx = tid; idx < NCP * 3; idx += blockDim.x) {
+            int i = idx % 3, cp = idx / 3;
+            int lz = cp % TC, ly = (cp / TC) % TC, lx = cp / (TC * TC);
+            double acc = S.Racc[idx];
+            for (int gg = 0; gg < 4; gg++) {
+                int e = base + gg;
+                if (e >= NEL) break;
+                int ex = e / (TE * TE), ey = (e / TE) % TE, ez = e % TE;
+                if (ex >= T.nv[0] || ey >= T.nv[1] || ez >= T.nv[2]) continue;
+                int ax = lx - ex, ay = ly - ey, az = lz - ez;
+                if (ax < 0 || ax > 2 || ay < 0 || ay > 2 || az < 0 || az > 2) continue;
+                acc += S.Re[gg][((ax * 3 + ay) * 3 + az) * 3 + i];
+            }
+            S.Racc[idx] = acc;
+        }
+        __syncthreads();
+    }
+    /* ---- add the tile into the global residual (no other tile of this colour touches these points) */
+    for (int idx = tid; idx < NCP * 3; idx += blockDim.x) {
+        int i = idx % 3, cp = idx / 3;
+        int lz = cp % TC, ly = (cp / TC) % TC, lx = cp / (TC * TC);
+        if (lx < T.nv[0] + 2 && ly < T.nv[1] + 2 && lz < T.nv[2] + 2) {
+            long gi = 3 * cp_index(g, T.e0[0] + lx, T.e0[1] + ly, T.e0[2] + lz) + i;
+            R[gi] += S.Racc[idx];
+        }
+    }
+}
+
+/* Neumann surface terms (src/snesiga_Residual.c:243-320): one thread per
+ * boundary dof, gathering every active (face, order) combo that reaches it. */
+__global__ void k_res_neumann(igab_geom g, long nrows, const int *__restrict__ row_dof,
+                              const int *__restrict__ ptr, const int4 *__restrict__ ent,
+                              const int *__restrict__ cinfo, const double *__restrict__ dnz,
+                              const double *__restrict__ hval, double *__restrict__ R)
+{
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= nrows) return;
+    double acc = 0.0;
+    for (int k = ptr[t]; k < ptr[t + 1]; k++) {
+        int4 e = ent[k];   /* (combo, layer slot, bx, by) */
+        const int *ci = cinfo + 8 * e.x;
+        int face = ci[0], order = ci[1], ne0 = ci[3], ne1 = ci[4];
+        long off = (long)(unsigned)ci[5] | ((long)ci[6] << 32);
+        int d0 = ci[7] & 3, d1 = (ci[7] >> 2) & 3;
+        double fz = order ? dnz[face * 2 + e.y] : 1.0;
+        int bx = e.z, by = e.w;
+        double s = 0.0;
+        for (int ex = bx - 2 > 0 ? bx - 2 : 0; ex <= bx && ex < ne0; ex++)
+            for (int ey = by - 2 > 0 ? by - 2 : 0; ey <= by && ey < ne1; ey++) {
+                const double *t0 = g.tab[d0] + (long)ex * IGAB_TAB1D;
+                const double *t1 = g.tab[d1] + (long)ey * IGAB_TAB1D;
+                const double *w0 = g.wh[d0] + (long)ex * IGAB_NQ;
+                const double *w1 = g.wh[d1] + (long)ey * IGAB_NQ;
+                const double *h = hval + off + ((long)ex * ne1 + ey) * 16;
+                for (int q0 = 0; q0 < 4; q0++)
+                    for (int q1 = 0; q1 < 4; q1++)
+                        s += w0[q0] * w1[q1] * t0[q0 * 9 + (bx - ex) * 3] * t1[q1 * 9 + (by - ey) * 3] * h[q0 * 4 + q1];
+            }
+        acc -= fz * s;
+    }
+    R[row_dof[t]] += acc;
+}
+
+/* Dirichlet rows R = U - g, written after all additions (src/snesiga_Residual.c:326-412) */
+__global__ void k_res_dirichlet(long nd, const int *__restrict__ drow, const double *__restrict__ dg,
+                                const double *__restrict__ U, double *__restrict__ R)
+{
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= nd) return;
+    int r = drow[t];
+    R[r] = U[r] - dg[t];
+}
+
+/* ============================================================ tangent */
+
+#define TAN_Q 4          /* Gauss points per batch */
+#define TAN_NPT 56       /* doubles of point data */
+#define TAN_NOWN 13      /* upper-triangle entries owned per thread (3321 / 256) */
+
+template <typename T, int TE>
+struct tan_smem {
+    static constexpr int TC = TE + 2;
+    static constexpr int NCP = TC * TC * TC;
+    double U[NCP * 3];
+    double tab[3][TE][IGAB_TAB1D];
+    double wh[3][TE][IGAB_NQ];
+    double xq[3][TE][IGAB_NQ];
+    double A[972];
+    double C[864];
+    double pt[IGAB_NQ3][TAN_NPT];   /* F 9, G 18, d2 12, d2ab 1, sig 3, d1[3..5] 3, tau 9, w 1 */
+    T N[TAN_Q][27][9];              /* N_a^{m+1} */
+    T Gv[TAN_Q][12][27];            /* dv/du_s */
+    T X[TAN_Q][12][81];
+    T Y[TAN_Q][12][81];
+    T GN[TAN_Q][9][27];             /* geo * N */
+};
+
+/* point data offsets */
+#define PT_F 0
+#define PT_G 9
+#define PT_D2 27
+#define PT_D2AB 39
+#define PT_SIG 40
+#define PT_D1S 43
+#define PT_TAU 46
+#define PT_W 55
+
+template <typename T>
+__device__ __forceinline__ void load_point(const double *pt, igab_ge_point<T> &P)
+{
+    for (int k = 0; k < 3; k++)
+        for (int J = 0; J < 3; J++) P.F[k][J] = T(pt[PT_F + 3 * k + J]);
+    for (int k = 0; k < 3; k++)
+        for (int c = 0; c < 6; c++) P.G[k][c] = T(pt[PT_G + 6 * k + c]);
+}
+
+template <typename T, int TE>
+__global__ void __launch_bounds__(256) k_tan_volume(igab_geom g, const double *__restrict__ U,
+                                                    T *__restrict__ vals, int colour)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    tan_smem<T, TE> &S = *reinterpret_cast<tan_smem<T, TE> *>(smem_raw);
+    constexpr int TC = TE + 2;
+    constexpr int NCP = TC * TC * TC;
+    constexpr int NEL = TE * TE * TE;
+    tile_t Tl;
+    if (!decode_tile(g, TE, colour, blockIdx.x, Tl)) return;
+    const int tid = threadIdx.x;
+
+    /* owned upper-triangle entries (c1 <= c2), c = 3a + k */
+    int own[TAN_NOWN];
+#pragma unroll
+    for (int j = 0; j < TAN_NOWN; j++) {
+        int idx = tid + 256 * j;
+        int c1 = 0, rem = idx;
+        while (c1 < 81 && rem >= 81 - c1) { rem -= 81 - c1; c1++; }
+        own[j] = c1 < 81 ? (c1 << 8) | (c1 + rem) : -1;
+    }
+    /* owned geometric entries (a1 <= a2), 378 */
+    int gown[2];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        int idx = tid + 256 * j;
+        int a1 = 0, rem = idx;
+        while (a1 < 27 && rem >= 27 - a1) { rem -= 27 - a1; a1++; }
+        gown[j] = a1 < 27 ? (a1 << 8) | (a1 + rem) : -1;
+    }
+
+    for (int idx = tid; idx < NCP * 3; idx += blockDim.x) {
+        int i = idx % 3, cp = idx / 3;
+        int lz = cp % TC, ly = (cp / TC) % TC, lx = cp / (TC * TC);
+        double v = 0.0;
+        if (lx < Tl.nv[0] + 2 && ly < Tl.nv[1] + 2 && lz < Tl.nv[2] + 2)
+            v = U[3 * cp_index(g, Tl.e0[0] + lx, Tl.e0[1] + ly, Tl.e0[2] + lz) + i];
+        S.U[idx] = v;
+    }
+    for (int idx = tid; idx < 3 * TE * IGAB_TAB1D; idx += blockDim.x) {
+        int d = idx / (TE * IGAB_TAB1D), r = idx % (TE * IGAB_TAB1D), le = r / IGAB_TAB1D, o = r % IGAB_TAB1D;
+        S.tab[d][le][o] = le < Tl.nv[d] ? g.tab[d][(long)(Tl.e0[d] + le) * IGAB_TAB1D + o] : 0.0;
+    }
+    for (int idx = tid; idx < 3 * TE * IGAB_NQ; idx += blockDim.x) {
+        int d = idx / (TE * IGAB_NQ), r = idx % (TE * IGAB_NQ), le = r / IGAB_NQ, q = r % IGAB_NQ;
+        bool ok = le < Tl.nv[d];
+        S.wh[d][le][q] = ok ? g.wh[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
+        S.xq[d][le][q] = ok ? g.xq[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
+    }
+    __syncthreads();
+
+    for (int le = 0; le < NEL; le++) {
+        const int lex = le / (TE * TE), ley = (le / TE) % TE, lez = le % TE;
+        if (!(lex < Tl.nv[0] && ley < Tl.nv[1] && lez < Tl.nv[2])) continue;   /* uniform over the block */
+        const double *Bx = S.tab[0][lex];
+        const double *By = S.tab[1][ley];
+        const double *Bz = S.tab[2][lez];
+        /* ---- interpolation (as the residual, all 256 threads for stages A and C) */
+        for (int o = tid; o < 972; o += 256) {
+            int i = o % 3, kz = (o / 3) % 3, ay = (o / 9) % 3, ax = (o / 27) % 3, q = o / 81;
+            const double *u0 = &S.U[(((lex + ax) * TC + (ley + ay)) * TC + lez) * 3 + i];
+            S.A[o] = Bz[q * 9 + kz] * u0[0] + Bz[q * 9 + 3 + kz] * u0[3] + Bz[q * 9 + 6 + kz] * u0[6];
+        }
+        __syncthreads();
+        for (int o = tid; o < 864; o += 256) {
+            int i = o % 3, kk = (o / 3) % 6, ax = (o / 18) % 3, qq = o / 54;
+            int qyy = qq & 3, qzz = qq >> 2;
+            int ky = kk_ky(kk), kz = kk_kz(kk);
+            const double *a0 = &S.A[((qzz * 3 + ax) * 3) * 9 + kz * 3 + i];
+            S.C[o] = By[qyy * 9 + ky] * a0[0] + By[qyy * 9 + 3 + ky] * a0[9] + By[qyy * 9 + 6 + ky] * a0[18];
+        }
+        __syncthreads();
+        if (tid < IGAB_NQ3) {
+            const int qx = tid & 3, qy = (tid >> 2) & 3, qz = tid >> 4, qq = qy + 4 * qz;
+            double u[30];
+#pragma unroll
+            for (int a = 0; a < 10; a++)
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int ax = 0; ax < 3; ax++)
+                        s += Bx[qx * 9 + ax * 3 + a_kx(a)] * S.C[((qq * 3 + ax) * 6 + a_kk(a)) * 3 + i];
+                    u[10 * i + a] = s;
+                }
+            if (g.periodic) {
+#pragma unroll
+                for (int i = 0; i < 3; i++)
+#pragma unroll
+                    for (int J = 0; J < 3; J++) u[10 * i + 1 + J] += g.pp[3 * i + J];
+            }
+            igab_ge_point<T> P;
+            T uT[30];
+#pragma unroll
+            for (int k = 0; k < 30; k++) uT[k] = T(u[k]);
+            igab_ge_eval(uT, g.coef, P);
+            double *pt = S.pt[tid];
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+#pragma unroll
+                for (int J = 0; J < 3; J++) pt[PT_F + 3 * k + J] = double(P.F[k][J]);
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+#pragma unroll
+                for (int c = 0; c < 6; c++) pt[PT_G + 6 * k + c] = double(P.G[k][c]);
+#pragma unroll
+            for (int v = 0; v < 12; v++) pt[PT_D2 + v] = double(P.d2[v]);
+            pt[PT_D2AB] = double(P.d2ab);
+#pragma unroll
+            for (int I = 0; I < 3; I++) pt[PT_SIG + I] = double(P.sig[I]);
+#pragma unroll
+            for (int I = 0; I < 3; I++) pt[PT_D1S + I] = double(P.d1[3 + I]);
+#pragma unroll
+            for (int I = 0; I < 3; I++)
+#pragma unroll
+                for (int K = 0; K < 3; K++) pt[PT_TAU + 3 * I + K] = double(P.tau[I][K]);
+            pt[PT_W] = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz];
+        }
+        __syncthreads();
+
+        T acc[TAN_NOWN];
+#pragma unroll
+        for (int j = 0; j < TAN_NOWN; j++) acc[j] = T(0);
+        T gacc[2] = {T(0), T(0)};
+
+        for (int q0 = 0; q0 < IGAB_NQ3; q0 += TAN_Q) {
+            /* (a) basis products and variable gradients for the batch */
+            for (int o = tid; o < TAN_Q * 27 * 9; o += 256) {
+                int m = o % 9, a = (o / 9) % 27, qb = o / 243;
+                int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
+                int ax = a / 9, ay = (a / 3) % 3, az = a % 3;
+                int al = m + 1;
+                double v = Bx[qx * 9 + ax * 3 + a_kx(al)] * By[qy * 9 + ay * 3 + a_ky(al)] * Bz[qz * 9 + az * 3 + a_kz(al)];
+                S.N[qb][a][m] = T(v);
+            }
+            for (int o = tid; o < TAN_Q * 12 * 3; o += 256) {
+                int k = o % 3, v = (o / 3) % 12, qb = o / 36;
+                igab_ge_point<T> P;
+                load_point(S.pt[q0 + qb], P);
+                T gg[9];
+                igab_ge_grad_var(P, v, k, gg);
+#pragma unroll
+                for (int m = 0; m < 9; m++) S.Gv[qb][v][9 * k + m] = gg[m];
+            }
+            /* geometric block times N: GN[m][b] = sum_n geo[m][n] N_b^{n} */
+            for (int o = tid; o < TAN_Q * 9 * 27; o += 256) {
+                int b = o % 27, m = (o / 27) % 9, qb = o / 243;
+                const double *pt = S.pt[q0 + qb];
+                T s = T(0);
+                if (m < 3) {
+                    s = T(pt[PT_SIG + m]) * S.N[qb][b][m];
+                    int o1 = (m + 1) % 3, o2 = (m + 2) % 3;
+                    /* off-diagonal E terms: (0,1)->d1[3], (0,2)->d1[4], (1,2)->d1[5] */
+                    int pr1 = (m == 0 || o1 == 0) ? ((m + o1 == 1) ? 0 : 1) : 2;
+                    int pr2 = (m == 0 || o2 == 0) ? ((m + o2 == 1) ? 0 : 1) : 2;
+                    s += T(0.5) * T(pt[PT_D1S + pr1]) * S.N[qb][b][o1];
+                    s += T(0.5) * T(pt[PT_D1S + pr2]) * S.N[qb][b][o2];
+                    for (int K = 0; K < 3; K++) s += T(pt[PT_TAU + 3 * m + K]) * S.N[qb][b][3 + igab_idx6(m, K)];
+                } else {
+                    int c = m - 3;
+                    for (int I = 0; I < 3; I++)
+                        for (int K = 0; K < 3; K++)
+                            if (igab_idx6(I, K) == c) s += T(pt[PT_TAU + 3 * I + K]) * S.N[qb][b][I];
+                }
+                S.GN[qb][m][b] = s;
+            }
+            __syncthreads();
+            /* (b) X = Gv . N and Y = w Phi'' X */
+            for (int o = tid; o < TAN_Q * 12 * 81; o += 256) {
+                int c = o % 81, v = (o / 81) % 12, qb = o / 972;
+                int a = c / 3, k = c % 3;
+                T s = T(0);
+#pragma unroll
+                for (int m = 0; m < 9; m++) s += S.Gv[qb][v][9 * k + m] * S.N[qb][a][m];
+                S.X[qb][v][c] = s;
+            }
+            __syncthreads();
+            for (int o = tid; o < TAN_Q * 12 * 81; o += 256) {
+                int c = o % 81, v = (o / 81) % 12, qb = o / 972;
+                const double *pt = S.pt[q0 + qb];
+                T w = T(pt[PT_W]);
+                T s = T(pt[PT_D2 + v]) * S.X[qb][v][c];
+                if (v == 1) s += T(pt[PT_D2AB]) * S.X[qb][2][c];
+                if (v == 2) s += T(pt[PT_D2AB]) * S.X[qb][1][c];
+                S.Y[qb][v][c] = w * s;
+            }
+            __syncthreads();
+            /* (c) accumulate owned entries */
+#pragma unroll
+            for (int j = 0; j < TAN_NOWN; j++) {
+                if (own[j] < 0) continue;
+                int c1 = own[j] >> 8, c2 = own[j] & 255;
+                T s = acc[j];
+                for (int qb = 0; qb < TAN_Q; qb++)
+#pragma unroll
+                    for (int v = 0; v < 12; v++) s += S.X[qb][v][c1] * S.Y[qb][v][c2];
+                acc[j] = s;
+            }
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                if (gown[j] < 0) continue;
+                int a1 = gown[j] >> 8, a2 = gown[j] & 255;
+                T s = gacc[j];
+                for (int qb = 0; qb < TAN_Q; qb++) {
+                    T w = T(S.pt[q0 + qb][PT_W]);
+                    T t = T(0);
+#pragma unroll
+                    for (int m = 0; m < 9; m++) t += S.N[qb][a1][m] * S.GN[qb][m][a2];
+                    s += w * t;
+                }
+                gacc[j] = s;
+            }
+            __syncthreads();
+        }
+        /* geometric block to shared memory (reuse X) */
+        T *Gam = &S.X[0][0][0];
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            if (gown[j] < 0) continue;
+            int a1 = gown[j] >> 8, a2 = gown[j] & 255;
+            Gam[a1 * 27 + a2] = gacc[j];
+            Gam[a2 * 27 + a1] = gacc[j];
+        }
+        __syncthreads();
+        /* ---- scatter into the CSR values (read-modify-write, conflict-free within a colour) */
+#pragma unroll
+        for (int j = 0; j < TAN_NOWN; j++) {
+            if (own[j] < 0) continue;
+            int c1 = own[j] >> 8, c2 = own[j] & 255;
+            int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
+            T val = acc[j];
+            if (k1 == k2) val += Gam[a1 * 27 + a2];
+            int x1 = Tl.e0[0] + lex + a1 / 9, y1 = Tl.e0[1] + ley + (a1 / 3) % 3, z1 = Tl.e0[2] + lez + a1 % 3;
+            int x2 = Tl.e0[0] + lex + a2 / 9, y2 = Tl.e0[1] + ley + (a2 / 3) % 3, z2 = Tl.e0[2] + lez + a2 % 3;
+            long r1 = 3 * cp_index(g, x1, y1, z1) + k1;
+            long o1 = g.rowptr[r1] + csr_pos(g, x1, y1, z1, x2, y2, z2, k2);
+            vals[o1] += val;
+            if (c1 != c2) {
+                long r2 = 3 * cp_index(g, x2, y2, z2) + k2;
+                long o2 = g.rowptr[r2] + csr_pos(g, x2, y2, z2, x1, y1, z1, k1);
+                vals[o2] += val;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+/* MatZeroRowsColumns(P, rows, 1.0) on the structured pattern (src/snesiga_Tangent.c:270):
+ * one thread per (Dirichlet row, entry of that row). */
+template <typename T>
+__global__ void k_tan_dirichlet(igab_geom g, long nd, const int *__restrict__ drow, T *__restrict__ vals)
+{
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long j = t / 375;
+    int s = (int)(t % 375);
+    if (j >= nd) return;
+    int r = drow[j];
+    int cp = r / 3;
+    int z = cp % g.nb[2], y = (cp / g.nb[2]) % g.nb[1], x = cp / (g.nb[2] * g.nb[1]);
+    int nc = g.rowptr[r + 1] - g.rowptr[r];
+    if (s >= nc) return;
+    int x0 = x > 2 ? x - 2 : 0;
+    int y0 = y > 2 ? y - 2 : 0, y1 = y + 2 < g.nb[1] - 1 ? y + 2 : g.nb[1] - 1;
+    int z0 = z > 2 ? z - 2 : 0, z1 = z + 2 < g.nb[2] - 1 ? z + 2 : g.nb[2] - 1;
+    int nyb = y1 - y0 + 1, nzb = z1 - z0 + 1;
+    int k2 = s % 3, q = s / 3;
+    int cz = z0 + q % nzb, cy = y0 + (q / nzb) % nyb, cx = x0 + q / (nzb * nyb);
+    long c = 3 * cp_index(g, cx, cy, cz) + k2;
+    vals[g.rowptr[r] + s] = (c == r) ? T(1) : T(0);
+    if (c != r) vals[g.rowptr[c] + csr_pos(g, cx, cy, cz, x, y, z, r % 3)] = T(0);
+}
+
+/* column indices of the CSR pattern, one thread per row */
+__global__ void k_csr_cols(igab_geom g, int *__restrict__ cols)
+{
+    long r = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (r >= g.ndof) return;
+    int cp = (int)(r / 3);
+    int z = cp % g.nb[2], y = (cp / g.nb[2]) % g.nb[1], x = cp / (g.nb[2] * g.nb[1]);
+    int x0 = x > 2 ? x - 2 : 0, x1 = x + 2 < g.nb[0] - 1 ? x + 2 : g.nb[0] - 1;
+    int y0 = y > 2 ? y - 2 : 0, y1 = y + 2 < g.nb[1] - 1 ? y + 2 : g.nb[1] - 1;
+    int z0 = z > 2 ? z - 2 : 0, z1 = z + 2 < g.nb[2] - 1 ? z + 2 : g.nb[2] - 1;
+    long o = g.rowptr[r];
+    for (int cx = x0; cx <= x1; cx++)
+        for (int cy = y0; cy <= y1; cy++)
+            for (int cz = z0; cz <= z1; cz++)
+                for (int k = 0; k < 3; k++) cols[o++] = (int)(3 * cp_index(g, cx, cy, cz) + k);
+}
+
+template <typename T>
+__global__ void k_check_finite(const T *__restrict__ v, long n, int *__restrict__ flag)
+{
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long stride = (long)gridDim.x * blockDim.x;
+    bool bad = false;
+    for (; i < n; i += stride) bad |= !isfinite(v[i]);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(flag, 1);
+}
+
+long tiles_of_colour(const igab_geom &g, int TE, int colour)
+{
+    long n = 1;
+    for (int d = 0; d < 3; d++) {
+        int c = (colour >> d) & 1;
+        int nt = (g.ne[d] + TE - 1) / TE;
+        n *= nt > c ? (nt - c + 1) / 2 : 0;
+    }
+    return n;
+}
+
+template <int TE>
+int launch_res_volume(igab_ctx *c, const igab_geom &g, const double *dU, double *dR)
+{
+    size_t sm = sizeof(res_smem<TE>);
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_res_volume<TE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    for (int colour = 0; colour < 8; colour++) {
+        long nblk = tiles_of_colour(g, TE, colour);
+        if (nblk == 0) continue;
+        k_res_volume<TE><<<(unsigned)nblk, 256, sm, c->stream>>>(g, dU, dR, colour);
+        c->last_launches++;
+    }
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+template <typename T, int TE>
+int launch_tan_volume(igab_ctx *c, const igab_geom &g, const double *dU, T *dv)
+{
+    size_t sm = sizeof(tan_smem<T, TE>);
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_volume<T, TE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    for (int colour = 0; colour < 8; colour++) {
+        long nblk = tiles_of_colour(g, TE, colour);
+        if (nblk == 0) continue;
+        k_tan_volume<T, TE><<<(unsigned)nblk, 256, sm, c->stream>>>(g, dU, dv, colour);
+        c->last_launches++;
+    }
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+template <typename T>
+int launch_tangent_t(igab_ctx *c, const double *dU, T *dv)
+{
+    igab_geom g = c->geom();
+    IGAB_CUDA_TRY(cudaMemsetAsync(dv, 0, (size_t)c->nnz * sizeof(T), c->stream));
+    igab_mark(c, 3);
+    int l0 = c->last_launches;
+    int e = launch_tan_volume<T, 2>(c, g, dU, dv);
+    if (e) return e;
+    c->nvol_tan = c->last_launches - l0;
+    igab_mark(c, 4);
+    if (c->nd > 0) {
+        long n = c->nd * 375;
+        k_tan_dirichlet<T><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(g, c->nd, c->d_drow, dv);
+        c->last_launches++;
+        IGAB_CUDA_TRY(cudaGetLastError());
+    }
+    igab_mark(c, 5);
+    c->ev_tan = c->profiling;
+    return 0;
+}
+
+} /* namespace */
+
+int igab_launch_residual(igab_ctx *c, const double *dU, double *dR)
+{
+    c->last_launches = 0;
+    igab_geom g = c->geom();
+    IGAB_CUDA_TRY(cudaMemsetAsync(dR, 0, (size_t)c->ndof * sizeof(double), c->stream));
+    igab_mark(c, 0);
+    int e = c->tile_res == 4 ? launch_res_volume<4>(c, g, dU, dR) : launch_res_volume<2>(c, g, dU, dR);
+    if (e) return e;
+    c->nvol_res = c->last_launches;
+    igab_mark(c, 1);
+    if (c->neumann_nonzero && c->n_neu_rows > 0) {
+        k_res_neumann<<<(unsigned)((c->n_neu_rows + 127) / 128), 128, 0, c->stream>>>(
+            g, c->n_neu_rows, c->d_neu_row, c->d_neu_ptr, c->d_neu_ent, c->d_combo_info, c->d_dnz, c->d_hval, dR);
+        c->last_launches++;
+        IGAB_CUDA_TRY(cudaGetLastError());
+    }
+    if (c->nd > 0) {
+        k_res_dirichlet<<<(unsigned)((c->nd + 255) / 256), 256, 0, c->stream>>>(c->nd, c->d_drow, c->d_dg, dU, dR);
+        c->last_launches++;
+        IGAB_CUDA_TRY(cudaGetLastError());
+    }
+    igab_mark(c, 2);
+    c->ev_res = c->profiling;
+    return 0;
+}
+
+int igab_launch_tangent(igab_ctx *c, const double *dU, void *dvals, int prec)
+{
+    c->last_launches = 0;
+    if (prec == IGAB_PREC_FP64) return launch_tangent_t<double>(c, dU, (double *)dvals);
+    if (prec == IGAB_PREC_FP32) return launch_tangent_t<float>(c, dU, (float *)dvals);
+    return IGAB_ERR_ARG;
+}
+
+int igab_launch_csr_cols(igab_ctx *c, int *dcols)
+{
+    igab_geom g = c->geom();
+    k_csr_cols<<<(unsigned)((c->ndof + 255) / 256), 256, 0, c->stream>>>(g, dcols);
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int igab_launch_check_finite(igab_ctx *c, const void *dev, long n, int prec, int *all_finite)
+{
+    int *dflag = nullptr;
+    IGAB_CUDA_TRY(cudaMallocAsync((void **)&dflag, sizeof(int), c->stream));
+    IGAB_CUDA_TRY(cudaMemsetAsync(dflag, 0, sizeof(int), c->stream));
+    unsigned nb = (unsigned)((n + 255) / 256);
+    if (nb > 148u * 16u) nb = 148u * 16u;
+    if (nb == 0) nb = 1;
+    if (prec == IGAB_PREC_FP64)
+        k_check_finite<double><<<nb, 256, 0, c->stream>>>((const double *)dev, n, dflag);
+    else
+        k_check_finite<float><<<nb, 256, 0, c->stream>>>((const float *)dev, n, dflag);
+    int h = 0;
+    IGAB_CUDA_TRY(cudaMemcpyAsync(&h, dflag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    IGAB_CUDA_TRY(cudaFreeAsync(dflag, c->stream));
+    IGAB_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    *all_finite = h == 0;
+    return 0;
+}
+
+/* ============================================================ set-up kernels */
+
+namespace {
+/* 1-D basis tables at the Gauss points of every element of one direction
+ * (mesh/nurbs/eval_Bspline.c:64-74 evaluated at src/snesiga_Residual.c:116-121 points) */
+__global__ void k_basis_tables(const double *__restrict__ kv, int ne, const double *__restrict__ gx,
+                               const double *__restrict__ gw, double *__restrict__ tab,
+                               double *__restrict__ wh, double *__restrict__ xq)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ne * IGAB_NQ) return;
+    int e = t / IGAB_NQ, q = t % IGAB_NQ;
+    double X0 = kv[e + 2], X1 = kv[e + 3];
+    double xi = gx[q];
+    double x = (-xi + 1.0) * X0 + xi * X1;
+    double out[3][3];
+    double win[6];
+    for (int i = 0; i < 6; i++) win[i] = kv[e + i];
+    igab_bspline_p2(win, x, out);
+    for (int l = 0; l < 3; l++)
+        for (int k = 0; k < 3; k++) tab[(long)e * IGAB_TAB1D + q * 9 + l * 3 + k] = out[l][k];
+    wh[(long)e * IGAB_NQ + q] = gw[q] * (X1 - X0);
+    xq[(long)e * IGAB_NQ + q] = x;
+}
+} /* namespace */
+
+int igab_launch_basis_tables(igab_ctx *c, int d, const double *dkv, const double *dgx, const double *dgw)
+{
+    int n = c->ne[d] * IGAB_NQ;
+    k_basis_tables<<<(n + 127) / 128, 128, 0, c->stream>>>(dkv, c->ne[d], dgx, dgw, c->d_tab[d], c->d_wh[d], c->d_xq[d]);
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+/* ============================================================ FMA peak probe */
+namespace {
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_peak(T *out, int iters, T b, T c)
+{
+    T a0 = T(threadIdx.x), a1 = a0 + T(1), a2 = a0 + T(2), a3 = a0 + T(3);
+    T a4 = a0 + T(4), a5 = a0 + T(5), a6 = a0 + T(6), a7 = a0 + T(7);
+    for (int i = 0; i < iters; i++) {
+        a0 = a0 * b + c; a1 = a1 * b + c; a2 = a2 * b + c; a3 = a3 * b + c;
+        a4 = a4 * b + c; a5 = a5 * b + c; a6 = a6 * b + c; a7 = a7 * b + c;
+    }
+    T s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == T(-12345)) out[0] = s;   /* keeps the chains live */
+}
+
+template <typename T>
+int fma_peak_t(double *tflops)
+{
+    int dev = 0, nsm = 0;
+    IGAB_CUDA_TRY(cudaGetDevice(&dev));
+    IGAB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    T *out = nullptr;
+    IGAB_CUDA_TRY(cudaMalloc((void **)&out, sizeof(T)));
+    cudaEvent_t e0, e1;
+    IGAB_CUDA_TRY(cudaEventCreate(&e0));
+    IGAB_CUDA_TRY(cudaEventCreate(&e1));
+    const int iters = 1 << 14;
+    unsigned nblk = (unsigned)nsm * 8u;
+    k_fma_peak<T><<<nblk, 256>>>(out, iters, T(0.999999), T(1e-7));   /* warm-up */
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; rep++) {
+        cudaEventRecord(e0);
+        k_fma_peak<T><<<nblk, 256>>>(out, iters, T(0.999999), T(1e-7));
+        cudaEventRecord(e1);
+        IGAB_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) best = ms;
+    }
+    IGAB_CUDA_TRY(cudaGetLastError());
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    double flops = 2.0 * 8.0 * iters * (double)nblk * 256.0;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return 0;
+}
+} /* namespace */
+
+int igab_launch_fma_peak(int prec, double *tflops)
+{
+    return prec == IGAB_PREC_FP64 ? fma_peak_t<double>(tflops) : fma_peak_t<float>(tflops);
+}

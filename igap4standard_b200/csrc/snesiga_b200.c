@@ -1,0 +1,453 @@
+/*
+ * PETSc SNES callbacks on top of libigap4_b200 (include/snesiga_b200.h).
+ *
+ * Host C only: PETSc objects are read and written through their public API
+ * (VecGetArrayRead, VecGetArray, MatSeqAIJGetArray, MatGetRowIJ), the
+ * assembly itself happens on the GPU through the igab C ABI.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include "petscsnes.h"
+#include "igap4_structs.h"
+#include "igab.h"
+#include "snesiga_b200.h"
+
+#ifndef PETSC_ERR_SUP
+#define PETSC_ERR_SUP 56
+#endif
+#ifndef PETSC_ERR_FP
+#define PETSC_ERR_FP 72
+#endif
+#ifndef PETSC_ERR_LIB
+#define PETSC_ERR_LIB 76
+#endif
+
+/* the application's traction hook; weak so that the library loads without one */
+extern void neumann(double *neumann_, double par_neumann[], int face_id, int bc_order, int idof, double xq[]) __attribute__((weak));
+
+typedef void (*neumann_fn)(double *, double[], int, int, int, double[]);
+
+typedef struct gpu_state {
+    IGA *app;
+    igab_ctx *ctx;
+    int device;
+    long ndof, nnz;
+    neumann_fn nfn;
+    int npol, nwatch, neu_done;
+    double *nwatch_copy;
+    long npts;
+    double *nxyz;   /* 3 per point */
+    int *nmeta;     /* face, order, dof per point */
+    double *nval;
+    Mat pattern_ok; /* last matrix whose pattern was checked */
+    int prec;
+    double *vals32; /* host widening buffer for the FP32 mode (floats) */
+    double ms[4];
+    struct gpu_state *next;
+} gpu_state;
+
+static gpu_state *g_states = NULL;
+
+static double now_ms(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
+}
+
+static gpu_state *find_state(void *app)
+{
+    for (gpu_state *s = g_states; s; s = s->next)
+        if (s->app == (IGA *)app) return s;
+    return NULL;
+}
+
+static PetscErrorCode map_err(int rc)
+{
+    if (rc == IGAB_OK) return 0;
+    if (rc == IGAB_ERR_NONFINITE) return PETSC_ERR_FP;
+    if (rc == IGAB_ERR_UNSUPPORTED || rc == IGAB_ERR_ARG) return PETSC_ERR_SUP;
+    if (rc == IGAB_ERR_NOMEM) return PETSC_ERR_MEM;
+    return PETSC_ERR_LIB;
+}
+
+static int create_state(IGA *app, int device, gpu_state **out)
+{
+    Phys *phys = app->phys;
+    Nurbs *nurbs = app->nurbs;
+    BC *bc = app->bc;
+    int nproc = 1;
+    MPI_Comm_size(MPI_COMM_WORLD, &nproc);
+    if (nproc != 1 || nurbs->nsendPart != 0 || nurbs->nrecvPart != 0) {
+        fprintf(stderr, "snesiga_b200: only single-rank, non-periodic meshes are supported\n");
+        return PETSC_ERR_SUP;
+    }
+    if (phys->ndim != 3 || phys->ndof != 3 || nurbs->porder != 2 || (phys->torder != 0 && phys->torder != 2)) {
+        fprintf(stderr, "snesiga_b200: needs ndim = ndof = 3, porder = 2 and torder 0 (ge) or 2 (getime)\n");
+        return PETSC_ERR_SUP;
+    }
+    igab_mesh_desc d;
+    memset(&d, 0, sizeof(d));
+    d.phys = phys->torder == 0 ? IGAB_PHYS_GE : IGAB_PHYS_GETIME;
+    long nk = 0;
+    for (int i = 0; i < 3; i++) { d.nelem[i] = nurbs->nelem[i]; nk += nurbs->nelem[i] + 5; }
+    double *knots = (double *)malloc((size_t)nk * sizeof(double));
+    if (!knots) return PETSC_ERR_MEM;
+    long o = 0;
+    for (int i = 0; i < 3; i++) {
+        if (nurbs->nknot[i] != nurbs->nelem[i] + 5) { free(knots); return PETSC_ERR_SUP; }
+        memcpy(knots + o, nurbs->knotVector[i], (size_t)nurbs->nknot[i] * sizeof(double));
+        o += nurbs->nknot[i];
+    }
+    d.knots = knots;
+    memcpy(d.par_mat, phys->par_mat, 9 * sizeof(double));
+    memcpy(d.bc_type, bc->bc_type, 36 * sizeof(int));
+    memcpy(d.par_periodic, bc->par_periodic, 9 * sizeof(double));
+    memcpy(d.par_dirichlet, bc->par_dirichlet, 9 * sizeof(double));
+    gpu_state *s = (gpu_state *)calloc(1, sizeof(gpu_state));
+    if (!s) { free(knots); return PETSC_ERR_MEM; }
+    int rc = igab_create(&d, device, &s->ctx);
+    free(knots);
+    if (rc) {
+        fprintf(stderr, "snesiga_b200: igab_create failed: %s\n", igab_last_error());
+        free(s);
+        return map_err(rc);
+    }
+    s->app = app;
+    s->device = device;
+    igab_sizes(s->ctx, &s->ndof, &s->nnz, NULL);
+    if (s->ndof != app->nselfIdx) {
+        fprintf(stderr, "snesiga_b200: dof count %ld does not match nselfIdx %d\n", s->ndof, app->nselfIdx);
+        igab_destroy(s->ctx);
+        free(s);
+        return PETSC_ERR_SUP;
+    }
+    s->nfn = neumann;
+    igab_neumann_points(s->ctx, &s->npts, NULL, NULL);
+    if (s->npts > 0) {
+        s->nxyz = (double *)malloc((size_t)s->npts * 3 * sizeof(double));
+        s->nmeta = (int *)malloc((size_t)s->npts * 3 * sizeof(int));
+        s->nval = (double *)malloc((size_t)s->npts * sizeof(double));
+        if (!s->nxyz || !s->nmeta || !s->nval) { igab_destroy(s->ctx); free(s); return PETSC_ERR_MEM; }
+        igab_neumann_points(s->ctx, &s->npts, s->nxyz, s->nmeta);
+    }
+    s->next = g_states;
+    g_states = s;
+    *out = s;
+    return 0;
+}
+
+static int get_state(void *app, gpu_state **out)
+{
+    gpu_state *s = find_state(app);
+    if (s) { *out = s; return 0; }
+    return create_state((IGA *)app, 0, out);
+}
+
+PetscErrorCode snesiga_gpu_init(void *app_, int device)
+{
+    if (find_state(app_)) return 0;
+    gpu_state *s;
+    return create_state((IGA *)app_, device, &s);
+}
+
+PetscErrorCode snesiga_gpu_free(void *app_)
+{
+    gpu_state **pp = &g_states;
+    while (*pp) {
+        if ((*pp)->app == (IGA *)app_) {
+            gpu_state *s = *pp;
+            *pp = s->next;
+            igab_destroy(s->ctx);
+            free(s->nxyz); free(s->nmeta); free(s->nval); free(s->nwatch_copy); free(s->vals32);
+            free(s);
+            return 0;
+        }
+        pp = &(*pp)->next;
+    }
+    return 0;
+}
+
+int snesiga_gpu_set_neumann(void *app_, neumann_fn fn)
+{
+    gpu_state *s;
+    int rc = get_state(app_, &s);
+    if (rc) return rc;
+    s->nfn = fn;
+    s->neu_done = 0;
+    return 0;
+}
+
+int snesiga_gpu_set_neumann_policy(void *app_, int policy, int n_watch)
+{
+    gpu_state *s;
+    int rc = get_state(app_, &s);
+    if (rc) return rc;
+    if (policy < 0 || policy > 2 || (policy == 2 && n_watch < 1)) return PETSC_ERR_SUP;
+    s->npol = policy;
+    s->nwatch = n_watch;
+    free(s->nwatch_copy);
+    s->nwatch_copy = NULL;
+    s->neu_done = 0;
+    return 0;
+}
+
+int snesiga_gpu_set_tangent_precision(void *app_, int prec)
+{
+    gpu_state *s;
+    int rc = get_state(app_, &s);
+    if (rc) return rc;
+    if (prec != IGAB_PREC_FP64 && prec != IGAB_PREC_FP32) return PETSC_ERR_SUP;
+    s->prec = prec;
+    return 0;
+}
+
+void *snesiga_gpu_context(void *app_)
+{
+    gpu_state *s = find_state(app_);
+    return s ? (void *)s->ctx : NULL;
+}
+
+int snesiga_gpu_last_timings(void *app_, double ms[4])
+{
+    gpu_state *s = find_state(app_);
+    if (!s) return PETSC_ERR_SUP;
+    memcpy(ms, s->ms, sizeof(s->ms));
+    return 0;
+}
+
+/* parameters the application may change between callbacks */
+static int sync_params(gpu_state *s)
+{
+    IGA *app = s->app;
+    int rc = igab_set_par_mat(s->ctx, app->phys->par_mat);
+    if (!rc) rc = igab_set_par_dirichlet(s->ctx, app->bc->par_dirichlet);
+    if (!rc) rc = igab_set_par_periodic(s->ctx, app->bc->par_periodic);
+    if (!rc && app->phys->torder > 0)
+        for (int lev = 1; lev <= app->phys->torder && !rc; lev++)
+            rc = igab_set_history(s->ctx, lev, app->U_hist + (size_t)lev * (size_t)app->nselfIdx, 0);
+    return rc;
+}
+
+/* evaluate the application's traction at the surface Gauss points
+ * (the neumann() calls of src/snesiga_Residual.c:264 and :304) */
+static int sync_neumann(gpu_state *s)
+{
+    if (s->npts == 0) return 0;
+    double *pn = s->app->bc->par_neumann;
+    if (s->neu_done) {
+        if (s->npol == 1) return 0;
+        if (s->npol == 2 && s->nwatch_copy && memcmp(s->nwatch_copy, pn, (size_t)s->nwatch * sizeof(double)) == 0) return 0;
+    }
+    if (!s->nfn) {
+        fprintf(stderr, "snesiga_b200: Neumann boundaries present but no neumann() hook is defined\n");
+        return IGAB_ERR_ARG;
+    }
+    for (long k = 0; k < s->npts; k++) {
+        double xq[3] = {s->nxyz[3 * k], s->nxyz[3 * k + 1], s->nxyz[3 * k + 2]};
+        double v = 0.0;
+        s->nfn(&v, pn, s->nmeta[3 * k], s->nmeta[3 * k + 1], s->nmeta[3 * k + 2], xq);
+        s->nval[k] = v;
+    }
+    if (s->npol == 2) {
+        if (!s->nwatch_copy) s->nwatch_copy = (double *)malloc((size_t)s->nwatch * sizeof(double));
+        if (s->nwatch_copy) memcpy(s->nwatch_copy, pn, (size_t)s->nwatch * sizeof(double));
+    }
+    s->neu_done = 1;
+    return igab_set_neumann_values(s->ctx, s->nval);
+}
+
+static void keep_history(IGA *app, const PetscScalar *u)
+{
+    memcpy(app->U_hist, u, (size_t)app->nselfIdx * sizeof(double));
+}
+
+PetscErrorCode snesiga_b200_Residual(SNES snes, Vec U_, Vec Residual_, void *app_)
+{
+    (void)snes;
+    double t0 = now_ms();
+    gpu_state *s;
+    int rc = get_state(app_, &s);
+    if (rc) return rc;
+    const PetscScalar *u;
+    PetscScalar *r;
+    VecGetArrayRead(U_, &u);
+    keep_history(s->app, u);
+    rc = sync_params(s);
+    if (!rc) rc = sync_neumann(s);
+    if (!rc) {
+        VecGetArray(Residual_, &r);
+        rc = igab_residual(s->ctx, u, r);
+        VecRestoreArray(Residual_, &r);
+    }
+    VecRestoreArrayRead(U_, &u);
+    VecAssemblyBegin(Residual_);
+    VecAssemblyEnd(Residual_);
+    s->ms[0] = now_ms() - t0;
+    if (rc) fprintf(stderr, "snesiga_b200: residual failed: %s\n", igab_last_error());
+    return map_err(rc);
+}
+
+/* Put the structured AIJ pattern into P the first time (as the reference's
+ * first MatSetValues pass does) and check that P's CSR is exactly it. */
+static int ensure_pattern(gpu_state *s, Mat P)
+{
+    if (s->pattern_ok == P) return 0;
+    PetscBool assembled = PETSC_FALSE;
+    MatAssembled(P, &assembled);
+    long ndof = s->ndof, nnz = s->nnz;
+    int *rowptr = (int *)malloc(((size_t)ndof + 1) * sizeof(int));
+    int *cols = (int *)malloc((size_t)nnz * sizeof(int));
+    if (!rowptr || !cols) { free(rowptr); free(cols); return IGAB_ERR_NOMEM; }
+    int rc = igab_csr_pattern(s->ctx, rowptr, cols);
+    if (rc) { free(rowptr); free(cols); return rc; }
+    if (!assembled) {
+        int maxc = 0;
+        for (long r = 0; r < ndof; r++)
+            if (rowptr[r + 1] - rowptr[r] > maxc) maxc = rowptr[r + 1] - rowptr[r];
+        double *zeros = (double *)calloc((size_t)maxc, sizeof(double));
+        if (!zeros) { free(rowptr); free(cols); return IGAB_ERR_NOMEM; }
+        for (long r = 0; r < ndof; r++) {
+            PetscInt row = (PetscInt)r;
+            MatSetValues(P, 1, &row, rowptr[r + 1] - rowptr[r], cols + rowptr[r], zeros, INSERT_VALUES);
+        }
+        free(zeros);
+        MatAssemblyBegin(P, MAT_FINAL_ASSEMBLY);
+        MatAssemblyEnd(P, MAT_FINAL_ASSEMBLY);
+    }
+    PetscInt n;
+    const PetscInt *ia, *ja;
+    PetscBool done;
+    MatGetRowIJ(P, 0, PETSC_FALSE, PETSC_FALSE, &n, &ia, &ja, &done);
+    int same = done && n == ndof && ia[ndof] == nnz;
+    if (same) same = memcmp(ia, rowptr, ((size_t)ndof + 1) * sizeof(int)) == 0 &&
+                     memcmp(ja, cols, (size_t)nnz * sizeof(int)) == 0;
+    MatRestoreRowIJ(P, 0, PETSC_FALSE, PETSC_FALSE, &n, &ia, &ja, &done);
+    free(rowptr);
+    free(cols);
+    if (!same) {
+        fprintf(stderr, "snesiga_b200: the tangent matrix does not have the structured AIJ pattern\n");
+        return IGAB_ERR_ARG;
+    }
+    s->pattern_ok = P;
+    return 0;
+}
+
+PetscErrorCode snesiga_b200_Tangent(SNES snes, Vec U_, Mat Tangent_, Mat Pmat_, void *app_)
+{
+    (void)snes;
+    double t0 = now_ms();
+    gpu_state *s;
+    int rc = get_state(app_, &s);
+    if (rc) return rc;
+    const PetscScalar *u;
+    VecGetArrayRead(U_, &u);
+    keep_history(s->app, u);
+    rc = sync_params(s);
+    if (!rc) rc = ensure_pattern(s, Pmat_);
+    if (!rc) {
+        PetscScalar *a;
+        MatSeqAIJGetArray(Pmat_, &a);
+        if (s->prec == IGAB_PREC_FP64) {
+            rc = igab_tangent(s->ctx, u, a, IGAB_PREC_FP64);
+        } else {
+            /* FP32 values land in the upper half of the double array (bytes 4*nnz..8*nnz);
+             * widening in ascending order reads f[k] before any write reaches it */
+            float *f = (float *)((char *)a + 4 * (size_t)s->nnz);
+            rc = igab_tangent(s->ctx, u, f, IGAB_PREC_FP32);
+            if (!rc)
+                for (long k = 0; k < s->nnz; k++) a[k] = (double)f[k];
+        }
+        MatSeqAIJRestoreArray(Pmat_, &a);
+    }
+    VecRestoreArrayRead(U_, &u);
+    if (!rc && Tangent_ != Pmat_) {
+        MatAssemblyBegin(Tangent_, MAT_FINAL_ASSEMBLY);
+        MatAssemblyEnd(Tangent_, MAT_FINAL_ASSEMBLY);
+    }
+    s->ms[1] = now_ms() - t0;
+    if (rc) fprintf(stderr, "snesiga_b200: tangent failed: %s\n", igab_last_error());
+    return map_err(rc);
+}
+
+PetscErrorCode snesiga_Residual(SNES snes, Vec U_, Vec Residual_, void *app_)
+{
+    return snesiga_b200_Residual(snes, U_, Residual_, app_);
+}
+
+PetscErrorCode snesiga_Tangent(SNES snes, Vec U_, Mat Tangent_, Mat Pmat_, void *app_)
+{
+    return snesiga_b200_Tangent(snes, U_, Tangent_, Pmat_, app_);
+}
+
+/* Single-rank snesiga_init (src/snesiga_init.c:12-132 with nproc = 1 and
+ * no halo parts): identity index maps, universal = local ordering, one
+ * sequential AIJ matrix preallocated with the per-row count of
+ * src/snesiga_init.c:341-359, callbacks installed. */
+void snesiga_init(void *app_, void *phys_, void *nurbs_, void *bc_, void *snesassmbl_, void *iocomm_)
+{
+    IGA *app = (IGA *)app_;
+    Phys *phys = (Phys *)phys_;
+    Nurbs *nurbs = (Nurbs *)nurbs_;
+    SNESAssmbl *sa = (SNESAssmbl *)snesassmbl_;
+    IOcomm *io = (IOcomm *)iocomm_;
+    int ndof = phys->ndof, p = nurbs->porder;
+    int *nb = nurbs->nbasis;
+    app->phys = phys;
+    app->nurbs = nurbs;
+    app->bc = (BC *)bc_;
+    int nproc = 1;
+    MPI_Comm_size(MPI_COMM_WORLD, &nproc);
+    if (nproc != 1 || nurbs->nsendPart != 0 || nurbs->nrecvPart != 0)
+        fprintf(stderr, "snesiga_b200: snesiga_init supports one rank without halo parts; callbacks will fail\n");
+    int n = ndof * nb[0] * nb[1] * nb[2];
+    app->nselfIdx = n;
+    app->selfIdx = (int *)malloc((size_t)n * sizeof(int));
+    for (int i = 0; i < n; i++) app->selfIdx[i] = i;
+    app->nsendIdx = 0;
+    app->sendIdx = (int *)malloc(sizeof(int));
+    app->sendPtr = (int *)calloc(1, sizeof(int));
+    app->nrecvIdx = 0;
+    app->recvIdx = (int *)malloc(sizeof(int));
+    app->recvPtr = (int *)calloc(1, sizeof(int));
+    io->nDof = n;
+    io->nDof_array = (int *)malloc(sizeof(int));
+    io->nDof_array[0] = n;
+    io->iDof_displ_array = (int *)malloc(2 * sizeof(int));
+    io->iDof_displ_array[0] = 0;
+    io->iDof_displ_array[1] = n;
+    io->nDof_global = n;
+    io->universalIdx = (int *)malloc((size_t)n * sizeof(int));
+    for (int c = 0, ia = 0; c < nb[0] * nb[1] * nb[2]; c++)
+        for (int d = 0; d < ndof; d++) io->universalIdx[ia++] = ndof * nurbs->universalIdx_temp[c] + d;
+    free(nurbs->universalIdx_temp);
+    nurbs->universalIdx_temp = NULL;
+    app->U_hist = (double *)malloc((size_t)(phys->torder + 1) * (size_t)n * sizeof(double));
+    app->globalIdx = (int *)malloc((size_t)n * sizeof(int));
+    for (int i = 0; i < n; i++) app->globalIdx[i] = i;
+    VecCreateMPI(MPI_COMM_WORLD, n, n, &sa->Residual_);
+    VecDuplicate(sa->Residual_, &sa->U);
+    int *d_nz = (int *)malloc((size_t)n * sizeof(int));
+    int ia = 0;
+    for (int x = 0; x < nb[0]; x++)
+        for (int y = 0; y < nb[1]; y++)
+            for (int z = 0; z < nb[2]; z++) {
+                int cx = (x < p ? x : p) + 1 + (x > nb[0] - 1 - p ? nb[0] - 1 - x : p);
+                int cy = (y < p ? y : p) + 1 + (y > nb[1] - 1 - p ? nb[1] - 1 - y : p);
+                int cz = (z < p ? z : p) + 1 + (z > nb[2] - 1 - p ? nb[2] - 1 - z : p);
+                for (int d = 0; d < ndof; d++) d_nz[ia++] = ndof * cx * cy * cz;
+            }
+    MatCreateAIJ(MPI_COMM_WORLD, n, n, n, n, 0, d_nz, 0, NULL, &sa->Tangent_);
+    free(d_nz);
+    free(nurbs->sendBlock);
+    free(nurbs->recvBlock);
+    nurbs->sendBlock = NULL;
+    nurbs->recvBlock = NULL;
+    MatSetOption(sa->Tangent_, MAT_KEEP_NONZERO_PATTERN, PETSC_TRUE);
+    MatSetOption(sa->Tangent_, MAT_NO_OFF_PROC_ZERO_ROWS, PETSC_TRUE);
+    MatSetOption(sa->Tangent_, MAT_SUBSET_OFF_PROC_ENTRIES, PETSC_TRUE);
+    sa->snes_Residual = snesiga_b200_Residual;
+    sa->snes_Tangent = snesiga_b200_Tangent;
+}

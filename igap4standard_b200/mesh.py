@@ -1,0 +1,94 @@
+"""Mesh, material and boundary-condition set-up for single-rank IGA cases.
+
+The reference builds open uniform knot vectors (mesh/nurbs/nurbs_genuniform.c:36-38)
+with 2^mref elements; here any element count is allowed and interior knots can
+be perturbed (the reference's disabled hook at nurbs_genuniform.c:37 perturbs
+knots the same way), because physical coordinates are knot coordinates
+(mesh/nurbs/eval_Bspline.c:64-74) and there is no separate geometry map.
+"""
+import numpy as np
+
+P = 2  # quadratic C1 B-splines (eval_Bspline requires p == 2)
+
+# par_mat of phys/ge/init.c:17-18 and phys/getime/init.c:17-18
+PAR_MAT_DEFAULT = np.array([0.25, 0.50, 500.0, 250.0, 0.025, 1.0, 1.0, 1.0e-3 * 0.5, 0.0])
+
+
+def open_knot_vector(n, perturb=0.0, rng=None, length=1.0):
+    """Open knot vector on [0, length] with n elements: p+1 repeated end knots.
+
+    perturb: interior knots move by uniform(-perturb*h, +perturb*h), h = length/n
+    (must stay below 0.5 so the knots stay increasing)."""
+    if n < 1:
+        raise ValueError("n must be >= 1")
+    if not 0.0 <= perturb < 0.5:
+        raise ValueError("perturb must be in [0, 0.5)")
+    h = length / n
+    inner = np.arange(1, n) * h
+    if perturb > 0 and n > 1:
+        rng = rng if rng is not None else np.random.default_rng(0)
+        inner = inner + rng.uniform(-perturb * h, perturb * h, size=n - 1)
+    return np.concatenate([np.zeros(P + 1), inner, np.full(P + 1, length)])
+
+
+def knots_for(nelem, perturb=0.0, seed=0):
+    """Three knot vectors back to back (the igab_mesh_desc.knots layout)."""
+    rng = np.random.default_rng(seed)
+    return np.concatenate([open_knot_vector(int(n), perturb, rng) for n in nelem])
+
+
+def par_mat_from_lame(lam, mu, ell, r=10.0, base=PAR_MAT_DEFAULT):
+    """Map (lambda, mu, strain-gradient length) onto phys/ge's par_mat.
+
+    The quadratic part of the ge energy (phys/ge/density.c:49) is
+    e0*vvol^2 + e345*(E01^2+E02^2+E12^2) + c37*(va^2+vb^2); matching the
+    St-Venant-Kirchhoff energy lambda/2 tr(E)^2 + mu E:E gives e0 = 3 lambda/2 + mu,
+    e345 = 2 mu, c37 = mu.  c37 = -6 curv / (r^2 (1 + 2 curv)) (phys/ge/residual.c:45-47),
+    so curv = -mu r^2 / (6 + 2 mu r^2); le = ell."""
+    pm = np.array(base, dtype=np.float64).copy()
+    curv = -mu * r * r / (6.0 + 2.0 * mu * r * r)
+    pm[0] = r
+    pm[1] = curv
+    pm[2] = 1.5 * lam + mu
+    pm[3] = 2.0 * mu
+    pm[4] = ell
+    return pm
+
+
+def ge_coefficients(par):
+    """(c36, c37, c38) of the energy for a par_mat (phys/ge/residual.c:36-38)."""
+    r, cu = par[0], par[1]
+    q = 1.3333333333333333 * r - 1.3333333333333333 * r * cu
+    den = r * r - 2 * (r * r) * cu - r * q
+    return (-(q / ((r * r) * den)), (2 * cu) / den, -(1 / ((r * r) * den)))
+
+
+def bc_config0():
+    """BCs of the static configs: face 0 (x=0) u = 0 and du/dn = 0; face 1 (x=1)
+    u_x Dirichlet, the rest traction-free; faces 2-5 traction-free.
+    Returns (bc_type[36], par_dirichlet[9]) with u_x = 0.01 X on the Dirichlet faces."""
+    bc = np.ones(36, dtype=np.int32)
+    bc[0:6] = 0
+    bc[6] = 0
+    pd = np.zeros(9)
+    pd[0] = 0.01
+    return bc, pd
+
+
+def bc_example():
+    """bc_init of the reference example (example/ex1/main.c:69-95): u = 0 on every
+    face, high-order Neumann everywhere."""
+    row = [0, 0, 0, 1, 1, 1]
+    return np.array(row * 6, dtype=np.int32), np.zeros(9)
+
+
+def n_dof(nelem):
+    return 3 * int(np.prod(np.asarray(nelem) + P))
+
+
+def nnz_of(nelem):
+    nnz = 9
+    for n in nelem:
+        m = int(n) + P
+        nnz *= m + 2 * max(m - 1, 0) + 2 * max(m - 2, 0)
+    return nnz

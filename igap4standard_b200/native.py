@@ -1,0 +1,142 @@
+"""ctypes bindings of the in-tree native libraries (built by igap4standard_b200.build).
+
+There is no CPU fallback: if a library is missing, loading raises
+NativeLibraryMissing and the caller must build it.
+"""
+import ctypes
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIBDIR = os.path.join(_PKG, "lib")
+LIB_CUDA = os.path.join(LIBDIR, "libigap4_b200.so")
+LIB_SUBSET = os.path.join(LIBDIR, "libpetsc_subset.so")
+LIB_DROPIN = os.path.join(LIBDIR, "libsnesiga_b200.so")
+
+c_int_p = ctypes.POINTER(ctypes.c_int)
+c_long_p = ctypes.POINTER(ctypes.c_long)
+c_double_p = ctypes.POINTER(ctypes.c_double)
+vp = ctypes.c_void_p
+
+
+class NativeLibraryMissing(RuntimeError):
+    pass
+
+
+class IgabError(RuntimeError):
+    def __init__(self, where, code, msg=""):
+        super().__init__("%s failed with status %d%s" % (where, code, (": " + msg) if msg else ""))
+        self.code = code
+
+
+class IgabMeshDesc(ctypes.Structure):
+    """igab_mesh_desc of include/igab.h"""
+    _fields_ = [
+        ("phys", ctypes.c_int),
+        ("nelem", ctypes.c_int * 3),
+        ("knots", c_double_p),
+        ("par_mat", ctypes.c_double * 9),
+        ("bc_type", ctypes.c_int * 36),
+        ("par_periodic", ctypes.c_double * 9),
+        ("par_dirichlet", ctypes.c_double * 9),
+    ]
+
+
+# (name, restype, argtypes) of every entry point declared in include/igab.h
+IGAB_API = [
+    ("igab_create", ctypes.c_int, [ctypes.POINTER(IgabMeshDesc), ctypes.c_int, ctypes.POINTER(vp)]),
+    ("igab_destroy", ctypes.c_int, [vp]),
+    ("igab_last_error", ctypes.c_char_p, []),
+    ("igab_version", ctypes.c_int, []),
+    ("igab_sizes", ctypes.c_int, [vp, c_long_p, c_long_p, c_long_p]),
+    ("igab_csr_pattern", ctypes.c_int, [vp, vp, vp]),
+    ("igab_csr_offset", ctypes.c_long, [vp, ctypes.c_long, ctypes.c_long]),
+    ("igab_set_par_mat", ctypes.c_int, [vp, vp]),
+    ("igab_set_par_dirichlet", ctypes.c_int, [vp, vp]),
+    ("igab_set_par_periodic", ctypes.c_int, [vp, vp]),
+    ("igab_neumann_points", ctypes.c_int, [vp, c_long_p, vp, vp]),
+    ("igab_set_neumann_values", ctypes.c_int, [vp, vp]),
+    ("igab_set_history", ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int]),
+    ("igab_residual", ctypes.c_int, [vp, vp, vp]),
+    ("igab_residual_device", ctypes.c_int, [vp, vp, vp]),
+    ("igab_tangent", ctypes.c_int, [vp, vp, vp, ctypes.c_int]),
+    ("igab_tangent_device", ctypes.c_int, [vp, vp, vp, ctypes.c_int]),
+    ("igab_set_stream", ctypes.c_int, [vp, vp]),
+    ("igab_sync", ctypes.c_int, [vp]),
+    ("igab_device_buffers", ctypes.c_int, [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_int]),
+    ("igab_check_finite", ctypes.c_int, [vp, vp, ctypes.c_long, ctypes.c_int, c_int_p]),
+    ("igab_set_tile", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+    ("igab_last_launch_count", ctypes.c_int, [vp, c_int_p]),
+    ("igab_set_profiling", ctypes.c_int, [vp, ctypes.c_int]),
+    ("igab_last_kernel_ms", ctypes.c_int, [vp, c_double_p]),
+    ("igab_fma_peak", ctypes.c_int, [ctypes.c_int, ctypes.c_int, c_double_p]),
+]
+
+# entry points of include/snesiga_b200.h and include/iga_case.h
+DROPIN_API = [
+    ("snesiga_Residual", ctypes.c_int, [vp, vp, vp, vp]),
+    ("snesiga_Tangent", ctypes.c_int, [vp, vp, vp, vp, vp]),
+    ("snesiga_init", None, [vp, vp, vp, vp, vp, vp]),
+    ("snesiga_b200_Residual", ctypes.c_int, [vp, vp, vp, vp]),
+    ("snesiga_b200_Tangent", ctypes.c_int, [vp, vp, vp, vp, vp]),
+    ("snesiga_gpu_init", ctypes.c_int, [vp, ctypes.c_int]),
+    ("snesiga_gpu_free", ctypes.c_int, [vp]),
+    ("snesiga_gpu_set_neumann", ctypes.c_int, [vp, vp]),
+    ("snesiga_gpu_set_neumann_policy", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+    ("snesiga_gpu_set_tangent_precision", ctypes.c_int, [vp, ctypes.c_int]),
+    ("snesiga_gpu_context", vp, [vp]),
+    ("snesiga_gpu_last_timings", ctypes.c_int, [vp, c_double_p]),
+]
+
+CASE_API = [
+    ("iga_case_create", vp, [ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int]),
+    ("iga_case_destroy", None, [vp]),
+    ("iga_case_ndof", ctypes.c_int, [vp]),
+    ("iga_case_set_history", ctypes.c_int, [vp, ctypes.c_int, vp]),
+    ("iga_case_get_history", ctypes.c_int, [vp, ctypes.c_int, vp]),
+    ("iga_case_set_par_neumann", ctypes.c_int, [vp, vp, ctypes.c_int]),
+    ("iga_case_set_par_dirichlet", ctypes.c_int, [vp, vp]),
+    ("iga_case_set_par_mat", ctypes.c_int, [vp, vp]),
+    ("iga_case_residual", ctypes.c_int, [vp, vp, vp]),
+    ("iga_case_tangent", ctypes.c_int, [vp, vp]),
+    ("iga_case_tangent_nnz", ctypes.c_long, [vp]),
+    ("iga_case_tangent_csr", ctypes.c_int, [vp, vp, vp, vp]),
+    ("iga_case_app", vp, [vp]),
+    ("iga_case_snesassmbl", vp, [vp]),
+    ("iga_case_neumann", None, [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]),
+]
+
+_cache = {}
+
+
+def bind(lib, api):
+    for name, res, args in api:
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+def _load(path, api, mode=ctypes.RTLD_GLOBAL):
+    if path in _cache:
+        return _cache[path]
+    if not os.path.exists(path):
+        raise NativeLibraryMissing("%s is not built; run `python -m igap4standard_b200.build`" % path)
+    lib = bind(ctypes.CDLL(path, mode=mode), api)
+    _cache[path] = lib
+    return lib
+
+
+def lib_cuda():
+    return _load(LIB_CUDA, IGAB_API)
+
+
+def lib_dropin():
+    lib_cuda()
+    _load(LIB_SUBSET, [])
+    return _load(LIB_DROPIN, DROPIN_API + CASE_API, mode=ctypes.RTLD_LOCAL)
+
+
+def check(lib, where, rc):
+    if rc != 0:
+        msg = lib.igab_last_error()
+        raise IgabError(where, rc, msg.decode() if msg else "")

@@ -1,0 +1,124 @@
+/*
+ * igab.h -- plain C ABI of the B200 element-assembly library (libigap4_b200.so).
+ *
+ * One context = one single-rank IGA mesh (quadratic C1 B-splines, p = 2,
+ * 4x4x4 Gauss points per element) plus its physics, boundary tables and
+ * device buffers.  Entry points take plain pointers and sizes; every one
+ * returns 0 on success or a nonzero igab_status.  Nothing here needs PETSc.
+ *
+ * The reference interface each entry point replaces (IGAP4STANDARD paths):
+ *   igab_create              snesiga_init            src/snesiga_init.c:12-132
+ *                            (index maps, AIJ preallocation; single rank)
+ *   igab_csr_pattern         MatCreateAIJ + first MatSetValues pattern
+ *                            src/snesiga_init.c:115-124, :341-359
+ *   igab_residual[_device]   snesiga_Residual        src/snesiga_Residual.c:13-417
+ *   igab_tangent[_device]    snesiga_Tangent         src/snesiga_Tangent.c:13-284
+ *   igab_set_history         app->U_hist levels 1..torder   include/iga.h:14
+ *   igab_neumann_points /    the neumann() hook evaluated at the surface
+ *   igab_set_neumann_values  Gauss points            src/snesiga_Residual.c:243-320
+ *   igab_set_par_*           Phys.par_mat, BC.par_dirichlet/par_periodic
+ *                            include/phys.h:16, include/bc.h:6-8
+ *
+ * Numbering: dof = 3*(nb1*nb2*ix + nb2*iy + iz) + d with nb = nelem + 2
+ * (src/snesiga_init.c:89-94, one rank).  The tangent is a CSR matrix with
+ * ascending column indices per row and the exact AIJ pattern the reference
+ * creates (every pair of control points whose supports overlap, 3x3 dofs).
+ */
+#ifndef IGAB_H
+#define IGAB_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct igab_ctx igab_ctx;
+
+enum igab_status {
+    IGAB_OK = 0,
+    IGAB_ERR_ARG = 1,        /* bad argument (size, pointer, enum) */
+    IGAB_ERR_CUDA = 2,       /* a CUDA call failed; message in igab_last_error() */
+    IGAB_ERR_NOMEM = 3,      /* host or device allocation failed */
+    IGAB_ERR_NONFINITE = 4,  /* residual or tangent contains NaN/Inf */
+    IGAB_ERR_UNSUPPORTED = 5 /* physics / order / precision not built */
+};
+
+enum igab_phys { IGAB_PHYS_GE = 0, IGAB_PHYS_GETIME = 1 };
+enum igab_prec { IGAB_PREC_FP64 = 0, IGAB_PREC_FP32 = 1 };
+
+typedef struct {
+    int phys;                 /* igab_phys */
+    int nelem[3];             /* elements per direction */
+    const double *knots;      /* 3 open knot vectors back to back, nelem[d]+5 values each */
+    double par_mat[9];        /* {r, curv, e0, e345, le, rho, cii, dt, t} (phys/ge/init.c:17-18) */
+    int bc_type[36];          /* [face][order][dof], 0 Dirichlet, 1 Neumann (include/bc.h:6) */
+    double par_periodic[9];   /* affine F0 added at Gauss points (src/snesiga_Residual.c:140-144) */
+    double par_dirichlet[9];  /* affine map of the Dirichlet values (src/iga_dirichlet.c:10-12) */
+} igab_mesh_desc;
+
+/* ---- lifetime */
+int igab_create(const igab_mesh_desc *desc, int device, igab_ctx **out);
+int igab_destroy(igab_ctx *ctx);
+const char *igab_last_error(void);
+int igab_version(void);
+
+/* ---- sizes and pattern */
+int igab_sizes(const igab_ctx *ctx, long *ndof, long *nnz, long *nelem_total);
+/* rowptr[ndof+1], cols[nnz] (host arrays; either may be NULL) */
+int igab_csr_pattern(igab_ctx *ctx, int *rowptr, int *cols);
+/* position of entry (row, col) in the CSR value array, or -1 if not in the pattern */
+long igab_csr_offset(const igab_ctx *ctx, long row, long col);
+
+/* ---- parameters (take effect at the next assembly) */
+int igab_set_par_mat(igab_ctx *ctx, const double par_mat[9]);
+int igab_set_par_dirichlet(igab_ctx *ctx, const double par_dirichlet[9]);
+int igab_set_par_periodic(igab_ctx *ctx, const double par_periodic[9]);
+
+/* ---- Neumann data: the caller evaluates its traction at the surface Gauss
+ * points and hands the values over.  n_points = total point count; xyz
+ * receives 3 coordinates per point, meta 3 ints per point (face, order, dof),
+ * in the order the values must be given.  All-zero values skip the kernel. */
+int igab_neumann_points(const igab_ctx *ctx, long *n_points, double *xyz, int *meta);
+int igab_set_neumann_values(igab_ctx *ctx, const double *values);
+
+/* ---- history levels 1..torder of U (transient physics): host or device pointer */
+int igab_set_history(igab_ctx *ctx, int level, const double *U, int on_device);
+
+/* ---- assembly.  _device variants take device pointers and enqueue on the
+ * context stream; the host variants copy U in and the result out. */
+int igab_residual(igab_ctx *ctx, const double *U_host, double *R_host);
+int igab_residual_device(igab_ctx *ctx, const double *U_dev, double *R_dev);
+/* vals: nnz doubles (IGAB_PREC_FP64) or floats (IGAB_PREC_FP32) */
+int igab_tangent(igab_ctx *ctx, const double *U_host, void *vals_host, int prec);
+int igab_tangent_device(igab_ctx *ctx, const double *U_dev, void *vals_dev, int prec);
+
+/* ---- stream / sync / device scratch */
+int igab_set_stream(igab_ctx *ctx, void *cuda_stream);
+int igab_sync(igab_ctx *ctx);
+/* device buffers owned by the context, sized ndof / nnz, for callers without an allocator */
+int igab_device_buffers(igab_ctx *ctx, double **U_dev, double **R_dev, void **vals_dev, int prec);
+/* check a device vector for NaN/Inf (1 = all finite) */
+int igab_check_finite(igab_ctx *ctx, const void *dev, long n, int prec, int *all_finite);
+
+/* ---- tuning: elements per tile edge of the 8-colour schedule (2 or 4), 0 = auto */
+int igab_set_tile(igab_ctx *ctx, int residual_tile, int tangent_tile);
+/* launches issued by the last assembly call (kernel count) */
+int igab_last_launch_count(const igab_ctx *ctx, int *n);
+
+/* ---- measurement: with profiling on, assembly calls record CUDA events on
+ * the context stream around their kernel phases; igab_last_kernel_ms waits
+ * for the stream and returns milliseconds of the last calls:
+ * ms[0] residual volume kernels, ms[1] residual boundary kernels,
+ * ms[2] tangent volume kernels, ms[3] tangent Dirichlet row/column zeroing,
+ * ms[4] number of residual volume launches, ms[5] number of tangent volume launches */
+int igab_set_profiling(igab_ctx *ctx, int on);
+int igab_last_kernel_ms(igab_ctx *ctx, double ms[6]);
+/* FMA throughput probe of the device (TFLOP/s, 2 flops per FMA), prec = igab_prec */
+int igab_fma_peak(int device, int prec, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,82 @@
+"""Seeded cases shared by the parity tests."""
+import zlib
+
+import numpy as np
+
+from igap4standard_b200 import mesh
+
+
+def neumann_values(xyz, meta, pn):
+    """The case builder's traction hook (iga_case_neumann) evaluated in numpy."""
+    f, o, d = meta[:, 0], meta[:, 1], meta[:, 2]
+    s = 1.0 + pn[36] * xyz[:, 0] + pn[37] * xyz[:, 1] + pn[38] * xyz[:, 2]
+    return pn[6 * f + 3 * o + d] * s
+
+
+def make_case(name):
+    """Returns dict(phys, nelem, knots, par_mat, bc_type, par_dirichlet, par_periodic, par_neumann, U)."""
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    if name == "tiny_default":          # 1 element, reference default material, example BCs
+        nelem = (1, 1, 1)
+        kn = mesh.knots_for(nelem)
+        pm = mesh.PAR_MAT_DEFAULT.copy()
+        bc, pd = mesh.bc_example()
+        pp = np.zeros(9)
+        pn = np.zeros(39)
+        amp = 1e-3
+    elif name == "ragged_config0":      # ragged tiles, config-0 BCs, default material
+        nelem = (2, 3, 5)
+        kn = mesh.knots_for(nelem)
+        pm = mesh.PAR_MAT_DEFAULT.copy()
+        bc, pd = mesh.bc_config0()
+        pp = np.zeros(9)
+        pn = np.zeros(39)
+        amp = 1e-3
+    elif name == "perturbed_lame":      # perturbed knots, (lambda, mu, l) mapping, traction + periodic term
+        nelem = (4, 4, 4)
+        kn = mesh.knots_for(nelem, perturb=0.1, seed=1)
+        pm = mesh.par_mat_from_lame(1.0, 1.0, 0.1)
+        bc, pd = mesh.bc_config0()
+        pd = rng.uniform(-0.02, 0.02, 9)
+        pp = rng.uniform(-0.01, 0.01, 9)
+        pn = rng.uniform(-0.05, 0.05, 39)
+        pn[36:39] = rng.uniform(-0.5, 0.5, 3)
+        amp = 1e-2
+    elif name == "mixed_bc":            # every face mixes Dirichlet/Neumann per dof and order
+        nelem = (3, 2, 4)
+        kn = mesh.knots_for(nelem, perturb=0.2, seed=7)
+        pm = mesh.par_mat_from_lame(0.7, 1.3, 0.15)
+        bc = rng.integers(0, 2, 36).astype(np.int32)
+        pd = rng.uniform(-0.05, 0.05, 9)
+        pp = np.zeros(9)
+        pn = rng.uniform(-0.1, 0.1, 39)
+        amp = 5e-2
+    elif name == "config0_8":           # BASELINE config 0 shape (8^3), seeded state in +-1e-3
+        nelem = (8, 8, 8)
+        kn = mesh.knots_for(nelem)
+        pm = mesh.par_mat_from_lame(1.0, 1.0, 0.1)
+        bc, pd = mesh.bc_config0()
+        pp = np.zeros(9)
+        pn = np.zeros(39)
+        amp = 1e-3
+    else:
+        raise KeyError(name)
+    ndof = mesh.n_dof(nelem)
+    U = np.random.default_rng(0).uniform(-amp, amp, ndof)
+    return dict(phys="ge", nelem=nelem, knots=kn, par_mat=pm, bc_type=bc, par_dirichlet=pd,
+                par_periodic=pp, par_neumann=pn, U=U)
+
+
+def residual_tolerance(ref):
+    """Per-entry bound |gpu - ref| <= 1e-12 * max(|ref_i|, scale): the reference sums
+    element contributions whose size is ~||R||_inf, so an entry that cancels to ~0
+    carries rounding of that size (survey parity criterion with a cancellation floor)."""
+    scale = np.max(np.abs(ref)) if ref.size else 0.0
+    return 1e-12 * np.maximum(np.abs(ref), scale)
+
+
+def tangent_tolerance(rowptr, vals_ref):
+    """|gpu - ref| <= 1e-12 * max(|ref|, ||ref row||_inf)."""
+    rowmax = np.maximum.reduceat(np.abs(vals_ref), rowptr[:-1]) if vals_ref.size else np.zeros(0)
+    per = np.repeat(rowmax, np.diff(rowptr))
+    return 1e-12 * np.maximum(np.abs(vals_ref), per)

@@ -117,6 +117,16 @@ int igab_last_kernel_ms(igab_ctx *ctx, double ms[6]);
 /* FMA throughput probe of the device (TFLOP/s, 2 flops per FMA), prec = igab_prec */
 int igab_fma_peak(int device, int prec, double *tflops);
 
+/* ---- residual for callers that cannot have the library allocate device memory.
+ * No counterpart in the reference.  Same result as igab_residual, but U and R
+ * are staged in a file-scope device array (2 x 8 MiB, held by every GPU that
+ * loads the library) instead of context buffers obtained with cudaMalloc; a
+ * call allocates nothing.  Meshes above 1,048,576 dofs are rejected
+ * (IGAB_ERR_ARG).  All calls share the array: calls that overlap on the GPU
+ * race.  The first call on a device looks up the array's address and should
+ * come before any stream capture. */
+int igab_residual_noalloc(igab_ctx *ctx, const double *U_host, double *R_host);
+
 #ifdef __cplusplus
 }
 #endif

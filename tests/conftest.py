@@ -36,3 +36,52 @@ def oracle_lib():
     if not ref.available():
         pytest.skip("reference oracle library oracle/_ref/libref_iga.so not built")
     return ref
+
+
+@pytest.fixture(scope="session")
+def golden():
+    path = os.path.join(REPO, "tests", "golden", "reference_vectors.npz")
+    return dict(np.load(path))
+
+
+@pytest.fixture(scope="session")
+def port_oracle():
+    from oracle import port
+    port.lib()
+    return port
+
+
+@pytest.fixture(scope="session")
+def host_math():
+    """igab_math.cuh compiled for the host (the device kernels' point mathematics)."""
+    import ctypes
+    import subprocess
+    src = os.path.join(REPO, "tests", "host", "igab_math_host.cpp")
+    inc = os.path.join(REPO, "igap4standard_b200", "csrc")
+    out_dir = os.path.join(REPO, "tests", "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    out = os.path.join(out_dir, "libigab_math_host.so")
+    deps = [src, os.path.join(inc, "igab_math.cuh")]
+    if not os.path.exists(out) or os.path.getmtime(out) < max(os.path.getmtime(d) for d in deps):
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", inc, src, "-o", out], check=True)
+    L = ctypes.CDLL(out)
+    vp = ctypes.c_void_p
+    L.host_ge_point.argtypes = [vp, vp, vp, vp]
+    L.host_bspline_p2.argtypes = [vp, ctypes.c_double, vp]
+    return L
+
+
+@pytest.fixture(scope="session")
+def checker():
+    """Factory of reference cases: the reference's own code (oracle/_ref) when it
+    is built, else the CPU restatement (oracle/port), pinned to the same
+    golden vectors.  Returns f(phys, nelem, knots, par_mat, bc_type, pp, pd, pn)."""
+    from oracle import ref, port
+    if ref.available():
+        return lambda *a: ref.case(*a)
+    port.lib()
+
+    def make(phys, *a):
+        assert phys == "ge"
+        return port.PortCase(*a)
+    return make

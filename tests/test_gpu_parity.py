@@ -23,9 +23,9 @@ def _assembly(c):
     return A
 
 
-def _ref_case(ref, c):
-    return ref.case("ge", c["nelem"], c["knots"], c["par_mat"], c["bc_type"], c["par_periodic"],
-                    c["par_dirichlet"], c["par_neumann"])
+def _ref_case(checker, c):
+    return checker("ge", c["nelem"], c["knots"], c["par_mat"], c["bc_type"], c["par_periodic"],
+                   c["par_dirichlet"], c["par_neumann"])
 
 
 def _report(name, err, tol):
@@ -35,9 +35,9 @@ def _report(name, err, tol):
 
 
 @pytest.mark.parametrize("name", CASES + ["config0_8"])
-def test_residual_parity(built, oracle_lib, name):
+def test_residual_parity(built, checker, name):
     c = make_case(name)
-    R_ref = _ref_case(oracle_lib, c).residual(c["U"])
+    R_ref = _ref_case(checker, c).residual(c["U"])
     A = _assembly(c)
     R = A.residual(c["U"])
     err = np.abs(R - R_ref)
@@ -45,9 +45,9 @@ def test_residual_parity(built, oracle_lib, name):
 
 
 @pytest.mark.parametrize("name", CASES)
-def test_tangent_parity(built, oracle_lib, name):
+def test_tangent_parity(built, checker, name):
     c = make_case(name)
-    rp_ref, cols_ref, v_ref = _ref_case(oracle_lib, c).tangent(c["U"])
+    rp_ref, cols_ref, v_ref = _ref_case(checker, c).tangent(c["U"])
     A = _assembly(c)
     rp, cols = A.pattern()
     assert np.array_equal(rp, rp_ref)
@@ -57,10 +57,10 @@ def test_tangent_parity(built, oracle_lib, name):
     assert _report(name, err, tangent_tolerance(rp_ref, v_ref)) <= 1.0
 
 
-def test_tangent_fp32_close(built, oracle_lib):
+def test_tangent_fp32_close(built, checker):
     """FP32-built tangent: an inexact-Newton Jacobian, compared rowwise in norm."""
     c = make_case("perturbed_lame")
-    rp_ref, _, v_ref = _ref_case(oracle_lib, c).tangent(c["U"])
+    rp_ref, _, v_ref = _ref_case(checker, c).tangent(c["U"])
     A = _assembly(c)
     v = A.tangent(c["U"], "fp32").astype(np.float64)
     rowmax = np.maximum.reduceat(np.abs(v_ref), rp_ref[:-1])
@@ -68,14 +68,14 @@ def test_tangent_fp32_close(built, oracle_lib):
     assert np.all(err <= 1e-5 * rowmax)
 
 
-def test_dropin_matches_reference(built, oracle_lib):
+def test_dropin_matches_reference(built, checker):
     """The PETSc drop-in (snesiga_Residual/snesiga_Tangent of libsnesiga_b200) on
     the same PETSc-subset objects the reference callbacks fill."""
     from igap4standard_b200 import gpu_case
     c = make_case("perturbed_lame")
     args = ("ge", c["nelem"], c["knots"], c["par_mat"], c["bc_type"], c["par_periodic"], c["par_dirichlet"],
             c["par_neumann"])
-    ref = oracle_lib.case(*args)
+    ref = checker(*args)
     gpu = gpu_case(*args)
     R_ref = ref.residual(c["U"])
     R = gpu.residual(c["U"])
@@ -93,13 +93,13 @@ def test_dropin_matches_reference(built, oracle_lib):
     assert _report("dropin tangent 2", np.abs(v2 - v_ref2), tangent_tolerance(rp_ref2, v_ref2)) <= 1.0
 
 
-def test_dropin_traction_update(built, oracle_lib):
+def test_dropin_traction_update(built, checker):
     """par_neumann changed between calls (a time-dependent traction) is picked up."""
     from igap4standard_b200 import gpu_case
     c = make_case("perturbed_lame")
     args = ("ge", c["nelem"], c["knots"], c["par_mat"], c["bc_type"], c["par_periodic"], c["par_dirichlet"],
             c["par_neumann"])
-    ref = oracle_lib.case(*args)
+    ref = checker(*args)
     gpu = gpu_case(*args)
     gpu.residual(c["U"])
     pn2 = c["par_neumann"] * -3.0

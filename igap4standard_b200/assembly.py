@@ -7,6 +7,7 @@ from .native import IgabMeshDesc, check, vp
 
 PHYS = {"ge": 0, "getime": 1}
 PREC = {"fp64": 0, "fp32": 1}
+OPT_TANGENT_FP64_KERNEL = 1
 
 
 def _ptr(a):
@@ -98,6 +99,14 @@ class Assembly:
     def set_history(self, level, U):
         a = np.ascontiguousarray(U, dtype=np.float64)
         check(self.lib, "igab_set_history", self.lib.igab_set_history(self.h, int(level), _ptr(a), 0))
+
+    def set_option(self, option, value):
+        check(self.lib, "igab_set_option", self.lib.igab_set_option(self.h, int(option), int(value)))
+
+    def get_option(self, option):
+        v = ctypes.c_int()
+        check(self.lib, "igab_get_option", self.lib.igab_get_option(self.h, int(option), ctypes.byref(v)))
+        return v.value
 
     def set_tile(self, residual_tile=0, tangent_tile=0):
         check(self.lib, "igab_set_tile", self.lib.igab_set_tile(self.h, residual_tile, tangent_tile))

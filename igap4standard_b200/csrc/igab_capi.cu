@@ -735,3 +735,28 @@ extern "C" int igab_fma_peak(int device, int prec, double *tflops)
     IGAB_CUDA_TRY(cudaSetDevice(device));
     return igab_launch_fma_peak(prec, tflops);
 }
+
+extern "C" int igab_set_option(igab_ctx *ctx, int option, int value)
+{
+    ARG_CHECK(ctx, "igab_set_option: null context");
+    switch (option) {
+    case IGAB_OPT_TANGENT_FP64_KERNEL:
+        ARG_CHECK(value == 0 || value == 1, "igab_set_option: tangent kernel must be 0 or 1");
+        ctx->tan_kernel = value;
+        return 0;
+    default:
+        igab_set_error("igab_set_option: unknown option %d", option);
+        return IGAB_ERR_ARG;
+    }
+}
+
+extern "C" int igab_get_option(const igab_ctx *ctx, int option, int *value)
+{
+    ARG_CHECK(ctx && value, "igab_get_option: null argument");
+    switch (option) {
+    case IGAB_OPT_TANGENT_FP64_KERNEL: *value = ctx->tan_kernel; return 0;
+    default:
+        igab_set_error("igab_get_option: unknown option %d", option);
+        return IGAB_ERR_ARG;
+    }
+}

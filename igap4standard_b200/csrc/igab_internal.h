@@ -85,6 +85,7 @@ struct igab_ctx {
     int vals_prec = -1;
 
     int tile_res = 2, tile_tan = 2;
+    int tan_kernel = 1;   /* FP64 tangent: 1 tensor-core (mma f64), 0 SIMT */
     int last_launches = 0;
 
     /* profiling events: [0..2] residual (start, after volume, end), [3..5] tangent */
@@ -103,6 +104,7 @@ int igab_launch_csr_cols(igab_ctx *c, int *dcols);
 int igab_launch_check_finite(igab_ctx *c, const void *dev, long n, int prec, int *all_finite);
 int igab_launch_basis_tables(igab_ctx *c, int d, const double *dkv, const double *dgx, const double *dgw);
 int igab_launch_fma_peak(int prec, double *tflops);
+int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv);
 /* record profiling event k on the context stream if profiling is on */
 static inline void igab_mark(igab_ctx *c, int k)
 {

@@ -26,72 +26,9 @@
 #include <stdint.h>
 #include "igab_internal.h"
 
+#include "igab_device.cuh"
+
 namespace {
-
-/* derivative multi-index of component alpha (eval_Bspline order):
- * 0:(0,0,0) 1:(1,0,0) 2:(0,1,0) 3:(0,0,1) 4:(2,0,0) 5:(1,1,0) 6:(1,0,1) 7:(0,2,0) 8:(0,1,1) 9:(0,0,2) */
-__host__ __device__ constexpr int a_kx(int a) { return a == 1 || a == 5 || a == 6 ? 1 : (a == 4 ? 2 : 0); }
-__host__ __device__ constexpr int a_ky(int a) { return a == 2 || a == 5 || a == 8 ? 1 : (a == 7 ? 2 : 0); }
-__host__ __device__ constexpr int a_kz(int a) { return a == 3 || a == 6 || a == 8 ? 1 : (a == 9 ? 2 : 0); }
-/* (ky,kz) pair index: 0:(0,0) 1:(1,0) 2:(0,1) 3:(2,0) 4:(1,1) 5:(0,2) */
-__host__ __device__ constexpr int kk_of(int ky, int kz)
-{
-    return (ky == 0 && kz == 0) ? 0 : (ky == 1 && kz == 0) ? 1 : (ky == 0 && kz == 1) ? 2
-         : (ky == 2 && kz == 0) ? 3 : (ky == 1 && kz == 1) ? 4 : 5;
-}
-__host__ __device__ constexpr int kk_ky(int kk) { return kk == 1 || kk == 4 ? 1 : (kk == 3 ? 2 : 0); }
-__host__ __device__ constexpr int kk_kz(int kk) { return kk == 2 || kk == 4 ? 1 : (kk == 5 ? 2 : 0); }
-__host__ __device__ constexpr int a_kk(int a) { return kk_of(a_ky(a), a_kz(a)); }
-
-__device__ __forceinline__ void group_sync(int group)
-{
-    asm volatile("bar.sync %0, %1;" ::"r"(group + 1), "r"(64) : "memory");
-}
-
-__device__ __forceinline__ double shfl_xor(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
-
-/* tile bookkeeping for one colour */
-struct tile_t {
-    int t[3];   /* tile coordinates */
-    int e0[3];  /* first element */
-    int nv[3];  /* valid elements per direction */
-};
-
-__device__ __forceinline__ bool decode_tile(const igab_geom &g, int TE, int colour, int bid, tile_t &T)
-{
-    int c[3] = {colour & 1, (colour >> 1) & 1, (colour >> 2) & 1};
-    int nc[3];
-    for (int d = 0; d < 3; d++) {
-        int nt = (g.ne[d] + TE - 1) / TE;
-        nc[d] = nt > c[d] ? (nt - c[d] + 1) / 2 : 0;
-    }
-    int i2 = bid % nc[2];
-    int i1 = (bid / nc[2]) % nc[1];
-    int i0 = bid / (nc[2] * nc[1]);
-    if (i0 >= nc[0]) return false;
-    T.t[0] = 2 * i0 + c[0]; T.t[1] = 2 * i1 + c[1]; T.t[2] = 2 * i2 + c[2];
-    for (int d = 0; d < 3; d++) {
-        T.e0[d] = T.t[d] * TE;
-        int r = g.ne[d] - T.e0[d];
-        T.nv[d] = r < TE ? r : TE;
-    }
-    return true;
-}
-
-__device__ __forceinline__ long cp_index(const igab_geom &g, int x, int y, int z)
-{
-    return ((long)x * g.nb[1] + y) * g.nb[2] + z;
-}
-
-/* position of column (cx,cy,cz,k2) inside the CSR row of control point (x,y,z) */
-__device__ __forceinline__ int csr_pos(const igab_geom &g, int x, int y, int z, int cx, int cy, int cz, int k2)
-{
-    int x0 = x > 2 ? x - 2 : 0;
-    int y0 = y > 2 ? y - 2 : 0, y1 = y + 2 < g.nb[1] - 1 ? y + 2 : g.nb[1] - 1;
-    int z0 = z > 2 ? z - 2 : 0, z1 = z + 2 < g.nb[2] - 1 ? z + 2 : g.nb[2] - 1;
-    int nyb = y1 - y0 + 1, nzb = z1 - z0 + 1;
-    return (((cx - x0) * nyb + (cy - y0)) * nzb + (cz - z0)) * 3 + k2;
-}
 
 /* ============================================================ residual */
 
@@ -713,17 +650,6 @@ __global__ void k_check_finite(const T *__restrict__ v, long n, int *__restrict_
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(flag, 1);
 }
 
-long tiles_of_colour(const igab_geom &g, int TE, int colour)
-{
-    long n = 1;
-    for (int d = 0; d < 3; d++) {
-        int c = (colour >> d) & 1;
-        int nt = (g.ne[d] + TE - 1) / TE;
-        n *= nt > c ? (nt - c + 1) / 2 : 0;
-    }
-    return n;
-}
-
 template <int TE>
 int launch_res_volume(igab_ctx *c, const igab_geom &g, const double *dU, double *dR)
 {
@@ -761,7 +687,8 @@ int launch_tangent_t(igab_ctx *c, const double *dU, T *dv)
     IGAB_CUDA_TRY(cudaMemsetAsync(dv, 0, (size_t)c->nnz * sizeof(T), c->stream));
     igab_mark(c, 3);
     int l0 = c->last_launches;
-    int e = launch_tan_volume<T, 2>(c, g, dU, dv);
+    int e = (sizeof(T) == 8 && c->tan_kernel == 1) ? igab_launch_tan_dmma(c, dU, (double *)dv)
+                                                   : launch_tan_volume<T, 2>(c, g, dU, dv);
     if (e) return e;
     c->nvol_tan = c->last_launches - l0;
     igab_mark(c, 4);

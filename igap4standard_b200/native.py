@@ -70,6 +70,8 @@ IGAB_API = [
     ("igab_last_kernel_ms", ctypes.c_int, [vp, c_double_p]),
     ("igab_fma_peak", ctypes.c_int, [ctypes.c_int, ctypes.c_int, c_double_p]),
     ("igab_residual_noalloc", ctypes.c_int, [vp, vp, vp]),
+    ("igab_set_option", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+    ("igab_get_option", ctypes.c_int, [vp, ctypes.c_int, c_int_p]),
 ]
 
 # entry points of include/snesiga_b200.h and include/iga_case.h

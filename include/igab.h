@@ -103,6 +103,10 @@ int igab_check_finite(igab_ctx *ctx, const void *dev, long n, int prec, int *all
 
 /* ---- tuning: elements per tile edge of the 8-colour schedule (2 or 4), 0 = auto */
 int igab_set_tile(igab_ctx *ctx, int residual_tile, int tangent_tile);
+/* kernel choices: IGAB_OPT_TANGENT_FP64_KERNEL 1 = FP64 tensor path (mma f64), 0 = FP64 FMA pipe */
+enum igab_option { IGAB_OPT_TANGENT_FP64_KERNEL = 1 };
+int igab_set_option(igab_ctx *ctx, int option, int value);
+int igab_get_option(const igab_ctx *ctx, int option, int *value);
 /* launches issued by the last assembly call (kernel count) */
 int igab_last_launch_count(const igab_ctx *ctx, int *n);
 

@@ -44,11 +44,14 @@ def test_residual_parity(built, checker, name):
     assert _report(name, err, residual_tolerance(R_ref)) <= 1.0
 
 
+@pytest.mark.parametrize("kernel", [1, 0])
 @pytest.mark.parametrize("name", CASES)
-def test_tangent_parity(built, checker, name):
+def test_tangent_parity(built, checker, name, kernel):
+    """kernel 1: FP64 tensor path (mma f64), kernel 0: FP64 FMA pipe."""
     c = make_case(name)
     rp_ref, cols_ref, v_ref = _ref_case(checker, c).tangent(c["U"])
     A = _assembly(c)
+    A.set_option(1, kernel)
     rp, cols = A.pattern()
     assert np.array_equal(rp, rp_ref)
     assert np.array_equal(cols, cols_ref)

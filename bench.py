@@ -38,9 +38,9 @@ METRIC = "Newton-step assembly ms & adjoint grads/s at 64^3, mixed vs FP64, 1xB2
 #  residual 64 * 2 * (27*30 + 27*30) + 64 * 270 (interpolation, test contraction, basis)
 TAN_ALG_FLOPS = 64 * 2 * (30 * 81 * 10 + 81 * 81 * 10)
 RES_ALG_FLOPS = 64 * (2 * (27 * 30 + 27 * 30) + 270)
-# flops the tangent kernel executes per element (rank-12 form, upper triangle):
-#  K += X^T Y (3321 x 12), X (972 x 9), Gamma (378 x 9), geometric block (243 x 4)
-TAN_EXEC_FLOPS = 64 * 2 * (3321 * 12 + 972 * 9 + 378 * 9 + 243 * 4)
+# flops the tangent kernel executes per element on the tensor path: 66 upper 8x8 tiles
+# x 12 variables per point, plus 10 upper 8x8 tiles of the geometric block x 9 per point
+TAN_EXEC_FLOPS = 64 * 2 * (66 * 64 * 12 + 10 * 64 * 9)
 
 
 def parse():
@@ -338,9 +338,10 @@ def run_ours(args):
                 traffic = traffic * nel / nlaunch
         except Exception:
             traffic = None
-    roofline = {"bound": "tensor", "pipe": "FP64 FMA (SIMT)", "achieved": round(achieved, 3), "peak": round(peak64, 3),
+    roofline = {"bound": "tensor", "pipe": "FP64 tensor (mma.sync m8n8k4 f64) + FP64 FMA", "achieved": round(achieved, 3),
+                "peak": round(peak64, 3),
                 "unit": "TFLOP/s", "frac": round(achieved / peak64, 4), "traffic": traffic,
-                "kernel": "k_tan_volume<double,2>", "avg_launch_ms": round(tan_ms / nlaunch, 3),
+                "kernel": "k_tan_dmma<2>", "avg_launch_ms": round(tan_ms / nlaunch, 3),
                 "flops_per_launch": nel * TAN_ALG_FLOPS / nlaunch,
                 "flops_definition": "algorithmic B^T D B per element = 64*2*(30*81*10+81*81*10) (effective: the "
                                     "kernel executes %d flops per element)" % TAN_EXEC_FLOPS,

@@ -4,19 +4,22 @@
  * Per element (src/snesiga_Tangent.c:104-190), with the energy written as
  * W = Phi(v(u)) over 12 variables (igab_math.cuh):
  *   K_e = sum_q w_q X_q^T Phi''_q X_q  +  blockdiag_k(Gamma),
- *   X_q[v][3a+k] = sum_m dv/du_{k,m}(q) N_a^{m}(q).
+ *   X_q[v][3a+k] = sum_m dv/du_{k,m}(q) N_a^{m}(q),
+ *   Gamma(a,b)   = sum_q sum_{m,n} N_a^m(q) (w_q geo_q[m][n]) N_b^n(q).
  * Phi'' is diagonal except for the (va, vb) pair; rotating those two rows by
  * the eigenvectors of that 2x2 block makes it diagonal, so
  *   K_e = X'^T diag(s) X',   s = w_q * eigenvalues.
- * X' (96 rows = 8 Gauss points x 12 variables, 88 padded columns) sits in
- * shared memory once; a warp loads its A fragments from it and forms the B
- * fragments by scaling the same registers with s.  The 66 upper-triangle 8x8
- * tiles of the 88x88 element matrix are spread over the 8 warps (<= 9 tiles,
- * <= 5 fragment blocks each, table below); the lower triangle is written by
- * symmetry.  The geometric block Gamma (same for the three displacement
- * components) is accumulated on the FP64 pipe by its owning threads.
- * Scatter: read-modify-write into the CSR values, conflict-free within one
- * of the 8 tile colours (see igab_kernels.cu).
+ * Both products run on DMMA tiles:
+ *   - X' (48 rows = 4 Gauss points x 12 variables, 88 padded columns) sits in
+ *     shared memory once; a warp loads its A fragments from it and forms its
+ *     B fragments by scaling the same registers with s.  The 66 upper 8x8
+ *     tiles of the 88x88 element matrix are spread over the 4 warps (table in
+ *     igab_warp_tiles.inc), the lower triangle follows by symmetry.
+ *   - Gamma (32x32 padded, 10 upper tiles) from N^T and w geo N.
+ * 128 threads and ~108 KB of shared memory per block let two blocks share
+ * an SM, so one block's scalar work (field, point integrand, X') overlaps the
+ * other's tensor work.  Scatter: read-modify-write into the CSR values,
+ * conflict-free within one of the 8 tile colours (igab_kernels.cu).
  */
 #include <cuda_runtime.h>
 #include "igab_device.cuh"
@@ -25,40 +28,47 @@ namespace {
 
 #include "igab_warp_tiles.inc"
 
-#define DQ 8            /* Gauss points per batch */
-#define DROWS (DQ * 12) /* k rows per batch */
-#define XS 100          /* row stride of X' in doubles: 100 = 4 (mod 16) keeps fragment loads conflict-free */
+#define NTHR 128
+#define DQ 4            /* Gauss points per batch */
+#define DROWS (DQ * 12) /* k rows of X' per batch */
+#define GROWS (DQ * 9)  /* k rows of the geometric product per batch */
+#define XS 100          /* X' row stride (doubles): = 4 mod 16 keeps fragment loads conflict-free */
+#define GS 36           /* N^T / GN row stride: = 4 mod 16 */
 
+/* point data */
 #define PT_F 0
 #define PT_G 9
-#define PT_D2 27
-#define PT_D2AB 39
-#define PT_SIG 40
-#define PT_D1S 43
-#define PT_TAU 46
-#define PT_W 55
-#define PT_ROT 56 /* cs, sn, l1, l2 of the (va, vb) block */
-#define PT_N 60
+#define PT_LAM 27   /* 12 diagonal values of the rotated Phi'' */
+#define PT_CS 39
+#define PT_SN 40
+#define PT_SIG 41
+#define PT_D1S 44
+#define PT_TAU 47
+#define PT_W 56
+#define PT_N 57
+
+/* work buffer: interpolation A[972] C[864] | X'[48][100] + points[64][57] | K[88][88] */
+#define W_A 0
+#define W_C 972
+#define W_X 0
+#define W_PT (DROWS * XS)
+#define W_SIZE (DROWS * XS + IGAB_NQ3 * PT_N)
 
 template <int TE>
 struct dmma_smem {
     static constexpr int TC = TE + 2;
     static constexpr int NCP = TC * TC * TC;
+    double W[W_SIZE > 88 * 88 ? W_SIZE : 88 * 88];
+    double NT[GROWS][GS];     /* N^T: row 9 qb + m, column a (a >= 27 zero); Gamma[32][32] at the end */
+    double GN[GROWS][GS];     /* w geo N: row 9 qb + m, column b (b >= 27 zero) */
+    double Gv[DQ][12][27];    /* rotated dv/du_s */
+    double geo[DQ][81];
+    double sc[DROWS];
     double U[NCP * 3];
     double tab[3][TE][IGAB_TAB1D];
     double wh[3][TE][IGAB_NQ];
-    double A[972];
-    double C[864];
-    double pt[IGAB_NQ3][PT_N];
-    double N[DQ][27][9];      /* N_a^{m+1} */
-    double Gv[DQ][12][27];    /* rotated dv/du_s */
-    double GN[DQ][9][27];     /* w * geo * N */
-    double geo[DQ][9][9];     /* geometric block per Gauss point */
-    double gcoef[12][9];      /* dv/du_{k,m} = gcoef[v][m] * src_k[gsrc[v][m]] */
-    int gsrc[12][9];          /* src_k = (F_k0, F_k1, F_k2, G_k0..G_k5), -1 = zero */
-    double sc[DROWS];         /* w * eigenvalue per k row */
-    double X[DROWS][XS];
-    double Gam[27 * 27];
+    double gcoef[12][9];
+    int gsrc[12][9];
 };
 
 __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
@@ -85,15 +95,17 @@ __device__ __forceinline__ void sym2_eig(double a, double b, double c, double &c
 }
 
 template <int W>
-__device__ __forceinline__ void warp_mma(const double *__restrict__ X, const double *__restrict__ sc, int lane,
-                                         double (&acc)[9][2])
+__device__ __forceinline__ void warp_mma(const double *__restrict__ X, const double *__restrict__ sc,
+                                         const double *__restrict__ NT, const double *__restrict__ GN, int lane,
+                                         double (&acc)[17][2], double (&gacc)[3][2])
 {
     using WT = warp_tiles<W>;
+    const int r4 = lane & 3, c8 = lane >> 2;
 #pragma unroll 2
     for (int kb = 0; kb < DROWS / 4; kb++) {
-        const int kr = 4 * kb + (lane & 3);
+        const int kr = 4 * kb + r4;
         const double s = sc[kr];
-        const double *row = X + kr * XS + (lane >> 2);
+        const double *row = X + kr * XS + c8;
         double f[WT::NB], g[WT::NB];
 #pragma unroll
         for (int b = 0; b < WT::NB; b++) {
@@ -103,37 +115,51 @@ __device__ __forceinline__ void warp_mma(const double *__restrict__ X, const dou
 #pragma unroll
         for (int t = 0; t < WT::NT; t++) dmma(acc[t][0], acc[t][1], f[WT::ti(t)], g[WT::tj(t)]);
     }
+#pragma unroll 3
+    for (int kb = 0; kb < GROWS / 4; kb++) {
+        const int kr = 4 * kb + r4;
+        double fa[WT::NGA], fb[WT::NGB];
+#pragma unroll
+        for (int b = 0; b < WT::NGA; b++) fa[b] = NT[kr * GS + 8 * WT::gablk(b) + c8];
+#pragma unroll
+        for (int b = 0; b < WT::NGB; b++) fb[b] = GN[kr * GS + 8 * WT::gbblk(b) + c8];
+#pragma unroll
+        for (int t = 0; t < WT::NGT; t++) dmma(gacc[t][0], gacc[t][1], fa[WT::gti(t)], fb[WT::gtj(t)]);
+    }
 }
 
-/* accumulator tiles -> shared K[c1][c2] (upper triangle tiles only) */
+/* accumulator tiles -> shared K[c1][c2] (stride 88) and Gamma[a1][a2] (stride 32) */
 template <int W>
-__device__ __forceinline__ void warp_dump(double *__restrict__ K, int lane, const double (&acc)[9][2])
+__device__ __forceinline__ void warp_dump(double *__restrict__ K, double *__restrict__ Gam, int lane,
+                                          const double (&acc)[17][2], const double (&gacc)[3][2])
 {
     using WT = warp_tiles<W>;
+    const int r = lane >> 2, c = 2 * (lane & 3);
 #pragma unroll
     for (int t = 0; t < WT::NT; t++) {
-        const int c1 = 8 * WT::blk(WT::ti(t)) + (lane >> 2);
-        const int c2 = 8 * WT::blk(WT::tj(t)) + 2 * (lane & 3);
+        const int c1 = 8 * WT::blk(WT::ti(t)) + r, c2 = 8 * WT::blk(WT::tj(t)) + c;
         K[c1 * 88 + c2] = acc[t][0];
         K[c1 * 88 + c2 + 1] = acc[t][1];
     }
+#pragma unroll
+    for (int t = 0; t < WT::NGT; t++) {
+        const int a1 = 8 * WT::gablk(WT::gti(t)) + r, a2 = 8 * WT::gbblk(WT::gtj(t)) + c;
+        Gam[a1 * 32 + a2] = gacc[t][0];
+        Gam[a1 * 32 + a2 + 1] = gacc[t][1];
+    }
 }
 
-#define WARP_SWITCH(CALL)          \
-    switch (warp) {                \
-    case 0: CALL(0); break;        \
-    case 1: CALL(1); break;        \
-    case 2: CALL(2); break;        \
-    case 3: CALL(3); break;        \
-    case 4: CALL(4); break;        \
-    case 5: CALL(5); break;        \
-    case 6: CALL(6); break;        \
-    default: CALL(7); break;       \
+#define WARP_SWITCH(CALL)    \
+    switch (warp) {          \
+    case 0: CALL(0); break;  \
+    case 1: CALL(1); break;  \
+    case 2: CALL(2); break;  \
+    default: CALL(3); break; \
     }
 
 template <int TE>
-__global__ void __launch_bounds__(256, 1) k_tan_dmma(igab_geom g, const double *__restrict__ U,
-                                                     double *__restrict__ vals, int colour)
+__global__ void __launch_bounds__(NTHR, 2) k_tan_dmma(igab_geom g, const double *__restrict__ U,
+                                                      double *__restrict__ vals, int colour)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     dmma_smem<TE> &S = *reinterpret_cast<dmma_smem<TE> *>(smem_raw);
@@ -143,18 +169,10 @@ __global__ void __launch_bounds__(256, 1) k_tan_dmma(igab_geom g, const double *
     tile_t Tl;
     if (!decode_tile(g, TE, colour, blockIdx.x, Tl)) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    double *const Xb = S.W + W_X;
+    double *const PTb = S.W + W_PT;
 
-    /* owned geometric entries (a1 <= a2), 378 over 256 threads */
-    int gown[2];
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-        int idx = tid + 256 * j;
-        int a1 = 0, rem = idx;
-        while (a1 < 27 && rem >= 27 - a1) { rem -= 27 - a1; a1++; }
-        gown[j] = a1 < 27 ? (a1 << 8) | (a1 + rem) : -1;
-    }
-
-    for (int idx = tid; idx < NCP * 3; idx += 256) {
+    for (int idx = tid; idx < NCP * 3; idx += NTHR) {
         int i = idx % 3, cp = idx / 3;
         int lz = cp % TC, ly = (cp / TC) % TC, lx = cp / (TC * TC);
         double v = 0.0;
@@ -162,11 +180,11 @@ __global__ void __launch_bounds__(256, 1) k_tan_dmma(igab_geom g, const double *
             v = U[3 * cp_index(g, Tl.e0[0] + lx, Tl.e0[1] + ly, Tl.e0[2] + lz) + i];
         S.U[idx] = v;
     }
-    for (int idx = tid; idx < 3 * TE * IGAB_TAB1D; idx += 256) {
+    for (int idx = tid; idx < 3 * TE * IGAB_TAB1D; idx += NTHR) {
         int d = idx / (TE * IGAB_TAB1D), r = idx % (TE * IGAB_TAB1D), le = r / IGAB_TAB1D, o = r % IGAB_TAB1D;
         S.tab[d][le][o] = le < Tl.nv[d] ? g.tab[d][(long)(Tl.e0[d] + le) * IGAB_TAB1D + o] : 0.0;
     }
-    for (int idx = tid; idx < 3 * TE * IGAB_NQ; idx += 256) {
+    for (int idx = tid; idx < 3 * TE * IGAB_NQ; idx += NTHR) {
         int d = idx / (TE * IGAB_NQ), r = idx % (TE * IGAB_NQ), le = r / IGAB_NQ, q = r % IGAB_NQ;
         S.wh[d][le][q] = le < Tl.nv[d] ? g.wh[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
     }
@@ -202,8 +220,11 @@ __global__ void __launch_bounds__(256, 1) k_tan_dmma(igab_geom g, const double *
         S.gsrc[v][m] = src;
         S.gcoef[v][m] = cf;
     }
-    /* padding columns 81..99 of X' stay zero */
-    for (int idx = tid; idx < DROWS * XS; idx += 256) (&S.X[0][0])[idx] = 0.0;
+    /* padding (a, b >= 27) of N^T and GN stays zero */
+    for (int idx = tid; idx < GROWS * GS; idx += NTHR) {
+        (&S.NT[0][0])[idx] = 0.0;
+        (&S.GN[0][0])[idx] = 0.0;
+    }
     __syncthreads();
 
     for (int le = 0; le < NEL; le++) {
@@ -212,21 +233,24 @@ __global__ void __launch_bounds__(256, 1) k_tan_dmma(igab_geom g, const double *
         const double *Bx = S.tab[0][lex];
         const double *By = S.tab[1][ley];
         const double *Bz = S.tab[2][lez];
+        double *const A = S.W + W_A;
+        double *const C = S.W + W_C;
         /* ---- field at the 64 Gauss points (sum-factorised, as the residual) */
-        for (int o = tid; o < 972; o += 256) {
+        for (int o = tid; o < 972; o += NTHR) {
             int i = o % 3, kz = (o / 3) % 3, ay = (o / 9) % 3, ax = (o / 27) % 3, q = o / 81;
             const double *u0 = &S.U[(((lex + ax) * TC + (ley + ay)) * TC + lez) * 3 + i];
-            S.A[o] = Bz[q * 9 + kz] * u0[0] + Bz[q * 9 + 3 + kz] * u0[3] + Bz[q * 9 + 6 + kz] * u0[6];
+            A[o] = Bz[q * 9 + kz] * u0[0] + Bz[q * 9 + 3 + kz] * u0[3] + Bz[q * 9 + 6 + kz] * u0[6];
         }
         __syncthreads();
-        for (int o = tid; o < 864; o += 256) {
+        for (int o = tid; o < 864; o += NTHR) {
             int i = o % 3, kk = (o / 3) % 6, ax = (o / 18) % 3, qq = o / 54;
             int qyy = qq & 3, qzz = qq >> 2;
-            const double *a0 = &S.A[((qzz * 3 + ax) * 3) * 9 + kk_kz(kk) * 3 + i];
-            S.C[o] = By[qyy * 9 + kk_ky(kk)] * a0[0] + By[qyy * 9 + 3 + kk_ky(kk)] * a0[9] +
-                     By[qyy * 9 + 6 + kk_ky(kk)] * a0[18];
+            const double *a0 = &A[((qzz * 3 + ax) * 3) * 9 + kk_kz(kk) * 3 + i];
+            C[o] = By[qyy * 9 + kk_ky(kk)] * a0[0] + By[qyy * 9 + 3 + kk_ky(kk)] * a0[9] +
+                   By[qyy * 9 + 6 + kk_ky(kk)] * a0[18];
         }
         __syncthreads();
+        /* ---- point integrand data (64 threads), point order q = 16 qz + 4 qy + qx */
         if (tid < IGAB_NQ3) {
             const int qx = tid & 3, qy = (tid >> 2) & 3, qz = tid >> 4, qq = qy + 4 * qz;
             double u[30];
@@ -237,7 +261,7 @@ __global__ void __launch_bounds__(256, 1) k_tan_dmma(igab_geom g, const double *
                     double s = 0.0;
 #pragma unroll
                     for (int ax = 0; ax < 3; ax++)
-                        s += Bx[qx * 9 + ax * 3 + a_kx(a)] * S.C[((qq * 3 + ax) * 6 + a_kk(a)) * 3 + i];
+                        s += Bx[qx * 9 + ax * 3 + a_kx(a)] * C[((qq * 3 + ax) * 6 + a_kk(a)) * 3 + i];
                     u[10 * i + a] = s;
                 }
             if (g.periodic) {
@@ -248,8 +272,7 @@ __global__ void __launch_bounds__(256, 1) k_tan_dmma(igab_geom g, const double *
             }
             igab_ge_point<double> P;
             igab_ge_eval(u, g.coef, P);
-            /* point order q = 16 qz + 4 qy + qx */
-            double *pt = S.pt[tid];
+            double *pt = PTb + tid * PT_N;
 #pragma unroll
             for (int k = 0; k < 3; k++)
 #pragma unroll
@@ -258,9 +281,12 @@ __global__ void __launch_bounds__(256, 1) k_tan_dmma(igab_geom g, const double *
             for (int k = 0; k < 3; k++)
 #pragma unroll
                 for (int c = 0; c < 6; c++) pt[PT_G + 6 * k + c] = P.G[k][c];
+            double cs, sn, l1, l2;
+            sym2_eig(P.d2[1], P.d2ab, P.d2[2], cs, sn, l1, l2);
 #pragma unroll
-            for (int v = 0; v < 12; v++) pt[PT_D2 + v] = P.d2[v];
-            pt[PT_D2AB] = P.d2ab;
+            for (int v = 0; v < 12; v++) pt[PT_LAM + v] = v == 1 ? l1 : (v == 2 ? l2 : P.d2[v]);
+            pt[PT_CS] = cs;
+            pt[PT_SN] = sn;
 #pragma unroll
             for (int I = 0; I < 3; I++) pt[PT_SIG + I] = P.sig[I];
 #pragma unroll
@@ -270,141 +296,121 @@ __global__ void __launch_bounds__(256, 1) k_tan_dmma(igab_geom g, const double *
 #pragma unroll
                 for (int K = 0; K < 3; K++) pt[PT_TAU + 3 * I + K] = P.tau[I][K];
             pt[PT_W] = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz];
-            sym2_eig(P.d2[1], P.d2ab, P.d2[2], pt[PT_ROT], pt[PT_ROT + 1], pt[PT_ROT + 2], pt[PT_ROT + 3]);
         }
         __syncthreads();
 
-        double acc[9][2];
+        double acc[17][2], gacc[3][2];
 #pragma unroll
-        for (int t = 0; t < 9; t++) acc[t][0] = acc[t][1] = 0.0;
-        double gacc[2] = {0.0, 0.0};
+        for (int t = 0; t < 17; t++) acc[t][0] = acc[t][1] = 0.0;
+#pragma unroll
+        for (int t = 0; t < 3; t++) gacc[t][0] = gacc[t][1] = 0.0;
 
         for (int q0 = 0; q0 < IGAB_NQ3; q0 += DQ) {
-            /* (a) basis products, rotated variable gradients, scales, geometric blocks */
-            for (int o = tid; o < DQ * 243; o += 256) {
+            /* (a) basis products (as N^T), rotated variable gradients, scales, geometric blocks */
+            if (q0 == 0)   /* the interpolation / staging data under X' is dead: padding columns back to zero */
+                for (int idx = tid; idx < DROWS * (XS - 81); idx += NTHR)
+                    Xb[(idx / (XS - 81)) * XS + 81 + idx % (XS - 81)] = 0.0;
+            for (int o = tid; o < DQ * 243; o += NTHR) {
                 int m = o % 9, a = (o / 9) % 27, qb = o / 243;
                 int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
                 int al = m + 1;
-                S.N[qb][a][m] = Bx[qx * 9 + (a / 9) * 3 + a_kx(al)] * By[qy * 9 + ((a / 3) % 3) * 3 + a_ky(al)] *
-                                Bz[qz * 9 + (a % 3) * 3 + a_kz(al)];
+                S.NT[9 * qb + m][a] = Bx[qx * 9 + (a / 9) * 3 + a_kx(al)] * By[qy * 9 + ((a / 3) % 3) * 3 + a_ky(al)] *
+                                      Bz[qz * 9 + (a % 3) * 3 + a_kz(al)];
             }
-            for (int o = tid; o < DQ * 12 * 27; o += 256) {
+            for (int o = tid; o < DQ * 12 * 27; o += NTHR) {
                 const int sidx = o % 27, v = (o / 27) % 12, qb = o / 324;
                 const int k = sidx / 9, m = sidx % 9;
-                const double *pt = S.pt[q0 + qb];
+                const double *pt = PTb + (q0 + qb) * PT_N;
                 double val;
                 if (v == 1 || v == 2) {
                     const int i1 = S.gsrc[1][m], i2 = S.gsrc[2][m];
                     const double g1 = i1 < 0 ? 0.0 : S.gcoef[1][m] * (i1 < 3 ? pt[PT_F + 3 * k + i1] : pt[PT_G + 6 * k + i1 - 3]);
                     const double g2 = i2 < 0 ? 0.0 : S.gcoef[2][m] * (i2 < 3 ? pt[PT_F + 3 * k + i2] : pt[PT_G + 6 * k + i2 - 3]);
-                    const double cs = pt[PT_ROT], sn = pt[PT_ROT + 1];
+                    const double cs = pt[PT_CS], sn = pt[PT_SN];
                     val = v == 1 ? cs * g1 - sn * g2 : sn * g1 + cs * g2;
-                    if (sidx == 0) S.sc[qb * 12 + v] = pt[PT_W] * pt[PT_ROT + 1 + v];
                 } else {
                     const int i0 = S.gsrc[v][m];
                     val = i0 < 0 ? 0.0 : S.gcoef[v][m] * (i0 < 3 ? pt[PT_F + 3 * k + i0] : pt[PT_G + 6 * k + i0 - 3]);
-                    if (sidx == 0) S.sc[qb * 12 + v] = pt[PT_W] * pt[PT_D2 + v];
                 }
+                if (sidx == 0) S.sc[qb * 12 + v] = pt[PT_W] * pt[PT_LAM + v];
                 S.Gv[qb][v][sidx] = val;
             }
-            for (int o = tid; o < DQ * 81; o += 256) {
+            for (int o = tid; o < DQ * 81; o += NTHR) {
                 const int n = o % 9, m = (o / 9) % 9, qb = o / 81;
-                const double *pt = S.pt[q0 + qb];
+                const double *pt = PTb + (q0 + qb) * PT_N;
                 const int lo = m < n ? m : n, hi = m < n ? n : m;
                 double gv = 0.0;
                 if (hi < 3) {
                     gv = lo == hi ? pt[PT_SIG + lo] : 0.5 * pt[PT_D1S + (lo == 0 ? hi - 1 : 2)];
                 } else if (lo < 3) {
-                    /* slot hi = 3 + idx6(lo, K) for exactly one K, if any */
 #pragma unroll
                     for (int K = 0; K < 3; K++)
                         if (3 + igab_idx6(lo, K) == hi) gv = pt[PT_TAU + 3 * lo + K];
                 }
-                S.geo[qb][m][n] = gv;
+                S.geo[qb][m * 9 + n] = pt[PT_W] * gv;
             }
             __syncthreads();
-            /* (b) X' = Gv' . N (rows of 9 outputs per task) and GN = w geo N */
-            for (int o = tid; o < DQ * 12 * 3 * 3; o += 256) {
+            /* (b) X' = Gv' . N (9 outputs per task) and GN = (w geo) N */
+            for (int o = tid; o < DQ * 12 * 3 * 3; o += NTHR) {
                 const int part = o % 3, k = (o / 3) % 3, v = (o / 9) % 12, qb = o / 108;
                 double gr[9];
 #pragma unroll
                 for (int m = 0; m < 9; m++) gr[m] = S.Gv[qb][v][9 * k + m];
-                double *xr = &S.X[qb * 12 + v][0];
+                double *xr = Xb + (qb * 12 + v) * XS;
+                const double *nt = &S.NT[9 * qb][0];
                 if (v < 6) {
 #pragma unroll
                     for (int j = 0; j < 9; j++) {
                         const int a = 9 * part + j;
-                        const double *nr = S.N[qb][a];
-                        xr[3 * a + k] = gr[0] * nr[0] + gr[1] * nr[1] + gr[2] * nr[2];
+                        xr[3 * a + k] = gr[0] * nt[a] + gr[1] * nt[GS + a] + gr[2] * nt[2 * GS + a];
                     }
                 } else {
 #pragma unroll
                     for (int j = 0; j < 9; j++) {
                         const int a = 9 * part + j;
-                        const double *nr = S.N[qb][a];
                         double t = 0.0;
 #pragma unroll
-                        for (int m = 0; m < 9; m++) t += gr[m] * nr[m];
+                        for (int m = 0; m < 9; m++) t += gr[m] * nt[m * GS + a];
                         xr[3 * a + k] = t;
                     }
                 }
             }
-            for (int o = tid; o < DQ * 243; o += 256) {
+            for (int o = tid; o < DQ * 243; o += NTHR) {
                 const int b = o % 27, m = (o / 27) % 9, qb = o / 243;
-                const double *gr = S.geo[qb][m];
-                const double *nr = S.N[qb][b];
+                const double *gr = &S.geo[qb][m * 9];
+                const double *nt = &S.NT[9 * qb][b];
                 double t = 0.0;
 #pragma unroll
-                for (int n = 0; n < 9; n++) t += gr[n] * nr[n];
-                S.GN[qb][m][b] = S.pt[q0 + qb][PT_W] * t;
+                for (int n = 0; n < 9; n++) t += gr[n] * nt[n * GS];
+                S.GN[9 * qb + m][b] = t;
             }
             __syncthreads();
-            /* (c) tensor-core accumulation K += X'^T diag(sc) X' */
-#define MMA_CALL(Wn) warp_mma<Wn>(&S.X[0][0], S.sc, lane, acc)
+            /* (c) tensor-core accumulation K += X'^T diag(sc) X', Gamma += N^T GN */
+#define MMA_CALL(Wn) warp_mma<Wn>(Xb, S.sc, &S.NT[0][0], &S.GN[0][0], lane, acc, gacc)
             WARP_SWITCH(MMA_CALL)
 #undef MMA_CALL
-            /* geometric block for the owned entries (FP64 pipe, overlaps the tensor work of other warps) */
-#pragma unroll
-            for (int j = 0; j < 2; j++) {
-                if (gown[j] < 0) continue;
-                int a1 = gown[j] >> 8, a2 = gown[j] & 255;
-                double t = gacc[j];
-                for (int qb = 0; qb < DQ; qb++)
-#pragma unroll
-                    for (int m = 0; m < 9; m++) t += S.N[qb][a1][m] * S.GN[qb][m][a2];
-                gacc[j] = t;
-            }
             __syncthreads();
         }
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            if (gown[j] < 0) continue;
-            int a1 = gown[j] >> 8, a2 = gown[j] & 255;
-            S.Gam[a1 * 27 + a2] = gacc[j];
-            S.Gam[a2 * 27 + a1] = gacc[j];
-        }
-        __syncthreads();
-#define DUMP_CALL(Wn) warp_dump<Wn>(&S.X[0][0], lane, acc)
+        /* ---- stage K and Gamma in shared memory, then scatter the 81 x 81 element matrix */
+        double *const K = S.W;
+        double *const Gam = &S.NT[0][0];
+#define DUMP_CALL(Wn) warp_dump<Wn>(K, Gam, lane, acc, gacc)
         WARP_SWITCH(DUMP_CALL)
 #undef DUMP_CALL
         __syncthreads();
-        /* ---- scatter the full 81 x 81 element matrix row by row (lower half mirrored) */
-        {
-            const double *K = &S.X[0][0];
-            for (int idx = tid; idx < 81 * 81; idx += 256) {
-                const int c1 = idx / 81, c2 = idx % 81;
-                const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
-                double val = c1 <= c2 ? K[c1 * 88 + c2] : K[c2 * 88 + c1];
-                if (k1 == k2) val += S.Gam[a1 * 27 + a2];
-                const int x1 = Tl.e0[0] + lex + a1 / 9, y1 = Tl.e0[1] + ley + (a1 / 3) % 3, z1 = Tl.e0[2] + lez + a1 % 3;
-                const int x2 = Tl.e0[0] + lex + a2 / 9, y2 = Tl.e0[1] + ley + (a2 / 3) % 3, z2 = Tl.e0[2] + lez + a2 % 3;
-                const long r1 = 3 * cp_index(g, x1, y1, z1) + k1;
-                vals[g.rowptr[r1] + csr_pos(g, x1, y1, z1, x2, y2, z2, k2)] += val;
-            }
+        for (int idx = tid; idx < 81 * 81; idx += NTHR) {
+            const int c1 = idx / 81, c2 = idx % 81;
+            const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
+            double val = c1 <= c2 ? K[c1 * 88 + c2] : K[c2 * 88 + c1];
+            if (k1 == k2) val += a1 <= a2 ? Gam[a1 * 32 + a2] : Gam[a2 * 32 + a1];
+            const int x1 = Tl.e0[0] + lex + a1 / 9, y1 = Tl.e0[1] + ley + (a1 / 3) % 3, z1 = Tl.e0[2] + lez + a1 % 3;
+            const int x2 = Tl.e0[0] + lex + a2 / 9, y2 = Tl.e0[1] + ley + (a2 / 3) % 3, z2 = Tl.e0[2] + lez + a2 % 3;
+            const long r1 = 3 * cp_index(g, x1, y1, z1) + k1;
+            vals[g.rowptr[r1] + csr_pos(g, x1, y1, z1, x2, y2, z2, k2)] += val;
         }
         __syncthreads();
-        /* the staged K overwrote padding columns of X'; they must be zero again */
-        for (int idx = tid; idx < DROWS * (XS - 81); idx += 256) S.X[idx / (XS - 81)][81 + idx % (XS - 81)] = 0.0;
+        /* Gamma overwrote N^T: restore the zero padding of N^T */
+        for (int idx = tid; idx < GROWS * GS; idx += NTHR) (&S.NT[0][0])[idx] = 0.0;
         __syncthreads();
     }
 }
@@ -419,7 +425,7 @@ int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv)
     for (int colour = 0; colour < 8; colour++) {
         long nblk = tiles_of_colour(g, 2, colour);
         if (nblk == 0) continue;
-        k_tan_dmma<2><<<(unsigned)nblk, 256, sm, c->stream>>>(g, dU, dv, colour);
+        k_tan_dmma<2><<<(unsigned)nblk, NTHR, sm, c->stream>>>(g, dU, dv, colour);
         c->last_launches++;
     }
     IGAB_CUDA_TRY(cudaGetLastError());

@@ -603,7 +603,6 @@ extern "C" int igab_device_buffers(igab_ctx *ctx, double **U_dev, double **R_dev
 extern "C" int igab_residual_device(igab_ctx *ctx, const double *U_dev, double *R_dev)
 {
     ARG_CHECK(ctx && U_dev && R_dev, "igab_residual_device: null argument");
-    ARG_CHECK(ctx->phys == IGAB_PHYS_GE, "igab_residual_device: only phys/ge is built in this version");
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     return igab_launch_residual(ctx, U_dev, R_dev);
 }
@@ -628,7 +627,6 @@ extern "C" int igab_tangent_device(igab_ctx *ctx, const double *U_dev, void *val
 {
     ARG_CHECK(ctx && U_dev && vals_dev, "igab_tangent_device: null argument");
     ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_tangent_device: bad precision");
-    ARG_CHECK(ctx->phys == IGAB_PHYS_GE, "igab_tangent_device: only phys/ge is built in this version");
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     return igab_launch_tangent(ctx, U_dev, vals_dev, prec);
 }

@@ -105,6 +105,7 @@ int igab_launch_check_finite(igab_ctx *c, const void *dev, long n, int prec, int
 int igab_launch_basis_tables(igab_ctx *c, int d, const double *dkv, const double *dgx, const double *dgw);
 int igab_launch_fma_peak(int prec, double *tflops);
 int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv);
+int igab_launch_tan_getime(igab_ctx *c, const double *dU, void *dv, int prec);
 /* record profiling event k on the context stream if profiling is on */
 static inline void igab_mark(igab_ctx *c, int k)
 {

@@ -32,11 +32,11 @@ namespace {
 
 /* ============================================================ residual */
 
-template <int TE>
+template <int TE, int NL>
 struct res_smem {
     static constexpr int TC = TE + 2;
     static constexpr int NCP = TC * TC * TC;
-    double U[NCP * 3];
+    double U[NL][NCP * 3];   /* history levels: t_{n+1}, t_n, t_{n-1} (transient) */
     double Racc[NCP * 3];
     double tab[3][TE][IGAB_TAB1D];
     double wh[3][TE][IGAB_NQ];
@@ -47,12 +47,59 @@ struct res_smem {
     double Re[4][81];
 };
 
-template <int TE>
+/* field and derivatives at this thread's Gauss point from one staged level:
+ * z then y contraction in shared memory, x in registers (sum factorisation) */
+template <int TE, int NL>
+__device__ __forceinline__ void res_interp(res_smem<TE, NL> &S, const double *__restrict__ Ul, int group, int gt,
+                                           int lex, int ley, int lez, const double *Bx, const double *By,
+                                           const double *Bz, int qx, int qy, int qz, double u[30])
+{
+    constexpr int TC = TE + 2;
+    for (int o = gt; o < 972; o += 64) {
+        int i = o % 3, kz = (o / 3) % 3, ay = (o / 9) % 3, ax = (o / 27) % 3, q = o / 81;
+        const double *u0 = &Ul[(((lex + ax) * TC + (ley + ay)) * TC + lez) * 3 + i];
+        S.A[group][o] = Bz[q * 9 + 0 * 3 + kz] * u0[0] + Bz[q * 9 + 1 * 3 + kz] * u0[3] + Bz[q * 9 + 2 * 3 + kz] * u0[6];
+    }
+    group_sync(group);
+    for (int o = gt; o < 864; o += 64) {
+        int i = o % 3, kk = (o / 3) % 6, ax = (o / 18) % 3, qq = o / 54;
+        int qyy = qq & 3, qzz = qq >> 2;
+        int ky = kk_ky(kk), kz = kk_kz(kk);
+        const double *a0 = &S.A[group][((qzz * 3 + ax) * 3) * 9 + kz * 3 + i];
+        S.C[group][o] = By[qyy * 9 + 0 * 3 + ky] * a0[0] + By[qyy * 9 + 1 * 3 + ky] * a0[9] + By[qyy * 9 + 2 * 3 + ky] * a0[18];
+    }
+    group_sync(group);
+    const int qq = qy + 4 * qz;
+#pragma unroll
+    for (int a = 0; a < 10; a++) {
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            double s = 0.0;
+#pragma unroll
+            for (int ax = 0; ax < 3; ax++) s += Bx[qx * 9 + ax * 3 + a_kx(a)] * S.C[group][((qq * 3 + ax) * 6 + a_kk(a)) * 3 + i];
+            u[10 * i + a] = s;
+        }
+    }
+    group_sync(group);   /* A and C are reused by the next level */
+}
+
+__device__ __forceinline__ void add_periodic(const igab_geom &g, const double X[3], double u[30])
+{
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        u[10 * i] += g.pp[3 * i] * X[0] + g.pp[3 * i + 1] * X[1] + g.pp[3 * i + 2] * X[2];
+#pragma unroll
+        for (int J = 0; J < 3; J++) u[10 * i + 1 + J] += g.pp[3 * i + J];
+    }
+}
+
+template <int TE, bool GT>
 __global__ void __launch_bounds__(256) k_res_volume(igab_geom g, const double *__restrict__ U,
                                                     double *__restrict__ R, int colour)
 {
+    constexpr int NL = GT ? 3 : 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    res_smem<TE> &S = *reinterpret_cast<res_smem<TE> *>(smem_raw);
+    res_smem<TE, NL> &S = *reinterpret_cast<res_smem<TE, NL> *>(smem_raw);
     constexpr int TC = TE + 2;
     constexpr int NCP = TC * TC * TC;
     constexpr int NEL = TE * TE * TE;
@@ -60,14 +107,17 @@ __global__ void __launch_bounds__(256) k_res_volume(igab_geom g, const double *_
     if (!decode_tile(g, TE, colour, blockIdx.x, T)) return;
     const int tid = threadIdx.x;
 
-    /* ---- stage control-point values and 1-D tables of the tile */
+    /* ---- stage control-point values (all history levels) and 1-D tables of the tile */
     for (int idx = tid; idx < NCP * 3; idx += blockDim.x) {
         int i = idx % 3, cp = idx / 3;
         int lz = cp % TC, ly = (cp / TC) % TC, lx = cp / (TC * TC);
-        double v = 0.0;
-        if (lx < T.nv[0] + 2 && ly < T.nv[1] + 2 && lz < T.nv[2] + 2)
-            v = U[3 * cp_index(g, T.e0[0] + lx, T.e0[1] + ly, T.e0[2] + lz) + i];
-        S.U[idx] = v;
+        const bool in = lx < T.nv[0] + 2 && ly < T.nv[1] + 2 && lz < T.nv[2] + 2;
+        const long gi = in ? 3 * cp_index(g, T.e0[0] + lx, T.e0[1] + ly, T.e0[2] + lz) + i : 0;
+#pragma unroll
+        for (int l = 0; l < NL; l++) {
+            const double *src = l == 0 ? U : (l == 1 ? g.hist1 : g.hist0);
+            S.U[l][idx] = in ? src[gi] : 0.0;
+        }
         S.Racc[idx] = 0.0;
     }
     for (int idx = tid; idx < 3 * TE * IGAB_TAB1D; idx += blockDim.x) {
@@ -94,50 +144,22 @@ __global__ void __launch_bounds__(256) k_res_volume(igab_geom g, const double *_
             const double *Bx = S.tab[0][lex];
             const double *By = S.tab[1][ley];
             const double *Bz = S.tab[2][lez];
-            /* stage A: contract z.  A[qz][ax][ay][kz][i] */
-            for (int o = gt; o < 972; o += 64) {
-                int i = o % 3, kz = (o / 3) % 3, ay = (o / 9) % 3, ax = (o / 27) % 3, q = o / 81;
-                const double *u0 = &S.U[(((lex + ax) * TC + (ley + ay)) * TC + lez) * 3 + i];
-                S.A[group][o] = Bz[q * 9 + 0 * 3 + kz] * u0[0] + Bz[q * 9 + 1 * 3 + kz] * u0[3] +
-                                Bz[q * 9 + 2 * 3 + kz] * u0[6];
-            }
-            group_sync(group);
-            /* stage C: contract y.  C[qy + 4 qz][ax][kk][i] */
-            for (int o = gt; o < 864; o += 64) {
-                int i = o % 3, kk = (o / 3) % 6, ax = (o / 18) % 3, qq = o / 54;
-                int qyy = qq & 3, qzz = qq >> 2;
-                int ky = kk_ky(kk), kz = kk_kz(kk);
-                const double *a0 = &S.A[group][((qzz * 3 + ax) * 3) * 9 + kz * 3 + i];
-                S.C[group][o] = By[qyy * 9 + 0 * 3 + ky] * a0[0] + By[qyy * 9 + 1 * 3 + ky] * a0[9] +
-                                By[qyy * 9 + 2 * 3 + ky] * a0[18];
-            }
-            group_sync(group);
-            /* stage X: one Gauss point per thread */
             double u[30];
-            const int qq = qy + 4 * qz;
-#pragma unroll
-            for (int a = 0; a < 10; a++) {
-#pragma unroll
-                for (int i = 0; i < 3; i++) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int ax = 0; ax < 3; ax++)
-                        s += Bx[qx * 9 + ax * 3 + a_kx(a)] * S.C[group][((qq * 3 + ax) * 6 + a_kk(a)) * 3 + i];
-                    u[10 * i + a] = s;
-                }
-            }
-            if (g.periodic) {
-                double X[3] = {S.xq[0][lex][qx], S.xq[1][ley][qy], S.xq[2][lez][qz]};
-#pragma unroll
-                for (int i = 0; i < 3; i++) {
-                    u[10 * i] += g.pp[3 * i] * X[0] + g.pp[3 * i + 1] * X[1] + g.pp[3 * i + 2] * X[2];
-#pragma unroll
-                    for (int J = 0; J < 3; J++) u[10 * i + 1 + J] += g.pp[3 * i + J];
-                }
-            }
+            const double X[3] = {S.xq[0][lex][qx], S.xq[1][ley][qy], S.xq[2][lez][qz]};
+            res_interp<TE, NL>(S, S.U[0], group, gt, lex, ley, lez, Bx, By, Bz, qx, qy, qz, u);
+            if (g.periodic) add_periodic(g, X, u);
             /* integrand */
             double r[30];
-            {
+            if (GT) {
+                double u1[30], u0[30];
+                res_interp<TE, NL>(S, S.U[NL > 1 ? 1 : 0], group, gt, lex, ley, lez, Bx, By, Bz, qx, qy, qz, u1);
+                res_interp<TE, NL>(S, S.U[NL > 2 ? 2 : 0], group, gt, lex, ley, lez, Bx, By, Bz, qx, qy, qz, u0);
+                if (g.periodic) {
+                    add_periodic(g, X, u1);
+                    add_periodic(g, X, u0);
+                }
+                igab_getime_residual(u, u1, u0, g.coef, g.rho, g.cii, g.dt, r);
+            } else {
                 igab_ge_point<double> P;
                 igab_ge_eval(u, g.coef, P);
                 igab_ge_residual(P, r);
@@ -650,15 +672,15 @@ __global__ void k_check_finite(const T *__restrict__ v, long n, int *__restrict_
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(flag, 1);
 }
 
-template <int TE>
-int launch_res_volume(igab_ctx *c, const igab_geom &g, const double *dU, double *dR)
+template <int TE, bool GT>
+int launch_res_volume_t(igab_ctx *c, const igab_geom &g, const double *dU, double *dR)
 {
-    size_t sm = sizeof(res_smem<TE>);
-    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_res_volume<TE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    size_t sm = sizeof(res_smem<TE, GT ? 3 : 1>);
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_res_volume<TE, GT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     for (int colour = 0; colour < 8; colour++) {
         long nblk = tiles_of_colour(g, TE, colour);
         if (nblk == 0) continue;
-        k_res_volume<TE><<<(unsigned)nblk, 256, sm, c->stream>>>(g, dU, dR, colour);
+        k_res_volume<TE, GT><<<(unsigned)nblk, 256, sm, c->stream>>>(g, dU, dR, colour);
         c->last_launches++;
     }
     IGAB_CUDA_TRY(cudaGetLastError());
@@ -687,8 +709,13 @@ int launch_tangent_t(igab_ctx *c, const double *dU, T *dv)
     IGAB_CUDA_TRY(cudaMemsetAsync(dv, 0, (size_t)c->nnz * sizeof(T), c->stream));
     igab_mark(c, 3);
     int l0 = c->last_launches;
-    int e = (sizeof(T) == 8 && c->tan_kernel == 1) ? igab_launch_tan_dmma(c, dU, (double *)dv)
-                                                   : launch_tan_volume<T, 2>(c, g, dU, dv);
+    int e;
+    if (c->phys == IGAB_PHYS_GETIME)
+        e = igab_launch_tan_getime(c, dU, dv, sizeof(T) == 8 ? IGAB_PREC_FP64 : IGAB_PREC_FP32);
+    else if (sizeof(T) == 8 && c->tan_kernel == 1)
+        e = igab_launch_tan_dmma(c, dU, (double *)dv);
+    else
+        e = launch_tan_volume<T, 2>(c, g, dU, dv);
     if (e) return e;
     c->nvol_tan = c->last_launches - l0;
     igab_mark(c, 4);
@@ -711,7 +738,11 @@ int igab_launch_residual(igab_ctx *c, const double *dU, double *dR)
     igab_geom g = c->geom();
     IGAB_CUDA_TRY(cudaMemsetAsync(dR, 0, (size_t)c->ndof * sizeof(double), c->stream));
     igab_mark(c, 0);
-    int e = c->tile_res == 4 ? launch_res_volume<4>(c, g, dU, dR) : launch_res_volume<2>(c, g, dU, dR);
+    int e;
+    if (c->phys == IGAB_PHYS_GETIME)
+        e = c->tile_res == 4 ? launch_res_volume_t<4, true>(c, g, dU, dR) : launch_res_volume_t<2, true>(c, g, dU, dR);
+    else
+        e = c->tile_res == 4 ? launch_res_volume_t<4, false>(c, g, dU, dR) : launch_res_volume_t<2, false>(c, g, dU, dR);
     if (e) return e;
     c->nvol_res = c->last_launches;
     igab_mark(c, 1);

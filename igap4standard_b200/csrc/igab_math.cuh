@@ -34,6 +34,7 @@
 #define IGAB_HD __host__ __device__ __forceinline__
 #else
 #define IGAB_HD inline
+
 #endif
 
 #define IGAB_INV_SQRT2 0.70710678118654752440
@@ -256,4 +257,110 @@ IGAB_HD void igab_ge_dense_tangent(const igab_ge_point<T> &P, T D[27][27])
         }
 }
 
+
+/* ------------------------------------------------------------- Taylor arithmetic */
+
+/* Truncated univariate Taylor polynomials c[0] + c[1] s + ... + c[N-1] s^(N-1).
+ * Running the energy code on u(s) = m + s h with this type yields the Taylor
+ * coefficients of dW/du (or of the point data) along the segment, which is how
+ * the transient integrand below is formed. */
+template <int N>
+struct igab_tay {
+    double c[N];
+    IGAB_HD igab_tay() {}
+    IGAB_HD igab_tay(double x)
+    {
+        c[0] = x;
+        for (int i = 1; i < N; i++) c[i] = 0.0;
+    }
+};
+template <int N>
+IGAB_HD igab_tay<N> operator+(const igab_tay<N> &a, const igab_tay<N> &b)
+{
+    igab_tay<N> r;
+    for (int i = 0; i < N; i++) r.c[i] = a.c[i] + b.c[i];
+    return r;
+}
+template <int N>
+IGAB_HD igab_tay<N> operator-(const igab_tay<N> &a, const igab_tay<N> &b)
+{
+    igab_tay<N> r;
+    for (int i = 0; i < N; i++) r.c[i] = a.c[i] - b.c[i];
+    return r;
+}
+template <int N>
+IGAB_HD igab_tay<N> operator-(const igab_tay<N> &a)
+{
+    igab_tay<N> r;
+    for (int i = 0; i < N; i++) r.c[i] = -a.c[i];
+    return r;
+}
+template <int N>
+IGAB_HD igab_tay<N> operator*(const igab_tay<N> &a, const igab_tay<N> &b)
+{
+    igab_tay<N> r;
+    for (int i = 0; i < N; i++) {
+        double t = 0.0;
+        for (int j = 0; j <= i; j++) t += a.c[j] * b.c[i - j];
+        r.c[i] = t;
+    }
+    return r;
+}
+template <int N>
+IGAB_HD igab_tay<N> &operator+=(igab_tay<N> &a, const igab_tay<N> &b)
+{
+    a = a + b;
+    return a;
+}
+
+/* ------------------------------------------------------------- phys/getime */
+
+/* The transient integrand of phys/getime (torder = 2, U_hist levels: u at t_{n+1},
+ * u1 at t_n, u0 at t_{n-1}; par = {.., rho = par[5], c = par[6], dt = par[7]}):
+ *   value components:  c (u - u0) / (2 dt) + rho (u + u0 - 2 u1) / dt^2
+ *   field derivatives: sum_{n=0..3} g_n / (n + 1),  g(s) = dW/du(m + s h) = sum g_n s^n,
+ *                      m = (u0 + u1)/2, h = (u - u0)/2,
+ * i.e. the average of dW/du over the segment from the mid-state of (t_{n-1}, t_n)
+ * to that of (t_n, t_{n+1}), truncated after the cubic term of its Taylor series
+ * (the expression phys/getime/residual.c:4127-4156 expands).  Its derivative is
+ *   d r / d u = 1/2 (H_0/2 + H_1/3 + H_2/4) + diag(rho/dt^2 + c/(2 dt)) on values,
+ * H(s) = d2W/du2(m + s h) = sum H_j s^j. */
+template <typename T>
+IGAB_HD void igab_getime_residual(const T *u, const T *u1, const T *u0, const igab_ge_coef &c,
+                                  double rho, double cii, double dt, T *r)
+{
+    igab_tay<4> ut[30];
+    for (int i = 0; i < 30; i++) {
+        ut[i].c[0] = double((u0[i] + u1[i]) * T(0.5));
+        ut[i].c[1] = double((u[i] - u0[i]) * T(0.5));
+        ut[i].c[2] = 0.0;
+        ut[i].c[3] = 0.0;
+    }
+    igab_ge_point<igab_tay<4>> P;
+    igab_ge_eval(ut, c, P);
+    igab_tay<4> rt[30];
+    igab_ge_residual(P, rt);
+    for (int i = 0; i < 30; i++) r[i] = T(rt[i].c[0] + rt[i].c[1] / 2.0 + rt[i].c[2] / 3.0 + rt[i].c[3] / 4.0);
+    for (int k = 0; k < 3; k++)
+        r[10 * k] = T(cii) * (u[10 * k] - u0[10 * k]) / T(2.0 * dt) +
+                    T(rho) * (u[10 * k] + u0[10 * k] - T(2) * u1[10 * k]) / T(dt * dt);
+}
+
+/* dense getime tangent on the 27 field-derivative components (check path) */
+template <typename T>
+IGAB_HD void igab_getime_dense_tangent(const T *u, const T *u1, const T *u0, const igab_ge_coef &c, T D[27][27])
+{
+    igab_tay<3> ut[30];
+    for (int i = 0; i < 30; i++) {
+        ut[i].c[0] = double((u0[i] + u1[i]) * T(0.5));
+        ut[i].c[1] = double((u[i] - u0[i]) * T(0.5));
+        ut[i].c[2] = 0.0;
+    }
+    igab_ge_point<igab_tay<3>> P;
+    igab_ge_eval(ut, c, P);
+    igab_tay<3> H[27][27];
+    igab_ge_dense_tangent(P, H);
+    for (int s = 0; s < 27; s++)
+        for (int t = 0; t < 27; t++) D[s][t] = T(0.5 * (H[s][t].c[0] / 2.0 + H[s][t].c[1] / 3.0 + H[s][t].c[2] / 4.0));
+}
 #endif

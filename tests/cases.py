@@ -80,3 +80,31 @@ def tangent_tolerance(rowptr, vals_ref):
     rowmax = np.maximum.reduceat(np.abs(vals_ref), rowptr[:-1]) if vals_ref.size else np.zeros(0)
     per = np.repeat(rowmax, np.diff(rowptr))
     return 1e-12 * np.maximum(np.abs(vals_ref), per)
+
+
+def make_transient_case(name):
+    """Seeded phys/getime cases: dict as make_case plus U1 (t_n) and U0 (t_{n-1})."""
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    if name == "getime_small":        # reference default material (dt = 5e-4), example BCs
+        nelem = (2, 3, 2)
+        kn = mesh.knots_for(nelem, perturb=0.1, seed=4)
+        pm = mesh.PAR_MAT_DEFAULT.copy()
+        bc, pd = mesh.bc_example()
+        amp = 1e-3
+    elif name == "getime_config2":    # BASELINE config-2 physics: rho = 1, dt = 1e-3, traction on x = 1
+        nelem = (3, 2, 3)
+        kn = mesh.knots_for(nelem)
+        pm = mesh.par_mat_from_lame(1.0, 1.0, 0.1)
+        pm[5], pm[6], pm[7] = 1.0, 1.0, 1e-3
+        bc, pd = mesh.bc_config0()
+        amp = 2e-2
+    else:
+        raise KeyError(name)
+    pn = np.zeros(39)
+    pn[6 + 0] = 0.01                  # face 1, standard order, x-dof traction
+    ndof = mesh.n_dof(nelem)
+    U0 = rng.uniform(-amp, amp, ndof)
+    U1 = U0 + rng.uniform(-amp, amp, ndof) * 0.3
+    U = U1 + rng.uniform(-amp, amp, ndof) * 0.3
+    return dict(phys="getime", nelem=nelem, knots=kn, par_mat=pm, bc_type=bc, par_dirichlet=pd,
+                par_periodic=np.zeros(9), par_neumann=pn, U=U, U1=U1, U0=U0)

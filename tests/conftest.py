@@ -68,6 +68,7 @@ def host_math():
     vp = ctypes.c_void_p
     L.host_ge_point.argtypes = [vp, vp, vp, vp]
     L.host_bspline_p2.argtypes = [vp, ctypes.c_double, vp]
+    L.host_getime_point.argtypes = [vp, vp, vp, vp]
     return L
 
 

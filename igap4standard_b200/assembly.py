@@ -133,6 +133,17 @@ class Assembly:
         check(self.lib, "igab_tangent_device",
               self.lib.igab_tangent_device(self.h, vp(U_ptr), vp(vals_ptr), PREC[prec]))
 
+    def graph_capture(self, U_ptr, R_ptr=None, vals_ptr=None, prec="fp64"):
+        what = (1 if R_ptr is not None else 0) | (2 if vals_ptr is not None else 0)
+        check(self.lib, "igab_graph_capture",
+              self.lib.igab_graph_capture(self.h, vp(U_ptr), vp(R_ptr or 0), vp(vals_ptr or 0), PREC[prec], what))
+
+    def graph_launch(self):
+        check(self.lib, "igab_graph_launch", self.lib.igab_graph_launch(self.h))
+
+    def graph_destroy(self):
+        check(self.lib, "igab_graph_destroy", self.lib.igab_graph_destroy(self.h))
+
     def set_stream(self, stream_ptr):
         check(self.lib, "igab_set_stream", self.lib.igab_set_stream(self.h, vp(stream_ptr)))
 

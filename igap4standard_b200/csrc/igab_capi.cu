@@ -208,12 +208,18 @@ static int build_dirichlet(igab_ctx *c)
     std::vector<double> gv;
     for (long r = 0; r < c->ndof; r++)
         if (is[r]) { rows.push_back((int)r); gv.push_back(g[r]); }
-    if (c->d_drow) { cudaFree(c->d_drow); c->d_drow = nullptr; }
-    if (c->d_dg) { cudaFree(c->d_dg); c->d_dg = nullptr; }
-    c->nd = (long)rows.size();
+    /* the Dirichlet row set depends only on bc_type; values change with par_dirichlet.
+     * Existing buffers are refilled in place so captured graphs stay valid. */
+    if ((long)rows.size() != c->nd || !c->d_drow) {
+        if (c->d_drow) { cudaFree(c->d_drow); c->d_drow = nullptr; }
+        if (c->d_dg) { cudaFree(c->d_dg); c->d_dg = nullptr; }
+        c->nd = (long)rows.size();
+        if (c->nd > 0) {
+            IGAB_CUDA_TRY(cudaMalloc((void **)&c->d_drow, rows.size() * sizeof(int)));
+            IGAB_CUDA_TRY(cudaMalloc((void **)&c->d_dg, gv.size() * sizeof(double)));
+        }
+    }
     if (c->nd > 0) {
-        IGAB_CUDA_TRY(cudaMalloc((void **)&c->d_drow, rows.size() * sizeof(int)));
-        IGAB_CUDA_TRY(cudaMalloc((void **)&c->d_dg, gv.size() * sizeof(double)));
         IGAB_CUDA_TRY(cudaMemcpy(c->d_drow, rows.data(), rows.size() * sizeof(int), cudaMemcpyHostToDevice));
         IGAB_CUDA_TRY(cudaMemcpy(c->d_dg, gv.data(), gv.size() * sizeof(double), cudaMemcpyHostToDevice));
     }
@@ -317,6 +323,8 @@ static void free_ctx(igab_ctx *c)
     cudaFree(c->d_hval); cudaFree(c->d_neu_row); cudaFree(c->d_neu_ptr); cudaFree(c->d_neu_ent);
     cudaFree(c->d_dnz); cudaFree(c->d_combo_info); cudaFree(c->d_hist);
     cudaFree(c->d_U); cudaFree(c->d_R); cudaFree(c->d_vals);
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
     for (int k = 0; k < 6; k++)
         if (c->ev[k]) cudaEventDestroy(c->ev[k]);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -554,8 +562,10 @@ extern "C" int igab_set_neumann_values(igab_ctx *ctx, const double *values)
     for (long i = 0; i < ctx->n_neu_points; i++)
         if (values[i] != 0.0) { nz = true; break; }
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
-    if (nz) IGAB_CUDA_TRY(cudaMemcpyAsync(ctx->d_hval, values, (size_t)ctx->n_neu_points * sizeof(double),
-                                          cudaMemcpyHostToDevice, ctx->stream));
+    /* zeros are copied too while a captured graph (which always runs the Neumann kernel) exists */
+    if (nz || ctx->graph_exec)
+        IGAB_CUDA_TRY(cudaMemcpyAsync(ctx->d_hval, values, (size_t)ctx->n_neu_points * sizeof(double),
+                                      cudaMemcpyHostToDevice, ctx->stream));
     IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     ctx->neumann_nonzero = nz;
     return 0;
@@ -757,4 +767,68 @@ extern "C" int igab_get_option(const igab_ctx *ctx, int option, int *value)
         igab_set_error("igab_get_option: unknown option %d", option);
         return IGAB_ERR_ARG;
     }
+}
+
+extern "C" int igab_graph_destroy(igab_ctx *ctx)
+{
+    ARG_CHECK(ctx, "igab_graph_destroy: null context");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
+    if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+    return 0;
+}
+
+extern "C" int igab_graph_capture(igab_ctx *ctx, const double *U_dev, double *R_dev, void *vals_dev, int prec, int what)
+{
+    ARG_CHECK(ctx && U_dev, "igab_graph_capture: null argument");
+    ARG_CHECK(what >= 1 && what <= 3, "igab_graph_capture: what must be 1, 2 or 3");
+    ARG_CHECK(!(what & 1) || R_dev, "igab_graph_capture: residual output missing");
+    ARG_CHECK(!(what & 2) || vals_dev, "igab_graph_capture: tangent output missing");
+    ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_graph_capture: bad precision");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    int rc = igab_graph_destroy(ctx);
+    if (rc) return rc;
+    ARG_CHECK(ctx->stream != nullptr, "igab_graph_capture: the context stream must not be the legacy default stream");
+    /* the graph always runs the Neumann kernel: zero values skipped by the last upload */
+    if (!ctx->neumann_nonzero && ctx->d_hval)
+        IGAB_CUDA_TRY(cudaMemsetAsync(ctx->d_hval, 0, (size_t)ctx->n_neu_points * sizeof(double), ctx->stream));
+    /* one eager run first: kernel attributes are set outside the capture */
+    const bool prof = ctx->profiling;
+    ctx->profiling = false;
+    ctx->force_neumann = true;
+    if (what & 1) rc = igab_launch_residual(ctx, U_dev, R_dev);
+    if (!rc && (what & 2)) rc = igab_launch_tangent(ctx, U_dev, vals_dev, prec);
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) { igab_set_error("igab_graph_capture: %s", cudaGetErrorString(e)); rc = IGAB_ERR_CUDA; }
+    }
+    if (!rc) {
+        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) { igab_set_error("cudaStreamBeginCapture: %s", cudaGetErrorString(e)); rc = IGAB_ERR_CUDA; }
+        else {
+            int rc2 = 0;
+            if (what & 1) rc2 = igab_launch_residual(ctx, U_dev, R_dev);
+            if (!rc2 && (what & 2)) rc2 = igab_launch_tangent(ctx, U_dev, vals_dev, prec);
+            cudaGraph_t gr = nullptr;
+            e = cudaStreamEndCapture(ctx->stream, &gr);
+            if (rc2) { rc = rc2; if (gr) cudaGraphDestroy(gr); }
+            else if (e != cudaSuccess) { igab_set_error("cudaStreamEndCapture: %s", cudaGetErrorString(e)); rc = IGAB_ERR_CUDA; }
+            else {
+                ctx->graph = gr;
+                e = cudaGraphInstantiate(&ctx->graph_exec, gr, 0);
+                if (e != cudaSuccess) { igab_set_error("cudaGraphInstantiate: %s", cudaGetErrorString(e)); rc = IGAB_ERR_CUDA; }
+            }
+        }
+    }
+    ctx->profiling = prof;
+    ctx->force_neumann = false;
+    return rc;
+}
+
+extern "C" int igab_graph_launch(igab_ctx *ctx)
+{
+    ARG_CHECK(ctx && ctx->graph_exec, "igab_graph_launch: no captured graph");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    IGAB_CUDA_TRY(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+    return 0;
 }

@@ -94,6 +94,11 @@ struct igab_ctx {
     bool ev_res = false, ev_tan = false;
     int nvol_res = 0, nvol_tan = 0;
 
+    /* captured assembly graph */
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    bool force_neumann = false;   /* graph capture keeps the Neumann kernel in whatever the values become */
+
     igab_geom geom() const;
 };
 

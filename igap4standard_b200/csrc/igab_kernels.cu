@@ -746,7 +746,7 @@ int igab_launch_residual(igab_ctx *c, const double *dU, double *dR)
     if (e) return e;
     c->nvol_res = c->last_launches;
     igab_mark(c, 1);
-    if (c->neumann_nonzero && c->n_neu_rows > 0) {
+    if ((c->neumann_nonzero || c->force_neumann) && c->n_neu_rows > 0) {
         k_res_neumann<<<(unsigned)((c->n_neu_rows + 127) / 128), 128, 0, c->stream>>>(
             g, c->n_neu_rows, c->d_neu_row, c->d_neu_ptr, c->d_neu_ent, c->d_combo_info, c->d_dnz, c->d_hval, dR);
         c->last_launches++;

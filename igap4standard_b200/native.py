@@ -71,6 +71,9 @@ IGAB_API = [
     ("igab_fma_peak", ctypes.c_int, [ctypes.c_int, ctypes.c_int, c_double_p]),
     ("igab_residual_noalloc", ctypes.c_int, [vp, vp, vp]),
     ("igab_set_option", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+    ("igab_graph_capture", ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int, ctypes.c_int]),
+    ("igab_graph_launch", ctypes.c_int, [vp]),
+    ("igab_graph_destroy", ctypes.c_int, [vp]),
     ("igab_get_option", ctypes.c_int, [vp, ctypes.c_int, c_int_p]),
 ]
 

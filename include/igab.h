@@ -121,6 +121,15 @@ int igab_last_kernel_ms(igab_ctx *ctx, double ms[6]);
 /* FMA throughput probe of the device (TFLOP/s, 2 flops per FMA), prec = igab_prec */
 int igab_fma_peak(int device, int prec, double *tflops);
 
+/* ---- CUDA graphs: capture one assembly at fixed device pointers, replay it.
+ * what: 1 residual, 2 tangent, 3 both (residual then tangent).  Parameters
+ * changed later with igab_set_par_dirichlet / igab_set_neumann_values /
+ * igab_set_history are picked up by replays (they update device buffers in
+ * place); igab_set_par_mat and igab_set_par_periodic need a new capture. */
+int igab_graph_capture(igab_ctx *ctx, const double *U_dev, double *R_dev, void *vals_dev, int prec, int what);
+int igab_graph_launch(igab_ctx *ctx);
+int igab_graph_destroy(igab_ctx *ctx);
+
 /* ---- residual for callers that cannot have the library allocate device memory.
  * No counterpart in the reference.  Same result as igab_residual, but U and R
  * are staged in a file-scope device array (2 x 8 MiB, held by every GPU that

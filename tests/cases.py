@@ -59,6 +59,16 @@ def make_case(name):
         pp = np.zeros(9)
         pn = np.zeros(39)
         amp = 1e-3
+    elif name == "newton_backtrack":    # strong Dirichlet pull: the first full Newton step is rejected
+        nelem = (3, 3, 3)
+        kn = mesh.knots_for(nelem, perturb=0.1, seed=3)
+        pm = mesh.par_mat_from_lame(1.0, 1.0, 0.1)
+        bc, pd = mesh.bc_config0()
+        pd = np.zeros(9)
+        pd[0] = 0.3
+        pp = np.zeros(9)
+        pn = np.zeros(39)
+        amp = 1e-3
     else:
         raise KeyError(name)
     ndof = mesh.n_dof(nelem)

@@ -46,6 +46,7 @@ class Assembly:
         self.ndof, self.nnz, self.nelem_total = nd.value, nz.value, ne.value
         self.nelem = tuple(int(n) for n in nelem)
         self.phys = phys
+        self.device = int(device)
 
     def close(self):
         if getattr(self, "h", None):
@@ -143,6 +144,52 @@ class Assembly:
 
     def graph_destroy(self):
         check(self.lib, "igab_graph_destroy", self.lib.igab_graph_destroy(self.h))
+
+    # ---- adjoint of the element-scaled problem (s_e = exp(g_e))
+    def set_element_log_scale(self, g):
+        """g: [nelem_total] log-scales in the reference's element order, or None for s = 1."""
+        if g is None:
+            check(self.lib, "igab_set_element_log_scale", self.lib.igab_set_element_log_scale(self.h, None, 0))
+            return
+        a = np.ascontiguousarray(g, dtype=np.float64)
+        if a.size != self.nelem_total:
+            raise ValueError("g needs one value per element")
+        check(self.lib, "igab_set_element_log_scale", self.lib.igab_set_element_log_scale(self.h, _ptr(a), 0))
+
+    def adjoint_forward_device(self, g_ptr, U_ptr, R_ptr=None, vals_ptr=None, prec="fp64"):
+        check(self.lib, "igab_adjoint_forward",
+              self.lib.igab_adjoint_forward(self.h, vp(g_ptr or 0), vp(U_ptr), vp(R_ptr or 0), vp(vals_ptr or 0),
+                                            PREC[prec]))
+
+    def adjoint_backward_device(self, U_ptr, vals_ptr, lam_ptr, KTlam_ptr=None, grad_ptr=None, prec="fp64"):
+        check(self.lib, "igab_adjoint_backward",
+              self.lib.igab_adjoint_backward(self.h, vp(U_ptr or 0), vp(vals_ptr or 0), PREC[prec], vp(lam_ptr),
+                                             vp(KTlam_ptr or 0), vp(grad_ptr or 0)))
+
+    def dRdg(self, U, lam):
+        """Host convenience: grad[e] = lam . dR/dg_e at U (Dirichlet rows of lam ignored)."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        Ud = torch.as_tensor(np.ascontiguousarray(U, dtype=np.float64)).to(dev)
+        Ld = torch.as_tensor(np.ascontiguousarray(lam, dtype=np.float64)).to(dev)
+        G = torch.empty(self.nelem_total, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        self.adjoint_backward_device(Ud.data_ptr(), None, Ld.data_ptr(), None, G.data_ptr())
+        self.sync()
+        return G.cpu().numpy()
+
+    def tangent_transpose_apply(self, vals, x, prec="fp64"):
+        """Host convenience: K^T x for CSR values vals of this mesh's pattern."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        dt = np.float64 if prec == "fp64" else np.float32
+        Vd = torch.as_tensor(np.ascontiguousarray(vals, dtype=dt)).to(dev)
+        Xd = torch.as_tensor(np.ascontiguousarray(x, dtype=np.float64)).to(dev)
+        Y = torch.empty(self.ndof, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        self.adjoint_backward_device(None, Vd.data_ptr(), Xd.data_ptr(), Y.data_ptr(), None, prec)
+        self.sync()
+        return Y.cpu().numpy()
 
     def set_stream(self, stream_ptr):
         check(self.lib, "igab_set_stream", self.lib.igab_set_stream(self.h, vp(stream_ptr)))

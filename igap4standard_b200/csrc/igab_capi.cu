@@ -56,6 +56,7 @@ igab_geom igab_ctx::geom() const
     g.cii = par_mat[6];
     g.dt = par_mat[7];
     g.phys = phys;
+    g.escale = escale_on ? d_escale : nullptr;
     return g;
 }
 
@@ -323,6 +324,7 @@ static void free_ctx(igab_ctx *c)
     cudaFree(c->d_hval); cudaFree(c->d_neu_row); cudaFree(c->d_neu_ptr); cudaFree(c->d_neu_ent);
     cudaFree(c->d_dnz); cudaFree(c->d_combo_info); cudaFree(c->d_hist);
     cudaFree(c->d_U); cudaFree(c->d_R); cudaFree(c->d_vals);
+    cudaFree(c->d_escale); cudaFree(c->d_lam);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     for (int k = 0; k < 6; k++)
@@ -831,4 +833,75 @@ extern "C" int igab_graph_launch(igab_ctx *ctx)
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     IGAB_CUDA_TRY(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
     return 0;
+}
+
+/* ------------------------------------------------------------------ adjoint */
+
+static int ensure_escale(igab_ctx *ctx)
+{
+    if (!ctx->d_escale) IGAB_CUDA_TRY(cudaMalloc((void **)&ctx->d_escale, (size_t)ctx->nel * sizeof(double)));
+    return 0;
+}
+
+extern "C" int igab_set_element_log_scale(igab_ctx *ctx, const double *g, int on_device)
+{
+    ARG_CHECK(ctx, "igab_set_element_log_scale: null context");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (!g) {
+        ctx->escale_on = false;
+        return 0;
+    }
+    int rc = ensure_escale(ctx);
+    if (rc) return rc;
+    double *dg = nullptr;
+    if (on_device) {
+        dg = const_cast<double *>(g);
+    } else {
+        IGAB_CUDA_TRY(cudaMallocAsync((void **)&dg, (size_t)ctx->nel * sizeof(double), ctx->stream));
+        IGAB_CUDA_TRY(cudaMemcpyAsync(dg, g, (size_t)ctx->nel * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    rc = igab_launch_exp_scale(ctx, dg);
+    if (!on_device) cudaFreeAsync(dg, ctx->stream);
+    if (rc) return rc;
+    IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    ctx->escale_on = true;
+    return 0;
+}
+
+extern "C" int igab_adjoint_forward(igab_ctx *ctx, const double *g_dev, const double *U_dev, double *R_dev,
+                                    void *vals_dev, int prec)
+{
+    ARG_CHECK(ctx && U_dev, "igab_adjoint_forward: null argument");
+    ARG_CHECK(R_dev || vals_dev, "igab_adjoint_forward: nothing to compute");
+    ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_adjoint_forward: bad precision");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    int rc = 0;
+    if (g_dev) {
+        rc = ensure_escale(ctx);
+        if (!rc) rc = igab_launch_exp_scale(ctx, g_dev);
+        if (rc) return rc;
+        ctx->escale_on = true;
+    }
+    if (R_dev) rc = igab_launch_residual(ctx, U_dev, R_dev);
+    if (!rc && vals_dev) rc = igab_launch_tangent(ctx, U_dev, vals_dev, prec);
+    return rc;
+}
+
+extern "C" int igab_adjoint_backward(igab_ctx *ctx, const double *U_dev, const void *vals_dev, int prec,
+                                     const double *lam_dev, double *KTlam_dev, double *grad_dev)
+{
+    ARG_CHECK(ctx && lam_dev, "igab_adjoint_backward: null argument");
+    ARG_CHECK(KTlam_dev || grad_dev, "igab_adjoint_backward: nothing to compute");
+    ARG_CHECK(!KTlam_dev || vals_dev, "igab_adjoint_backward: K^T lam needs the tangent values");
+    ARG_CHECK(!grad_dev || U_dev, "igab_adjoint_backward: dR/dg needs U");
+    ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_adjoint_backward: bad precision");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    ctx->last_launches = 0;
+    int rc = 0;
+    if (KTlam_dev) rc = igab_launch_tangent_transpose(ctx, vals_dev, prec, lam_dev, KTlam_dev);
+    if (!rc && grad_dev) {
+        if (!ctx->d_lam) IGAB_CUDA_TRY(cudaMalloc((void **)&ctx->d_lam, (size_t)ctx->ndof * sizeof(double)));
+        rc = igab_launch_adjoint_dRdg(ctx, U_dev, lam_dev, grad_dev);
+    }
+    return rc;
 }

@@ -75,6 +75,11 @@ __device__ __forceinline__ int csr_pos(const igab_geom &g, int x, int y, int z, 
     return (((cx - x0) * nyb + (cy - y0)) * nzb + (cz - z0)) * 3 + k2;
 }
 
+/* per-element integrand scale (1 when no scaling is set) */
+__device__ __forceinline__ double elem_scale(const igab_geom &g, int ex, int ey, int ez)
+{
+    return g.escale ? g.escale[((long)ex * g.ne[1] + ey) * g.ne[2] + ez] : 1.0;
+}
 
 long tiles_of_colour(const igab_geom &g, int TE, int colour)
 {

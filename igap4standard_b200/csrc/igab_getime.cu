@@ -229,7 +229,8 @@ __global__ void __launch_bounds__(256) k_tan_getime(igab_geom g, const double *_
                 for (int K = 0; K < 3; K++)
                     pt[GP_TAU + 3 * I + K] = cw[0] * P.tau[I][K].c[0] + cw[1] * P.tau[I][K].c[1] + cw[2] * P.tau[I][K].c[2];
             }
-            pt[GP_W] = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz];
+            pt[GP_W] = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz] *
+                       elem_scale(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez);
             pt[GP_MASS] = g.rho / (g.dt * g.dt) + g.cii / (2.0 * g.dt);
         }
         __syncthreads();

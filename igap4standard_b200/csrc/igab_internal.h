@@ -32,6 +32,8 @@ struct igab_geom {
     const double *hist0;  /* U at t_{n-1} (U_hist level 2) */
     double rho, cii, dt;
     int phys;
+    /* per-element integrand scale s_e = exp(g_e), element e = (ex*ne1 + ey)*ne2 + ez; null: 1 */
+    const double *escale;
 };
 
 struct igab_ctx {
@@ -94,6 +96,11 @@ struct igab_ctx {
     bool ev_res = false, ev_tan = false;
     int nvol_res = 0, nvol_tan = 0;
 
+    /* adjoint: element scales and the masked adjoint vector */
+    double *d_escale = nullptr;        /* [nel] exp(g_e) */
+    bool escale_on = false;
+    double *d_lam = nullptr;           /* [ndof] lambda with Dirichlet rows zeroed */
+
     /* captured assembly graph */
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -111,6 +118,9 @@ int igab_launch_basis_tables(igab_ctx *c, int d, const double *dkv, const double
 int igab_launch_fma_peak(int prec, double *tflops);
 int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv);
 int igab_launch_tan_getime(igab_ctx *c, const double *dU, void *dv, int prec);
+int igab_launch_exp_scale(igab_ctx *c, const double *dg);
+int igab_launch_adjoint_dRdg(igab_ctx *c, const double *dU, const double *dlam, double *dgrad);
+int igab_launch_tangent_transpose(igab_ctx *c, const void *dvals, int prec, const double *dx, double *dy);
 /* record profiling event k on the context stream if profiling is on */
 static inline void igab_mark(igab_ctx *c, int k)
 {

@@ -93,9 +93,14 @@ __device__ __forceinline__ void add_periodic(const igab_geom &g, const double X[
     }
 }
 
-template <int TE, bool GT>
+/* VJP = false: add the tile's element residuals into R.
+ * VJP = true: adjoint mode; nothing is added to R, instead grad[e] = lam_e . R_e
+ * for every element of the tile (lam with Dirichlet rows already zeroed), i.e.
+ * the vector-Jacobian product lam^T dR/dg_e of the scaled residual. */
+template <int TE, bool GT, bool VJP>
 __global__ void __launch_bounds__(256) k_res_volume(igab_geom g, const double *__restrict__ U,
-                                                    double *__restrict__ R, int colour)
+                                                    double *__restrict__ R, int colour,
+                                                    const double *__restrict__ lam, double *__restrict__ grad)
 {
     constexpr int NL = GT ? 3 : 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -118,7 +123,7 @@ __global__ void __launch_bounds__(256) k_res_volume(igab_geom g, const double *_
             const double *src = l == 0 ? U : (l == 1 ? g.hist1 : g.hist0);
             S.U[l][idx] = in ? src[gi] : 0.0;
         }
-        S.Racc[idx] = 0.0;
+        S.Racc[idx] = VJP ? (in ? lam[gi] : 0.0) : 0.0;   /* adjoint mode keeps lam here */
     }
     for (int idx = tid; idx < 3 * TE * IGAB_TAB1D; idx += blockDim.x) {
         int d = idx / (TE * IGAB_TAB1D), r = idx % (TE * IGAB_TAB1D), le = r / IGAB_TAB1D, o = r % IGAB_TAB1D;
@@ -164,7 +169,8 @@ __global__ void __launch_bounds__(256) k_res_volume(igab_geom g, const double *_
                 igab_ge_eval(u, g.coef, P);
                 igab_ge_residual(P, r);
             }
-            const double w = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz];
+            const double w = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz] *
+                             elem_scale(g, T.e0[0] + lex, T.e0[1] + ley, T.e0[2] + lez);
 #pragma unroll
             for (int k = 0; k < 30; k++) r[k] *= w;
 
@@ -255,6 +261,27 @@ __global__ void __launch_bounds__(256) k_res_volume(igab_geom g, const double *_
                 for (int s = 0; s < 9; s++) S.Re[group][(qx * 3 + qy) * 9 + s] = P3[s] + S.red[group][(qx * 3 + qy) * 9 + s];
         }
         __syncthreads();
+        if (VJP) {
+            /* one warp per element: grad_e = sum_k Re[k] lam[k], fixed order */
+            const int w = tid >> 5, lane = tid & 31;
+            if (w < 4) {
+                const int e = base + w;
+                const int ex = e / (TE * TE), ey = (e / TE) % TE, ez = e % TE;
+                if (e < NEL && ex < T.nv[0] && ey < T.nv[1] && ez < T.nv[2]) {
+                    double s = 0.0;
+                    for (int k = lane; k < 81; k += 32) {
+                        const int i = k % 3, az = (k / 3) % 3, ay = (k / 9) % 3, ax = k / 27;
+                        s += S.Re[w][k] * S.Racc[(((ex + ax) * TC + (ey + ay)) * TC + (ez + az)) * 3 + i];
+                    }
+#pragma unroll
+                    for (int m = 16; m >= 1; m >>= 1) s += shfl_xor(s, m);
+                    if (lane == 0)
+                        grad[((long)(T.e0[0] + ex) * g.ne[1] + (T.e0[1] + ey)) * g.ne[2] + (T.e0[2] + ez)] = s;
+                }
+            }
+            __syncthreads();
+            continue;
+        }
         /* ---- fixed-order accumulation of the (up to) 4 element vectors into the tile */
         for (int idx = tid; idx < NCP * 3; idx += blockDim.x) {
             int i = idx % 3, cp = idx / 3;
@@ -273,6 +300,7 @@ __global__ void __launch_bounds__(256) k_res_volume(igab_geom g, const double *_
         }
         __syncthreads();
     }
+    if (VJP) return;
     /* ---- add the tile into the global residual (no other tile of this colour touches these points) */
     for (int idx = tid; idx < NCP * 3; idx += blockDim.x) {
         int i = idx % 3, cp = idx / 3;
@@ -489,7 +517,8 @@ __global__ void __launch_bounds__(256) k_tan_volume(igab_geom g, const double *_
             for (int I = 0; I < 3; I++)
 #pragma unroll
                 for (int K = 0; K < 3; K++) pt[PT_TAU + 3 * I + K] = double(P.tau[I][K]);
-            pt[PT_W] = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz];
+            pt[PT_W] = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz] *
+                       elem_scale(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez);
         }
         __syncthreads();
 
@@ -662,6 +691,78 @@ __global__ void k_csr_cols(igab_geom g, int *__restrict__ cols)
                 for (int k = 0; k < 3; k++) cols[o++] = (int)(3 * cp_index(g, cx, cy, cz) + k);
 }
 
+/* y = K^T x on the structured CSR values (vals).  One block per output
+ * segment: control points (cx, cy, z) for z in [zlo, zhi], all 3 components.
+ * Column (cx,cy,z,k) of K is held by the rows of the 25 neighbouring z-lines
+ * (sx, sy); each such row stores its entries for line (cx, cy) as one
+ * contiguous run of <= 15 values (5 z x 3 k, columns ascending).  The block
+ * stages those runs line by line in shared memory with coalesced loads and
+ * every output row sums its column in a fixed order. */
+#define KT_ZMAX 32
+template <typename T>
+__global__ void __launch_bounds__(128) k_tangent_transpose(igab_geom g, const T *__restrict__ vals,
+                                                           const double *__restrict__ x, double *__restrict__ y,
+                                                           int nchunk)
+{
+    __shared__ T band[(KT_ZMAX + 4) * 3][15];
+    __shared__ double xs[(KT_ZMAX + 4) * 3];
+    const int nz = g.nb[2];
+    const int chunk = blockIdx.x % nchunk;
+    const int line = blockIdx.x / nchunk;
+    const int cy = line % g.nb[1], cx = line / g.nb[1];
+    const int zlo = (int)(((long)chunk * nz) / nchunk);
+    const int zhi = (int)(((long)(chunk + 1) * nz) / nchunk) - 1;
+    const int slo = zlo - 2 > 0 ? zlo - 2 : 0, shi = zhi + 2 < nz - 1 ? zhi + 2 : nz - 1;
+    const int nsrc = (shi - slo + 1) * 3;
+    const int tid = threadIdx.x;
+    const int oz = zlo + tid / 3, ok = tid % 3;
+    const bool owner = oz <= zhi;
+    double acc = 0.0;
+    const int sx0 = cx - 2 > 0 ? cx - 2 : 0, sx1 = cx + 2 < g.nb[0] - 1 ? cx + 2 : g.nb[0] - 1;
+    const int sy0 = cy - 2 > 0 ? cy - 2 : 0, sy1 = cy + 2 < g.nb[1] - 1 ? cy + 2 : g.nb[1] - 1;
+    for (int sx = sx0; sx <= sx1; sx++)
+        for (int sy = sy0; sy <= sy1; sy++) {
+            for (int idx = tid; idx < nsrc * 15; idx += blockDim.x) {
+                const int r = idx / 15, t = idx % 15;
+                const int sz = slo + r / 3, sk = r % 3;
+                /* columns of this row inside line (cx,cy) and inside [zlo, zhi] */
+                const int c0 = sz - 2 > zlo ? sz - 2 : zlo;
+                const int c1 = sz + 2 < zhi ? sz + 2 : zhi;
+                if (t < (c1 - c0 + 1) * 3) {
+                    const long j = 3 * cp_index(g, sx, sy, sz) + sk;
+                    band[r][(c0 - sz + 2) * 3 + t] = vals[g.rowptr[j] + csr_pos(g, sx, sy, sz, cx, cy, c0, 0) + t];
+                }
+            }
+            for (int idx = tid; idx < nsrc; idx += blockDim.x)
+                xs[idx] = x[3 * cp_index(g, sx, sy, slo + idx / 3) + idx % 3];
+            __syncthreads();
+            if (owner) {
+                const int z0 = oz - 2 > 0 ? oz - 2 : 0, z1 = oz + 2 < nz - 1 ? oz + 2 : nz - 1;
+                for (int sz = z0; sz <= z1; sz++)
+#pragma unroll
+                    for (int sk = 0; sk < 3; sk++) {
+                        const int r = (sz - slo) * 3 + sk;
+                        acc += double(band[r][(oz - sz + 2) * 3 + ok]) * xs[r];
+                    }
+            }
+            __syncthreads();
+        }
+    if (owner) y[3 * cp_index(g, cx, cy, oz) + ok] = acc;
+}
+
+__global__ void k_exp_scale(const double *__restrict__ gl, double *__restrict__ s, long n)
+{
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i < n) s[i] = exp(gl[i]);
+}
+
+/* lam with the Dirichlet rows zeroed (those rows of R do not depend on g) */
+__global__ void k_zero_rows(long nd, const int *__restrict__ rows, double *__restrict__ v)
+{
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t < nd) v[rows[t]] = 0.0;
+}
+
 template <typename T>
 __global__ void k_check_finite(const T *__restrict__ v, long n, int *__restrict__ flag)
 {
@@ -672,15 +773,16 @@ __global__ void k_check_finite(const T *__restrict__ v, long n, int *__restrict_
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(flag, 1);
 }
 
-template <int TE, bool GT>
-int launch_res_volume_t(igab_ctx *c, const igab_geom &g, const double *dU, double *dR)
+template <int TE, bool GT, bool VJP = false>
+int launch_res_volume_t(igab_ctx *c, const igab_geom &g, const double *dU, double *dR,
+                        const double *dlam = nullptr, double *dgrad = nullptr)
 {
     size_t sm = sizeof(res_smem<TE, GT ? 3 : 1>);
-    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_res_volume<TE, GT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_res_volume<TE, GT, VJP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     for (int colour = 0; colour < 8; colour++) {
         long nblk = tiles_of_colour(g, TE, colour);
         if (nblk == 0) continue;
-        k_res_volume<TE, GT><<<(unsigned)nblk, 256, sm, c->stream>>>(g, dU, dR, colour);
+        k_res_volume<TE, GT, VJP><<<(unsigned)nblk, 256, sm, c->stream>>>(g, dU, dR, colour, dlam, dgrad);
         c->last_launches++;
     }
     IGAB_CUDA_TRY(cudaGetLastError());
@@ -768,6 +870,45 @@ int igab_launch_tangent(igab_ctx *c, const double *dU, void *dvals, int prec)
     if (prec == IGAB_PREC_FP64) return launch_tangent_t<double>(c, dU, (double *)dvals);
     if (prec == IGAB_PREC_FP32) return launch_tangent_t<float>(c, dU, (float *)dvals);
     return IGAB_ERR_ARG;
+}
+
+int igab_launch_exp_scale(igab_ctx *c, const double *dg)
+{
+    k_exp_scale<<<(unsigned)((c->nel + 255) / 256), 256, 0, c->stream>>>(dg, c->d_escale, c->nel);
+    c->last_launches++;
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+/* grad_e = lam~^T dR/dg_e with lam~ = lam outside the Dirichlet rows (c->d_lam is scratch) */
+int igab_launch_adjoint_dRdg(igab_ctx *c, const double *dU, const double *dlam, double *dgrad)
+{
+    igab_geom g = c->geom();
+    IGAB_CUDA_TRY(cudaMemcpyAsync(c->d_lam, dlam, (size_t)c->ndof * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    if (c->nd > 0) {
+        k_zero_rows<<<(unsigned)((c->nd + 255) / 256), 256, 0, c->stream>>>(c->nd, c->d_drow, c->d_lam);
+        c->last_launches++;
+        IGAB_CUDA_TRY(cudaGetLastError());
+    }
+    if (c->phys == IGAB_PHYS_GETIME)
+        return c->tile_res == 4 ? launch_res_volume_t<4, true, true>(c, g, dU, nullptr, c->d_lam, dgrad)
+                                : launch_res_volume_t<2, true, true>(c, g, dU, nullptr, c->d_lam, dgrad);
+    return c->tile_res == 4 ? launch_res_volume_t<4, false, true>(c, g, dU, nullptr, c->d_lam, dgrad)
+                            : launch_res_volume_t<2, false, true>(c, g, dU, nullptr, c->d_lam, dgrad);
+}
+
+int igab_launch_tangent_transpose(igab_ctx *c, const void *dvals, int prec, const double *dx, double *dy)
+{
+    igab_geom g = c->geom();
+    const int nchunk = (c->nb[2] + KT_ZMAX - 1) / KT_ZMAX;
+    const long nblk = (long)c->nb[0] * c->nb[1] * nchunk;
+    if (prec == IGAB_PREC_FP64)
+        k_tangent_transpose<double><<<(unsigned)nblk, 128, 0, c->stream>>>(g, (const double *)dvals, dx, dy, nchunk);
+    else
+        k_tangent_transpose<float><<<(unsigned)nblk, 128, 0, c->stream>>>(g, (const float *)dvals, dx, dy, nchunk);
+    c->last_launches++;
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
 }
 
 int igab_launch_csr_cols(igab_ctx *c, int *dcols)

@@ -295,7 +295,8 @@ __global__ void __launch_bounds__(NTHR, 2) k_tan_dmma(igab_geom g, const double 
             for (int I = 0; I < 3; I++)
 #pragma unroll
                 for (int K = 0; K < 3; K++) pt[PT_TAU + 3 * I + K] = P.tau[I][K];
-            pt[PT_W] = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz];
+            pt[PT_W] = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz] *
+                       elem_scale(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez);
         }
         __syncthreads();
 

@@ -74,6 +74,9 @@ IGAB_API = [
     ("igab_graph_capture", ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int, ctypes.c_int]),
     ("igab_graph_launch", ctypes.c_int, [vp]),
     ("igab_graph_destroy", ctypes.c_int, [vp]),
+    ("igab_set_element_log_scale", ctypes.c_int, [vp, vp, ctypes.c_int]),
+    ("igab_adjoint_forward", ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int]),
+    ("igab_adjoint_backward", ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp, vp, vp]),
     ("igab_get_option", ctypes.c_int, [vp, ctypes.c_int, c_int_p]),
 ]
 

@@ -130,6 +130,23 @@ int igab_graph_capture(igab_ctx *ctx, const double *U_dev, double *R_dev, void *
 int igab_graph_launch(igab_ctx *ctx);
 int igab_graph_destroy(igab_ctx *ctx);
 
+/* ---- discrete adjoint of the element-scaled problem (no reference counterpart).
+ * Every element integrand (volume residual and tangent) is multiplied by
+ * s_e = exp(g_e); element e = (ex*ne1 + ey)*ne2 + ez, the reference's element
+ * loop order (src/snesiga_Residual.c:104-106).  Neumann and Dirichlet rows are
+ * not scaled.
+ *   forward : s = exp(g) (g_dev NULL keeps the current scales), then R and/or
+ *             the CSR tangent at U, as igab_residual_device / igab_tangent_device.
+ *   backward: KTlam = K^T lam on CSR values vals_dev (structured pattern) and/or
+ *             grad[e] = sum_r lam_r dR_r/dg_e = s_e lam_e . R_e(U), Dirichlet rows
+ *             of lam ignored (there R = U - g does not depend on g).
+ * With K^T lam = dJ/dU solved by the caller, dJ/dg = -grad. */
+int igab_set_element_log_scale(igab_ctx *ctx, const double *g, int on_device);   /* g NULL: s = 1 */
+int igab_adjoint_forward(igab_ctx *ctx, const double *g_dev, const double *U_dev, double *R_dev,
+                         void *vals_dev, int prec);
+int igab_adjoint_backward(igab_ctx *ctx, const double *U_dev, const void *vals_dev, int prec,
+                          const double *lam_dev, double *KTlam_dev, double *grad_dev);
+
 /* ---- residual for callers that cannot have the library allocate device memory.
  * No counterpart in the reference.  Same result as igab_residual, but U and R
  * are staged in a file-scope device array (2 x 8 MiB, held by every GPU that

@@ -26,6 +26,9 @@ with -std=gnu99 (the non-static ``inline`` of include/mathutil.h needs GNU
 semantics here) and -march=x86-64-v3 instead of -march=native so that the
 library also runs on the GPU hosts' CPUs.
 
+oracle/elem_scale.c wraps the reference's integrand pointers with a per-element
+scale (the adjoint tests' oracle of the element-scaled problem).
+
 The struct-layout probe (oracle/layout_probe.c) is compiled twice, once with
 the reference's headers and once with include/igap4_structs.h, so the tests
 can check that both declare byte-identical structs.
@@ -84,6 +87,7 @@ def main():
     newest_src = max(os.path.getmtime(p) for p in
                      [os.path.join(ref, s) for s in REF_SOURCES] +
                      [CASE_SRC, os.path.join(SUBSET, "petsc_subset.c"), __file__,
+                      os.path.join(HERE, "elem_scale.c"),
                       os.path.join(HERE, "layout_probe.c"), os.path.join(OUR_INC, "igap4_structs.h")])
     if os.path.exists(LIB) and os.path.getmtime(LIB) > newest_src and not args.force:
         print("build_ref: %s is up to date" % LIB)
@@ -101,10 +105,13 @@ def main():
     jobs.append(["gcc"] + CFLAGS + ref_inc + ["-DPROBE_REFERENCE_HEADERS", "-c", probe,
                                              "-o", os.path.join(OBJ_DIR, "layout_ref.o")])
     jobs.append(["gcc"] + CFLAGS + our_inc + ["-c", probe, "-o", os.path.join(OBJ_DIR, "layout_ours.o")])
+    jobs.append(["gcc"] + CFLAGS + ref_inc + ["-c", os.path.join(HERE, "elem_scale.c"),
+                                             "-o", os.path.join(OBJ_DIR, "elem_scale.o")])
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         list(ex.map(run, jobs))
     objs = [obj_name(r) for r in REF_SOURCES] + [os.path.join(OBJ_DIR, n) for n in
-                                                 ("iga_case.o", "petsc_subset.o", "layout_ref.o", "layout_ours.o")]
+                                                 ("iga_case.o", "petsc_subset.o", "layout_ref.o", "layout_ours.o",
+                                                  "elem_scale.o")]
     run(["gcc", "-shared", "-o", LIB] + objs + ["-lm"])
     print("build_ref: built %s" % LIB)
     return 0

@@ -44,6 +44,14 @@ def lib():
         L.iga_dirichlet.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int,
                                     ctypes.c_int]
         L.iga_dirichlet.restype = None
+        L.oracle_scale_install.argtypes = [vp, vp, ctypes.c_long]
+        L.oracle_scale_install.restype = None
+        L.oracle_scale_remove.argtypes = [vp]
+        L.oracle_scale_remove.restype = None
+        L.oracle_scale_reset.argtypes = []
+        L.oracle_scale_reset.restype = None
+        L.oracle_scale_calls.restype = ctypes.c_long
+        L.oracle_scale_overflow.restype = ctypes.c_long
         L.layout_probe_reference.argtypes = [vp]
         L.layout_probe_ours.argtypes = [vp]
         _lib = L
@@ -120,3 +128,31 @@ def layouts():
     na = lib().layout_probe_reference(_p(a))
     nb = lib().layout_probe_ours(_p(b))
     return a[:na], b[:nb]
+
+
+class ScaledCase:
+    """A reference case whose element integrands are multiplied by s_e = exp(g_e)
+    (oracle/elem_scale.c).  residual()/tangent() as Case."""
+
+    def __init__(self, case, g):
+        self.case = case
+        self.ndof = case.ndof
+        self.s = np.ascontiguousarray(np.exp(np.asarray(g, dtype=np.float64)))
+        lib().oracle_scale_install(case.app, _p(self.s), int(self.s.size))
+
+    def _checked(self, fn, *a):
+        L = lib()
+        L.oracle_scale_reset()
+        out = fn(*a)
+        if L.oracle_scale_overflow() != 0 or L.oracle_scale_calls() != 64 * self.s.size:
+            raise RuntimeError("integrand call count does not match the element count")
+        return out
+
+    def residual(self, U):
+        return self._checked(self.case.residual, U)
+
+    def tangent(self, U):
+        return self._checked(self.case.tangent, U)
+
+    def close(self):
+        lib().oracle_scale_remove(self.case.app)

@@ -324,7 +324,7 @@ static void free_ctx(igab_ctx *c)
     cudaFree(c->d_hval); cudaFree(c->d_neu_row); cudaFree(c->d_neu_ptr); cudaFree(c->d_neu_ent);
     cudaFree(c->d_dnz); cudaFree(c->d_combo_info); cudaFree(c->d_hist);
     cudaFree(c->d_U); cudaFree(c->d_R); cudaFree(c->d_vals);
-    cudaFree(c->d_escale); cudaFree(c->d_lam);
+    cudaFree(c->d_escale); cudaFree(c->d_lam); cudaFree(c->d_status);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     for (int k = 0; k < 6; k++)
@@ -411,6 +411,8 @@ extern "C" int igab_create(const igab_mesh_desc *desc, int device, igab_ctx **ou
             return _e == cudaErrorMemoryAllocation ? IGAB_ERR_NOMEM : IGAB_ERR_CUDA; \
         }                                                                    \
     } while (0)
+    TRY(cudaMalloc((void **)&c->d_status, sizeof(int)));
+    TRY(cudaMemset(c->d_status, 0, sizeof(int)));
     TRY(cudaMalloc((void **)&c->d_rowptr, c->rowptr_h.size() * sizeof(int)));
     TRY(cudaMemcpy(c->d_rowptr, c->rowptr_h.data(), c->rowptr_h.size() * sizeof(int), cudaMemcpyHostToDevice));
 
@@ -583,6 +585,8 @@ extern "C" int igab_set_history(igab_ctx *ctx, int level, const double *U, int o
     return 0;
 }
 
+static int check_status(igab_ctx *ctx);
+
 static int ensure_buffers(igab_ctx *ctx, int prec)
 {
     if (!ctx->d_U) IGAB_CUDA_TRY(cudaMalloc((void **)&ctx->d_U, (size_t)ctx->ndof * sizeof(double)));
@@ -659,6 +663,8 @@ extern "C" int igab_tangent(igab_ctx *ctx, const double *U_host, void *vals_host
     size_t es = prec == IGAB_PREC_FP64 ? sizeof(double) : sizeof(float);
     IGAB_CUDA_TRY(cudaMemcpyAsync(vals_host, ctx->d_vals, (size_t)ctx->nnz * es, cudaMemcpyDeviceToHost, ctx->stream));
     IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    rc = check_status(ctx);
+    if (rc) return rc;
     if (!fin) { igab_set_error("igab_tangent: non-finite entry"); return IGAB_ERR_NONFINITE; }
     return 0;
 }
@@ -676,12 +682,25 @@ extern "C" int igab_set_stream(igab_ctx *ctx, void *cuda_stream)
     return 0;
 }
 
+/* after a stream synchronisation: report (and clear) a kernel's bounded-wait failure */
+static int check_status(igab_ctx *ctx)
+{
+    int st = 0;
+    IGAB_CUDA_TRY(cudaMemcpy(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st) {
+        IGAB_CUDA_TRY(cudaMemset(ctx->d_status, 0, sizeof(int)));
+        igab_set_error("tensor-core tangent kernel: a completion wait gave up (status %d)", st);
+        return IGAB_ERR_CUDA;
+    }
+    return 0;
+}
+
 extern "C" int igab_sync(igab_ctx *ctx)
 {
     ARG_CHECK(ctx, "igab_sync: null context");
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return 0;
+    return check_status(ctx);
 }
 
 extern "C" int igab_check_finite(igab_ctx *ctx, const void *dev, long n, int prec, int *all_finite)
@@ -754,6 +773,10 @@ extern "C" int igab_set_option(igab_ctx *ctx, int option, int value)
         ARG_CHECK(value == 0 || value == 1, "igab_set_option: tangent kernel must be 0 or 1");
         ctx->tan_kernel = value;
         return 0;
+    case IGAB_OPT_TANGENT_FP32_KERNEL:
+        ARG_CHECK(value == 0 || value == 1, "igab_set_option: tangent kernel must be 0 or 1");
+        ctx->tan32_kernel = value;
+        return 0;
     default:
         igab_set_error("igab_set_option: unknown option %d", option);
         return IGAB_ERR_ARG;
@@ -765,6 +788,7 @@ extern "C" int igab_get_option(const igab_ctx *ctx, int option, int *value)
     ARG_CHECK(ctx && value, "igab_get_option: null argument");
     switch (option) {
     case IGAB_OPT_TANGENT_FP64_KERNEL: *value = ctx->tan_kernel; return 0;
+    case IGAB_OPT_TANGENT_FP32_KERNEL: *value = ctx->tan32_kernel; return 0;
     default:
         igab_set_error("igab_get_option: unknown option %d", option);
         return IGAB_ERR_ARG;

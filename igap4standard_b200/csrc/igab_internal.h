@@ -88,6 +88,8 @@ struct igab_ctx {
 
     int tile_res = 2, tile_tan = 2;
     int tan_kernel = 1;   /* FP64 tangent: 1 tensor-core (mma f64), 0 SIMT */
+    int tan32_kernel = 1; /* FP32 tangent: 1 tcgen05 tensor cores (TF32 hi/lo), 0 SIMT */
+    int *d_status = nullptr;   /* device status word: nonzero after a bounded wait gave up */
     int last_launches = 0;
 
     /* profiling events: [0..2] residual (start, after volume, end), [3..5] tangent */
@@ -117,6 +119,7 @@ int igab_launch_check_finite(igab_ctx *c, const void *dev, long n, int prec, int
 int igab_launch_basis_tables(igab_ctx *c, int d, const double *dkv, const double *dgx, const double *dgw);
 int igab_launch_fma_peak(int prec, double *tflops);
 int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv);
+int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv);
 int igab_launch_tan_getime(igab_ctx *c, const double *dU, void *dv, int prec);
 int igab_launch_exp_scale(igab_ctx *c, const double *dg);
 int igab_launch_adjoint_dRdg(igab_ctx *c, const double *dU, const double *dlam, double *dgrad);

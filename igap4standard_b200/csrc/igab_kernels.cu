@@ -816,6 +816,8 @@ int launch_tangent_t(igab_ctx *c, const double *dU, T *dv)
         e = igab_launch_tan_getime(c, dU, dv, sizeof(T) == 8 ? IGAB_PREC_FP64 : IGAB_PREC_FP32);
     else if (sizeof(T) == 8 && c->tan_kernel == 1)
         e = igab_launch_tan_dmma(c, dU, (double *)dv);
+    else if (sizeof(T) == 4 && c->tan32_kernel == 1)
+        e = igab_launch_tan_tc32(c, dU, (float *)dv);
     else
         e = launch_tan_volume<T, 2>(c, g, dU, dv);
     if (e) return e;

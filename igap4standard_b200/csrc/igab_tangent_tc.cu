@@ -1,0 +1,655 @@
+/*
+ * FP32 tangent volume kernel on the 5th-generation tensor cores (tcgen05,
+ * TF32 operands in shared memory, FP32 accumulators in tensor memory): the
+ * tangent of the mixed-precision Newton path (FP32 Jacobian, FP64 residual).
+ *
+ * Per element (src/snesiga_Tangent.c:104-190), with the energy written as
+ * W = Phi(v(u)) over 12 variables (igab_math.cuh):
+ *   K_e = sum_q sum_v s_qv x_qv x_qv^T + blockdiag_k(Gamma),
+ * where x_qv[3a+k] = sum_m dv'/du_{k,m}(q) N_a^m(q) uses the variables after the
+ * per-point rotation that diagonalises Phi'' (its one 2x2 block), and
+ * s_qv = w_q lambda_v(q).  With y = sqrt|s| x and the rows split by the sign
+ * of s,  K_main = Y_+^T Y_+ - Y_-^T Y_-.  A Gram product Y^T Y needs only two
+ * TF32 MMAs per k-step for FP32 accuracy: with y = y_hi + y_lo (both TF32),
+ *   E = Y_hi^T Y_hi + Y_hi^T (2 Y_lo),   Y^T Y = (E + E^T)/2 + O(2^-22),
+ * so the symmetric part taken at read-out recovers the cross term Y_lo^T Y_hi.
+ * The geometric block, identical for the three displacement components, is
+ *   Gamma(a,b) = sum_q sum_m,n N_a^m (w geo_q)[m][n] N_b^n = sum_q sum_i U_qi[a] V_qi[b]
+ * with six rows per point (geo = [[S, T], [T^T, 0]], S the 3x3 first-derivative
+ * block, T the 3x6 coupling to second derivatives):
+ *   U_i = d_i N_a,  V_i = (S grad N_a)_i + (T H_a)_i        (i < 3)
+ *   U_i = (T H_a)_I, V_i = d_I N_a                          (i = 3 + I)
+ * and three MMAs per k-step (hi hi, hi lo, lo hi).
+ *
+ * Work per CTA: a 2x2x2 tile of elements of one of the 8 colours (the scatter
+ * is conflict-free within a colour).  Per element: sum-factorised field at the
+ * 64 Gauss points (FP64), the point integrand (FP64, 64 threads), sign buckets
+ * of the 768 (point, variable) rows, then chunks of 32 rows are built into a
+ * double-buffered shared-memory stage (TF32 hi/lo in the K-major layout of
+ * igab_tc.cuh) by all 288 threads, and one thread issues the chunk's MMAs into
+ * a fresh tensor-memory accumulator: 4 k-steps x 2 MMAs (M 128, N 96) for
+ * element-matrix rows, 4 x 3 MMAs (M 128, N 32) for Gamma rows.  While the
+ * tensor core works on chunk c, the accumulator of chunk c-1 is added into
+ * FP32 registers (round to nearest; subtracted for negative-curvature rows):
+ * the tensor core sums only one chunk's products per entry, which keeps the
+ * FP32 accumulation error at the level of the FMA-pipe kernel.  Tensor
+ * memory: 256 columns per CTA (element matrix 2 x 96, Gamma 2 x 32, double
+ * buffered); at most two CTAs per SM.  Rows 81-127 of the M side and columns
+ * 81-95 of the N side read whatever lies behind the operand in the stage;
+ * they only feed accumulator rows and columns that are never read.  At the
+ * end of an element: the register accumulators go to shared memory, the
+ * symmetric part is taken, Gamma is added on the k1 = k2 blocks and the
+ * 81 x 81 values are read-modify-written into the FP32 CSR values.
+ */
+#include <cuda_runtime.h>
+#include "igab_device.cuh"
+#include "igab_tc.cuh"
+
+namespace {
+
+#define TCN_THR 288            /* 9 warps: one builder task per thread per chunk */
+#define TC_STAGE 24576         /* bytes per operand stage */
+#define TC_MAIN_LO 11264       /* 2 Y_lo after Y_hi (11 groups of 8 rows) */
+#define TC_G_ULO 4096          /* Gamma chunk: U_hi 0, U_lo, V_hi, V_lo (4 groups each) */
+#define TC_G_VHI 8192
+#define TC_G_VLO 12288
+#define TC_TMEM_COLS 256u
+#define TC_COL_MAIN 0u         /* two 96-column element-matrix accumulators */
+#define TC_COL_GAM 192u        /* two 32-column Gamma accumulators */
+#define TC_NGCHUNK 12          /* 64 points x 6 Gamma rows / 32 */
+
+/* float point data per Gauss point */
+#define TP_F 0      /* F[k][J], 9 */
+#define TP_G 9      /* G[k][c], 18 */
+#define TP_CS 27    /* rotation of the (va, vb) block */
+#define TP_SN 28
+#define TP_RS 29    /* sign(s) sqrt|s|, 12 */
+#define TP_S 41     /* w * (sig0, sig1, sig2, d1[3]/2, d1[4]/2, d1[5]/2) */
+#define TP_T 47     /* w * tau[I][K], 9 */
+#define TP_N 57
+
+template <int TE>
+struct tc_smem {
+    static constexpr int TC = TE + 2;
+    static constexpr int NCP = TC * TC * TC;
+    unsigned char stage[2][TC_STAGE];   /* operand stages; E and Gamma staging at read-out */
+    double A[972];                      /* interpolation temporaries */
+    double C[864];
+    double U[NCP * 3];
+    double tab[3][TE][IGAB_TAB1D];
+    double wh[3][TE][IGAB_NQ];
+    float tabf[3][TE][IGAB_TAB1D];
+    float pt[IGAB_NQ3][TP_N];
+    unsigned short map[2][768];         /* bucket slot -> 12 q + v (positive, negative) */
+    int cnt[2];
+    int part[2][2];                     /* per-warp bucket counts for the scan */
+    unsigned long long mbar[2];
+    unsigned int tmem_base;
+    int abort_flag;
+};
+
+/* eigen-rotation of [[a, b], [b, c]]: [[a,b],[b,c]] = l1 e1 e1^T + l2 e2 e2^T,
+ * e1 = (cs, -sn), e2 = (sn, cs) (same convention as the FP64 tensor kernel) */
+__device__ __forceinline__ void tc_sym2_eig(double a, double b, double c, double &cs, double &sn, double &l1,
+                                            double &l2)
+{
+    if (b == 0.0) {
+        cs = 1.0; sn = 0.0; l1 = a; l2 = c;
+        return;
+    }
+    double zeta = (c - a) / (2.0 * b);
+    double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+    cs = 1.0 / sqrt(1.0 + t * t);
+    sn = t * cs;
+    l1 = a - t * b;
+    l2 = c + t * b;
+}
+
+/* gradient of rotated variable v with respect to the 9 strain components of
+ * displacement component k (igab_ge_grad_var, then the (va, vb) rotation) */
+__device__ __forceinline__ void tc_grad_var(const float *p, int v, int k, float g[9])
+{
+#pragma unroll
+    for (int m = 0; m < 9; m++) g[m] = 0.f;
+    const float is2 = (float)IGAB_INV_SQRT2, is3 = (float)IGAB_INV_SQRT3, is6 = (float)IGAB_INV_SQRT6;
+    const float F0 = p[TP_F + 3 * k], F1 = p[TP_F + 3 * k + 1], F2 = p[TP_F + 3 * k + 2];
+    const float *G = p + TP_G + 6 * k;
+    if (v == 0) {
+        g[0] = F0 * is3; g[1] = F1 * is3; g[2] = F2 * is3;
+    } else if (v <= 2) {
+        const float cs = p[TP_CS], sn = p[TP_SN];
+        const float a0 = F0 * is2, a1 = -F1 * is2;                        /* va */
+        const float b0 = F0 * is6, b1 = F1 * is6, b2 = -2.f * F2 * is6;   /* vb */
+        if (v == 1) { g[0] = cs * a0 - sn * b0; g[1] = cs * a1 - sn * b1; g[2] = -sn * b2; }
+        else        { g[0] = sn * a0 + cs * b0; g[1] = sn * a1 + cs * b1; g[2] = cs * b2; }
+    } else if (v == 3) {
+        g[0] = 0.5f * F1; g[1] = 0.5f * F0;
+    } else if (v == 4) {
+        g[0] = 0.5f * F2; g[2] = 0.5f * F0;
+    } else if (v == 5) {
+        g[1] = 0.5f * F2; g[2] = 0.5f * F1;
+    } else if (v == 6) {   /* strain-gradient variables: constant indices keep g[] in registers */
+        g[0] = G[0] * is2; g[1] = -G[1] * is2; g[3] = F0 * is2; g[4] = -F1 * is2;
+    } else if (v == 7) {
+        g[0] = G[1] * is2; g[1] = -G[3] * is2; g[4] = F0 * is2; g[6] = -F1 * is2;
+    } else if (v == 8) {
+        g[0] = G[2] * is2; g[1] = -G[4] * is2; g[5] = F0 * is2; g[7] = -F1 * is2;
+    } else if (v == 9) {
+        g[0] = G[0] * is6; g[1] = G[1] * is6; g[2] = -2.f * G[2] * is6;
+        g[3] = F0 * is6; g[4] = F1 * is6; g[5] = -2.f * F2 * is6;
+    } else if (v == 10) {
+        g[0] = G[1] * is6; g[1] = G[3] * is6; g[2] = -2.f * G[4] * is6;
+        g[4] = F0 * is6; g[6] = F1 * is6; g[7] = -2.f * F2 * is6;
+    } else {
+        g[0] = G[2] * is6; g[1] = G[4] * is6; g[2] = -2.f * G[5] * is6;
+        g[5] = F0 * is6; g[7] = F1 * is6; g[8] = -2.f * F2 * is6;
+    }
+}
+
+__device__ __forceinline__ void st_pair(unsigned char *hi_base, unsigned char *lo_base, uint32_t off, float y,
+                                        float lo_scale)
+{
+    float h, l;
+    tc_split(y, h, l);
+    *reinterpret_cast<float *>(hi_base + off) = h;
+    *reinterpret_cast<float *>(lo_base + off) = lo_scale * l;
+}
+
+/* Add the accumulator of one finished chunk into the FP32 registers (round to
+ * nearest): element-matrix chunks go to warps 0-2 / 4-6 (TMEM lanes = rows
+ * 0-95, columns 0-47 / 48-95 of the 96-column accumulator, subtracted for
+ * rows of negative curvature), Gamma chunks to warp 8 (lanes 0-31, 32 columns).
+ * Each chunk starts a fresh accumulator, so the tensor core sums only the 8
+ * (12) products of one chunk per entry. */
+__device__ __forceinline__ void tc_accumulate(uint32_t tmem, int buf, int kind, int warp, float (&acc)[48])
+{
+    if (kind < 2) {
+        if (warp == 3 || warp >= 7) return;   /* lanes 96-127: rows beyond 80; warp 8 holds Gamma */
+        const int lb = 32 * (warp & 3), half = warp >> 2;
+        const float sg = kind == 0 ? 1.f : -1.f;
+        const uint32_t ta = tmem + ((uint32_t)lb << 16) + TC_COL_MAIN + (uint32_t)buf * 96u + 48u * half;
+#pragma unroll
+        for (int part = 0; part < 3; part++) {
+            float v[16];
+            tc_ld16(ta + 16u * part, v);
+#pragma unroll
+            for (int i = 0; i < 16; i++) acc[16 * part + i] += sg * v[i];
+        }
+    } else if (warp == 8) {
+        const uint32_t ta = tmem + TC_COL_GAM + (uint32_t)buf * 32u;
+#pragma unroll
+        for (int part = 0; part < 2; part++) {
+            float v[16];
+            tc_ld16(ta + 16u * part, v);
+#pragma unroll
+            for (int i = 0; i < 16; i++) acc[16 * part + i] += v[i];
+        }
+    }
+}
+
+template <int TE>
+__global__ void __maxnreg__(112) k_tan_tc32(igab_geom g, const double *__restrict__ U,
+                                                         float *__restrict__ vals, int colour, int *status)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    tc_smem<TE> &S = *reinterpret_cast<tc_smem<TE> *>(smem_raw);
+    constexpr int TC = TE + 2;
+    constexpr int NCP = TC * TC * TC;
+    constexpr int NEL = TE * TE * TE;
+    tile_t Tl;
+    if (!decode_tile(g, TE, colour, blockIdx.x, Tl)) return;   /* block-uniform, before any barrier */
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    /* ---- set-up: barriers, tensor memory, tile data */
+    if (tid == 0) {
+        tc_mbar_init(&S.mbar[0], 1);
+        tc_mbar_init(&S.mbar[1], 1);
+        tc_fence_mbar_init();
+        S.abort_flag = 0;
+    }
+    if (warp == 0) tc_alloc(&S.tmem_base, TC_TMEM_COLS);
+    for (int idx = tid; idx < NCP * 3; idx += TCN_THR) {
+        int i = idx % 3, cp = idx / 3;
+        int lz = cp % TC, ly = (cp / TC) % TC, lx = cp / (TC * TC);
+        double v = 0.0;
+        if (lx < Tl.nv[0] + 2 && ly < Tl.nv[1] + 2 && lz < Tl.nv[2] + 2)
+            v = U[3 * cp_index(g, Tl.e0[0] + lx, Tl.e0[1] + ly, Tl.e0[2] + lz) + i];
+        S.U[idx] = v;
+    }
+    for (int idx = tid; idx < 3 * TE * IGAB_TAB1D; idx += TCN_THR) {
+        int d = idx / (TE * IGAB_TAB1D), r = idx % (TE * IGAB_TAB1D), le = r / IGAB_TAB1D, o = r % IGAB_TAB1D;
+        double t = le < Tl.nv[d] ? g.tab[d][(long)(Tl.e0[d] + le) * IGAB_TAB1D + o] : 0.0;
+        S.tab[d][le][o] = t;
+        S.tabf[d][le][o] = (float)t;
+    }
+    for (int idx = tid; idx < 3 * TE * IGAB_NQ; idx += TCN_THR) {
+        int d = idx / (TE * IGAB_NQ), r = idx % (TE * IGAB_NQ), le = r / IGAB_NQ, q = r % IGAB_NQ;
+        S.wh[d][le][q] = le < Tl.nv[d] ? g.wh[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
+    }
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    const uint32_t tmem = S.tmem_base;
+
+    bool pend[2] = {false, false};
+    int kind[2] = {0, 0};    /* chunk in flight per stage: 0 positive rows, 1 negative rows, 2 Gamma */
+    uint32_t ph[2] = {0u, 0u};
+    int gc = 0;          /* chunks issued by this CTA */
+    bool aborted = false;
+
+    for (int le = 0; le < NEL && !aborted; le++) {
+        const int lex = le / (TE * TE), ley = (le / TE) % TE, lez = le % TE;
+        if (!(lex < Tl.nv[0] && ley < Tl.nv[1] && lez < Tl.nv[2])) continue;   /* block-uniform */
+        const double *Bx = S.tab[0][lex];
+        const double *By = S.tab[1][ley];
+        const double *Bz = S.tab[2][lez];
+        /* ---- field at the 64 Gauss points (sum-factorised: z, then y, then x) */
+        for (int o = tid; o < 972; o += TCN_THR) {
+            int i = o % 3, kz = (o / 3) % 3, ay = (o / 9) % 3, ax = (o / 27) % 3, q = o / 81;
+            const double *u0 = &S.U[(((lex + ax) * TC + (ley + ay)) * TC + lez) * 3 + i];
+            S.A[o] = Bz[q * 9 + kz] * u0[0] + Bz[q * 9 + 3 + kz] * u0[3] + Bz[q * 9 + 6 + kz] * u0[6];
+        }
+        __syncthreads();
+        for (int o = tid; o < 864; o += TCN_THR) {
+            int i = o % 3, kk = (o / 3) % 6, ax = (o / 18) % 3, qq = o / 54;
+            int qyy = qq & 3, qzz = qq >> 2;
+            const double *a0 = &S.A[((qzz * 3 + ax) * 3) * 9 + kk_kz(kk) * 3 + i];
+            S.C[o] = By[qyy * 9 + kk_ky(kk)] * a0[0] + By[qyy * 9 + 3 + kk_ky(kk)] * a0[9] +
+                     By[qyy * 9 + 6 + kk_ky(kk)] * a0[18];
+        }
+        __syncthreads();
+        /* ---- point integrand (FP64), rotated curvatures, sign masks; q = 16 qz + 4 qy + qx */
+        unsigned pmask = 0, nmask = 0;
+        if (tid < IGAB_NQ3) {
+            const int qx = tid & 3, qy = (tid >> 2) & 3, qz = tid >> 4, qq = qy + 4 * qz;
+            double u[30];
+#pragma unroll
+            for (int a = 0; a < 10; a++)
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int ax = 0; ax < 3; ax++)
+                        s += Bx[qx * 9 + ax * 3 + a_kx(a)] * S.C[((qq * 3 + ax) * 6 + a_kk(a)) * 3 + i];
+                    u[10 * i + a] = s;
+                }
+            if (g.periodic) {
+#pragma unroll
+                for (int i = 0; i < 3; i++)
+#pragma unroll
+                    for (int J = 0; J < 3; J++) u[10 * i + 1 + J] += g.pp[3 * i + J];
+            }
+            igab_ge_point<double> P;
+            igab_ge_eval(u, g.coef, P);
+            const double w = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz] *
+                             elem_scale(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez);
+            double cs, sn, l1, l2;
+            tc_sym2_eig(P.d2[1], P.d2ab, P.d2[2], cs, sn, l1, l2);
+            float *pt = S.pt[tid];
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+#pragma unroll
+                for (int J = 0; J < 3; J++) pt[TP_F + 3 * k + J] = (float)P.F[k][J];
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+#pragma unroll
+                for (int c = 0; c < 6; c++) pt[TP_G + 6 * k + c] = (float)P.G[k][c];
+            pt[TP_CS] = (float)cs;
+            pt[TP_SN] = (float)sn;
+#pragma unroll
+            for (int v = 0; v < 12; v++) {
+                const double s = w * (v == 1 ? l1 : (v == 2 ? l2 : P.d2[v]));
+                const double r = sqrt(fabs(s));
+                pt[TP_RS + v] = (float)(s < 0.0 ? -r : r);
+                if (s > 0.0) pmask |= 1u << v;
+                if (s < 0.0) nmask |= 1u << v;
+            }
+#pragma unroll
+            for (int I = 0; I < 3; I++) pt[TP_S + I] = (float)(w * P.sig[I]);
+#pragma unroll
+            for (int I = 0; I < 3; I++) pt[TP_S + 3 + I] = (float)(w * 0.5 * P.d1[3 + I]);
+#pragma unroll
+            for (int I = 0; I < 3; I++)
+#pragma unroll
+                for (int K = 0; K < 3; K++) pt[TP_T + 3 * I + K] = (float)(w * P.tau[I][K]);
+        }
+        /* ---- sign buckets: exclusive scan of the per-point counts over the 64 points */
+        int pinc = __popc(pmask), ninc = __popc(nmask);
+        if (tid < IGAB_NQ3) {
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int tp = __shfl_up_sync(0xffffffffu, pinc, o), tn = __shfl_up_sync(0xffffffffu, ninc, o);
+                if (lane >= o) { pinc += tp; ninc += tn; }
+            }
+            if (lane == 31) { S.part[warp][0] = pinc; S.part[warp][1] = ninc; }
+        }
+        __syncthreads();
+        if (tid < IGAB_NQ3) {
+            int po = pinc - __popc(pmask) + (warp ? S.part[0][0] : 0);
+            int no = ninc - __popc(nmask) + (warp ? S.part[0][1] : 0);
+            for (int v = 0; v < 12; v++) {
+                if (pmask & (1u << v)) S.map[0][po++] = (unsigned short)(12 * tid + v);
+                if (nmask & (1u << v)) S.map[1][no++] = (unsigned short)(12 * tid + v);
+            }
+            if (tid == 0) {
+                S.cnt[0] = S.part[0][0] + S.part[1][0];
+                S.cnt[1] = S.part[0][1] + S.part[1][1];
+            }
+        }
+        __syncthreads();
+        const int npos = S.cnt[0], nneg = S.cnt[1];
+        const int cpos = (npos + TC_KC - 1) / TC_KC, cneg = (nneg + TC_KC - 1) / TC_KC;
+        const int nch = cpos + cneg + TC_NGCHUNK;
+
+        /* ---- chunk loop: chunk ch is built into stage gc & 1 and multiplied into
+         * accumulator gc & 1 while chunk ch-1's accumulator is added into registers */
+        float acc[48];
+#pragma unroll
+        for (int i = 0; i < 48; i++) acc[i] = 0.f;
+        for (int ch = 0; ch < nch; ch++) {
+            const int b = gc & 1;
+            unsigned char *st = S.stage[b];
+            if (ch < cpos + cneg) {
+                /* main rows: task (slot j, component k, ax) -> 9 outputs (ay, az) */
+                const int neg = ch >= cpos;
+                const int base = (neg ? ch - cpos : ch) * TC_KC;
+                const int cntb = neg ? nneg : npos;
+                const int j = tid / 9, k = (tid / 3) % 3, ax = tid % 3;
+                unsigned char *hi = st, *lo = st + TC_MAIN_LO;
+                const int slot = base + j;
+                if (slot < cntb) {
+                    const int id = S.map[neg][slot], q = id / 12, v = id % 12;
+                    const int qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
+                    const float *p = S.pt[q];
+                    float gv[9];
+                    tc_grad_var(p, v, k, gv);
+                    const float r = fabsf(p[TP_RS + v]);
+                    const float *bxp = &S.tabf[0][lex][qx * 9 + ax * 3];
+                    const float bx0 = bxp[0], bx1 = bxp[1], bx2 = bxp[2];
+                    /* coefficients of By[ky] By-term per kz: derivative m -> (kx, ky, kz) as eval_Bspline */
+                    const float t00 = r * (gv[0] * bx1 + gv[3] * bx2), t01 = r * (gv[1] * bx0 + gv[4] * bx1),
+                                t02 = r * (gv[6] * bx0);
+                    const float t10 = r * (gv[2] * bx0 + gv[5] * bx1), t11 = r * (gv[7] * bx0);
+                    const float t20 = r * (gv[8] * bx0);
+#pragma unroll
+                    for (int ay = 0; ay < 3; ay++) {
+                        const float *byp = &S.tabf[1][ley][qy * 9 + ay * 3];
+                        const float cy0 = t00 * byp[0] + t01 * byp[1] + t02 * byp[2];
+                        const float cy1 = t10 * byp[0] + t11 * byp[1];
+                        const float cy2 = t20 * byp[0];
+#pragma unroll
+                        for (int az = 0; az < 3; az++) {
+                            const float *bzp = &S.tabf[2][lez][qz * 9 + az * 3];
+                            const float y = cy0 * bzp[0] + cy1 * bzp[1] + cy2 * bzp[2];
+                            const int c = 3 * (9 * ax + 3 * ay + az) + k;
+                            st_pair(hi, lo, tc_off(c, j), y, 2.f);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int ay = 0; ay < 3; ay++)
+#pragma unroll
+                        for (int az = 0; az < 3; az++) {
+                            const uint32_t off = tc_off(3 * (9 * ax + 3 * ay + az) + k, j);
+                            *reinterpret_cast<float *>(hi + off) = 0.f;
+                            *reinterpret_cast<float *>(lo + off) = 0.f;
+                        }
+                }
+            } else {
+                /* Gamma rows: task (slot j, ax, ay) -> 3 outputs (az) of U and V */
+                const int gch = ch - cpos - cneg;
+                const int j = tid / 9, ax = (tid / 3) % 3, ay = tid % 3;
+                const int srow = gch * TC_KC + j, q = srow / 6, i = srow % 6;
+                const int qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
+                const float *p = S.pt[q];
+                const float *bxp = &S.tabf[0][lex][qx * 9 + ax * 3];
+                const float *byp = &S.tabf[1][ley][qy * 9 + ay * 3];
+                const float bx0 = bxp[0], bx1 = bxp[1], bx2 = bxp[2];
+                const float by0 = byp[0], by1 = byp[1], by2 = byp[2];
+                const int I = i < 3 ? i : i - 3;
+                const float s00 = p[TP_S], s11 = p[TP_S + 1], s22 = p[TP_S + 2];
+                const float s01 = p[TP_S + 3], s02 = p[TP_S + 4], s12 = p[TP_S + 5];
+                const float tI0 = p[TP_T + 3 * I], tI1 = p[TP_T + 3 * I + 1], tI2 = p[TP_T + 3 * I + 2];
+#pragma unroll
+                for (int az = 0; az < 3; az++) {
+                    const float *bzp = &S.tabf[2][lez][qz * 9 + az * 3];
+                    const float bz0 = bzp[0], bz1 = bzp[1], bz2 = bzp[2];
+                    const float dx = bx1 * by0 * bz0, dy = bx0 * by1 * bz0, dz = bx0 * by0 * bz1;
+                    /* second derivatives H[idx6(I, K)], K = 0..2 */
+                    float h0, h1, h2;
+                    if (I == 0) { h0 = bx2 * by0 * bz0; h1 = bx1 * by1 * bz0; h2 = bx1 * by0 * bz1; }
+                    else if (I == 1) { h0 = bx1 * by1 * bz0; h1 = bx0 * by2 * bz0; h2 = bx0 * by1 * bz1; }
+                    else { h0 = bx1 * by0 * bz1; h1 = bx0 * by1 * bz1; h2 = bx0 * by0 * bz2; }
+                    const float th = tI0 * h0 + tI1 * h1 + tI2 * h2;   /* (T H_a)_I */
+                    const float dI = I == 0 ? dx : (I == 1 ? dy : dz);
+                    float uval, vval;
+                    if (i < 3) {
+                        const float sg = I == 0 ? s00 * dx + s01 * dy + s02 * dz
+                                       : (I == 1 ? s01 * dx + s11 * dy + s12 * dz : s02 * dx + s12 * dy + s22 * dz);
+                        uval = dI;
+                        vval = sg + th;
+                    } else {
+                        uval = th;
+                        vval = dI;
+                    }
+                    const uint32_t off = tc_off(9 * ax + 3 * ay + az, j);
+                    st_pair(st, st + TC_G_ULO, off, uval, 1.f);
+                    st_pair(st + TC_G_VHI, st + TC_G_VLO, off, vval, 1.f);
+                }
+            }
+            tc_fence_proxy_async();
+            __syncthreads();
+            if (tid == 0) {
+                tc_fence_after_sync();
+                const uint32_t sb = tc_smem_u32(st);
+                if (ch < cpos + cneg) {
+                    constexpr uint32_t idm = tc_idesc_tf32(128, 96);
+                    const uint32_t d = tmem + TC_COL_MAIN + (uint32_t)b * 96u;
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++) {
+                        const uint64_t ah = tc_sdesc(sb + kk * TC_KSTEP_BYTES);
+                        const uint64_t bl = tc_sdesc(sb + TC_MAIN_LO + kk * TC_KSTEP_BYTES);
+                        tc_mma_tf32(d, ah, ah, idm, kk == 0 ? 0u : 1u);
+                        tc_mma_tf32(d, ah, bl, idm, 1u);
+                    }
+                } else {
+                    constexpr uint32_t idg = tc_idesc_tf32(128, 32);
+                    const uint32_t d = tmem + TC_COL_GAM + (uint32_t)b * 32u;
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++) {
+                        const uint32_t o = kk * TC_KSTEP_BYTES;
+                        const uint64_t uh = tc_sdesc(sb + o), ul = tc_sdesc(sb + TC_G_ULO + o);
+                        const uint64_t vh = tc_sdesc(sb + TC_G_VHI + o), vl = tc_sdesc(sb + TC_G_VLO + o);
+                        tc_mma_tf32(d, uh, vh, idg, kk == 0 ? 0u : 1u);
+                        tc_mma_tf32(d, uh, vl, idg, 1u);
+                        tc_mma_tf32(d, ul, vh, idg, 1u);
+                    }
+                }
+                tc_commit(&S.mbar[b]);
+            }
+            pend[b] = true;
+            kind[b] = ch < cpos ? 0 : (ch < cpos + cneg ? 1 : 2);
+            /* chunk ch-1 (stage and accumulator 1-b): wait for its MMAs, add its
+             * accumulator into the registers; stage 1-b is then free for chunk ch+1 */
+            if (pend[b ^ 1]) {
+                if (tid == 0 && !tc_mbar_wait(&S.mbar[b ^ 1], ph[b ^ 1])) S.abort_flag = 1;
+                ph[b ^ 1] ^= 1u;
+                pend[b ^ 1] = false;
+                __syncthreads();
+                if (S.abort_flag) { aborted = true; break; }
+                tc_fence_after_sync();
+                tc_accumulate(tmem, b ^ 1, kind[b ^ 1], warp, acc);
+                tc_fence_before_sync();
+            }
+            gc++;
+        }
+        if (aborted) break;
+
+        /* ---- last chunk, then the element matrix and Gamma to shared memory */
+        {
+            const int b = (gc - 1) & 1;
+            if (tid == 0 && !tc_mbar_wait(&S.mbar[b], ph[b])) S.abort_flag = 1;
+            ph[b] ^= 1u;
+            pend[b] = false;
+            __syncthreads();
+            if (S.abort_flag) { aborted = true; break; }
+            tc_fence_after_sync();
+            tc_accumulate(tmem, b, kind[b], warp, acc);
+        }
+        float *E = reinterpret_cast<float *>(&S.stage[0][0]);   /* [81][81] */
+        float *Gm = E + 81 * 81;                                  /* [27][27] */
+        if (warp < 8) {
+            const int lb = 32 * (warp & 3), half = warp >> 2, row = lb + lane;
+            if (row < 81)
+#pragma unroll
+                for (int i = 0; i < 48; i++)
+                    if (48 * half + i < 81) E[row * 81 + 48 * half + i] = acc[i];
+        } else if (lane < 27) {
+#pragma unroll
+            for (int i = 0; i < 27; i++) Gm[lane * 27 + i] = acc[i];
+        }
+        tc_fence_before_sync();
+        __syncthreads();
+        /* ---- symmetric part + Gamma on the k1 = k2 blocks, scatter into the CSR values */
+        for (int idx = tid; idx < 81 * 81; idx += TCN_THR) {
+            const int c1 = idx / 81, c2 = idx % 81;
+            const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
+            float val = 0.5f * (E[c1 * 81 + c2] + E[c2 * 81 + c1]);
+            if (k1 == k2) val += 0.5f * (Gm[a1 * 27 + a2] + Gm[a2 * 27 + a1]);
+            const int x1 = Tl.e0[0] + lex + a1 / 9, y1 = Tl.e0[1] + ley + (a1 / 3) % 3, z1 = Tl.e0[2] + lez + a1 % 3;
+            const int x2 = Tl.e0[0] + lex + a2 / 9, y2 = Tl.e0[1] + ley + (a2 / 3) % 3, z2 = Tl.e0[2] + lez + a2 % 3;
+            const long r1 = 3 * cp_index(g, x1, y1, z1) + k1;
+            vals[g.rowptr[r1] + csr_pos(g, x1, y1, z1, x2, y2, z2, k2)] += val;
+        }
+        __syncthreads();
+    }
+
+    /* ---- release: every issued MMA has completed (or the wait gave up) */
+    if (aborted) {
+        if (tid == 0) {
+            atomicOr(status, 1);
+            for (int b = 0; b < 2; b++)
+                if (pend[b]) tc_mbar_wait(&S.mbar[b], ph[b]);
+        }
+    }
+    tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after_sync();
+        tc_dealloc(tmem, TC_TMEM_COLS);
+    }
+}
+
+/* ---------------------------------------------------------------- self-test
+ * One CTA: A (128 x 32) and B (96 x 32) of small exact values in the operand
+ * layout, D = A B^T with M 128 / N 96 (4 k-steps) into columns 0-95 and, for
+ * the Gamma shape, A B[0:32]^T with M 128 / N 32 into columns 96-127 (first
+ * k-step overwrite, then accumulate).  out[128][128] receives columns 0-127. */
+__global__ void __launch_bounds__(128) k_tc_selftest(float *out, int *status)
+{
+    __shared__ __align__(128) unsigned char sm[16384 + 12288];
+    __shared__ unsigned long long bar;
+    __shared__ unsigned int tbase;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    unsigned char *A = sm, *B = sm + 16384;
+    for (int idx = tid; idx < 128 * 32; idx += 128) {
+        const int m = idx / 32, k = idx % 32;
+        *reinterpret_cast<float *>(A + tc_off(m, k)) = (float)((m * 5 + k * 3) % 13 - 6) * 0.5f;
+    }
+    for (int idx = tid; idx < 96 * 32; idx += 128) {
+        const int n = idx / 32, k = idx % 32;
+        *reinterpret_cast<float *>(B + tc_off(n, k)) = (float)((n * 7 + k) % 11 - 5) * 0.25f;
+    }
+    if (tid == 0) {
+        tc_mbar_init(&bar, 1);
+        tc_fence_mbar_init();
+    }
+    if (warp == 0) tc_alloc(&tbase, 128);
+    tc_fence_proxy_async();
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    const uint32_t tm = tbase;
+    if (tid == 0) {
+        const uint32_t sa = tc_smem_u32(A), sb = tc_smem_u32(B);
+        for (int kk = 0; kk < 4; kk++)
+            tc_mma_tf32(tm, tc_sdesc(sa + kk * TC_KSTEP_BYTES), tc_sdesc(sb + kk * TC_KSTEP_BYTES),
+                        tc_idesc_tf32(128, 96), kk > 0);
+        for (int kk = 0; kk < 4; kk++)
+            tc_mma_tf32(tm + 96, tc_sdesc(sa + kk * TC_KSTEP_BYTES), tc_sdesc(sb + kk * TC_KSTEP_BYTES),
+                        tc_idesc_tf32(128, 32), kk > 0);
+        tc_commit(&bar);
+    }
+    __syncthreads();
+    if (tid == 0 && !tc_mbar_wait(&bar, 0)) atomicOr(status, 1);
+    __syncthreads();
+    tc_fence_after_sync();
+    for (int part = 0; part < 8; part++) {
+        float v[16];
+        tc_ld16(tm + ((uint32_t)(32 * warp) << 16) + 16u * part, v);
+        for (int i = 0; i < 16; i++) out[(32 * warp + lane) * 128 + 16 * part + i] = v[i];
+    }
+    tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after_sync();
+        tc_dealloc(tm, 128);
+    }
+}
+
+} /* namespace */
+
+int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv)
+{
+    igab_geom g = c->geom();
+    const size_t sm = sizeof(tc_smem<2>);
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_tc32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    /* 256 tensor-memory columns per CTA: at most two CTAs may share an SM */
+    int per_sm = 0;
+    IGAB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tan_tc32<2>, TCN_THR, sm));
+    if (per_sm > 2 || per_sm < 1) {
+        igab_set_error("k_tan_tc32: %d CTAs per SM (needs 1 or 2 for its tensor memory)", per_sm);
+        return IGAB_ERR_UNSUPPORTED;
+    }
+    for (int colour = 0; colour < 8; colour++) {
+        long nblk = tiles_of_colour(g, 2, colour);
+        if (nblk == 0) continue;
+        k_tan_tc32<2><<<(unsigned)nblk, TCN_THR, sm, c->stream>>>(g, dU, dv, colour, c->d_status);
+        c->last_launches++;
+    }
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+extern "C" int igab_tc_selftest(int device, float *out_host)
+{
+    if (!out_host) {
+        igab_set_error("igab_tc_selftest: null output");
+        return IGAB_ERR_ARG;
+    }
+    IGAB_CUDA_TRY(cudaSetDevice(device));
+    float *d_out = nullptr;
+    int *d_st = nullptr;
+    IGAB_CUDA_TRY(cudaMalloc((void **)&d_out, 128 * 128 * sizeof(float)));
+    cudaError_t e = cudaMalloc((void **)&d_st, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(d_st, 0, sizeof(int));
+    if (e == cudaSuccess) {
+        k_tc_selftest<<<1, 128>>>(d_out, d_st);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    int st = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(out_host, d_out, 128 * 128 * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&st, d_st, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d_out);
+    cudaFree(d_st);
+    if (e != cudaSuccess) {
+        igab_set_error("igab_tc_selftest: %s", cudaGetErrorString(e));
+        return IGAB_ERR_CUDA;
+    }
+    if (st) {
+        igab_set_error("igab_tc_selftest: tensor-core completion wait timed out");
+        return IGAB_ERR_CUDA;
+    }
+    return 0;
+}

@@ -78,6 +78,7 @@ IGAB_API = [
     ("igab_adjoint_forward", ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int]),
     ("igab_adjoint_backward", ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp, vp, vp]),
     ("igab_get_option", ctypes.c_int, [vp, ctypes.c_int, c_int_p]),
+    ("igab_tc_selftest", ctypes.c_int, [ctypes.c_int, vp]),
 ]
 
 # entry points of include/snesiga_b200.h and include/iga_case.h

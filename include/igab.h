@@ -103,8 +103,10 @@ int igab_check_finite(igab_ctx *ctx, const void *dev, long n, int prec, int *all
 
 /* ---- tuning: elements per tile edge of the 8-colour schedule (2 or 4), 0 = auto */
 int igab_set_tile(igab_ctx *ctx, int residual_tile, int tangent_tile);
-/* kernel choices: IGAB_OPT_TANGENT_FP64_KERNEL 1 = FP64 tensor path (mma f64), 0 = FP64 FMA pipe */
-enum igab_option { IGAB_OPT_TANGENT_FP64_KERNEL = 1 };
+/* kernel choices: IGAB_OPT_TANGENT_FP64_KERNEL 1 = FP64 tensor path (mma f64), 0 = FP64 FMA pipe;
+ * IGAB_OPT_TANGENT_FP32_KERNEL 1 = tcgen05 tensor cores (TF32 hi/lo split, FP32 accumulation in
+ * tensor memory), 0 = FP32 FMA pipe */
+enum igab_option { IGAB_OPT_TANGENT_FP64_KERNEL = 1, IGAB_OPT_TANGENT_FP32_KERNEL = 2 };
 int igab_set_option(igab_ctx *ctx, int option, int value);
 int igab_get_option(const igab_ctx *ctx, int option, int *value);
 /* launches issued by the last assembly call (kernel count) */
@@ -120,6 +122,11 @@ int igab_set_profiling(igab_ctx *ctx, int on);
 int igab_last_kernel_ms(igab_ctx *ctx, double ms[6]);
 /* FMA throughput probe of the device (TFLOP/s, 2 flops per FMA), prec = igab_prec */
 int igab_fma_peak(int device, int prec, double *tflops);
+/* Check of the tcgen05 operand layout and descriptors used by the FP32 tensor-core tangent
+ * (no reference counterpart): one CTA computes A B^T for fixed small-integer A (128 x 32) and
+ * B (96 x 32) with the M 128 / N 96 and M 128 / N 32 instruction shapes; out (128 x 128 floats,
+ * row-major) receives accumulator columns 0-95 (A B^T) and 96-127 (A B[0:32]^T). */
+int igab_tc_selftest(int device, float *out);
 
 /* ---- CUDA graphs: capture one assembly at fixed device pointers, replay it.
  * what: 1 residual, 2 tangent, 3 both (residual then tangent).  Parameters

@@ -75,6 +75,24 @@ __device__ __forceinline__ int csr_pos(const igab_geom &g, int x, int y, int z, 
     return (((cx - x0) * nyb + (cy - y0)) * nzb + (cz - z0)) * 3 + k2;
 }
 
+/* CSR bases of row c1 (= 3 a1 + k1) of the element matrix of the element whose first
+ * control point is (ex, ey, ez): entry (c1, c2), c2 = 3 (9 ax + 3 ay + az) + k2, lies at
+ *   rb + ax * rsx + ay * rsy + 3 az + k2
+ * (csr_pos with the row's window fixed; one rowptr load per row instead of per entry). */
+__device__ __forceinline__ void elem_row_base(const igab_geom &g, int ex, int ey, int ez, int c1, long &rb, int &rsx,
+                                              int &rsy)
+{
+    const int a1 = c1 / 3, k1 = c1 % 3;
+    const int x1 = ex + a1 / 9, y1 = ey + (a1 / 3) % 3, z1 = ez + a1 % 3;
+    const int x0 = x1 > 2 ? x1 - 2 : 0;
+    const int y0 = y1 > 2 ? y1 - 2 : 0, ye = y1 + 2 < g.nb[1] - 1 ? y1 + 2 : g.nb[1] - 1;
+    const int z0 = z1 > 2 ? z1 - 2 : 0, ze = z1 + 2 < g.nb[2] - 1 ? z1 + 2 : g.nb[2] - 1;
+    const int nyb = ye - y0 + 1, nzb = ze - z0 + 1;
+    rb = (long)g.rowptr[3 * cp_index(g, x1, y1, z1) + k1] + (((ex - x0) * nyb + (ey - y0)) * nzb + (ez - z0)) * 3;
+    rsx = nyb * nzb * 3;
+    rsy = nzb * 3;
+}
+
 /* per-element integrand scale (1 when no scaling is set) */
 __device__ __forceinline__ double elem_scale(const igab_geom &g, int ex, int ey, int ez)
 {

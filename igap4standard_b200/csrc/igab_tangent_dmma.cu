@@ -69,6 +69,8 @@ struct dmma_smem {
     double wh[3][TE][IGAB_NQ];
     double gcoef[12][9];
     int gsrc[12][9];
+    long rbase[81];       /* CSR row bases of the element matrix (elem_row_base) */
+    int rsx[81], rsy[81];
 };
 
 __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
@@ -398,16 +400,32 @@ __global__ void __launch_bounds__(NTHR, 2) k_tan_dmma(igab_geom g, const double 
 #define DUMP_CALL(Wn) warp_dump<Wn>(K, Gam, lane, acc, gacc)
         WARP_SWITCH(DUMP_CALL)
 #undef DUMP_CALL
+        if (tid < 81)
+            elem_row_base(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez, tid, S.rbase[tid], S.rsx[tid], S.rsy[tid]);
         __syncthreads();
-        for (int idx = tid; idx < 81 * 81; idx += NTHR) {
-            const int c1 = idx / 81, c2 = idx % 81;
-            const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
-            double val = c1 <= c2 ? K[c1 * 88 + c2] : K[c2 * 88 + c1];
-            if (k1 == k2) val += a1 <= a2 ? Gam[a1 * 32 + a2] : Gam[a2 * 32 + a1];
-            const int x1 = Tl.e0[0] + lex + a1 / 9, y1 = Tl.e0[1] + ley + (a1 / 3) % 3, z1 = Tl.e0[2] + lez + a1 % 3;
-            const int x2 = Tl.e0[0] + lex + a2 / 9, y2 = Tl.e0[1] + ley + (a2 / 3) % 3, z2 = Tl.e0[2] + lez + a2 % 3;
-            const long r1 = 3 * cp_index(g, x1, y1, z1) + k1;
-            vals[g.rowptr[r1] + csr_pos(g, x1, y1, z1, x2, y2, z2, k2)] += val;
+        /* read-modify-write into the CSR values, four independent entries per thread in flight */
+        for (int i0 = tid; i0 < 81 * 81; i0 += 4 * NTHR) {
+            long off[4];
+            double val[4], old[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int idx = i0 + u * NTHR;
+                off[u] = -1;
+                if (idx < 81 * 81) {
+                    const int c1 = idx / 81, c2 = idx % 81;
+                    const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
+                    double v = c1 <= c2 ? K[c1 * 88 + c2] : K[c2 * 88 + c1];
+                    if (k1 == k2) v += a1 <= a2 ? Gam[a1 * 32 + a2] : Gam[a2 * 32 + a1];
+                    val[u] = v;
+                    off[u] = S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (off[u] >= 0) old[u] = vals[off[u]];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (off[u] >= 0) vals[off[u]] = old[u] + val[u];
         }
         __syncthreads();
         /* Gamma overwrote N^T: restore the zero padding of N^T */

@@ -83,6 +83,8 @@ struct tc_smem {
     unsigned short map[2][768];         /* bucket slot -> 12 q + v (positive, negative) */
     int cnt[2];
     int part[2][2];                     /* per-warp bucket counts for the scan */
+    long rbase[81];                     /* CSR row bases of the element matrix (elem_row_base) */
+    int rsx[81], rsy[81];
     unsigned long long mbar[2];
     unsigned int tmem_base;
     int abort_flag;
@@ -188,7 +190,7 @@ __device__ __forceinline__ void tc_accumulate(uint32_t tmem, int buf, int kind, 
 }
 
 template <int TE>
-__global__ void __maxnreg__(112) k_tan_tc32(igab_geom g, const double *__restrict__ U,
+__global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32(igab_geom g, const double *__restrict__ U,
                                                          float *__restrict__ vals, int colour, int *status)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -504,22 +506,40 @@ __global__ void __maxnreg__(112) k_tan_tc32(igab_geom g, const double *__restric
 #pragma unroll
                 for (int i = 0; i < 48; i++)
                     if (48 * half + i < 81) E[row * 81 + 48 * half + i] = acc[i];
-        } else if (lane < 27) {
+        } else {
+            if (lane < 27)
 #pragma unroll
-            for (int i = 0; i < 27; i++) Gm[lane * 27 + i] = acc[i];
+                for (int i = 0; i < 27; i++) Gm[lane * 27 + i] = acc[i];
         }
+        if (tid >= 192 && tid < 192 + 81)
+            elem_row_base(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez, tid - 192, S.rbase[tid - 192],
+                          S.rsx[tid - 192], S.rsy[tid - 192]);
         tc_fence_before_sync();
         __syncthreads();
-        /* ---- symmetric part + Gamma on the k1 = k2 blocks, scatter into the CSR values */
-        for (int idx = tid; idx < 81 * 81; idx += TCN_THR) {
-            const int c1 = idx / 81, c2 = idx % 81;
-            const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
-            float val = 0.5f * (E[c1 * 81 + c2] + E[c2 * 81 + c1]);
-            if (k1 == k2) val += 0.5f * (Gm[a1 * 27 + a2] + Gm[a2 * 27 + a1]);
-            const int x1 = Tl.e0[0] + lex + a1 / 9, y1 = Tl.e0[1] + ley + (a1 / 3) % 3, z1 = Tl.e0[2] + lez + a1 % 3;
-            const int x2 = Tl.e0[0] + lex + a2 / 9, y2 = Tl.e0[1] + ley + (a2 / 3) % 3, z2 = Tl.e0[2] + lez + a2 % 3;
-            const long r1 = 3 * cp_index(g, x1, y1, z1) + k1;
-            vals[g.rowptr[r1] + csr_pos(g, x1, y1, z1, x2, y2, z2, k2)] += val;
+        /* ---- symmetric part + Gamma on the k1 = k2 blocks, read-modify-write into the CSR
+         * values, four independent entries per thread in flight */
+        for (int i0 = tid; i0 < 81 * 81; i0 += 4 * TCN_THR) {
+            long off[4];
+            float val[4], old[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int idx = i0 + u * TCN_THR;
+                off[u] = -1;
+                if (idx < 81 * 81) {
+                    const int c1 = idx / 81, c2 = idx % 81;
+                    const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
+                    float v = 0.5f * (E[c1 * 81 + c2] + E[c2 * 81 + c1]);
+                    if (k1 == k2) v += 0.5f * (Gm[a1 * 27 + a2] + Gm[a2 * 27 + a1]);
+                    val[u] = v;
+                    off[u] = S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (off[u] >= 0) old[u] = vals[off[u]];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (off[u] >= 0) vals[off[u]] = old[u] + val[u];
         }
         __syncthreads();
     }
@@ -604,6 +624,7 @@ int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv)
     igab_geom g = c->geom();
     const size_t sm = sizeof(tc_smem<2>);
     IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_tc32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_tc32<2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     /* 256 tensor-memory columns per CTA: at most two CTAs may share an SM */
     int per_sm = 0;
     IGAB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tan_tc32<2>, TCN_THR, sm));

@@ -9,8 +9,9 @@ from .native import NativeLibraryMissing, IgabError, lib_cuda, lib_dropin
 from .mesh import (open_knot_vector, knots_for, par_mat_from_lame, bc_config0, bc_example,
                    n_dof, nnz_of, PAR_MAT_DEFAULT)
 from .assembly import Assembly
+from .batch import Batch
 from .case import Case, gpu_case
 
 __all__ = ["NativeLibraryMissing", "IgabError", "lib_cuda", "lib_dropin", "open_knot_vector", "knots_for",
            "par_mat_from_lame", "bc_config0", "bc_example", "n_dof", "nnz_of", "PAR_MAT_DEFAULT",
-           "Assembly", "Case", "gpu_case"]
+           "Assembly", "Batch", "Case", "gpu_case"]

@@ -99,6 +99,59 @@ __device__ __forceinline__ double elem_scale(const igab_geom &g, int ex, int ey,
     return g.escale ? g.escale[((long)ex * g.ne[1] + ey) * g.ne[2] + ez] : 1.0;
 }
 
+/* ---- persistent batched launches: one work item (a tile of one instance) at a time */
+#define IGAB_BATCH_SPIN (1L << 22)   /* polls (with a 128 ns sleep) before a dependency wait gives up */
+
+struct batch_slot {
+    igab_geom g;      /* geometry of the current item's instance */
+    int item, inst, colour, tile;
+};
+
+/* all threads: fetch the next item, wait until every earlier colour of its
+ * instance is complete, stage the instance geometry in shared memory.
+ * Returns false when the list is exhausted (block-uniform). */
+__device__ __forceinline__ bool batch_next(const igab_batch_dev &B, batch_slot &sl)
+{
+    if (threadIdx.x == 0) {
+        const int it = atomicAdd(B.counter, 1);
+        sl.item = it;
+        if (it < B.nitems) {
+            const int4 w = B.items[it];
+            sl.inst = w.x;
+            sl.colour = w.y;
+            sl.tile = w.z;
+            int *done = B.done + 8 * w.x;
+            const int *need = B.need + 8 * w.x;
+            for (int c = 0; c < w.y; c++) {
+                long spins = 0;
+                while (atomicOr(&done[c], 0) < need[c]) {
+                    if (++spins > IGAB_BATCH_SPIN) {
+                        atomicOr(B.status, 2);
+                        break;
+                    }
+                    __nanosleep(128);
+                }
+            }
+            __threadfence();
+        }
+    }
+    __syncthreads();
+    if (sl.item >= B.nitems) return false;
+    const int *src = reinterpret_cast<const int *>(B.geoms + sl.inst);
+    int *dst = reinterpret_cast<int *>(&sl.g);
+    for (int i = threadIdx.x; i < (int)(sizeof(igab_geom) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    return true;
+}
+
+/* all threads, after the item's last global write: publish the finished tile */
+__device__ __forceinline__ void batch_done(const igab_batch_dev &B, const batch_slot &sl)
+{
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(&B.done[8 * sl.inst + sl.colour], 1);
+}
+
 long tiles_of_colour(const igab_geom &g, int TE, int colour)
 {
     long n = 1;

@@ -36,6 +36,24 @@ struct igab_geom {
     const double *escale;
 };
 
+/* Batched assembly: the work list of a persistent launch over many meshes.
+ * item = (instance, colour, tile, 0), ordered colour-major; done[8 i + c]
+ * counts the finished tiles of colour c of instance i, need[8 i + c] how many
+ * there are.  A tile of colour c starts once every earlier colour of its
+ * instance is complete (bounded wait), so tiles of one instance never overlap
+ * in time unless they are of one colour. */
+struct igab_batch_dev {
+    const igab_geom *geoms;
+    const int4 *items;
+    int nitems;
+    int *counter;          /* next item; zeroed before each launch (with done) */
+    int *done;
+    const int *need;
+    const long *dof_off;   /* [n] offsets of the instances in U / R */
+    const long *nnz_off;   /* [n] offsets in the CSR values */
+    int *status;           /* bit 1: a dependency wait gave up */
+};
+
 struct igab_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -120,6 +138,19 @@ int igab_launch_basis_tables(igab_ctx *c, int d, const double *dkv, const double
 int igab_launch_fma_peak(int prec, double *tflops);
 int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv);
 int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv);
+/* persistent batched launches (igab_batch.cu builds the work list) */
+int igab_launch_res_batch(const igab_batch_dev &B, int grid, cudaStream_t s, const double *dU, double *dR);
+int igab_launch_tan_dmma_batch(const igab_batch_dev &B, int grid, cudaStream_t s, const double *dU, double *dv);
+int igab_launch_tan_tc32_batch(const igab_batch_dev &B, int grid, cudaStream_t s, const double *dU, float *dv);
+int igab_launch_tan_dirichlet_batch(const igab_batch_dev &B, long nd, const int *dinst, const int *drow, void *dv,
+                                    int prec, cudaStream_t s);
+/* R = U - g on a list of (global) Dirichlet rows */
+int igab_launch_res_dirichlet_rows(long nd, const int *drow, const double *dg, const double *dU, double *dR,
+                                   cudaStream_t s);
+/* CTAs per SM the persistent kernels can hold (occupancy; the FP32 tangent is capped at 2 by its tensor memory) */
+int igab_batch_occupancy_res(int *per_sm);
+int igab_batch_occupancy_dmma(int *per_sm);
+int igab_batch_occupancy_tc32(int *per_sm);
 int igab_launch_tan_getime(igab_ctx *c, const double *dU, void *dv, int prec);
 int igab_launch_exp_scale(igab_ctx *c, const double *dg);
 int igab_launch_adjoint_dRdg(igab_ctx *c, const double *dU, const double *dlam, double *dgrad);

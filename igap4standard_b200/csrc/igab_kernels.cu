@@ -98,18 +98,14 @@ __device__ __forceinline__ void add_periodic(const igab_geom &g, const double X[
  * for every element of the tile (lam with Dirichlet rows already zeroed), i.e.
  * the vector-Jacobian product lam^T dR/dg_e of the scaled residual. */
 template <int TE, bool GT, bool VJP>
-__global__ void __launch_bounds__(256) k_res_volume(igab_geom g, const double *__restrict__ U,
-                                                    double *__restrict__ R, int colour,
-                                                    const double *__restrict__ lam, double *__restrict__ grad)
+__device__ __forceinline__ void res_tile(const igab_geom &g, const tile_t &T, const double *__restrict__ U,
+                                         double *__restrict__ R, const double *__restrict__ lam,
+                                         double *__restrict__ grad, res_smem<TE, GT ? 3 : 1> &S)
 {
     constexpr int NL = GT ? 3 : 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    res_smem<TE, NL> &S = *reinterpret_cast<res_smem<TE, NL> *>(smem_raw);
     constexpr int TC = TE + 2;
     constexpr int NCP = TC * TC * TC;
     constexpr int NEL = TE * TE * TE;
-    tile_t T;
-    if (!decode_tile(g, TE, colour, blockIdx.x, T)) return;
     const int tid = threadIdx.x;
 
     /* ---- stage control-point values (all history levels) and 1-D tables of the tile */
@@ -307,9 +303,21 @@ __global__ void __launch_bounds__(256) k_res_volume(igab_geom g, const double *_
         int lz = cp % TC, ly = (cp / TC) % TC, lx = cp / (TC * TC);
         if (lx < T.nv[0] + 2 && ly < T.nv[1] + 2 && lz < T.nv[2] + 2) {
             long gi = 3 * cp_index(g, T.e0[0] + lx, T.e0[1] + ly, T.e0[2] + lz) + i;
-            R[gi] += S.Racc[idx];
+            R[gi] = __ldcg(&R[gi]) + S.Racc[idx];   /* L2 read: another CTA may have written it */
         }
     }
+}
+
+template <int TE, bool GT, bool VJP>
+__global__ void __launch_bounds__(256) k_res_volume(igab_geom g, const double *__restrict__ U,
+                                                    double *__restrict__ R, int colour,
+                                                    const double *__restrict__ lam, double *__restrict__ grad)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    res_smem<TE, GT ? 3 : 1> &S = *reinterpret_cast<res_smem<TE, GT ? 3 : 1> *>(smem_raw);
+    tile_t T;
+    if (!decode_tile(g, TE, colour, blockIdx.x, T)) return;
+    res_tile<TE, GT, VJP>(g, T, U, R, lam, grad, S);
 }
 
 /* Neumann surface terms (src/snesiga_Residual.c:243-320): one thread per
@@ -652,13 +660,8 @@ __global__ void __launch_bounds__(256) k_tan_volume(igab_geom g, const double *_
 /* MatZeroRowsColumns(P, rows, 1.0) on the structured pattern (src/snesiga_Tangent.c:270):
  * one thread per (Dirichlet row, entry of that row). */
 template <typename T>
-__global__ void k_tan_dirichlet(igab_geom g, long nd, const int *__restrict__ drow, T *__restrict__ vals)
+__device__ __forceinline__ void tan_dirichlet_entry(const igab_geom &g, int r, int s, T *__restrict__ vals)
 {
-    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    long j = t / 375;
-    int s = (int)(t % 375);
-    if (j >= nd) return;
-    int r = drow[j];
     int cp = r / 3;
     int z = cp % g.nb[2], y = (cp / g.nb[2]) % g.nb[1], x = cp / (g.nb[2] * g.nb[1]);
     int nc = g.rowptr[r + 1] - g.rowptr[r];
@@ -672,6 +675,45 @@ __global__ void k_tan_dirichlet(igab_geom g, long nd, const int *__restrict__ dr
     long c = 3 * cp_index(g, cx, cy, cz) + k2;
     vals[g.rowptr[r] + s] = (c == r) ? T(1) : T(0);
     if (c != r) vals[g.rowptr[c] + csr_pos(g, cx, cy, cz, x, y, z, r % 3)] = T(0);
+}
+
+template <typename T>
+__global__ void k_tan_dirichlet(igab_geom g, long nd, const int *__restrict__ drow, T *__restrict__ vals)
+{
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long j = t / 375;
+    int s = (int)(t % 375);
+    if (j >= nd) return;
+    tan_dirichlet_entry<T>(g, drow[j], s, vals);
+}
+
+/* the same over the Dirichlet rows of all instances of a batch (row j of instance dinst[j]) */
+template <typename T>
+__global__ void k_tan_dirichlet_batch(igab_batch_dev B, long nd, const int *__restrict__ dinst,
+                                      const int *__restrict__ drow, T *__restrict__ vals)
+{
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long j = t / 375;
+    int s = (int)(t % 375);
+    if (j >= nd) return;
+    const int inst = dinst[j];
+    tan_dirichlet_entry<T>(B.geoms[inst], drow[j], s, vals + B.nnz_off[inst]);
+}
+
+/* persistent residual over the tiles of every instance of a batch (TE = 2, phys/ge) */
+__global__ void __launch_bounds__(256, 2) k_res_batch(igab_batch_dev B, const double *__restrict__ U,
+                                                   double *__restrict__ R)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    res_smem<2, 1> &S = *reinterpret_cast<res_smem<2, 1> *>(smem_raw);
+    __shared__ batch_slot sl;
+    while (batch_next(B, sl)) {
+        tile_t T;
+        decode_tile(sl.g, 2, sl.colour, sl.tile, T);
+        const long off = B.dof_off[sl.inst];
+        res_tile<2, false, false>(sl.g, T, U + off, R + off, nullptr, nullptr, S);
+        batch_done(B, sl);
+    }
 }
 
 /* column indices of the CSR pattern, one thread per row */
@@ -909,6 +951,45 @@ int igab_launch_tangent_transpose(igab_ctx *c, const void *dvals, int prec, cons
     else
         k_tangent_transpose<float><<<(unsigned)nblk, 128, 0, c->stream>>>(g, (const float *)dvals, dx, dy, nchunk);
     c->last_launches++;
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int igab_launch_res_batch(const igab_batch_dev &B, int grid, cudaStream_t st, const double *dU, double *dR)
+{
+    const size_t sm = sizeof(res_smem<2, 1>);
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_res_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_res_batch<<<grid, 256, sm, st>>>(B, dU, dR);
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int igab_batch_occupancy_res(int *per_sm)
+{
+    const size_t sm = sizeof(res_smem<2, 1>);
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_res_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    IGAB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_res_batch, 256, sm));
+    return 0;
+}
+
+int igab_launch_res_dirichlet_rows(long nd, const int *drow, const double *dg, const double *dU, double *dR,
+                                   cudaStream_t st)
+{
+    if (nd <= 0) return 0;
+    k_res_dirichlet<<<(unsigned)((nd + 255) / 256), 256, 0, st>>>(nd, drow, dg, dU, dR);
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int igab_launch_tan_dirichlet_batch(const igab_batch_dev &B, long nd, const int *dinst, const int *drow, void *dv,
+                                    int prec, cudaStream_t st)
+{
+    if (nd <= 0) return 0;
+    const long n = nd * 375;
+    if (prec == IGAB_PREC_FP64)
+        k_tan_dirichlet_batch<double><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(B, nd, dinst, drow, (double *)dv);
+    else
+        k_tan_dirichlet_batch<float><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(B, nd, dinst, drow, (float *)dv);
     IGAB_CUDA_TRY(cudaGetLastError());
     return 0;
 }

@@ -159,17 +159,14 @@ __device__ __forceinline__ void warp_dump(double *__restrict__ K, double *__rest
     default: CALL(3); break; \
     }
 
+/* one tile: all NTHR threads of the block, uniformly */
 template <int TE>
-__global__ void __launch_bounds__(NTHR, 2) k_tan_dmma(igab_geom g, const double *__restrict__ U,
-                                                      double *__restrict__ vals, int colour)
+__device__ __forceinline__ void dmma_tile(const igab_geom &g, const tile_t &Tl, const double *__restrict__ U,
+                                          double *__restrict__ vals, dmma_smem<TE> &S)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    dmma_smem<TE> &S = *reinterpret_cast<dmma_smem<TE> *>(smem_raw);
     constexpr int TC = TE + 2;
     constexpr int NCP = TC * TC * TC;
     constexpr int NEL = TE * TE * TE;
-    tile_t Tl;
-    if (!decode_tile(g, TE, colour, blockIdx.x, Tl)) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     double *const Xb = S.W + W_X;
     double *const PTb = S.W + W_PT;
@@ -422,7 +419,7 @@ __global__ void __launch_bounds__(NTHR, 2) k_tan_dmma(igab_geom g, const double 
             }
 #pragma unroll
             for (int u = 0; u < 4; u++)
-                if (off[u] >= 0) old[u] = vals[off[u]];
+                if (off[u] >= 0) old[u] = __ldcg(&vals[off[u]]);   /* L2: written by other CTAs */
 #pragma unroll
             for (int u = 0; u < 4; u++)
                 if (off[u] >= 0) vals[off[u]] = old[u] + val[u];
@@ -434,7 +431,50 @@ __global__ void __launch_bounds__(NTHR, 2) k_tan_dmma(igab_geom g, const double 
     }
 }
 
+template <int TE>
+__global__ void __launch_bounds__(NTHR, 2) k_tan_dmma(igab_geom g, const double *__restrict__ U,
+                                                      double *__restrict__ vals, int colour)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    dmma_smem<TE> &S = *reinterpret_cast<dmma_smem<TE> *>(smem_raw);
+    tile_t Tl;
+    if (!decode_tile(g, TE, colour, blockIdx.x, Tl)) return;
+    dmma_tile<TE>(g, Tl, U, vals, S);
+}
+
+/* persistent FP64 tangent over the tiles of every instance of a batch */
+__global__ void __launch_bounds__(NTHR, 2) k_tan_dmma_batch(igab_batch_dev B, const double *__restrict__ U,
+                                                            double *__restrict__ vals)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    dmma_smem<2> &S = *reinterpret_cast<dmma_smem<2> *>(smem_raw);
+    __shared__ batch_slot sl;
+    while (batch_next(B, sl)) {
+        tile_t Tl;
+        decode_tile(sl.g, 2, sl.colour, sl.tile, Tl);
+        dmma_tile<2>(sl.g, Tl, U + B.dof_off[sl.inst], vals + B.nnz_off[sl.inst], S);
+        batch_done(B, sl);
+    }
+}
+
 } /* namespace */
+
+int igab_launch_tan_dmma_batch(const igab_batch_dev &B, int grid, cudaStream_t st, const double *dU, double *dv)
+{
+    const size_t sm = sizeof(dmma_smem<2>);
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_dmma_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_tan_dmma_batch<<<grid, NTHR, sm, st>>>(B, dU, dv);
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int igab_batch_occupancy_dmma(int *per_sm)
+{
+    const size_t sm = sizeof(dmma_smem<2>);
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_dmma_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    IGAB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_tan_dmma_batch, NTHR, sm));
+    return 0;
+}
 
 int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv)
 {

@@ -189,20 +189,21 @@ __device__ __forceinline__ void tc_accumulate(uint32_t tmem, int buf, int kind, 
     }
 }
 
-template <int TE>
-__global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32(igab_geom g, const double *__restrict__ U,
-                                                         float *__restrict__ vals, int colour, int *status)
-{
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    tc_smem<TE> &S = *reinterpret_cast<tc_smem<TE> *>(smem_raw);
-    constexpr int TC = TE + 2;
-    constexpr int NCP = TC * TC * TC;
-    constexpr int NEL = TE * TE * TE;
-    tile_t Tl;
-    if (!decode_tile(g, TE, colour, blockIdx.x, Tl)) return;   /* block-uniform, before any barrier */
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+/* pipeline state of a CTA, carried across the tiles it processes */
+struct tc_state {
+    bool pend[2];      /* a commit on stage/accumulator b is not yet waited for */
+    int kind[2];       /* chunk in flight per stage: 0 positive rows, 1 negative rows, 2 Gamma */
+    uint32_t ph[2];    /* parity of the next phase to wait for on mbar[b] */
+    int gc;            /* chunks issued by this CTA */
+    bool aborted;
+    uint32_t tmem;
+};
 
-    /* ---- set-up: barriers, tensor memory, tile data */
+/* barriers and tensor memory of the CTA (all threads) */
+template <int TE>
+__device__ __forceinline__ void tc_setup(tc_smem<TE> &S, tc_state &Q)
+{
+    const int tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0) {
         tc_mbar_init(&S.mbar[0], 1);
         tc_mbar_init(&S.mbar[1], 1);
@@ -210,6 +211,52 @@ __global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32(igab_geom g, const doub
         S.abort_flag = 0;
     }
     if (warp == 0) tc_alloc(&S.tmem_base, TC_TMEM_COLS);
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    Q.tmem = S.tmem_base;
+    Q.pend[0] = Q.pend[1] = false;
+    Q.kind[0] = Q.kind[1] = 0;
+    Q.ph[0] = Q.ph[1] = 0u;
+    Q.gc = 0;
+    Q.aborted = false;
+}
+
+/* release: wait (bounded) for MMAs still in flight after an abort, free the tensor memory */
+template <int TE>
+__device__ __forceinline__ void tc_release(tc_smem<TE> &S, tc_state &Q, int *status)
+{
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (Q.aborted && tid == 0) {
+        atomicOr(status, 1);
+        for (int b = 0; b < 2; b++)
+            if (Q.pend[b]) tc_mbar_wait(&S.mbar[b], Q.ph[b]);
+    }
+    tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after_sync();
+        tc_dealloc(Q.tmem, TC_TMEM_COLS);
+    }
+}
+
+/* one tile of up to TE^3 elements: all TCN_THR threads of the block, uniformly */
+template <int TE>
+__device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, const double *__restrict__ U,
+                                        float *__restrict__ vals, tc_smem<TE> &S, tc_state &Q)
+{
+    constexpr int TC = TE + 2;
+    constexpr int NCP = TC * TC * TC;
+    constexpr int NEL = TE * TE * TE;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    /* local copies of the pipeline state (registers), written back at the end */
+    bool pend[2] = {Q.pend[0], Q.pend[1]};
+    int kind[2] = {Q.kind[0], Q.kind[1]};
+    uint32_t ph[2] = {Q.ph[0], Q.ph[1]};
+    int gc = Q.gc;
+    bool aborted = Q.aborted;
+    const uint32_t tmem = Q.tmem;
+
     for (int idx = tid; idx < NCP * 3; idx += TCN_THR) {
         int i = idx % 3, cp = idx / 3;
         int lz = cp % TC, ly = (cp / TC) % TC, lx = cp / (TC * TC);
@@ -228,16 +275,7 @@ __global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32(igab_geom g, const doub
         int d = idx / (TE * IGAB_NQ), r = idx % (TE * IGAB_NQ), le = r / IGAB_NQ, q = r % IGAB_NQ;
         S.wh[d][le][q] = le < Tl.nv[d] ? g.wh[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
     }
-    tc_fence_before_sync();
     __syncthreads();
-    tc_fence_after_sync();
-    const uint32_t tmem = S.tmem_base;
-
-    bool pend[2] = {false, false};
-    int kind[2] = {0, 0};    /* chunk in flight per stage: 0 positive rows, 1 negative rows, 2 Gamma */
-    uint32_t ph[2] = {0u, 0u};
-    int gc = 0;          /* chunks issued by this CTA */
-    bool aborted = false;
 
     for (int le = 0; le < NEL && !aborted; le++) {
         const int lex = le / (TE * TE), ley = (le / TE) % TE, lez = le % TE;
@@ -536,28 +574,56 @@ __global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32(igab_geom g, const doub
             }
 #pragma unroll
             for (int u = 0; u < 4; u++)
-                if (off[u] >= 0) old[u] = vals[off[u]];
+                if (off[u] >= 0) old[u] = __ldcg(&vals[off[u]]);   /* L2: written by other CTAs */
 #pragma unroll
             for (int u = 0; u < 4; u++)
                 if (off[u] >= 0) vals[off[u]] = old[u] + val[u];
         }
         __syncthreads();
     }
+    for (int b = 0; b < 2; b++) {
+        Q.pend[b] = pend[b];
+        Q.kind[b] = kind[b];
+        Q.ph[b] = ph[b];
+    }
+    Q.gc = gc;
+    Q.aborted = aborted;
+}
 
-    /* ---- release: every issued MMA has completed (or the wait gave up) */
-    if (aborted) {
-        if (tid == 0) {
-            atomicOr(status, 1);
-            for (int b = 0; b < 2; b++)
-                if (pend[b]) tc_mbar_wait(&S.mbar[b], ph[b]);
+template <int TE>
+__global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32(igab_geom g, const double *__restrict__ U,
+                                                         float *__restrict__ vals, int colour, int *status)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    tc_smem<TE> &S = *reinterpret_cast<tc_smem<TE> *>(smem_raw);
+    tile_t Tl;
+    if (!decode_tile(g, TE, colour, blockIdx.x, Tl)) return;   /* block-uniform, before any barrier */
+    tc_state Q;
+    tc_setup<TE>(S, Q);
+    tc_tile<TE>(g, Tl, U, vals, S, Q);
+    tc_release<TE>(S, Q, status);
+}
+
+/* persistent FP32 tangent over the tiles of every instance of a batch: tensor
+ * memory and barriers are set up once per CTA; after an abort the remaining
+ * items are only published (their values are not computed) */
+__global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32_batch(igab_batch_dev B, const double *__restrict__ U,
+                                                               float *__restrict__ vals)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    tc_smem<2> &S = *reinterpret_cast<tc_smem<2> *>(smem_raw);
+    __shared__ batch_slot sl;
+    tc_state Q;
+    tc_setup<2>(S, Q);
+    while (batch_next(B, sl)) {
+        if (!Q.aborted) {
+            tile_t Tl;
+            decode_tile(sl.g, 2, sl.colour, sl.tile, Tl);
+            tc_tile<2>(sl.g, Tl, U + B.dof_off[sl.inst], vals + B.nnz_off[sl.inst], S, Q);
         }
+        batch_done(B, sl);
     }
-    tc_fence_before_sync();
-    __syncthreads();
-    if (warp == 0) {
-        tc_fence_after_sync();
-        tc_dealloc(tmem, TC_TMEM_COLS);
-    }
+    tc_release<2>(S, Q, B.status);
 }
 
 /* ---------------------------------------------------------------- self-test
@@ -639,6 +705,26 @@ int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv)
         c->last_launches++;
     }
     IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int igab_launch_tan_tc32_batch(const igab_batch_dev &B, int grid, cudaStream_t st, const double *dU, float *dv)
+{
+    const size_t sm = sizeof(tc_smem<2>);
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_tc32_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_tc32_batch, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    k_tan_tc32_batch<<<grid, TCN_THR, sm, st>>>(B, dU, dv);
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int igab_batch_occupancy_tc32(int *per_sm)
+{
+    const size_t sm = sizeof(tc_smem<2>);
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_tc32_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_tc32_batch, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    IGAB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_tan_tc32_batch, TCN_THR, sm));
+    if (*per_sm > 2) *per_sm = 2;   /* 256 tensor-memory columns per CTA */
     return 0;
 }
 

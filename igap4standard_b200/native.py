@@ -79,6 +79,20 @@ IGAB_API = [
     ("igab_adjoint_backward", ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp, vp, vp]),
     ("igab_get_option", ctypes.c_int, [vp, ctypes.c_int, c_int_p]),
     ("igab_tc_selftest", ctypes.c_int, [ctypes.c_int, vp]),
+    ("igab_batch_create", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]),
+    ("igab_batch_destroy", ctypes.c_int, [vp]),
+    ("igab_batch_sizes", ctypes.c_int, [vp, c_long_p, c_long_p, c_long_p, vp, vp]),
+    ("igab_batch_instance", vp, [vp, ctypes.c_int]),
+    ("igab_batch_refresh", ctypes.c_int, [vp]),
+    ("igab_batch_set_stream", ctypes.c_int, [vp, vp]),
+    ("igab_batch_set_schedule", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("igab_batch_get_schedule", ctypes.c_int, [vp, c_int_p, c_int_p, c_int_p, c_int_p]),
+    ("igab_batch_residual_device", ctypes.c_int, [vp, vp, vp]),
+    ("igab_batch_tangent_device", ctypes.c_int, [vp, vp, vp, ctypes.c_int]),
+    ("igab_batch_sync", ctypes.c_int, [vp]),
+    ("igab_batch_last_launch_count", ctypes.c_int, [vp, c_int_p]),
+    ("igab_batch_graph_capture", ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int]),
+    ("igab_batch_graph_launch", ctypes.c_int, [vp]),
 ]
 
 # entry points of include/snesiga_b200.h and include/iga_case.h

@@ -154,6 +154,35 @@ int igab_adjoint_forward(igab_ctx *ctx, const double *g_dev, const double *U_dev
 int igab_adjoint_backward(igab_ctx *ctx, const double *U_dev, const void *vals_dev, int prec,
                           const double *lam_dev, double *KTlam_dev, double *grad_dev);
 
+/* ---- batched assembly: many independent meshes of uneven size, each with its own
+ * material constants and boundary tables, assembled by one persistent launch per
+ * operator (no reference counterpart: the reference runs one mesh per process; each
+ * instance's result is the single-mesh result of igab_residual_device /
+ * igab_tangent_device bit for bit).  phys/ge only; Neumann tractions are zero.
+ * Instance i owns U/R[dof_offsets[i] .. dof_offsets[i+1]) and
+ * vals[nnz_offsets[i] .. nnz_offsets[i+1]) in its own numbering and AIJ pattern;
+ * igab_batch_instance returns its context for pattern queries and parameter
+ * changes (then call igab_batch_refresh).  Schedule knobs (the autotuner's search
+ * space): CTAs per SM of the residual / FP64 tangent / FP32 tangent persistent
+ * kernels (0 = as many as fit) and the instance order of the colour-major work
+ * list (0 natural, 1 largest first). */
+typedef struct igab_batch igab_batch;
+int igab_batch_create(const igab_mesh_desc *descs, int n, int device, igab_batch **out);
+int igab_batch_destroy(igab_batch *b);
+int igab_batch_sizes(const igab_batch *b, long *ndof, long *nnz, long *nelem, long *dof_offsets, long *nnz_offsets);
+igab_ctx *igab_batch_instance(igab_batch *b, int i);
+int igab_batch_refresh(igab_batch *b);
+int igab_batch_set_stream(igab_batch *b, void *cuda_stream);
+int igab_batch_set_schedule(igab_batch *b, int ctas_res, int ctas_tan64, int ctas_tan32, int order);
+int igab_batch_get_schedule(const igab_batch *b, int *ctas_res, int *ctas_tan64, int *ctas_tan32, int *order);
+int igab_batch_residual_device(igab_batch *b, const double *U_dev, double *R_dev);
+int igab_batch_tangent_device(igab_batch *b, const double *U_dev, void *vals_dev, int prec);
+int igab_batch_sync(igab_batch *b);
+int igab_batch_last_launch_count(const igab_batch *b, int *n);
+/* one Newton iteration's assembly (residual then tangent) captured in a CUDA graph */
+int igab_batch_graph_capture(igab_batch *b, const double *U_dev, double *R_dev, void *vals_dev, int prec);
+int igab_batch_graph_launch(igab_batch *b);
+
 /* ---- residual for callers that cannot have the library allocate device memory.
  * No counterpart in the reference.  Same result as igab_residual, but U and R
  * are staged in a file-scope device array (2 x 8 MiB, held by every GPU that

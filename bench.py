@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=4, help="elements per side of the CPU sample mesh")
+    ap.add_argument("--no-tune", action="store_true", help="skip the schedule autotuner")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 512-instance batched assembly")
+    ap.add_argument("--batch-instances", type=int, default=512)
     return ap.parse_args()
 
 
@@ -223,6 +227,73 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def bench_batch(args, dev, device, barrier):
+    """The 512-instance static workload (n^3 elements, n uniform 6..24, own material per
+    instance): one Newton iteration's assembly (FP64 residual + FP32 tangent) through the
+    persistent batched launch with the autotuned schedule, and the same work as one
+    single-mesh assembly per instance for comparison."""
+    import ctypes
+    import torch
+    from igap4standard_b200 import Batch, mesh
+    from igap4standard_b200.native import vp, check
+    inst = mesh.batch_config3(args.batch_instances, seed=3)
+    t0 = time.perf_counter()
+    B = Batch(inst, device=device)
+    setup_s = time.perf_counter() - t0
+    st = torch.cuda.Stream(device=dev)
+    B.set_stream(st.cuda_stream)
+    g = torch.Generator(device="cpu").manual_seed(0)
+    U = (torch.rand(B.ndof, dtype=torch.float64, generator=g) * 2e-3 - 1e-3).to(dev)
+    R = torch.empty(B.ndof, dtype=torch.float64, device=dev)
+    V = torch.empty(B.nnz, dtype=torch.float32, device=dev)
+    tune = B.autotune(U.data_ptr(), what=1 | 4, reps=1)
+    tune.pop("cached", None)
+
+    def step():
+        B.residual_device(U.data_ptr(), R.data_ptr())
+        B.tangent_device(U.data_ptr(), V.data_ptr(), "fp32")
+
+    step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    K = 2
+    e0.record(st)
+    for _ in range(K):
+        step()
+    e1.record(st)
+    barrier()
+    B.sync()
+    ms = e0.elapsed_time(e1) / K
+    # the same assembly as one single-mesh call pair per instance (8 colour launches each)
+    lib = B.lib
+    hs = [B.instance_handle(i) for i in range(B.n)]
+    offs = [(int(B.dof_offsets[i]) * 8, int(B.nnz_offsets[i]) * 4) for i in range(B.n)]
+
+    def loop_step():
+        for h, (od, on) in zip(hs, offs):
+            check(lib, "igab_residual_device", lib.igab_residual_device(h, vp(U.data_ptr() + od), vp(R.data_ptr() + od)))
+            check(lib, "igab_tangent_device",
+                  lib.igab_tangent_device(h, vp(U.data_ptr() + od), vp(V.data_ptr() + on), 1))
+
+    loop_step()
+    barrier()
+    e0.record(st)
+    loop_step()
+    e1.record(st)
+    barrier()
+    loop_ms = e0.elapsed_time(e1)
+    out = {"instances": B.n, "elements": B.nelem_total, "dofs": B.ndof, "nnz": B.nnz,
+           "ms_per_step": round(ms, 3), "elements_per_s": round(B.nelem_total / (ms * 1e-3), 1),
+           "per_instance_launches_ms": round(loop_ms, 3), "speedup_vs_per_instance": round(loop_ms / ms, 3),
+           "dtype": "f64 residual, f32 tangent", "schedule": tune, "setup_s": round(setup_s, 2),
+           "workload": "config 3: n^3 elements, n uniform 6..24 (seed 3), lambda, mu lognormal(0,0.25), "
+                       "l uniform [0.05,0.2], BCs of config 0; one residual + one FP32 tangent per step"}
+    B.close()
+    del V
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -286,6 +357,10 @@ def run_ours(args):
             t = float(tt.item())
         return t, kms / K, launches
 
+    schedule = None
+    if not args.no_tune:
+        schedule = A.autotune(U.data_ptr(), what=7, reps=2)
+        schedule.pop("cached", None)
     peak64 = fma_peak_tflops("fp64", local)
     peak32 = fma_peak_tflops("fp32", local)
     clocks = ClockSampler(local)
@@ -323,6 +398,44 @@ def run_ours(args):
                "d2h_bytes_per_step": ndof * 8 + nnz * 8, "ms_per_step": round(te, 3),
                "timing": "host wall clock around igab_residual + igab_tangent (FP64), pinned host buffers"}
 
+    # ---- adjoint gradient dJ/dg (s_e = exp(g_e) on every element) at this mesh: one
+    # backward pass = dR/dg vector-Jacobian product + K^T lambda on the FP64 tangent
+    adjoint = None
+    if not args.no_adjoint:
+        gen = torch.Generator(device="cpu").manual_seed(4)
+        gl = (torch.randn(nel, dtype=torch.float64, generator=gen) * 0.3).to(dev)
+        lam = (torch.rand(ndof, dtype=torch.float64, generator=gen) * 2 - 1).to(dev)
+        KTl = torch.empty(ndof, dtype=torch.float64, device=dev)
+        grad = torch.empty(nel, dtype=torch.float64, device=dev)
+        A.set_profiling(False)
+        A.adjoint_forward_device(gl.data_ptr(), U.data_ptr(), R.data_ptr(), V64.data_ptr(), "fp64")
+        for _ in range(2):
+            A.adjoint_backward_device(U.data_ptr(), V64.data_ptr(), lam.data_ptr(), KTl.data_ptr(), grad.data_ptr())
+        barrier()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(args.steps):
+            A.adjoint_backward_device(U.data_ptr(), V64.data_ptr(), lam.data_ptr(), KTl.data_ptr(), grad.data_ptr())
+        a1.record(stream)
+        barrier()
+        bms = a0.elapsed_time(a1) / args.steps
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        A.adjoint_forward_device(gl.data_ptr(), U.data_ptr(), R.data_ptr(), V64.data_ptr(), "fp64")
+        f1.record(stream)
+        barrier()
+        fms = f0.elapsed_time(f1)
+        A.set_element_log_scale(None)
+        adjoint = {"grads_per_s": round(1000.0 / bms, 2), "backward_ms": round(bms, 3),
+                   "forward_ms": round(fms, 3), "parameters": nel,
+                   "definition": "assembly-side adjoint: one gradient = dR/dg VJP (s_e = exp(g_e) per element) + "
+                                 "K^T lambda on the FP64 CSR tangent, lambda given; the adjoint linear solve "
+                                 "K^T lambda = dJ/dU is the caller's (PETSc KSP in the reference application)"}
+
+    batch = None
+    if not args.no_batch:
+        batch = bench_batch(args, dev, local, barrier)
+
     # ---- roofline of the dominant kernel (tangent volume, 8 colour launches per step)
     tan_ms = k64[2]
     nlaunch = max(k64[5], 1)
@@ -358,7 +471,8 @@ def run_ours(args):
             "phases_ms": {"residual_volume": round(k64[0], 3), "residual_bc": round(k64[1], 3),
                           "tangent_volume": round(k64[2], 3), "tangent_dirichlet": round(k64[3], 3)},
             "residual_tflops_alg": round(res_tf, 3) if res_tf else None,
-            "adjoint_grads_per_s": None,
+            "adjoint_grads_per_s": adjoint["grads_per_s"] if adjoint else None, "adjoint": adjoint,
+            "schedule": schedule, "batch_config3": batch,
             "clocks": clk, "gpu_launches": int(launches64), "roofline": roofline,
             "peaks_measured": {"fp64_tflops": round(peak64, 2), "fp32_tflops": round(peak32, 2)},
             "e2e": e2e}

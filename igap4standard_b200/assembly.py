@@ -8,6 +8,7 @@ from .native import IgabMeshDesc, check, vp
 PHYS = {"ge": 0, "getime": 1}
 PREC = {"fp64": 0, "fp32": 1}
 OPT_TANGENT_FP64_KERNEL = 1
+OPT_TANGENT_FP32_KERNEL = 2
 
 
 def _ptr(a):
@@ -111,6 +112,26 @@ class Assembly:
 
     def set_tile(self, residual_tile=0, tangent_tile=0):
         check(self.lib, "igab_set_tile", self.lib.igab_set_tile(self.h, residual_tile, tangent_tile))
+
+    def autotune(self, U_ptr=None, what=7, reps=3, cache=None):
+        """Time every candidate schedule (igab_autotune) and keep the fastest; with a
+        cache file, a schedule stored for this GPU and mesh is applied without timing.
+        Returns dict(residual_tile, tangent_fp64_kernel, tangent_fp32_kernel, *_ms, cached)."""
+        from . import tuning
+        key = tuning.mesh_key(self.device, self.nelem, self.phys, what) if cache else None
+        hit = tuning.load(cache).get(key) if cache else None
+        if hit:
+            self.set_tile(hit["residual_tile"], 0)
+            self.set_option(OPT_TANGENT_FP64_KERNEL, hit["tangent_fp64_kernel"])
+            self.set_option(OPT_TANGENT_FP32_KERNEL, hit["tangent_fp32_kernel"])
+            return dict(hit, cached=True)
+        r = native.IgabTuneResult()
+        check(self.lib, "igab_autotune",
+              self.lib.igab_autotune(self.h, vp(U_ptr or 0), int(what), int(reps), ctypes.byref(r)))
+        out = {f: getattr(r, f) for f, _ in native.IgabTuneResult._fields_}
+        if cache:
+            tuning.store(cache, key, out)
+        return dict(out, cached=False)
 
     # ---- host-pointer assembly
     def residual(self, U, out=None):

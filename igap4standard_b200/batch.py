@@ -37,6 +37,7 @@ class Batch:
         check(self.lib, "igab_batch_create", self.lib.igab_batch_create(descs, len(inst), int(device), ctypes.byref(h)))
         self.h = h
         self.n = len(inst)
+        self.sizes = [tuple(int(x) for x in c["nelem"]) for c in inst]
         self.device = int(device)
         nd, nz, ne = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()
         self.dof_offsets = np.zeros(self.n + 1, dtype=np.int64)
@@ -78,6 +79,23 @@ class Batch:
         v = [ctypes.c_int() for _ in range(4)]
         check(self.lib, "igab_batch_get_schedule", self.lib.igab_batch_get_schedule(self.h, *[ctypes.byref(x) for x in v]))
         return tuple(x.value for x in v)
+
+    def autotune(self, U_ptr=None, what=7, reps=2, cache=None):
+        """Time the candidate batch schedules (igab_batch_autotune) and keep the fastest;
+        with a cache file, a schedule stored for this GPU and batch shape is applied."""
+        from . import tuning
+        key = tuning.batch_key(self.device, self.sizes, what) if cache else None
+        hit = tuning.load(cache).get(key) if cache else None
+        if hit:
+            self.set_schedule(hit["ctas_res"], hit["ctas_tan64"], hit["ctas_tan32"], hit["order"])
+            return dict(hit, cached=True)
+        r = native.IgabBatchTuneResult()
+        check(self.lib, "igab_batch_autotune",
+              self.lib.igab_batch_autotune(self.h, vp(U_ptr or 0), int(what), int(reps), ctypes.byref(r)))
+        out = {f: getattr(r, f) for f, _ in native.IgabBatchTuneResult._fields_}
+        if cache:
+            tuning.store(cache, key, out)
+        return dict(out, cached=False)
 
     def set_stream(self, stream_ptr):
         check(self.lib, "igab_batch_set_stream", self.lib.igab_batch_set_stream(self.h, vp(stream_ptr)))

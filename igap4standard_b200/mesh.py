@@ -95,15 +95,16 @@ def nnz_of(nelem):
 
 
 def batch_config3(n_instances=512, seed=3, nmin=6, nmax=24, perturb=0.0):
-    """Seeded instances of the batched static workload: elements per side uniform in
-    [nmin, nmax] (per direction), lambda and mu lognormal(0, 0.25), strain-gradient
+    """Seeded instances of the batched static workload: n^3 elements with n uniform
+    in [nmin, nmax] per instance, lambda and mu lognormal(0, 0.25), strain-gradient
     length uniform in [0.05, 0.2], BCs of bc_config0.  Returns a list of dicts
     (nelem, knots, par_mat, bc_type, par_dirichlet)."""
     rng = np.random.default_rng(seed)
     out = []
     bc, pd = bc_config0()
     for _ in range(n_instances):
-        nelem = tuple(int(x) for x in rng.integers(nmin, nmax + 1, 3))
+        n = int(rng.integers(nmin, nmax + 1))
+        nelem = (n, n, n)
         lam, mu = np.exp(rng.normal(0.0, 0.25, 2))
         ell = rng.uniform(0.05, 0.2)
         kseed = int(rng.integers(0, 2 ** 31 - 1))

@@ -28,6 +28,20 @@ class IgabError(RuntimeError):
         self.code = code
 
 
+class IgabTuneResult(ctypes.Structure):
+    """igab_tune_result of include/igab.h"""
+    _fields_ = [("residual_tile", ctypes.c_int), ("tangent_fp64_kernel", ctypes.c_int),
+                ("tangent_fp32_kernel", ctypes.c_int), ("residual_ms", ctypes.c_double),
+                ("tangent_fp64_ms", ctypes.c_double), ("tangent_fp32_ms", ctypes.c_double)]
+
+
+class IgabBatchTuneResult(ctypes.Structure):
+    """igab_batch_tune_result of include/igab.h"""
+    _fields_ = [("ctas_res", ctypes.c_int), ("ctas_tan64", ctypes.c_int), ("ctas_tan32", ctypes.c_int),
+                ("order", ctypes.c_int), ("residual_ms", ctypes.c_double), ("tangent_fp64_ms", ctypes.c_double),
+                ("tangent_fp32_ms", ctypes.c_double)]
+
+
 class IgabMeshDesc(ctypes.Structure):
     """igab_mesh_desc of include/igab.h"""
     _fields_ = [
@@ -93,6 +107,8 @@ IGAB_API = [
     ("igab_batch_last_launch_count", ctypes.c_int, [vp, c_int_p]),
     ("igab_batch_graph_capture", ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int]),
     ("igab_batch_graph_launch", ctypes.c_int, [vp]),
+    ("igab_autotune", ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(IgabTuneResult)]),
+    ("igab_batch_autotune", ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(IgabBatchTuneResult)]),
 ]
 
 # entry points of include/snesiga_b200.h and include/iga_case.h

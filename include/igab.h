@@ -154,6 +154,17 @@ int igab_adjoint_forward(igab_ctx *ctx, const double *g_dev, const double *U_dev
 int igab_adjoint_backward(igab_ctx *ctx, const double *U_dev, const void *vals_dev, int prec,
                           const double *lam_dev, double *KTlam_dev, double *grad_dev);
 
+/* ---- autotuner (no reference counterpart): times every candidate schedule on this
+ * mesh and state (U_dev; NULL = zero state) with CUDA events on the context stream,
+ * reps timed runs after one warm-up, and leaves the fastest applied.  what: bit 0
+ * residual (tile edge 2 or 4), bit 1 FP64 tangent (tensor path or FMA pipe), bit 2
+ * FP32 tangent (tcgen05 or FMA pipe).  Times of the chosen candidates in ms. */
+typedef struct {
+    int residual_tile, tangent_fp64_kernel, tangent_fp32_kernel;
+    double residual_ms, tangent_fp64_ms, tangent_fp32_ms;
+} igab_tune_result;
+int igab_autotune(igab_ctx *ctx, const double *U_dev, int what, int reps, igab_tune_result *out);
+
 /* ---- batched assembly: many independent meshes of uneven size, each with its own
  * material constants and boundary tables, assembled by one persistent launch per
  * operator (no reference counterpart: the reference runs one mesh per process; each
@@ -182,6 +193,14 @@ int igab_batch_last_launch_count(const igab_batch *b, int *n);
 /* one Newton iteration's assembly (residual then tangent) captured in a CUDA graph */
 int igab_batch_graph_capture(igab_batch *b, const double *U_dev, double *R_dev, void *vals_dev, int prec);
 int igab_batch_graph_launch(igab_batch *b);
+/* autotuner of the batch schedule: CTAs per SM of each persistent kernel and the
+ * instance order (what: bit 0 residual, bit 1 FP64 tangent, bit 2 FP32 tangent);
+ * the fastest schedule is left applied. */
+typedef struct {
+    int ctas_res, ctas_tan64, ctas_tan32, order;
+    double residual_ms, tangent_fp64_ms, tangent_fp32_ms;
+} igab_batch_tune_result;
+int igab_batch_autotune(igab_batch *b, const double *U_dev, int what, int reps, igab_batch_tune_result *out);
 
 /* ---- residual for callers that cannot have the library allocate device memory.
  * No counterpart in the reference.  Same result as igab_residual, but U and R

@@ -102,6 +102,10 @@ class Assembly:
         a = np.ascontiguousarray(U, dtype=np.float64)
         check(self.lib, "igab_set_history", self.lib.igab_set_history(self.h, int(level), _ptr(a), 0))
 
+    def set_history_device(self, level, U_ptr):
+        """History level (1 = t_n, 2 = t_{n-1}) from a device pointer (copied in place)."""
+        check(self.lib, "igab_set_history", self.lib.igab_set_history(self.h, int(level), vp(U_ptr), 1))
+
     def set_option(self, option, value):
         check(self.lib, "igab_set_option", self.lib.igab_set_option(self.h, int(option), int(value)))
 

@@ -75,6 +75,15 @@ def bc_config0():
     return bc, pd
 
 
+def bc_transient():
+    """BCs of the transient workload: face 0 (x=0) u = 0 and du/dn = 0; every other
+    face traction-driven (the x = 1 traction is the Neumann value of face 1, order 0,
+    dof x).  Returns (bc_type[36], par_dirichlet[9] = 0)."""
+    bc = np.ones(36, dtype=np.int32)
+    bc[0:6] = 0
+    return bc, np.zeros(9)
+
+
 def bc_example():
     """bc_init of the reference example (example/ex1/main.c:69-95): u = 0 on every
     face, high-order Neumann everywhere."""

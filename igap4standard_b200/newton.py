@@ -50,6 +50,13 @@ class NewtonResult:
     line_search_lambdas: list = field(default_factory=list)
 
 
+def _norm(v):
+    """2-norm of a numpy array or a torch tensor (device-resident drivers pass tensors)."""
+    if hasattr(v, "detach"):
+        return float(v.norm())
+    return float(np.linalg.norm(v))
+
+
 class _Counted:
     def __init__(self, fn):
         self.fn, self.n = fn, 0
@@ -64,7 +71,7 @@ def backtrack(residual, X, F, fnorm, Y, JY, alpha=1e-4, minlambda=1e-12, maxstep
 
     JY is J @ Y with the Jacobian the step was solved with; the slope of
     0.5||F||^2 along -Y is -(F, JY), forced negative as PETSc does."""
-    ynorm = np.linalg.norm(Y)
+    ynorm = _norm(Y)
     if ynorm > maxstep:
         Y = Y * (maxstep / ynorm)
         JY = JY * (maxstep / ynorm)
@@ -76,7 +83,7 @@ def backtrack(residual, X, F, fnorm, Y, JY, alpha=1e-4, minlambda=1e-12, maxstep
     lam = 1.0
     W = X - Y
     G = residual(W)
-    gnorm = float(np.linalg.norm(G))
+    gnorm = _norm(G)
     if not np.isfinite(gnorm):
         return W, G, gnorm, lam, False
     if 0.5 * gnorm * gnorm <= 0.5 * fnorm * fnorm + lam * alpha * initslope:
@@ -88,7 +95,7 @@ def backtrack(residual, X, F, fnorm, Y, JY, alpha=1e-4, minlambda=1e-12, maxstep
     W = X - lam * Y
     G = residual(W)
     gprev, lamprev = gnorm, 1.0
-    gnorm = float(np.linalg.norm(G))
+    gnorm = _norm(G)
     if np.isfinite(gnorm) and 0.5 * gnorm * gnorm <= 0.5 * fnorm * fnorm + lam * alpha * initslope:
         return W, G, gnorm, lam, True
     # cubic backtracks
@@ -106,7 +113,7 @@ def backtrack(residual, X, F, fnorm, Y, JY, alpha=1e-4, minlambda=1e-12, maxstep
         lam = 0.1 * lam if lamtemp <= 0.1 * lam else lamtemp
         W = X - lam * Y
         G = residual(W)
-        gnorm = float(np.linalg.norm(G))
+        gnorm = _norm(G)
         if np.isfinite(gnorm) and 0.5 * gnorm * gnorm <= 0.5 * fnorm * fnorm + lam * alpha * initslope:
             return W, G, gnorm, lam, True
     return W, G, gnorm, lam, False

@@ -1,0 +1,234 @@
+"""Device-resident time stepping of the transient physics (phys/getime) with the
+reference application's solver semantics.
+
+Per time step the reference example (example/ex1/main.c:48-56) takes the
+previous solution as initial guess (initguess, :116-126), runs snes_solve
+(src/snes_solve.c:23-33: one Newton step per SNESSolve, absolute ||F||_2 <=
+1e-10, stagnation stop) and shifts the history levels, U_hist[k] <- U_hist[k-1]
+for k = torder..1 (:55).  This module does the same on the GPU:
+
+  - the residual + tangent assembly of one Newton iteration is captured once in a
+    CUDA graph at fixed device buffers (the iterate lives in the captured U
+    buffer) and replayed every iteration; history levels and tractions are
+    updated in place, which replays pick up;
+  - the line search is newton.backtrack (Dennis & Schnabel A6.3.1, as PETSc's
+    SNESLINESEARCHBT), on device tensors;
+  - the linear solve is Jacobi-preconditioned BiCGStab (van der Vorst, SIAM J.
+    Sci. Stat. Comput. 13 (1992) 631-644) whose operator is the library's own
+    structured K^T x kernel (K is symmetric after the symmetric Dirichlet
+    elimination, so K^T x = K x).  The reference solves with PETSc GMRES + ASM
+    (src/snes_init.c:24-39), which is outside the assembly path; this solver is
+    the driver's stand-in for it.
+
+The traction of the transient workload is 0.01 sin(2 pi t) on face x = 1 in
+the x direction (face 1, standard order, dof 0), evaluated at t_{n+1}.
+"""
+import numpy as np
+
+from . import newton
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class DeviceProblem:
+    """Residual / tangent / K x of one Assembly on device tensors (FP64 vectors)."""
+
+    def __init__(self, A, prec="fp32", use_graph=True):
+        torch = _torch()
+        self.A, self.prec = A, prec
+        self.dev = torch.device("cuda", A.device)
+        # a dedicated stream (graph capture needs one); torch vector work runs on it too
+        self.stream = torch.cuda.Stream(device=self.dev)
+        A.set_stream(self.stream.cuda_stream)
+        n, nnz = A.ndof, A.nnz
+        with torch.cuda.stream(self.stream):
+            self.X = torch.zeros(n, dtype=torch.float64, device=self.dev)     # captured U buffer (the iterate)
+            self.R = torch.zeros(n, dtype=torch.float64, device=self.dev)
+            self.V = torch.zeros(nnz, dtype=torch.float64 if prec == "fp64" else torch.float32, device=self.dev)
+            self.Rt = torch.zeros(n, dtype=torch.float64, device=self.dev)    # line-search residuals
+        self.stream.synchronize()
+        rowptr, cols = A.pattern()
+        rows = np.repeat(np.arange(n), np.diff(rowptr))
+        self.diag_pos = torch.as_tensor(np.nonzero(cols == rows)[0], device=self.dev)
+        self.use_graph = use_graph
+        self.captured = False
+        self.n_assembly = 0
+        self.n_residual = 0
+        self.krylov_its = []
+
+    def capture(self):
+        torch = _torch()
+        torch.cuda.synchronize(self.dev)
+        self.A.graph_capture(self.X.data_ptr(), self.R.data_ptr(), self.V.data_ptr(), self.prec)
+        self.captured = True
+
+    def assemble(self):
+        """R and the tangent at the iterate X (graph replay or eager launches)."""
+        if self.use_graph:
+            if not self.captured:
+                self.capture()
+            self.A.graph_launch()
+        else:
+            self.A.residual_device(self.X.data_ptr(), self.R.data_ptr())
+            self.A.tangent_device(self.X.data_ptr(), self.V.data_ptr(), self.prec)
+        self.n_assembly += 1
+        return self.R
+
+    def residual(self, W):
+        torch = _torch()
+        W = W.contiguous()
+        out = torch.empty_like(self.Rt)
+        self.A.residual_device(W.data_ptr(), out.data_ptr())
+        self.n_residual += 1
+        return out
+
+    def matvec(self, x, y=None):
+        torch = _torch()
+        x = x.contiguous()
+        y = torch.empty_like(x) if y is None else y
+        self.A.adjoint_backward_device(None, self.V.data_ptr(), x.data_ptr(), y.data_ptr(), None, self.prec)
+        return y
+
+    def diagonal(self):
+        return self.V[self.diag_pos].to(_torch().float64)
+
+
+def bicgstab(matvec, b, dinv, rtol=1e-5, atol=0.0, maxit=2000):
+    """Right-preconditioned BiCGStab (M = diag); returns (x, iterations, converged).
+    Stops when ||b - A x|| <= max(rtol ||b||, atol)."""
+    torch = _torch()
+    x = torch.zeros_like(b)
+    r = b.clone()
+    bnorm = float(b.norm())
+    if bnorm == 0.0:
+        return x, 0, True
+    tol = max(rtol * bnorm, atol)
+    rhat = r.clone()
+    rho = alpha = omega = 1.0
+    v = torch.zeros_like(b)
+    p = torch.zeros_like(b)
+    for it in range(1, maxit + 1):
+        rho_new = float(torch.dot(rhat, r))
+        if rho_new == 0.0:
+            return x, it, False
+        beta = (rho_new / rho) * (alpha / omega) if it > 1 else 0.0
+        p = r + beta * (p - omega * v) if it > 1 else r.clone()
+        phat = dinv * p
+        v = matvec(phat)
+        den = float(torch.dot(rhat, v))
+        if den == 0.0:
+            return x, it, False
+        alpha = rho_new / den
+        s = r - alpha * v
+        if float(s.norm()) <= tol:
+            x += alpha * phat
+            return x, it, True
+        shat = dinv * s
+        t = matvec(shat)
+        tt = float(torch.dot(t, t))
+        omega = float(torch.dot(t, s)) / tt if tt > 0 else 0.0
+        x += alpha * phat + omega * shat
+        r = s - omega * t
+        rho = rho_new
+        if float(r.norm()) <= tol:
+            return x, it, True
+        if omega == 0.0:
+            return x, it, False
+    return x, maxit, False
+
+
+def newton_device(P, rtol_lin=1e-5, max_subiter=newton.MAX_SUBITER):
+    """snes_solve semantics on device tensors; the iterate is P.X (updated in place)."""
+    torch = _torch()
+    res = newton.NewtonResult(U=None, converged=False, reason=newton.DIVERGED_MAX_IT, iterations=0)
+    f_old = 999.0
+    reason = newton.DIVERGED_MAX_IT
+    for _ in range(max_subiter):
+        F = P.assemble().clone()
+        fnorm = float(F.norm())
+        if not np.isfinite(fnorm):
+            reason = newton.DIVERGED_FNORM_NAN
+        elif fnorm < newton.ABS_TOL:
+            reason = newton.CONVERGED_FNORM_ABS
+        else:
+            ttol = fnorm * newton.REL_TOL
+            d = P.diagonal()
+            dinv = torch.where(d != 0, 1.0 / d, torch.ones_like(d))
+            Y, its, _ = bicgstab(P.matvec, F, dinv, rtol=rtol_lin)
+            P.krylov_its.append(its)
+            JY = P.matvec(Y)
+            xnorm = float(P.X.norm())
+            Xn, F, fnorm, lam, ok = newton.backtrack(P.residual, P.X, F, fnorm, Y, JY)
+            P.X.copy_(Xn)
+            res.line_search_lambdas.append(lam)
+            res.iterations += 1
+            snorm = lam * float(Y.norm())
+            if not ok:
+                reason = newton.DIVERGED_LINE_SEARCH
+            elif not np.isfinite(fnorm):
+                reason = newton.DIVERGED_FNORM_NAN
+            elif fnorm < newton.ABS_TOL:
+                reason = newton.CONVERGED_FNORM_ABS
+            elif fnorm <= ttol:
+                reason = newton.CONVERGED_FNORM_RELATIVE
+            elif snorm < newton.STEP_TOL * xnorm:
+                reason = newton.CONVERGED_SNORM_RELATIVE
+            else:
+                reason = newton.DIVERGED_MAX_IT
+        if abs(f_old - fnorm) / f_old < newton.STAGNATION:   # src/snes_solve.c:29
+            reason = newton.DIVERGED_LINE_SEARCH
+        f_old = fnorm
+        res.fnorms.append(fnorm)
+        if reason != newton.DIVERGED_MAX_IT:
+            break
+    res.reason = reason
+    res.converged = reason > 0
+    return res
+
+
+def traction_values(A, t, amplitude=0.01, face=1, order=0, dof=0):
+    """Surface-point values of the transient traction amplitude sin(2 pi t) on (face, order, dof)."""
+    xyz, meta = A.neumann_points()
+    val = amplitude * np.sin(2.0 * np.pi * t)
+    sel = (meta[:, 0] == face) & (meta[:, 1] == order) & (meta[:, 2] == dof)
+    return np.where(sel, val, 0.0)
+
+
+def run(A, nsteps, dt, prec="fp32", use_graph=True, rtol_lin=1e-5, traction=traction_values, U_init=None,
+        U_prev=None, callback=None):
+    """Time-step A (an Assembly with phys="getime") nsteps times from the history
+    (U_init at t_0, U_prev at t_{-1}; zeros by default).  Returns (history of U per
+    step as host arrays, per-step NewtonResults, DeviceProblem)."""
+    torch = _torch()
+    P = DeviceProblem(A, prec, use_graph)
+    with torch.cuda.stream(P.stream):
+        return _run(P, A, nsteps, dt, rtol_lin, traction, U_init, U_prev, callback)
+
+
+def _run(P, A, nsteps, dt, rtol_lin, traction, U_init, U_prev, callback):
+    torch = _torch()
+    n = A.ndof
+    h1 = torch.zeros(n, dtype=torch.float64, device=P.dev)   # U at t_n     (U_hist level 1)
+    h0 = torch.zeros(n, dtype=torch.float64, device=P.dev)   # U at t_{n-1} (U_hist level 2)
+    if U_init is not None:
+        h1.copy_(torch.as_tensor(np.asarray(U_init, dtype=np.float64)))
+    if U_prev is not None:
+        h0.copy_(torch.as_tensor(np.asarray(U_prev, dtype=np.float64)))
+    hist, results = [], []
+    for step in range(nsteps):
+        t = (step + 1) * dt
+        A.set_neumann_values(traction(A, t))
+        A.set_history_device(1, h1.data_ptr())
+        A.set_history_device(2, h0.data_ptr())
+        P.X.copy_(h1)                                   # initguess: U <- U_hist[1]
+        r = newton_device(P, rtol_lin=rtol_lin)
+        results.append(r)
+        h0.copy_(h1)                                    # history shift (main.c:55)
+        h1.copy_(P.X)
+        hist.append(P.X.cpu().numpy())
+        if callback:
+            callback(step, r)
+    return hist, results, P

@@ -338,7 +338,7 @@ def run_ours(args):
     dev = torch.device("cuda", local)
 
     from igap4standard_b200 import Assembly
-    from igap4standard_b200.assembly import fma_peak_tflops
+    from igap4standard_b200.assembly import fma_peak_tflops, tc_peak_tflops
 
     n = args.n
     nelem, kn, pm, bc, pd = workload(n)
@@ -394,6 +394,8 @@ def run_ours(args):
         schedule.pop("cached", None)
     peak64 = fma_peak_tflops("fp64", local)
     peak32 = fma_peak_tflops("fp32", local)
+    peak_tf32 = tc_peak_tflops(256, local)
+    peak_tf32_n96 = tc_peak_tflops(96, local)
     clocks = ClockSampler(local)
     clocks.start()
     t64, k64, launches64 = timed("fp64", args.steps, args.warmup)
@@ -493,6 +495,22 @@ def run_ours(args):
                 "executed_tflops": round(executed, 3),
                 "peak_source": "measured FP64 FMA probe (igab_fma_peak), burst; MEASURED_PEAKS.json has no FP64"}
     res_tf = nel * RES_ALG_FLOPS / (k64[0] * 1e-3) / 1e12 if k64[0] > 0 else None
+    # FP32 (mixed) tangent on tcgen05: per element 768 curvature rows in chunks of 32 (about 25 chunks,
+    # 8 MMAs M128 x N96 x K8 each) plus 12 geometric chunks of 12 MMAs M128 x N32 x K8
+    tc_exec_per_el = 25 * 8 * 2 * 128 * 96 * 8 + 12 * 12 * 2 * 128 * 32 * 8
+    tan32_ms = k32[2]
+    nl32 = max(k32[5], 1)
+    roofline_mixed = {"bound": "tensor", "pipe": "TF32 tcgen05 (hi/lo split, FP32 accumulation)",
+                      "kernel": "k_tan_tc32<2>", "avg_launch_ms": round(tan32_ms / nl32, 3),
+                      "achieved": round(nel * TAN_ALG_FLOPS / (tan32_ms * 1e-3) / 1e12, 3),
+                      "executed_tflops": round(nel * tc_exec_per_el / (tan32_ms * 1e-3) / 1e12, 3),
+                      "peak": round(peak_tf32, 1), "peak_at_kernel_shape": round(peak_tf32_n96, 1),
+                      "unit": "TFLOP/s",
+                      "frac": round(nel * TAN_ALG_FLOPS / (tan32_ms * 1e-3) / 1e12 / peak_tf32, 4),
+                      "frac_executed_of_shape_peak": round(nel * tc_exec_per_el / (tan32_ms * 1e-3) / 1e12
+                                                           / peak_tf32_n96, 4),
+                      "peak_source": "measured: igab_tc_peak (back-to-back tcgen05.mma kind::tf32, M128 x N256 / "
+                                     "N96, one CTA per SM)"}
 
     line = {"metric": METRIC, "value": round(t64 / world, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t64, 3), "higher_is_better": False, "scaling": "weak",
@@ -506,7 +524,9 @@ def run_ours(args):
             "adjoint_grads_per_s": adjoint["grads_per_s"] if adjoint else None, "adjoint": adjoint,
             "schedule": schedule, "batch_config3": batch, "transient_config2": trans,
             "clocks": clk, "gpu_launches": int(launches64), "roofline": roofline,
-            "peaks_measured": {"fp64_tflops": round(peak64, 2), "fp32_tflops": round(peak32, 2)},
+            "roofline_mixed": roofline_mixed,
+            "peaks_measured": {"fp64_tflops": round(peak64, 2), "fp32_tflops": round(peak32, 2),
+                               "tf32_tensor_tflops": round(peak_tf32, 1), "tf32_tensor_n96_tflops": round(peak_tf32_n96, 1)},
             "e2e": e2e}
 
     if rank == 0 and not args.no_cpu:

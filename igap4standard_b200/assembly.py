@@ -238,6 +238,14 @@ class Assembly:
         return list(ms)
 
 
+def tc_peak_tflops(n_cols=256, device=0):
+    """Measured dense TF32 tcgen05 throughput for M 128 x N n_cols MMAs (igab_tc_peak)."""
+    lib = native.lib_cuda()
+    t = ctypes.c_double()
+    check(lib, "igab_tc_peak", lib.igab_tc_peak(int(device), int(n_cols), ctypes.byref(t)))
+    return t.value
+
+
 def fma_peak_tflops(prec="fp64", device=0):
     lib = native.lib_cuda()
     t = ctypes.c_double()

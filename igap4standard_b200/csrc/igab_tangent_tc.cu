@@ -683,7 +683,101 @@ __global__ void __launch_bounds__(128) k_tc_selftest(float *out, int *status)
     }
 }
 
+/* ---------------------------------------------------------------- peak probe
+ * One CTA per SM, one thread issues `reps` back-to-back tcgen05.mma kind::tf32
+ * M 128 x N n x K 8 into one accumulator (operands: zeros in shared memory). */
+template <int N>
+__global__ void __launch_bounds__(128) k_tc_peak(int reps, int *status)
+{
+    extern __shared__ __align__(128) unsigned char sm[];
+    __shared__ unsigned long long bar;
+    __shared__ unsigned int tb;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    for (int i = tid; i < 49152 / 4; i += blockDim.x) reinterpret_cast<float *>(sm)[i] = 0.f;
+    if (tid == 0) {
+        tc_mbar_init(&bar, 1);
+        tc_fence_mbar_init();
+    }
+    if (warp == 0) tc_alloc(&tb, 256);
+    tc_fence_proxy_async();
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    const uint32_t tm = tb;
+    if (tid == 0) {
+        const uint32_t sa = tc_smem_u32(sm), sb = sa + 16384;
+        for (int r = 0; r < reps; r++)
+            tc_mma_tf32(tm, tc_sdesc(sa + (r & 3) * TC_KSTEP_BYTES), tc_sdesc(sb + (r & 3) * TC_KSTEP_BYTES),
+                        tc_idesc_tf32(128, N), r > 0);
+        tc_commit(&bar);
+        if (!tc_mbar_wait(&bar, 0)) atomicOr(status, 1);
+    }
+    tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after_sync();
+        tc_dealloc(tm, 256);
+    }
+}
+
+template <int N>
+int tc_peak_run(int nsm, double *tflops)
+{
+    const int reps = 4096;
+    const size_t smem = 200000;   /* one CTA per SM */
+    int *st = nullptr;
+    IGAB_CUDA_TRY(cudaMalloc((void **)&st, sizeof(int)));
+    cudaError_t e = cudaMemset(st, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_tc_peak<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    if (e == cudaSuccess) {
+        k_tc_peak<N><<<nsm, 128, smem>>>(reps, st);   /* warm-up */
+        cudaEventRecord(a);
+        k_tc_peak<N><<<nsm, 128, smem>>>(reps, st);
+        cudaEventRecord(b);
+        e = cudaEventSynchronize(b);
+    }
+    float ms = 0.f;
+    int hs = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    if (e == cudaSuccess) e = cudaMemcpy(&hs, st, sizeof(int), cudaMemcpyDeviceToHost);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    cudaFree(st);
+    if (e != cudaSuccess) {
+        igab_set_error("igab_tc_peak: %s", cudaGetErrorString(e));
+        return IGAB_ERR_CUDA;
+    }
+    if (hs) {
+        igab_set_error("igab_tc_peak: completion wait timed out");
+        return IGAB_ERR_CUDA;
+    }
+    *tflops = 2.0 * 128 * N * 8 * (double)reps * nsm / (ms * 1e-3) / 1e12;
+    return 0;
+}
+
 } /* namespace */
+
+extern "C" int igab_tc_peak(int device, int n_cols, double *tflops)
+{
+    if (!tflops) {
+        igab_set_error("igab_tc_peak: null output");
+        return IGAB_ERR_ARG;
+    }
+    IGAB_CUDA_TRY(cudaSetDevice(device));
+    int nsm = 0;
+    IGAB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    switch (n_cols) {
+    case 32: return tc_peak_run<32>(nsm, tflops);
+    case 96: return tc_peak_run<96>(nsm, tflops);
+    case 256: return tc_peak_run<256>(nsm, tflops);
+    default:
+        igab_set_error("igab_tc_peak: n_cols must be 32, 96 or 256");
+        return IGAB_ERR_ARG;
+    }
+}
 
 int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv)
 {

@@ -127,6 +127,10 @@ int igab_fma_peak(int device, int prec, double *tflops);
  * B (96 x 32) with the M 128 / N 96 and M 128 / N 32 instruction shapes; out (128 x 128 floats,
  * row-major) receives accumulator columns 0-95 (A B^T) and 96-127 (A B[0:32]^T). */
 int igab_tc_selftest(int device, float *out);
+/* TF32 tensor-core throughput probe (TFLOP/s, dense): one CTA per SM issuing back-to-back
+ * tcgen05.mma kind::tf32 M 128 x N n_cols x K 8 (n_cols 32, 96 = the FP32 tangent's
+ * shapes, or 256 = full width); no reference counterpart. */
+int igab_tc_peak(int device, int n_cols, double *tflops);
 
 /* ---- CUDA graphs: capture one assembly at fixed device pointers, replay it.
  * what: 1 residual, 2 tangent, 3 both (residual then tangent).  Parameters

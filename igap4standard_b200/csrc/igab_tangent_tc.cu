@@ -47,7 +47,9 @@
 
 namespace {
 
-#define TCN_THR 288            /* 9 warps: one builder task per thread per chunk */
+#define TCN_BLD 288            /* builder warps 0-8: one operand task per thread per chunk */
+#define TCN_THR 320            /* + warp 9: the MMA issuer */
+#define TC_BAR_BLD 1           /* named barrier of the builder warps */
 #define TC_STAGE 24576         /* bytes per operand stage */
 #define TC_MAIN_LO 11264       /* 2 Y_lo after Y_hi (11 groups of 8 rows) */
 #define TC_G_ULO 4096          /* Gamma chunk: U_hi 0, U_lo, V_hi, V_lo (4 groups each) */
@@ -85,7 +87,11 @@ struct tc_smem {
     int part[2][2];                     /* per-warp bucket counts for the scan */
     long rbase[81];                     /* CSR row bases of the element matrix (elem_row_base) */
     int rsx[81], rsy[81];
-    unsigned long long mbar[2];
+    unsigned long long full[2];         /* stage b written (288 builder arrivals) */
+    unsigned long long done[2];         /* MMAs of the chunk in stage / accumulator b completed (commit) */
+    unsigned long long freed[2];        /* accumulator b read out (288 builder arrivals) */
+    unsigned long long drain;           /* issuer: every MMA it issued has completed */
+    int ckind[2];                       /* chunk in stage b: 0 positive rows, 1 negative rows, 2 Gamma, 3 end of tile */
     unsigned int tmem_base;
     int abort_flag;
 };
@@ -189,12 +195,14 @@ __device__ __forceinline__ void tc_accumulate(uint32_t tmem, int buf, int kind, 
     }
 }
 
-/* pipeline state of a CTA, carried across the tiles it processes */
+/* pipeline state of a thread, carried across the tiles its CTA processes: the
+ * builders track the commits they wait for, the issuer the arrivals it waits for */
 struct tc_state {
-    bool pend[2];      /* a commit on stage/accumulator b is not yet waited for */
-    int kind[2];       /* chunk in flight per stage: 0 positive rows, 1 negative rows, 2 Gamma */
-    uint32_t ph[2];    /* parity of the next phase to wait for on mbar[b] */
-    int gc;            /* chunks issued by this CTA */
+    uint32_t ph_done[2];   /* builders: parity of the next wait on done[b] */
+    uint32_t ph_full[2];   /* issuer: parity of the next wait on full[b] */
+    uint32_t ph_free[2];   /* issuer: parity of the next wait on freed[b] */
+    uint32_t ph_drain;
+    int gc;                /* chunks (with MMAs) so far */
     bool aborted;
     uint32_t tmem;
 };
@@ -205,8 +213,12 @@ __device__ __forceinline__ void tc_setup(tc_smem<TE> &S, tc_state &Q)
 {
     const int tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0) {
-        tc_mbar_init(&S.mbar[0], 1);
-        tc_mbar_init(&S.mbar[1], 1);
+        for (int b = 0; b < 2; b++) {
+            tc_mbar_init(&S.full[b], TCN_BLD);
+            tc_mbar_init(&S.done[b], 1);
+            tc_mbar_init(&S.freed[b], TCN_BLD);
+        }
+        tc_mbar_init(&S.drain, 1);
         tc_fence_mbar_init();
         S.abort_flag = 0;
     }
@@ -215,32 +227,94 @@ __device__ __forceinline__ void tc_setup(tc_smem<TE> &S, tc_state &Q)
     __syncthreads();
     tc_fence_after_sync();
     Q.tmem = S.tmem_base;
-    Q.pend[0] = Q.pend[1] = false;
-    Q.kind[0] = Q.kind[1] = 0;
-    Q.ph[0] = Q.ph[1] = 0u;
+    Q.ph_done[0] = Q.ph_done[1] = Q.ph_full[0] = Q.ph_full[1] = Q.ph_free[0] = Q.ph_free[1] = 0u;
+    Q.ph_drain = 0u;
     Q.gc = 0;
     Q.aborted = false;
 }
 
-/* release: wait (bounded) for MMAs still in flight after an abort, free the tensor memory */
+/* release (all threads): the issuer has drained its MMAs; free the tensor memory */
 template <int TE>
 __device__ __forceinline__ void tc_release(tc_smem<TE> &S, tc_state &Q, int *status)
 {
     const int tid = threadIdx.x, warp = tid >> 5;
-    if (Q.aborted && tid == 0) {
-        atomicOr(status, 1);
-        for (int b = 0; b < 2; b++)
-            if (Q.pend[b]) tc_mbar_wait(&S.mbar[b], Q.ph[b]);
-    }
     tc_fence_before_sync();
     __syncthreads();
+    if (tid == 0 && S.abort_flag) atomicOr(status, 1);
     if (warp == 0) {
         tc_fence_after_sync();
         tc_dealloc(Q.tmem, TC_TMEM_COLS);
     }
 }
 
-/* one tile of up to TE^3 elements: all TCN_THR threads of the block, uniformly */
+/* the issuer warp for one tile: wait for each built chunk, issue its MMAs into a
+ * fresh accumulator once the builders have read that accumulator's previous
+ * chunk, commit; ends at the builders' end-of-tile chunk.  Before returning it
+ * waits (bounded) until every MMA it issued has completed. */
+template <int TE>
+__device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
+{
+    const int lane = threadIdx.x & 31;
+    const volatile int *abort = &S.abort_flag;
+    bool ok = !*abort;
+    while (ok) {
+        const int b = Q.gc & 1;
+        if (lane == 0) ok = tc_mbar_wait_abortable(&S.full[b], Q.ph_full[b], abort);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        Q.ph_full[b] ^= 1u;
+        if (!ok) break;
+        int kind = 0;
+        if (lane == 0) kind = S.ckind[b];   /* read by the thread that observed the arrival */
+        kind = __shfl_sync(0xffffffffu, kind, 0);
+        if (kind == 3) break;
+        if (Q.gc >= 2) {
+            if (lane == 0) ok = tc_mbar_wait_abortable(&S.freed[b], Q.ph_free[b], abort);
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            Q.ph_free[b] ^= 1u;
+            if (!ok) break;
+        }
+        if (lane == 0) {
+            tc_fence_after_sync();
+            const uint32_t sb = tc_smem_u32(S.stage[b]);
+            if (kind < 2) {
+                constexpr uint32_t idm = tc_idesc_tf32(128, 96);
+                const uint32_t d = Q.tmem + TC_COL_MAIN + (uint32_t)b * 96u;
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++) {
+                    const uint64_t ah = tc_sdesc(sb + kk * TC_KSTEP_BYTES);
+                    const uint64_t bl = tc_sdesc(sb + TC_MAIN_LO + kk * TC_KSTEP_BYTES);
+                    tc_mma_tf32(d, ah, ah, idm, kk == 0 ? 0u : 1u);
+                    tc_mma_tf32(d, ah, bl, idm, 1u);
+                }
+            } else {
+                constexpr uint32_t idg = tc_idesc_tf32(128, 32);
+                const uint32_t d = Q.tmem + TC_COL_GAM + (uint32_t)b * 32u;
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++) {
+                    const uint32_t o = kk * TC_KSTEP_BYTES;
+                    const uint64_t uh = tc_sdesc(sb + o), ul = tc_sdesc(sb + TC_G_ULO + o);
+                    const uint64_t vh = tc_sdesc(sb + TC_G_VHI + o), vl = tc_sdesc(sb + TC_G_VLO + o);
+                    tc_mma_tf32(d, uh, vh, idg, kk == 0 ? 0u : 1u);
+                    tc_mma_tf32(d, uh, vl, idg, 1u);
+                    tc_mma_tf32(d, ul, vh, idg, 1u);
+                }
+            }
+            tc_commit(&S.done[b]);
+        }
+        __syncwarp();
+        Q.gc++;
+    }
+    if (!ok && lane == 0) S.abort_flag = 1;
+    /* drain: the commit tracks every MMA this thread issued */
+    if (lane == 0) {
+        tc_commit(&S.drain);
+        if (!tc_mbar_wait(&S.drain, Q.ph_drain)) S.abort_flag = 1;
+    }
+    Q.ph_drain ^= 1u;
+    __syncwarp();
+}
+
+/* the builder warps (threads 0..287) for one tile of up to TE^3 elements */
 template <int TE>
 __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, const double *__restrict__ U,
                                         float *__restrict__ vals, tc_smem<TE> &S, tc_state &Q)
@@ -250,14 +324,14 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
     constexpr int NEL = TE * TE * TE;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     /* local copies of the pipeline state (registers), written back at the end */
-    bool pend[2] = {Q.pend[0], Q.pend[1]};
-    int kind[2] = {Q.kind[0], Q.kind[1]};
-    uint32_t ph[2] = {Q.ph[0], Q.ph[1]};
+    uint32_t ph[2] = {Q.ph_done[0], Q.ph_done[1]};
+    int kind[2] = {0, 0};
     int gc = Q.gc;
     bool aborted = Q.aborted;
     const uint32_t tmem = Q.tmem;
+    const volatile int *abort = &S.abort_flag;
 
-    for (int idx = tid; idx < NCP * 3; idx += TCN_THR) {
+    for (int idx = tid; idx < NCP * 3; idx += TCN_BLD) {
         int i = idx % 3, cp = idx / 3;
         int lz = cp % TC, ly = (cp / TC) % TC, lx = cp / (TC * TC);
         double v = 0.0;
@@ -265,17 +339,17 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
             v = U[3 * cp_index(g, Tl.e0[0] + lx, Tl.e0[1] + ly, Tl.e0[2] + lz) + i];
         S.U[idx] = v;
     }
-    for (int idx = tid; idx < 3 * TE * IGAB_TAB1D; idx += TCN_THR) {
+    for (int idx = tid; idx < 3 * TE * IGAB_TAB1D; idx += TCN_BLD) {
         int d = idx / (TE * IGAB_TAB1D), r = idx % (TE * IGAB_TAB1D), le = r / IGAB_TAB1D, o = r % IGAB_TAB1D;
         double t = le < Tl.nv[d] ? g.tab[d][(long)(Tl.e0[d] + le) * IGAB_TAB1D + o] : 0.0;
         S.tab[d][le][o] = t;
         S.tabf[d][le][o] = (float)t;
     }
-    for (int idx = tid; idx < 3 * TE * IGAB_NQ; idx += TCN_THR) {
+    for (int idx = tid; idx < 3 * TE * IGAB_NQ; idx += TCN_BLD) {
         int d = idx / (TE * IGAB_NQ), r = idx % (TE * IGAB_NQ), le = r / IGAB_NQ, q = r % IGAB_NQ;
         S.wh[d][le][q] = le < Tl.nv[d] ? g.wh[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
     }
-    __syncthreads();
+    tc_bar_sync(TC_BAR_BLD, TCN_BLD);
 
     for (int le = 0; le < NEL && !aborted; le++) {
         const int lex = le / (TE * TE), ley = (le / TE) % TE, lez = le % TE;
@@ -284,20 +358,20 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         const double *By = S.tab[1][ley];
         const double *Bz = S.tab[2][lez];
         /* ---- field at the 64 Gauss points (sum-factorised: z, then y, then x) */
-        for (int o = tid; o < 972; o += TCN_THR) {
+        for (int o = tid; o < 972; o += TCN_BLD) {
             int i = o % 3, kz = (o / 3) % 3, ay = (o / 9) % 3, ax = (o / 27) % 3, q = o / 81;
             const double *u0 = &S.U[(((lex + ax) * TC + (ley + ay)) * TC + lez) * 3 + i];
             S.A[o] = Bz[q * 9 + kz] * u0[0] + Bz[q * 9 + 3 + kz] * u0[3] + Bz[q * 9 + 6 + kz] * u0[6];
         }
-        __syncthreads();
-        for (int o = tid; o < 864; o += TCN_THR) {
+        tc_bar_sync(TC_BAR_BLD, TCN_BLD);
+        for (int o = tid; o < 864; o += TCN_BLD) {
             int i = o % 3, kk = (o / 3) % 6, ax = (o / 18) % 3, qq = o / 54;
             int qyy = qq & 3, qzz = qq >> 2;
             const double *a0 = &S.A[((qzz * 3 + ax) * 3) * 9 + kk_kz(kk) * 3 + i];
             S.C[o] = By[qyy * 9 + kk_ky(kk)] * a0[0] + By[qyy * 9 + 3 + kk_ky(kk)] * a0[9] +
                      By[qyy * 9 + 6 + kk_ky(kk)] * a0[18];
         }
-        __syncthreads();
+        tc_bar_sync(TC_BAR_BLD, TCN_BLD);
         /* ---- point integrand (FP64), rotated curvatures, sign masks; q = 16 qz + 4 qy + qx */
         unsigned pmask = 0, nmask = 0;
         if (tid < IGAB_NQ3) {
@@ -363,7 +437,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
             }
             if (lane == 31) { S.part[warp][0] = pinc; S.part[warp][1] = ninc; }
         }
-        __syncthreads();
+        tc_bar_sync(TC_BAR_BLD, TCN_BLD);
         if (tid < IGAB_NQ3) {
             int po = pinc - __popc(pmask) + (warp ? S.part[0][0] : 0);
             int no = ninc - __popc(nmask) + (warp ? S.part[0][1] : 0);
@@ -376,7 +450,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                 S.cnt[1] = S.part[0][1] + S.part[1][1];
             }
         }
-        __syncthreads();
+        tc_bar_sync(TC_BAR_BLD, TCN_BLD);
         const int npos = S.cnt[0], nneg = S.cnt[1];
         const int cpos = (npos + TC_KC - 1) / TC_KC, cneg = (nneg + TC_KC - 1) / TC_KC;
         const int nch = cpos + cneg + TC_NGCHUNK;
@@ -477,49 +551,22 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                     st_pair(st + TC_G_VHI, st + TC_G_VLO, off, vval, 1.f);
                 }
             }
+            /* hand the chunk to the issuer */
+            const int ck = ch < cpos ? 0 : (ch < cpos + cneg ? 1 : 2);
+            if (tid == 0) S.ckind[b] = ck;
             tc_fence_proxy_async();
-            __syncthreads();
-            if (tid == 0) {
-                tc_fence_after_sync();
-                const uint32_t sb = tc_smem_u32(st);
-                if (ch < cpos + cneg) {
-                    constexpr uint32_t idm = tc_idesc_tf32(128, 96);
-                    const uint32_t d = tmem + TC_COL_MAIN + (uint32_t)b * 96u;
-#pragma unroll
-                    for (int kk = 0; kk < 4; kk++) {
-                        const uint64_t ah = tc_sdesc(sb + kk * TC_KSTEP_BYTES);
-                        const uint64_t bl = tc_sdesc(sb + TC_MAIN_LO + kk * TC_KSTEP_BYTES);
-                        tc_mma_tf32(d, ah, ah, idm, kk == 0 ? 0u : 1u);
-                        tc_mma_tf32(d, ah, bl, idm, 1u);
-                    }
-                } else {
-                    constexpr uint32_t idg = tc_idesc_tf32(128, 32);
-                    const uint32_t d = tmem + TC_COL_GAM + (uint32_t)b * 32u;
-#pragma unroll
-                    for (int kk = 0; kk < 4; kk++) {
-                        const uint32_t o = kk * TC_KSTEP_BYTES;
-                        const uint64_t uh = tc_sdesc(sb + o), ul = tc_sdesc(sb + TC_G_ULO + o);
-                        const uint64_t vh = tc_sdesc(sb + TC_G_VHI + o), vl = tc_sdesc(sb + TC_G_VLO + o);
-                        tc_mma_tf32(d, uh, vh, idg, kk == 0 ? 0u : 1u);
-                        tc_mma_tf32(d, uh, vl, idg, 1u);
-                        tc_mma_tf32(d, ul, vh, idg, 1u);
-                    }
-                }
-                tc_commit(&S.mbar[b]);
-            }
-            pend[b] = true;
-            kind[b] = ch < cpos ? 0 : (ch < cpos + cneg ? 1 : 2);
-            /* chunk ch-1 (stage and accumulator 1-b): wait for its MMAs, add its
-             * accumulator into the registers; stage 1-b is then free for chunk ch+1 */
-            if (pend[b ^ 1]) {
-                if (tid == 0 && !tc_mbar_wait(&S.mbar[b ^ 1], ph[b ^ 1])) S.abort_flag = 1;
+            tc_mbar_arrive(&S.full[b]);
+            kind[b] = ck;
+            /* chunk ch-1 (accumulator 1-b): wait for its MMAs, add it into the registers,
+             * release the accumulator; its stage is then free for chunk ch+1 */
+            if (ch > 0) {
+                bool ok = tc_mbar_wait_abortable(&S.done[b ^ 1], ph[b ^ 1], abort);
                 ph[b ^ 1] ^= 1u;
-                pend[b ^ 1] = false;
-                __syncthreads();
-                if (S.abort_flag) { aborted = true; break; }
+                if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) { aborted = true; break; }
                 tc_fence_after_sync();
                 tc_accumulate(tmem, b ^ 1, kind[b ^ 1], warp, acc);
                 tc_fence_before_sync();
+                tc_mbar_arrive(&S.freed[b ^ 1]);
             }
             gc++;
         }
@@ -528,13 +575,13 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         /* ---- last chunk, then the element matrix and Gamma to shared memory */
         {
             const int b = (gc - 1) & 1;
-            if (tid == 0 && !tc_mbar_wait(&S.mbar[b], ph[b])) S.abort_flag = 1;
+            bool ok = tc_mbar_wait_abortable(&S.done[b], ph[b], abort);
             ph[b] ^= 1u;
-            pend[b] = false;
-            __syncthreads();
-            if (S.abort_flag) { aborted = true; break; }
+            if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) { aborted = true; break; }
             tc_fence_after_sync();
             tc_accumulate(tmem, b, kind[b], warp, acc);
+            tc_fence_before_sync();
+            tc_mbar_arrive(&S.freed[b]);
         }
         float *E = reinterpret_cast<float *>(&S.stage[0][0]);   /* [81][81] */
         float *Gm = E + 81 * 81;                                  /* [27][27] */
@@ -553,15 +600,15 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
             elem_row_base(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez, tid - 192, S.rbase[tid - 192],
                           S.rsx[tid - 192], S.rsy[tid - 192]);
         tc_fence_before_sync();
-        __syncthreads();
+        tc_bar_sync(TC_BAR_BLD, TCN_BLD);
         /* ---- symmetric part + Gamma on the k1 = k2 blocks, read-modify-write into the CSR
          * values, four independent entries per thread in flight */
-        for (int i0 = tid; i0 < 81 * 81; i0 += 4 * TCN_THR) {
+        for (int i0 = tid; i0 < 81 * 81; i0 += 4 * TCN_BLD) {
             long off[4];
             float val[4], old[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) {
-                const int idx = i0 + u * TCN_THR;
+                const int idx = i0 + u * TCN_BLD;
                 off[u] = -1;
                 if (idx < 81 * 81) {
                     const int c1 = idx / 81, c2 = idx % 81;
@@ -579,13 +626,17 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
             for (int u = 0; u < 4; u++)
                 if (off[u] >= 0) vals[off[u]] = old[u] + val[u];
         }
-        __syncthreads();
+        tc_bar_sync(TC_BAR_BLD, TCN_BLD);
     }
-    for (int b = 0; b < 2; b++) {
-        Q.pend[b] = pend[b];
-        Q.kind[b] = kind[b];
-        Q.ph[b] = ph[b];
+    /* end of tile for the issuer (also after an abort: it stops at the flag) */
+    if (aborted && tid == 0) S.abort_flag = 1;
+    if (!aborted) {
+        const int b = gc & 1;
+        if (tid == 0) S.ckind[b] = 3;
+        tc_mbar_arrive(&S.full[b]);
     }
+    Q.ph_done[0] = ph[0];
+    Q.ph_done[1] = ph[1];
     Q.gc = gc;
     Q.aborted = aborted;
 }
@@ -600,7 +651,8 @@ __global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32(igab_geom g, const doub
     if (!decode_tile(g, TE, colour, blockIdx.x, Tl)) return;   /* block-uniform, before any barrier */
     tc_state Q;
     tc_setup<TE>(S, Q);
-    tc_tile<TE>(g, Tl, U, vals, S, Q);
+    if (threadIdx.x < TCN_BLD) tc_tile<TE>(g, Tl, U, vals, S, Q);
+    else tc_issue<TE>(S, Q);
     tc_release<TE>(S, Q, status);
 }
 
@@ -616,10 +668,14 @@ __global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32_batch(igab_batch_dev B,
     tc_state Q;
     tc_setup<2>(S, Q);
     while (batch_next(B, sl)) {
-        if (!Q.aborted) {
-            tile_t Tl;
-            decode_tile(sl.g, 2, sl.colour, sl.tile, Tl);
-            tc_tile<2>(sl.g, Tl, U + B.dof_off[sl.inst], vals + B.nnz_off[sl.inst], S, Q);
+        if (!S.abort_flag) {
+            if (threadIdx.x < TCN_BLD) {
+                tile_t Tl;
+                decode_tile(sl.g, 2, sl.colour, sl.tile, Tl);
+                tc_tile<2>(sl.g, Tl, U + B.dof_off[sl.inst], vals + B.nnz_off[sl.inst], S, Q);
+            } else {
+                tc_issue<2>(S, Q);
+            }
         }
         batch_done(B, sl);
     }

@@ -98,6 +98,53 @@ __device__ __forceinline__ bool tc_mbar_wait(unsigned long long *bar, uint32_t p
     return false;
 }
 
+/* bounded wait that also gives up as soon as *abort is set (another role gave up) */
+__device__ __forceinline__ bool tc_mbar_wait_abortable(unsigned long long *bar, uint32_t parity,
+                                                       const volatile int *abort)
+{
+    const uint32_t a = tc_smem_u32(bar);
+    for (long i = 0; i < TC_WAIT_POLLS; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if ((i & 63) == 63 && *abort) return false;
+    }
+    return false;
+}
+
+/* one arrival on *bar (release: this thread's prior shared-memory writes are visible to the waiter) */
+__device__ __forceinline__ void tc_mbar_arrive(unsigned long long *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc_smem_u32(bar)) : "memory");
+}
+
+/* named barrier among `count` threads (a role's threads, not the whole block) */
+__device__ __forceinline__ void tc_bar_sync(int id, int count)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+/* named barrier with an AND vote over `count` threads */
+__device__ __forceinline__ bool tc_bar_and(int id, int count, bool v)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id), "r"(count)
+        : "memory");
+    return r != 0;
+}
+
 /* generic-proxy shared-memory writes -> visible to the tensor core (async proxy) */
 __device__ __forceinline__ void tc_fence_proxy_async()
 {

@@ -22,24 +22,25 @@
  * and three MMAs per k-step (hi hi, hi lo, lo hi).
  *
  * Work per CTA: a 2x2x2 tile of elements of one of the 8 colours (the scatter
- * is conflict-free within a colour).  Per element: sum-factorised field at the
- * 64 Gauss points (FP64), the point integrand (FP64, 64 threads), sign buckets
- * of the 768 (point, variable) rows, then chunks of 32 rows are built into a
- * double-buffered shared-memory stage (TF32 hi/lo in the K-major layout of
- * igab_tc.cuh) by all 288 threads, and one thread issues the chunk's MMAs into
- * a fresh tensor-memory accumulator: 4 k-steps x 2 MMAs (M 128, N 96) for
- * element-matrix rows, 4 x 3 MMAs (M 128, N 32) for Gamma rows.  While the
- * tensor core works on chunk c, the accumulator of chunk c-1 is added into
- * FP32 registers (round to nearest; subtracted for negative-curvature rows):
- * the tensor core sums only one chunk's products per entry, which keeps the
- * FP32 accumulation error at the level of the FMA-pipe kernel.  Tensor
- * memory: 256 columns per CTA (element matrix 2 x 96, Gamma 2 x 32, double
- * buffered); at most two CTAs per SM.  Rows 81-127 of the M side and columns
- * 81-95 of the N side read whatever lies behind the operand in the stage;
- * they only feed accumulator rows and columns that are never read.  At the
- * end of an element: the register accumulators go to shared memory, the
- * symmetric part is taken, Gamma is added on the k1 = k2 blocks and the
- * 81 x 81 values are read-modify-written into the FP32 CSR values.
+ * is conflict-free within a colour).  Warps 0-8 build, warp 9 issues MMAs.
+ * Per element the builders compute the sum-factorised field at the 64 Gauss
+ * points (FP64), the point integrand (FP64, 64 threads) and sign buckets of
+ * the 768 (point, variable) rows, then build chunks of 32 rows into a double-
+ * buffered shared-memory stage (TF32 hi/lo in the K-major layout of
+ * igab_tc.cuh) and hand each to the issuer through an mbarrier.  The issuer
+ * runs 4 k-steps x 2 MMAs (M 128, N 96; negate-A for negative-curvature rows)
+ * or x 3 (M 128, N 32, Gamma rows) per chunk and commits to the stage's
+ * mbarrier, which frees the stage for the chunk after next.  An element
+ * accumulates in two tensor-memory accumulators per class, by chunk parity:
+ * about 96 accumulating MMAs each, 5e-6 rowwise agreement with the FP64
+ * reference (one accumulator for all 192 gave 1e-5).  Tensor memory: 256
+ * columns per CTA (element matrix 2 x 96, Gamma 2 x 32); at most two CTAs per
+ * SM.  Rows 81-127 of the M side and columns 81-95 of the N side read whatever
+ * lies behind the operand in the stage; they only feed accumulator rows and
+ * columns that are never read.  At the end of an element the builders sum the
+ * accumulators into shared memory, release them to the issuer, take the
+ * symmetric part, add Gamma on the k1 = k2 blocks and read-modify-write the
+ * 81 x 81 values into the FP32 CSR values.
  */
 #include <cuda_runtime.h>
 #include "igab_device.cuh"
@@ -89,9 +90,10 @@ struct tc_smem {
     int rsx[81], rsy[81];
     unsigned long long full[2];         /* stage b written (288 builder arrivals) */
     unsigned long long done[2];         /* MMAs of the chunk in stage / accumulator b completed (commit) */
-    unsigned long long freed[2];        /* accumulator b read out (288 builder arrivals) */
+    unsigned long long freed;           /* the element's accumulators read out (288 builder arrivals) */
     unsigned long long drain;           /* issuer: every MMA it issued has completed */
-    int ckind[2];                       /* chunk in stage b: 0 positive rows, 1 negative rows, 2 Gamma, 3 end of tile */
+    int ckind[2];                       /* chunk in stage b: 0 positive rows, 1 negative rows, 2 Gamma,
+                                           3 end of tile; + 4 on an element's first chunk */
     unsigned int tmem_base;
     int abort_flag;
 };
@@ -163,46 +165,16 @@ __device__ __forceinline__ void st_pair(unsigned char *hi_base, unsigned char *l
     *reinterpret_cast<float *>(lo_base + off) = lo_scale * l;
 }
 
-/* Add the accumulator of one finished chunk into the FP32 registers (round to
- * nearest): element-matrix chunks go to warps 0-2 / 4-6 (TMEM lanes = rows
- * 0-95, columns 0-47 / 48-95 of the 96-column accumulator, subtracted for
- * rows of negative curvature), Gamma chunks to warp 8 (lanes 0-31, 32 columns).
- * Each chunk starts a fresh accumulator, so the tensor core sums only the 8
- * (12) products of one chunk per entry. */
-__device__ __forceinline__ void tc_accumulate(uint32_t tmem, int buf, int kind, int warp, float (&acc)[48])
-{
-    if (kind < 2) {
-        if (warp == 3 || warp >= 7) return;   /* lanes 96-127: rows beyond 80; warp 8 holds Gamma */
-        const int lb = 32 * (warp & 3), half = warp >> 2;
-        const float sg = kind == 0 ? 1.f : -1.f;
-        const uint32_t ta = tmem + ((uint32_t)lb << 16) + TC_COL_MAIN + (uint32_t)buf * 96u + 48u * half;
-#pragma unroll
-        for (int part = 0; part < 3; part++) {
-            float v[16];
-            tc_ld16(ta + 16u * part, v);
-#pragma unroll
-            for (int i = 0; i < 16; i++) acc[16 * part + i] += sg * v[i];
-        }
-    } else if (warp == 8) {
-        const uint32_t ta = tmem + TC_COL_GAM + (uint32_t)buf * 32u;
-#pragma unroll
-        for (int part = 0; part < 2; part++) {
-            float v[16];
-            tc_ld16(ta + 16u * part, v);
-#pragma unroll
-            for (int i = 0; i < 16; i++) acc[16 * part + i] += v[i];
-        }
-    }
-}
-
 /* pipeline state of a thread, carried across the tiles its CTA processes: the
  * builders track the commits they wait for, the issuer the arrivals it waits for */
 struct tc_state {
     uint32_t ph_done[2];   /* builders: parity of the next wait on done[b] */
+    bool pend[2];          /* builders: a chunk in stage b whose completion is not yet waited for */
     uint32_t ph_full[2];   /* issuer: parity of the next wait on full[b] */
-    uint32_t ph_free[2];   /* issuer: parity of the next wait on freed[b] */
+    uint32_t ph_free;      /* issuer: parity of the next wait on freed */
     uint32_t ph_drain;
     int gc;                /* chunks (with MMAs) so far */
+    int nelem;             /* elements (issuer: started) so far */
     bool aborted;
     uint32_t tmem;
 };
@@ -216,8 +188,8 @@ __device__ __forceinline__ void tc_setup(tc_smem<TE> &S, tc_state &Q)
         for (int b = 0; b < 2; b++) {
             tc_mbar_init(&S.full[b], TCN_BLD);
             tc_mbar_init(&S.done[b], 1);
-            tc_mbar_init(&S.freed[b], TCN_BLD);
         }
+        tc_mbar_init(&S.freed, TCN_BLD);
         tc_mbar_init(&S.drain, 1);
         tc_fence_mbar_init();
         S.abort_flag = 0;
@@ -227,9 +199,11 @@ __device__ __forceinline__ void tc_setup(tc_smem<TE> &S, tc_state &Q)
     __syncthreads();
     tc_fence_after_sync();
     Q.tmem = S.tmem_base;
-    Q.ph_done[0] = Q.ph_done[1] = Q.ph_full[0] = Q.ph_full[1] = Q.ph_free[0] = Q.ph_free[1] = 0u;
-    Q.ph_drain = 0u;
+    Q.ph_done[0] = Q.ph_done[1] = Q.ph_full[0] = Q.ph_full[1] = 0u;
+    Q.pend[0] = Q.pend[1] = false;
+    Q.ph_free = Q.ph_drain = 0u;
     Q.gc = 0;
+    Q.nelem = 0;
     Q.aborted = false;
 }
 
@@ -247,43 +221,56 @@ __device__ __forceinline__ void tc_release(tc_smem<TE> &S, tc_state &Q, int *sta
     }
 }
 
-/* the issuer warp for one tile: wait for each built chunk, issue its MMAs into a
- * fresh accumulator once the builders have read that accumulator's previous
- * chunk, commit; ends at the builders' end-of-tile chunk.  Before returning it
- * waits (bounded) until every MMA it issued has completed. */
+/* the issuer warp for one tile: wait for each built chunk and issue its MMAs.
+ * An element's chunks accumulate in two tensor-memory accumulators by chunk
+ * parity (element matrix: 96 columns each, Gamma: 32 each); negative-curvature
+ * chunks use the negate-A form.  Before the first MMA of an element the issuer
+ * waits until the builders have read the previous element's accumulators.  Ends
+ * at the builders' end-of-tile chunk; before returning it waits (bounded) until
+ * every MMA it issued has completed. */
 template <int TE>
 __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
 {
     const int lane = threadIdx.x & 31;
     const volatile int *abort = &S.abort_flag;
     bool ok = !*abort;
+    bool started[2][2] = {{false, false}, {false, false}};   /* [element matrix / Gamma][accumulator] */
     while (ok) {
         const int b = Q.gc & 1;
         if (lane == 0) ok = tc_mbar_wait_abortable(&S.full[b], Q.ph_full[b], abort);
         ok = __shfl_sync(0xffffffffu, ok, 0);
         Q.ph_full[b] ^= 1u;
         if (!ok) break;
-        int kind = 0;
-        if (lane == 0) kind = S.ckind[b];   /* read by the thread that observed the arrival */
-        kind = __shfl_sync(0xffffffffu, kind, 0);
-        if (kind == 3) break;
-        if (Q.gc >= 2) {
-            if (lane == 0) ok = tc_mbar_wait_abortable(&S.freed[b], Q.ph_free[b], abort);
-            ok = __shfl_sync(0xffffffffu, ok, 0);
-            Q.ph_free[b] ^= 1u;
-            if (!ok) break;
+        int ck = 0;
+        if (lane == 0) ck = S.ckind[b];   /* read by the thread that observed the arrival */
+        ck = __shfl_sync(0xffffffffu, ck, 0);
+        if (ck == 3) break;
+        if (ck & 4) {
+            /* first chunk of an element: the previous element's accumulators must be read out */
+            if (Q.nelem > 0) {
+                if (lane == 0) ok = tc_mbar_wait_abortable(&S.freed, Q.ph_free, abort);
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                Q.ph_free ^= 1u;
+                if (!ok) break;
+            }
+            Q.nelem++;
+            started[0][0] = started[0][1] = started[1][0] = started[1][1] = false;
         }
+        const int kind = ck & 3;
+        const int cls = kind == 2 ? 1 : 0;
+        const uint32_t acc0 = started[cls][b] ? 1u : 0u;
+        started[cls][b] = true;
         if (lane == 0) {
             tc_fence_after_sync();
             const uint32_t sb = tc_smem_u32(S.stage[b]);
             if (kind < 2) {
-                constexpr uint32_t idm = tc_idesc_tf32(128, 96);
+                const uint32_t idm = kind == 0 ? tc_idesc_tf32(128, 96) : tc_idesc_tf32(128, 96, true);
                 const uint32_t d = Q.tmem + TC_COL_MAIN + (uint32_t)b * 96u;
 #pragma unroll
                 for (int kk = 0; kk < 4; kk++) {
                     const uint64_t ah = tc_sdesc(sb + kk * TC_KSTEP_BYTES);
                     const uint64_t bl = tc_sdesc(sb + TC_MAIN_LO + kk * TC_KSTEP_BYTES);
-                    tc_mma_tf32(d, ah, ah, idm, kk == 0 ? 0u : 1u);
+                    tc_mma_tf32(d, ah, ah, idm, kk == 0 ? acc0 : 1u);
                     tc_mma_tf32(d, ah, bl, idm, 1u);
                 }
             } else {
@@ -294,7 +281,7 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
                     const uint32_t o = kk * TC_KSTEP_BYTES;
                     const uint64_t uh = tc_sdesc(sb + o), ul = tc_sdesc(sb + TC_G_ULO + o);
                     const uint64_t vh = tc_sdesc(sb + TC_G_VHI + o), vl = tc_sdesc(sb + TC_G_VLO + o);
-                    tc_mma_tf32(d, uh, vh, idg, kk == 0 ? 0u : 1u);
+                    tc_mma_tf32(d, uh, vh, idg, kk == 0 ? acc0 : 1u);
                     tc_mma_tf32(d, uh, vl, idg, 1u);
                     tc_mma_tf32(d, ul, vh, idg, 1u);
                 }
@@ -314,6 +301,57 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
     __syncwarp();
 }
 
+/* Sum the element's accumulators into shared memory (FP32, round to nearest):
+ * element-matrix rows by warps 0-2 / 4-6 (TMEM lanes = rows 0-95, columns
+ * 0-47 / 48-95), Gamma rows by warp 8 (lanes 0-31, 32 columns).  used[c][b]:
+ * accumulator b of class c (element matrix, Gamma) holds this element's sums. */
+__device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2][2], int warp, int lane, float *E,
+                                           float *Gm)
+{
+    if (warp < 8) {
+        if (warp == 3 || warp == 7) return;   /* lanes 96-127: rows beyond 80 */
+        const int lb = 32 * (warp & 3), half = warp >> 2, row = lb + lane;
+#pragma unroll 1
+        for (int part = 0; part < 3; part++) {
+            const int c0 = 48 * half + 16 * part;
+            float s[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) s[i] = 0.f;
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                if (!used[0][b]) continue;   /* warp-uniform */
+                float v[16];
+                tc_ld16(tmem + ((uint32_t)lb << 16) + TC_COL_MAIN + (uint32_t)b * 96u + (uint32_t)c0, v);
+#pragma unroll
+                for (int i = 0; i < 16; i++) s[i] += v[i];
+            }
+            if (row < 81)
+#pragma unroll
+                for (int i = 0; i < 16; i++)
+                    if (c0 + i < 81) E[row * 81 + c0 + i] = s[i];
+        }
+    } else {
+#pragma unroll 1
+        for (int part = 0; part < 2; part++) {
+            float s[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) s[i] = 0.f;
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                if (!used[1][b]) continue;
+                float v[16];
+                tc_ld16(tmem + TC_COL_GAM + (uint32_t)b * 32u + 16u * part, v);
+#pragma unroll
+                for (int i = 0; i < 16; i++) s[i] += v[i];
+            }
+            if (lane < 27)
+#pragma unroll
+                for (int i = 0; i < 16; i++)
+                    if (16 * part + i < 27) Gm[lane * 27 + 16 * part + i] = s[i];
+        }
+    }
+}
+
 /* the builder warps (threads 0..287) for one tile of up to TE^3 elements */
 template <int TE>
 __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, const double *__restrict__ U,
@@ -325,7 +363,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     /* local copies of the pipeline state (registers), written back at the end */
     uint32_t ph[2] = {Q.ph_done[0], Q.ph_done[1]};
-    int kind[2] = {0, 0};
+    bool pend[2] = {Q.pend[0], Q.pend[1]};
     int gc = Q.gc;
     bool aborted = Q.aborted;
     const uint32_t tmem = Q.tmem;
@@ -455,14 +493,17 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         const int cpos = (npos + TC_KC - 1) / TC_KC, cneg = (nneg + TC_KC - 1) / TC_KC;
         const int nch = cpos + cneg + TC_NGCHUNK;
 
-        /* ---- chunk loop: chunk ch is built into stage gc & 1 and multiplied into
-         * accumulator gc & 1 while chunk ch-1's accumulator is added into registers */
-        float acc[48];
-#pragma unroll
-        for (int i = 0; i < 48; i++) acc[i] = 0.f;
+        /* ---- chunk loop: chunk ch is built into stage gc & 1 while the tensor core
+         * works on the previous chunks; the element accumulates in tensor memory */
         for (int ch = 0; ch < nch; ch++) {
             const int b = gc & 1;
             unsigned char *st = S.stage[b];
+            if (pend[b]) {   /* stage b holds chunk gc-2: wait for its MMAs */
+                const bool ok = tc_mbar_wait_abortable(&S.done[b], ph[b], abort);
+                ph[b] ^= 1u;
+                pend[b] = false;
+                if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) { aborted = true; break; }
+            }
             if (ch < cpos + cneg) {
                 /* main rows: task (slot j, component k, ax) -> 9 outputs (ay, az) */
                 const int neg = ch >= cpos;
@@ -552,50 +593,38 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                 }
             }
             /* hand the chunk to the issuer */
-            const int ck = ch < cpos ? 0 : (ch < cpos + cneg ? 1 : 2);
+            const int ck = (ch < cpos ? 0 : (ch < cpos + cneg ? 1 : 2)) | (ch == 0 ? 4 : 0);
             if (tid == 0) S.ckind[b] = ck;
             tc_fence_proxy_async();
             tc_mbar_arrive(&S.full[b]);
-            kind[b] = ck;
-            /* chunk ch-1 (accumulator 1-b): wait for its MMAs, add it into the registers,
-             * release the accumulator; its stage is then free for chunk ch+1 */
-            if (ch > 0) {
-                bool ok = tc_mbar_wait_abortable(&S.done[b ^ 1], ph[b ^ 1], abort);
-                ph[b ^ 1] ^= 1u;
-                if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) { aborted = true; break; }
-                tc_fence_after_sync();
-                tc_accumulate(tmem, b ^ 1, kind[b ^ 1], warp, acc);
-                tc_fence_before_sync();
-                tc_mbar_arrive(&S.freed[b ^ 1]);
-            }
+            pend[b] = true;
             gc++;
         }
         if (aborted) break;
 
-        /* ---- last chunk, then the element matrix and Gamma to shared memory */
-        {
-            const int b = (gc - 1) & 1;
-            bool ok = tc_mbar_wait_abortable(&S.done[b], ph[b], abort);
+        /* ---- all chunks of the element done (older stage first), accumulators -> shared memory */
+        for (int k = 0; k < 2 && !aborted; k++) {
+            const int b = (gc + k) & 1;   /* chunk gc-2, then gc-1 */
+            if (!pend[b]) continue;
+            const bool ok = tc_mbar_wait_abortable(&S.done[b], ph[b], abort);
             ph[b] ^= 1u;
-            if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) { aborted = true; break; }
-            tc_fence_after_sync();
-            tc_accumulate(tmem, b, kind[b], warp, acc);
-            tc_fence_before_sync();
-            tc_mbar_arrive(&S.freed[b]);
+            pend[b] = false;
+            if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) aborted = true;
         }
+        if (aborted) break;
+        const int g0 = gc - nch;   /* the element's first chunk */
+        const int cmain = cpos + cneg;
+        bool used[2][2];
+        used[0][g0 & 1] = cmain > 0;
+        used[0][(g0 + 1) & 1] = cmain > 1;
+        used[1][(g0 + cmain) & 1] = true;                 /* TC_NGCHUNK >= 2 Gamma chunks */
+        used[1][(g0 + cmain + 1) & 1] = TC_NGCHUNK > 1;
         float *E = reinterpret_cast<float *>(&S.stage[0][0]);   /* [81][81] */
         float *Gm = E + 81 * 81;                                  /* [27][27] */
-        if (warp < 8) {
-            const int lb = 32 * (warp & 3), half = warp >> 2, row = lb + lane;
-            if (row < 81)
-#pragma unroll
-                for (int i = 0; i < 48; i++)
-                    if (48 * half + i < 81) E[row * 81 + 48 * half + i] = acc[i];
-        } else {
-            if (lane < 27)
-#pragma unroll
-                for (int i = 0; i < 27; i++) Gm[lane * 27 + i] = acc[i];
-        }
+        tc_fence_after_sync();
+        tc_readout(tmem, used, warp, lane, E, Gm);
+        tc_fence_before_sync();
+        tc_mbar_arrive(&S.freed);
         if (tid >= 192 && tid < 192 + 81)
             elem_row_base(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez, tid - 192, S.rbase[tid - 192],
                           S.rsx[tid - 192], S.rsy[tid - 192]);
@@ -637,6 +666,8 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
     }
     Q.ph_done[0] = ph[0];
     Q.ph_done[1] = ph[1];
+    Q.pend[0] = pend[0];
+    Q.pend[1] = pend[1];
     Q.gc = gc;
     Q.aborted = aborted;
 }
@@ -686,7 +717,8 @@ __global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32_batch(igab_batch_dev B,
  * One CTA: A (128 x 32) and B (96 x 32) of small exact values in the operand
  * layout, D = A B^T with M 128 / N 96 (4 k-steps) into columns 0-95 and, for
  * the Gamma shape, A B[0:32]^T with M 128 / N 32 into columns 96-127 (first
- * k-step overwrite, then accumulate).  out[128][128] receives columns 0-127. */
+ * k-step overwrite, then accumulate), and with negate-A on k-steps 2-3 into
+ * columns 128-159.  out[128][160] receives columns 0-159. */
 __global__ void __launch_bounds__(128) k_tc_selftest(float *out, int *status)
 {
     __shared__ __align__(128) unsigned char sm[16384 + 12288];
@@ -706,7 +738,7 @@ __global__ void __launch_bounds__(128) k_tc_selftest(float *out, int *status)
         tc_mbar_init(&bar, 1);
         tc_fence_mbar_init();
     }
-    if (warp == 0) tc_alloc(&tbase, 128);
+    if (warp == 0) tc_alloc(&tbase, 256);
     tc_fence_proxy_async();
     tc_fence_before_sync();
     __syncthreads();
@@ -720,22 +752,26 @@ __global__ void __launch_bounds__(128) k_tc_selftest(float *out, int *status)
         for (int kk = 0; kk < 4; kk++)
             tc_mma_tf32(tm + 96, tc_sdesc(sa + kk * TC_KSTEP_BYTES), tc_sdesc(sb + kk * TC_KSTEP_BYTES),
                         tc_idesc_tf32(128, 32), kk > 0);
+        /* negate-A: columns 128-159 = A B[0:32]^T for k-steps 0-1 minus it for k-steps 2-3 */
+        for (int kk = 0; kk < 4; kk++)
+            tc_mma_tf32(tm + 128, tc_sdesc(sa + kk * TC_KSTEP_BYTES), tc_sdesc(sb + kk * TC_KSTEP_BYTES),
+                        tc_idesc_tf32(128, 32, kk >= 2), kk > 0);
         tc_commit(&bar);
     }
     __syncthreads();
     if (tid == 0 && !tc_mbar_wait(&bar, 0)) atomicOr(status, 1);
     __syncthreads();
     tc_fence_after_sync();
-    for (int part = 0; part < 8; part++) {
+    for (int part = 0; part < 10; part++) {
         float v[16];
         tc_ld16(tm + ((uint32_t)(32 * warp) << 16) + 16u * part, v);
-        for (int i = 0; i < 16; i++) out[(32 * warp + lane) * 128 + 16 * part + i] = v[i];
+        for (int i = 0; i < 16; i++) out[(32 * warp + lane) * 160 + 16 * part + i] = v[i];
     }
     tc_fence_before_sync();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after_sync();
-        tc_dealloc(tm, 128);
+        tc_dealloc(tm, 256);
     }
 }
 
@@ -887,7 +923,7 @@ extern "C" int igab_tc_selftest(int device, float *out_host)
     IGAB_CUDA_TRY(cudaSetDevice(device));
     float *d_out = nullptr;
     int *d_st = nullptr;
-    IGAB_CUDA_TRY(cudaMalloc((void **)&d_out, 128 * 128 * sizeof(float)));
+    IGAB_CUDA_TRY(cudaMalloc((void **)&d_out, 128 * 160 * sizeof(float)));
     cudaError_t e = cudaMalloc((void **)&d_st, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(d_st, 0, sizeof(int));
     if (e == cudaSuccess) {
@@ -896,7 +932,7 @@ extern "C" int igab_tc_selftest(int device, float *out_host)
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     int st = 0;
-    if (e == cudaSuccess) e = cudaMemcpy(out_host, d_out, 128 * 128 * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(out_host, d_out, 128 * 160 * sizeof(float), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(&st, d_st, sizeof(int), cudaMemcpyDeviceToHost);
     cudaFree(d_out);
     cudaFree(d_st);

@@ -29,11 +29,12 @@ constexpr int TC_KSTEP_BYTES = 256;
 constexpr long TC_WAIT_POLLS = 1L << 22;
 
 /* Instruction descriptor of tcgen05.mma kind::tf32: D f32 (bits 4-5 = 1),
- * A and B tf32 (bits 7-9, 10-12 = 2), both K-major (bits 15, 16 = 0),
- * N >> 3 in bits 17-22, M >> 4 in bits 24-28, dense, no negation. */
-__host__ __device__ constexpr uint32_t tc_idesc_tf32(int M, int N)
+ * A and B tf32 (bits 7-9, 10-12 = 2), negate A (bit 13, optional), both
+ * K-major (bits 15, 16 = 0), N >> 3 in bits 17-22, M >> 4 in bits 24-28, dense. */
+__host__ __device__ constexpr uint32_t tc_idesc_tf32(int M, int N, bool negate_a = false)
 {
-    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+    return (1u << 4) | (2u << 7) | (2u << 10) | (negate_a ? (1u << 13) : 0u) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
 }
 
 __device__ __forceinline__ uint32_t tc_smem_u32(const void *p)

@@ -124,8 +124,9 @@ int igab_last_kernel_ms(igab_ctx *ctx, double ms[6]);
 int igab_fma_peak(int device, int prec, double *tflops);
 /* Check of the tcgen05 operand layout and descriptors used by the FP32 tensor-core tangent
  * (no reference counterpart): one CTA computes A B^T for fixed small-integer A (128 x 32) and
- * B (96 x 32) with the M 128 / N 96 and M 128 / N 32 instruction shapes; out (128 x 128 floats,
- * row-major) receives accumulator columns 0-95 (A B^T) and 96-127 (A B[0:32]^T). */
+ * B (96 x 32) with the M 128 / N 96 and M 128 / N 32 instruction shapes; out (128 x 160 floats,
+ * row-major) receives accumulator columns 0-95 (A B^T), 96-127 (A B[0:32]^T) and 128-159
+ * (A B[0:32]^T over K 0-15 minus it over K 16-31, the negate-A form). */
 int igab_tc_selftest(int device, float *out);
 /* TF32 tensor-core throughput probe (TFLOP/s, dense): one CTA per SM issuing back-to-back
  * tcgen05.mma kind::tf32 M 128 x N n_cols x K 8 (n_cols 32, 96 = the FP32 tangent's

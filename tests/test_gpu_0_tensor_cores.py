@@ -22,7 +22,7 @@ def test_tc_operand_layout_selftest(built):
     instruction shapes (M 128 / N 96 and M 128 / N 32); exact in FP32."""
     from igap4standard_b200 import native
     lib = native.lib_cuda()
-    out = np.zeros((128, 128), dtype=np.float32)
+    out = np.zeros((128, 160), dtype=np.float32)
     native.check(lib, "igab_tc_selftest", lib.igab_tc_selftest(0, out.ctypes.data_as(ctypes.c_void_p)))
     m = np.arange(128)[:, None]
     k = np.arange(32)[None, :]
@@ -31,7 +31,9 @@ def test_tc_operand_layout_selftest(built):
     B = (((n * 7 + k) % 11) - 5) * 0.25
     D = A @ B.T
     assert np.array_equal(out[:, :96], D.astype(np.float32))
-    assert np.array_equal(out[:, 96:], D[:, :32].astype(np.float32))
+    assert np.array_equal(out[:, 96:128], D[:, :32].astype(np.float32))
+    Dn = A[:, :16] @ B[:32, :16].T - A[:, 16:] @ B[:32, 16:].T      # negate-A on the last two k-steps
+    assert np.array_equal(out[:, 128:], Dn.astype(np.float32))
 
 
 def _assembly(c):

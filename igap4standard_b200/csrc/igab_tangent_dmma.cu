@@ -400,29 +400,16 @@ __device__ __forceinline__ void dmma_tile(const igab_geom &g, const tile_t &Tl, 
         if (tid < 81)
             elem_row_base(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez, tid, S.rbase[tid], S.rsx[tid], S.rsy[tid]);
         __syncthreads();
-        /* read-modify-write into the CSR values, four independent entries per thread in flight */
-        for (int i0 = tid; i0 < 81 * 81; i0 += 4 * NTHR) {
-            long off[4];
-            double val[4], old[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const int idx = i0 + u * NTHR;
-                off[u] = -1;
-                if (idx < 81 * 81) {
-                    const int c1 = idx / 81, c2 = idx % 81;
-                    const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
-                    double v = c1 <= c2 ? K[c1 * 88 + c2] : K[c2 * 88 + c1];
-                    if (k1 == k2) v += a1 <= a2 ? Gam[a1 * 32 + a2] : Gam[a2 * 32 + a1];
-                    val[u] = v;
-                    off[u] = S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9;
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-                if (off[u] >= 0) old[u] = __ldcg(&vals[off[u]]);   /* L2: written by other CTAs */
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-                if (off[u] >= 0) vals[off[u]] = old[u] + val[u];
+        /* added into the CSR values with fire-and-forget reductions (red.global.add):
+         * the tiles of one colour touch disjoint entries and the elements of a tile
+         * are separated by a barrier, so every entry receives its additions in a
+         * fixed order */
+        for (int idx = tid; idx < 81 * 81; idx += NTHR) {
+            const int c1 = idx / 81, c2 = idx % 81;
+            const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
+            double v = c1 <= c2 ? K[c1 * 88 + c2] : K[c2 * 88 + c1];
+            if (k1 == k2) v += a1 <= a2 ? Gam[a1 * 32 + a2] : Gam[a2 * 32 + a1];
+            atomicAdd(&vals[S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9], v);
         }
         __syncthreads();
         /* Gamma overwrote N^T: restore the zero padding of N^T */

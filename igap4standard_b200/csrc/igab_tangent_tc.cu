@@ -84,6 +84,8 @@ struct tc_smem {
     float tabf[3][TE][IGAB_TAB1D];
     float pt[IGAB_NQ3][TP_N];
     unsigned short map[2][768];         /* bucket slot -> 12 q + v (positive, negative) */
+    float gk[2][TC_KC][3][9];           /* per chunk parity: r * d v'/d u_{k,m} of each slot (pre-pass) */
+    int qs[2][TC_KC];                   /* point of each slot, -1 for padding rows */
     int cnt[2];
     int part[2][2];                     /* per-warp bucket counts for the scan */
     long rbase[81];                     /* CSR row bases of the element matrix (elem_row_base) */
@@ -352,6 +354,33 @@ __device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2][
     }
 }
 
+/* Pre-pass of an element-matrix chunk (threads 0-95, one (slot, component)
+ * each): the row's coefficients r * d v'/d u_{k,m} (m = 0..8) and its point,
+ * so that the 288 build tasks read them instead of each evaluating the
+ * variable gradient (which branches on the variable). */
+template <int TE>
+__device__ __forceinline__ void tc_prepass(tc_smem<TE> &S, int par, int bucket, int base, int cntb)
+{
+    const int t = threadIdx.x;
+    if (t >= 3 * TC_KC) return;
+    const int j = t / 3, k = t % 3, slot = base + j;
+    float *gout = S.gk[par][j][k];
+    if (slot < cntb) {
+        const int id = S.map[bucket][slot], q = id / 12, v = id % 12;
+        const float *p = S.pt[q];
+        float gv[9];
+        tc_grad_var(p, v, k, gv);
+        const float r = fabsf(p[TP_RS + v]);
+#pragma unroll
+        for (int m = 0; m < 9; m++) gout[m] = r * gv[m];
+        if (k == 0) S.qs[par][j] = q;
+    } else {
+#pragma unroll
+        for (int m = 0; m < 9; m++) gout[m] = 0.f;
+        if (k == 0) S.qs[par][j] = -1;
+    }
+}
+
 /* the builder warps (threads 0..287) for one tile of up to TE^3 elements */
 template <int TE>
 __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, const double *__restrict__ U,
@@ -495,37 +524,38 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
 
         /* ---- chunk loop: chunk ch is built into stage gc & 1 while the tensor core
          * works on the previous chunks; the element accumulates in tensor memory */
+        const int cmain = cpos + cneg;
+        if (cmain > 0) tc_prepass<TE>(S, 0, 0 < cpos ? 0 : 1, 0, 0 < cpos ? npos : nneg);
         for (int ch = 0; ch < nch; ch++) {
             const int b = gc & 1;
             unsigned char *st = S.stage[b];
-            if (pend[b]) {   /* stage b holds chunk gc-2: wait for its MMAs */
-                const bool ok = tc_mbar_wait_abortable(&S.done[b], ph[b], abort);
+            /* stage b holds chunk gc-2: wait for its MMAs; the barrier also publishes the pre-pass */
+            bool ok = true;
+            if (pend[b]) {
+                ok = tc_mbar_wait_abortable(&S.done[b], ph[b], abort);
                 ph[b] ^= 1u;
                 pend[b] = false;
-                if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) { aborted = true; break; }
             }
+            if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) { aborted = true; break; }
             if (ch < cpos + cneg) {
                 /* main rows: task (slot j, component k, ax) -> 9 outputs (ay, az) */
-                const int neg = ch >= cpos;
-                const int base = (neg ? ch - cpos : ch) * TC_KC;
-                const int cntb = neg ? nneg : npos;
+                const int par = ch & 1;
                 const int j = tid / 9, k = (tid / 3) % 3, ax = tid % 3;
                 unsigned char *hi = st, *lo = st + TC_MAIN_LO;
-                const int slot = base + j;
-                if (slot < cntb) {
-                    const int id = S.map[neg][slot], q = id / 12, v = id % 12;
+                const int q = S.qs[par][j];
+                if (q >= 0) {
                     const int qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
-                    const float *p = S.pt[q];
-                    float gv[9];
-                    tc_grad_var(p, v, k, gv);
-                    const float r = fabsf(p[TP_RS + v]);
+                    const float *gv = S.gk[par][j][k];
                     const float *bxp = &S.tabf[0][lex][qx * 9 + ax * 3];
                     const float bx0 = bxp[0], bx1 = bxp[1], bx2 = bxp[2];
-                    /* coefficients of By[ky] By-term per kz: derivative m -> (kx, ky, kz) as eval_Bspline */
-                    const float t00 = r * (gv[0] * bx1 + gv[3] * bx2), t01 = r * (gv[1] * bx0 + gv[4] * bx1),
-                                t02 = r * (gv[6] * bx0);
-                    const float t10 = r * (gv[2] * bx0 + gv[5] * bx1), t11 = r * (gv[7] * bx0);
-                    const float t20 = r * (gv[8] * bx0);
+                    /* coefficients of By[ky] per kz: derivative m -> (kx, ky, kz) as eval_Bspline */
+                    const float t00 = gv[0] * bx1 + gv[3] * bx2, t01 = gv[1] * bx0 + gv[4] * bx1, t02 = gv[6] * bx0;
+                    const float t10 = gv[2] * bx0 + gv[5] * bx1, t11 = gv[7] * bx0;
+                    const float t20 = gv[8] * bx0;
+                    const float *bzq = &S.tabf[2][lez][qz * 9];
+                    float bz[9];
+#pragma unroll
+                    for (int i = 0; i < 9; i++) bz[i] = bzq[i];
 #pragma unroll
                     for (int ay = 0; ay < 3; ay++) {
                         const float *byp = &S.tabf[1][ley][qy * 9 + ay * 3];
@@ -534,8 +564,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                         const float cy2 = t20 * byp[0];
 #pragma unroll
                         for (int az = 0; az < 3; az++) {
-                            const float *bzp = &S.tabf[2][lez][qz * 9 + az * 3];
-                            const float y = cy0 * bzp[0] + cy1 * bzp[1] + cy2 * bzp[2];
+                            const float y = cy0 * bz[3 * az] + cy1 * bz[3 * az + 1] + cy2 * bz[3 * az + 2];
                             const int c = 3 * (9 * ax + 3 * ay + az) + k;
                             st_pair(hi, lo, tc_off(c, j), y, 2.f);
                         }
@@ -592,6 +621,11 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                     st_pair(st + TC_G_VHI, st + TC_G_VLO, off, vval, 1.f);
                 }
             }
+            /* coefficients of the next element-matrix chunk (read after the next barrier) */
+            if (ch + 1 < cmain) {
+                const int nb = ch + 1 < cpos ? 0 : 1;
+                tc_prepass<TE>(S, (ch + 1) & 1, nb, (nb ? ch + 1 - cpos : ch + 1) * TC_KC, nb ? nneg : npos);
+            }
             /* hand the chunk to the issuer */
             const int ck = (ch < cpos ? 0 : (ch < cpos + cneg ? 1 : 2)) | (ch == 0 ? 4 : 0);
             if (tid == 0) S.ckind[b] = ck;
@@ -613,7 +647,6 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         }
         if (aborted) break;
         const int g0 = gc - nch;   /* the element's first chunk */
-        const int cmain = cpos + cneg;
         bool used[2][2];
         used[0][g0 & 1] = cmain > 0;
         used[0][(g0 + 1) & 1] = cmain > 1;
@@ -630,30 +663,16 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                           S.rsx[tid - 192], S.rsy[tid - 192]);
         tc_fence_before_sync();
         tc_bar_sync(TC_BAR_BLD, TCN_BLD);
-        /* ---- symmetric part + Gamma on the k1 = k2 blocks, read-modify-write into the CSR
-         * values, four independent entries per thread in flight */
-        for (int i0 = tid; i0 < 81 * 81; i0 += 4 * TCN_BLD) {
-            long off[4];
-            float val[4], old[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const int idx = i0 + u * TCN_BLD;
-                off[u] = -1;
-                if (idx < 81 * 81) {
-                    const int c1 = idx / 81, c2 = idx % 81;
-                    const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
-                    float v = 0.5f * (E[c1 * 81 + c2] + E[c2 * 81 + c1]);
-                    if (k1 == k2) v += 0.5f * (Gm[a1 * 27 + a2] + Gm[a2 * 27 + a1]);
-                    val[u] = v;
-                    off[u] = S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9;
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-                if (off[u] >= 0) old[u] = __ldcg(&vals[off[u]]);   /* L2: written by other CTAs */
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-                if (off[u] >= 0) vals[off[u]] = old[u] + val[u];
+        /* ---- symmetric part + Gamma on the k1 = k2 blocks, added into the CSR values
+         * with fire-and-forget reductions (red.global.add): the tiles of one colour
+         * touch disjoint entries and the elements of a tile are separated by a
+         * barrier, so every entry still receives its additions in a fixed order */
+        for (int idx = tid; idx < 81 * 81; idx += TCN_BLD) {
+            const int c1 = idx / 81, c2 = idx % 81;
+            const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
+            float v = 0.5f * (E[c1 * 81 + c2] + E[c2 * 81 + c1]);
+            if (k1 == k2) v += 0.5f * (Gm[a1 * 27 + a2] + Gm[a2 * 27 + a1]);
+            atomicAdd(&vals[S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9], v);
         }
         tc_bar_sync(TC_BAR_BLD, TCN_BLD);
     }

@@ -159,6 +159,20 @@ class Assembly:
         check(self.lib, "igab_tangent_device",
               self.lib.igab_tangent_device(self.h, vp(U_ptr), vp(vals_ptr), PREC[prec]))
 
+    def dirichlet_rows(self):
+        """Ascending dofs of the Dirichlet residual rows."""
+        n = ctypes.c_long()
+        check(self.lib, "igab_dirichlet_rows", self.lib.igab_dirichlet_rows(self.h, ctypes.byref(n), None))
+        rows = np.empty(n.value, dtype=np.int32)
+        if n.value:
+            check(self.lib, "igab_dirichlet_rows", self.lib.igab_dirichlet_rows(self.h, ctypes.byref(n), _ptr(rows)))
+        return rows
+
+    def history_jacobian_device(self, U_ptr, vals_ptr, level, prec="fp64"):
+        """CSR values of dR/dU_hist[level] (transient physics; Dirichlet rows zero)."""
+        check(self.lib, "igab_history_jacobian_device",
+              self.lib.igab_history_jacobian_device(self.h, vp(U_ptr), vp(vals_ptr), PREC[prec], int(level)))
+
     def graph_capture(self, U_ptr, R_ptr=None, vals_ptr=None, prec="fp64"):
         what = (1 if R_ptr is not None else 0) | (2 if vals_ptr is not None else 0)
         check(self.lib, "igab_graph_capture",

@@ -57,6 +57,11 @@ igab_geom igab_ctx::geom() const
     g.dt = par_mat[7];
     g.phys = phys;
     g.escale = escale_on ? d_escale : nullptr;
+    g.tw[0] = 0.25;
+    g.tw[1] = 1.0 / 6.0;
+    g.tw[2] = 0.125;
+    g.tw[3] = 0.0;
+    g.tmass = g.dt != 0.0 ? g.rho / (g.dt * g.dt) + g.cii / (2.0 * g.dt) : 0.0;
     return g;
 }
 
@@ -667,6 +672,37 @@ extern "C" int igab_tangent(igab_ctx *ctx, const double *U_host, void *vals_host
     if (rc) return rc;
     if (!fin) { igab_set_error("igab_tangent: non-finite entry"); return IGAB_ERR_NONFINITE; }
     return 0;
+}
+
+extern "C" int igab_dirichlet_rows(igab_ctx *ctx, long *n, int *rows)
+{
+    ARG_CHECK(ctx && n, "igab_dirichlet_rows: null argument");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (ctx->dirichlet_dirty) {
+        int rc = build_dirichlet(ctx);
+        if (rc) return rc;
+    }
+    *n = ctx->nd;
+    if (rows && ctx->nd > 0) {
+        IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        IGAB_CUDA_TRY(cudaMemcpy(rows, ctx->d_drow, (size_t)ctx->nd * sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    return 0;
+}
+
+extern "C" int igab_history_jacobian_device(igab_ctx *ctx, const double *U_dev, void *vals_dev, int prec, int level)
+{
+    ARG_CHECK(ctx && U_dev && vals_dev, "igab_history_jacobian_device: null argument");
+    ARG_CHECK(ctx->phys == IGAB_PHYS_GETIME, "igab_history_jacobian_device: needs the transient physics");
+    ARG_CHECK(level == 1 || level == 2, "igab_history_jacobian_device: level must be 1 or 2");
+    ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_history_jacobian_device: bad precision");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    ctx->last_launches = 0;
+    const size_t es = prec == IGAB_PREC_FP64 ? sizeof(double) : sizeof(float);
+    IGAB_CUDA_TRY(cudaMemsetAsync(vals_dev, 0, (size_t)ctx->nnz * es, ctx->stream));
+    int rc = igab_launch_tan_getime_level(ctx, U_dev, vals_dev, prec, level);
+    if (!rc) rc = igab_launch_zero_csr_rows(ctx, vals_dev, prec);
+    return rc;
 }
 
 extern "C" int igab_set_stream(igab_ctx *ctx, void *cuda_stream)

@@ -3,12 +3,18 @@
  *
  * With u(s) = m + s h (m = (u0 + u1)/2, h = (u - u0)/2, see igab_math.cuh),
  * the tangent of the truncated average gradient is
- *   D = 1/2 (H_0/2 + H_1/3 + H_2/4),   H(s) = d2W/du2(m + s h) = sum_j H_j s^j.
+ *   D = 1/2 (H_0/2 + H_1/3 + H_2/4),   H(s) = d2W/du2(m + s h) = sum_j H_j s^j,
+ * and its derivatives with respect to the history levels (the discrete adjoint
+ * of the time stepping) are, through m and h,
+ *   d r/d u1 = 1/2 (H_0 + H_1/2 + H_2/3 + H_3/4),
+ *   d r/d u0 = 1/2 (H_0/2 + H_1/6 + H_2/12 + H_3/4),
+ * all of the form sum_j w_j H_j (w = igab_geom::tw) plus a value-component mass
+ * term (inertia / damping coefficients of u, u1, u0; igab_geom::tmass).
  * Writing H(s) = G(s)^T Phi''(s) G(s) + geo(s) with G(s) = G0 + s G1 exactly linear
  * in s, D becomes a rank-24 form plus an effective geometric block:
  *   D = sum_{a,c in {0,1}} G_a^T M_ac G_c + geo_eff,
- *   M_ac = sum_b cw_{a+b+c} Phi''_b,  cw = (1/4, 1/6, 1/8),
- *   geo_eff = geo built from sum_j cw_j (Phi'_v)_j.
+ *   M_ac = sum_b w_{a+b+c} Phi''_b,
+ *   geo_eff = geo built from sum_j w_j (Phi'_v)_j.
  * M_ac is 2x2 per energy variable (4x4 for the coupled (va, vb) pair). The
  * inertia/damping term (rho/dt^2 + c/(2 dt)) N_a N_b joins the geometric block,
  * which is the same for the three displacement components.
@@ -186,14 +192,15 @@ __global__ void __launch_bounds__(256) k_tan_getime(igab_geom g, const double *_
         /* ---- point data along u(s) = m + s h */
         if (tid < IGAB_NQ3) {
             const int qx = tid & 3, qy = (tid >> 2) & 3, qz = tid >> 4;
-            igab_tay<3> ut[30];
+            igab_tay<4> ut[30];
 #pragma unroll
             for (int i = 0; i < 30; i++) {
                 ut[i].c[0] = 0.5 * (ul[2][i] + ul[1][i]);
                 ut[i].c[1] = 0.5 * (ul[0][i] - ul[2][i]);
                 ut[i].c[2] = 0.0;
+                ut[i].c[3] = 0.0;
             }
-            igab_ge_point<igab_tay<3>> P;
+            igab_ge_point<igab_tay<4>> P;
             igab_ge_eval(ut, g.coef, P);
             double *pt = S.pt[tid];
             for (int k = 0; k < 3; k++)
@@ -206,12 +213,12 @@ __global__ void __launch_bounds__(256) k_tan_getime(igab_geom g, const double *_
                     pt[GP_G0 + 6 * k + c] = P.G[k][c].c[0];
                     pt[GP_G1 + 6 * k + c] = P.G[k][c].c[1];
                 }
-            const double cw[3] = {0.25, 1.0 / 6.0, 0.125};
+            const double *cw = g.tw;
             for (int v = 0; v < 12; v++) {
                 const double *f = P.d2[v].c;
-                pt[GP_MD + 3 * v + 0] = cw[0] * f[0] + cw[1] * f[1] + cw[2] * f[2];
-                pt[GP_MD + 3 * v + 1] = cw[1] * f[0] + cw[2] * f[1];
-                pt[GP_MD + 3 * v + 2] = cw[2] * f[0];
+                pt[GP_MD + 3 * v + 0] = cw[0] * f[0] + cw[1] * f[1] + cw[2] * f[2] + cw[3] * f[3];
+                pt[GP_MD + 3 * v + 1] = cw[1] * f[0] + cw[2] * f[1] + cw[3] * f[2];
+                pt[GP_MD + 3 * v + 2] = cw[2] * f[0] + cw[3] * f[1];
             }
             /* (va, vb) x (G0, G1): row r = 2 i + a, i = 0 (va), 1 (vb) */
             for (int r = 0; r < 4; r++)
@@ -219,19 +226,22 @@ __global__ void __launch_bounds__(256) k_tan_getime(igab_geom g, const double *_
                     const int i1 = r >> 1, a = r & 1, i2 = c2 >> 1, c = c2 & 1;
                     const double *f = (i1 == i2) ? P.d2[1 + i1].c : P.d2ab.c;
                     double t = 0.0;
-                    for (int b = 0; b < 3; b++)
-                        if (a + b + c < 3) t += cw[a + b + c] * f[b];
+                    for (int b = 0; b < 4; b++)
+                        if (a + b + c < 4) t += cw[a + b + c] * f[b];
                     pt[GP_M12 + 4 * r + c2] = t;
                 }
             for (int I = 0; I < 3; I++) {
-                pt[GP_SIG + I] = cw[0] * P.sig[I].c[0] + cw[1] * P.sig[I].c[1] + cw[2] * P.sig[I].c[2];
-                pt[GP_D1S + I] = cw[0] * P.d1[3 + I].c[0] + cw[1] * P.d1[3 + I].c[1] + cw[2] * P.d1[3 + I].c[2];
+                pt[GP_SIG + I] = cw[0] * P.sig[I].c[0] + cw[1] * P.sig[I].c[1] + cw[2] * P.sig[I].c[2] +
+                                 cw[3] * P.sig[I].c[3];
+                pt[GP_D1S + I] = cw[0] * P.d1[3 + I].c[0] + cw[1] * P.d1[3 + I].c[1] + cw[2] * P.d1[3 + I].c[2] +
+                                 cw[3] * P.d1[3 + I].c[3];
                 for (int K = 0; K < 3; K++)
-                    pt[GP_TAU + 3 * I + K] = cw[0] * P.tau[I][K].c[0] + cw[1] * P.tau[I][K].c[1] + cw[2] * P.tau[I][K].c[2];
+                    pt[GP_TAU + 3 * I + K] = cw[0] * P.tau[I][K].c[0] + cw[1] * P.tau[I][K].c[1] +
+                                             cw[2] * P.tau[I][K].c[2] + cw[3] * P.tau[I][K].c[3];
             }
             pt[GP_W] = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz] *
                        elem_scale(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez);
-            pt[GP_MASS] = g.rho / (g.dt * g.dt) + g.cii / (2.0 * g.dt);
+            pt[GP_MASS] = g.tmass;
         }
         __syncthreads();
 
@@ -365,9 +375,18 @@ __global__ void __launch_bounds__(256) k_tan_getime(igab_geom g, const double *_
 }
 
 template <typename T>
-int launch_t(igab_ctx *c, const double *dU, T *dv)
+int launch_t(igab_ctx *c, const double *dU, T *dv, int level)
 {
     igab_geom g = c->geom();
+    if (level == 1) {          /* d r / d u1 */
+        const double w[4] = {0.5, 0.25, 1.0 / 6.0, 0.125};
+        for (int j = 0; j < 4; j++) g.tw[j] = w[j];
+        g.tmass = -2.0 * g.rho / (g.dt * g.dt);
+    } else if (level == 2) {   /* d r / d u0 */
+        const double w[4] = {0.25, 1.0 / 12.0, 1.0 / 24.0, 0.125};
+        for (int j = 0; j < 4; j++) g.tw[j] = w[j];
+        g.tmass = g.rho / (g.dt * g.dt) - g.cii / (2.0 * g.dt);
+    }
     size_t sm = sizeof(gt_smem<T, 2>);
     IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_getime<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     for (int colour = 0; colour < 8; colour++) {
@@ -384,5 +403,11 @@ int launch_t(igab_ctx *c, const double *dU, T *dv)
 
 int igab_launch_tan_getime(igab_ctx *c, const double *dU, void *dv, int prec)
 {
-    return prec == IGAB_PREC_FP64 ? launch_t<double>(c, dU, (double *)dv) : launch_t<float>(c, dU, (float *)dv);
+    return igab_launch_tan_getime_level(c, dU, dv, prec, 0);
+}
+
+int igab_launch_tan_getime_level(igab_ctx *c, const double *dU, void *dv, int prec, int level)
+{
+    return prec == IGAB_PREC_FP64 ? launch_t<double>(c, dU, (double *)dv, level)
+                                  : launch_t<float>(c, dU, (float *)dv, level);
 }

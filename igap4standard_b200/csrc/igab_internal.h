@@ -34,6 +34,11 @@ struct igab_geom {
     int phys;
     /* per-element integrand scale s_e = exp(g_e), element e = (ex*ne1 + ey)*ne2 + ez; null: 1 */
     const double *escale;
+    /* phys/getime tangent-type assembly: weights w_j of the Hessian Taylor coefficients H_j
+     * (j = 0..3) and the coefficient of the value-component mass term; the tangent d r/d u
+     * is w = (1/4, 1/6, 1/8, 0), mass rho/dt^2 + c/(2 dt) (igab_getime.cu) */
+    double tw[4];
+    double tmass;
 };
 
 /* Batched assembly: the work list of a persistent launch over many meshes.
@@ -152,6 +157,10 @@ int igab_batch_occupancy_res(int *per_sm);
 int igab_batch_occupancy_dmma(int *per_sm);
 int igab_batch_occupancy_tc32(int *per_sm);
 int igab_launch_tan_getime(igab_ctx *c, const double *dU, void *dv, int prec);
+/* zero the Dirichlet rows of CSR values (rows only) */
+int igab_launch_zero_csr_rows(igab_ctx *c, void *dv, int prec);
+/* the same kernel with explicit weights (history Jacobians); level 0 = tangent */
+int igab_launch_tan_getime_level(igab_ctx *c, const double *dU, void *dv, int prec, int level);
 int igab_launch_exp_scale(igab_ctx *c, const double *dg);
 int igab_launch_adjoint_dRdg(igab_ctx *c, const double *dU, const double *dlam, double *dgrad);
 int igab_launch_tangent_transpose(igab_ctx *c, const void *dvals, int prec, const double *dx, double *dy);

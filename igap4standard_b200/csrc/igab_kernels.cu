@@ -687,6 +687,19 @@ __global__ void k_tan_dirichlet(igab_geom g, long nd, const int *__restrict__ dr
     tan_dirichlet_entry<T>(g, drow[j], s, vals);
 }
 
+/* zero the Dirichlet rows of a CSR matrix (no column change, no diagonal): one thread per
+ * (row, entry of that row) */
+template <typename T>
+__global__ void k_zero_csr_rows(igab_geom g, long nd, const int *__restrict__ drow, T *__restrict__ vals)
+{
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    long j = t / 375;
+    int s = (int)(t % 375);
+    if (j >= nd) return;
+    const int r = drow[j];
+    if (s < g.rowptr[r + 1] - g.rowptr[r]) vals[g.rowptr[r] + s] = T(0);
+}
+
 /* the same over the Dirichlet rows of all instances of a batch (row j of instance dinst[j]) */
 template <typename T>
 __global__ void k_tan_dirichlet_batch(igab_batch_dev B, long nd, const int *__restrict__ dinst,
@@ -990,6 +1003,20 @@ int igab_launch_tan_dirichlet_batch(const igab_batch_dev &B, long nd, const int 
         k_tan_dirichlet_batch<double><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(B, nd, dinst, drow, (double *)dv);
     else
         k_tan_dirichlet_batch<float><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(B, nd, dinst, drow, (float *)dv);
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int igab_launch_zero_csr_rows(igab_ctx *c, void *dv, int prec)
+{
+    if (c->nd <= 0) return 0;
+    const igab_geom g = c->geom();
+    const long n = c->nd * 375;
+    if (prec == IGAB_PREC_FP64)
+        k_zero_csr_rows<double><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(g, c->nd, c->d_drow, (double *)dv);
+    else
+        k_zero_csr_rows<float><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(g, c->nd, c->d_drow, (float *)dv);
+    c->last_launches++;
     IGAB_CUDA_TRY(cudaGetLastError());
     return 0;
 }

@@ -94,6 +94,8 @@ IGAB_API = [
     ("igab_get_option", ctypes.c_int, [vp, ctypes.c_int, c_int_p]),
     ("igab_tc_selftest", ctypes.c_int, [ctypes.c_int, vp]),
     ("igab_tc_peak", ctypes.c_int, [ctypes.c_int, ctypes.c_int, c_double_p]),
+    ("igab_history_jacobian_device", ctypes.c_int, [vp, vp, vp, ctypes.c_int, ctypes.c_int]),
+    ("igab_dirichlet_rows", ctypes.c_int, [vp, c_long_p, vp]),
     ("igab_batch_create", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]),
     ("igab_batch_destroy", ctypes.c_int, [vp]),
     ("igab_batch_sizes", ctypes.c_int, [vp, c_long_p, c_long_p, c_long_p, vp, vp]),

@@ -140,8 +140,9 @@ def bicgstab(matvec, b, dinv, rtol=1e-5, atol=0.0, maxit=2000):
     return x, maxit, False
 
 
-def newton_device(P, rtol_lin=1e-5, max_subiter=newton.MAX_SUBITER):
-    """snes_solve semantics on device tensors; the iterate is P.X (updated in place)."""
+def newton_device(P, rtol_lin=1e-5, max_subiter=newton.MAX_SUBITER, abs_tol=newton.ABS_TOL):
+    """snes_solve semantics on device tensors; the iterate is P.X (updated in place).
+    abs_tol: the absolute ||F|| test (1e-10 in the reference, src/snes_init.c:18)."""
     torch = _torch()
     res = newton.NewtonResult(U=None, converged=False, reason=newton.DIVERGED_MAX_IT, iterations=0)
     f_old = 999.0
@@ -151,7 +152,7 @@ def newton_device(P, rtol_lin=1e-5, max_subiter=newton.MAX_SUBITER):
         fnorm = float(F.norm())
         if not np.isfinite(fnorm):
             reason = newton.DIVERGED_FNORM_NAN
-        elif fnorm < newton.ABS_TOL:
+        elif fnorm < abs_tol:
             reason = newton.CONVERGED_FNORM_ABS
         else:
             ttol = fnorm * newton.REL_TOL
@@ -170,7 +171,7 @@ def newton_device(P, rtol_lin=1e-5, max_subiter=newton.MAX_SUBITER):
                 reason = newton.DIVERGED_LINE_SEARCH
             elif not np.isfinite(fnorm):
                 reason = newton.DIVERGED_FNORM_NAN
-            elif fnorm < newton.ABS_TOL:
+            elif fnorm < abs_tol:
                 reason = newton.CONVERGED_FNORM_ABS
             elif fnorm <= ttol:
                 reason = newton.CONVERGED_FNORM_RELATIVE
@@ -198,17 +199,17 @@ def traction_values(A, t, amplitude=0.01, face=1, order=0, dof=0):
 
 
 def run(A, nsteps, dt, prec="fp32", use_graph=True, rtol_lin=1e-5, traction=traction_values, U_init=None,
-        U_prev=None, callback=None):
+        U_prev=None, callback=None, abs_tol=newton.ABS_TOL):
     """Time-step A (an Assembly with phys="getime") nsteps times from the history
     (U_init at t_0, U_prev at t_{-1}; zeros by default).  Returns (history of U per
     step as host arrays, per-step NewtonResults, DeviceProblem)."""
     torch = _torch()
     P = DeviceProblem(A, prec, use_graph)
     with torch.cuda.stream(P.stream):
-        return _run(P, A, nsteps, dt, rtol_lin, traction, U_init, U_prev, callback)
+        return _run(P, A, nsteps, dt, rtol_lin, traction, U_init, U_prev, callback, abs_tol)
 
 
-def _run(P, A, nsteps, dt, rtol_lin, traction, U_init, U_prev, callback):
+def _run(P, A, nsteps, dt, rtol_lin, traction, U_init, U_prev, callback, abs_tol=newton.ABS_TOL):
     torch = _torch()
     n = A.ndof
     h1 = torch.zeros(n, dtype=torch.float64, device=P.dev)   # U at t_n     (U_hist level 1)
@@ -224,7 +225,7 @@ def _run(P, A, nsteps, dt, rtol_lin, traction, U_init, U_prev, callback):
         A.set_history_device(1, h1.data_ptr())
         A.set_history_device(2, h0.data_ptr())
         P.X.copy_(h1)                                   # initguess: U <- U_hist[1]
-        r = newton_device(P, rtol_lin=rtol_lin)
+        r = newton_device(P, rtol_lin=rtol_lin, abs_tol=abs_tol)
         results.append(r)
         h0.copy_(h1)                                    # history shift (main.c:55)
         h1.copy_(P.X)
@@ -232,3 +233,112 @@ def _run(P, A, nsteps, dt, rtol_lin, traction, U_init, U_prev, callback):
         if callback:
             callback(step, r)
     return hist, results, P
+
+
+# ---------------------------------------------------------------------------
+# Discrete adjoint of the time stepping (element-scaled problem, s_e = exp(g_e))
+#
+# Steps n = 0..N-1 solve R_n(U_{n+1}; U_n, U_{n-1}, g) = 0 (levels: U_hist[1] = U_n,
+# U_hist[2] = U_{n-1}).  For an objective J(U_N), with L = J - sum_n lam_n . R_n,
+#   K_n^T lam_n = b_n,  b_n = dJ/dU_{n+1} - J1_{n+1}^T lam_{n+1} - J0_{n+2}^T lam_{n+2},
+#   dJ/dg = - sum_n lam_n . dR_n/dg,
+# K_n = dR_n/dU_{n+1} (the tangent), J1_n = dR_n/dU_n, J0_n = dR_n/dU_{n-1} (the history
+# Jacobians, igab_history_jacobian_device).  The Dirichlet rows of R_n do not depend on
+# g or on the history, so lam is zero there (b is zeroed on those rows; K is the
+# symmetric-eliminated tangent, identity there).  States are kept at checkpoints every
+# `every` steps (U_{s-1}, U_s) and each segment is recomputed forward before its
+# backward sweep, so memory is O(N / every + every) states.
+
+
+def _sym_solve(P, b, rtol):
+    torch = _torch()
+    d = P.diagonal()
+    dinv = torch.where(d != 0, 1.0 / d, torch.ones_like(d))
+    x, its, ok = bicgstab(P.matvec, b, dinv, rtol=rtol)
+    return x
+
+
+def _forward_steps(P, A, n0, n1, dt, states, rtol_lin, traction, abs_tol):
+    """Steps n0..n1-1 from states[n0-1], states[n0] (device tensors); fills states[n0+1..n1]."""
+    torch = _torch()
+    h1 = states[n0].clone()
+    h0 = states[n0 - 1].clone()
+    results = []
+    for n in range(n0, n1):
+        A.set_neumann_values(traction(A, (n + 1) * dt))
+        A.set_history_device(1, h1.data_ptr())
+        A.set_history_device(2, h0.data_ptr())
+        P.X.copy_(h1)
+        r = newton_device(P, rtol_lin=rtol_lin, abs_tol=abs_tol)
+        results.append(r)
+        h0, h1 = h1, P.X.clone()
+        states[n + 1] = h1
+    return results
+
+
+def adjoint(A, nsteps, dt, g, dJdU_final, every=10, rtol_lin=1e-12, traction=traction_values, abs_tol=1e-13,
+            U_init=None, U_prev=None, objective=None):
+    """Forward solve of nsteps steps with element log-scales g and checkpoints every
+    `every` steps, then the backward sweep.  dJdU_final(U_N) -> dJ/dU_N (host or device
+    array); objective(U_N) -> J (optional).  Returns dict(J, grad (dJ/dg, host), U_N,
+    checkpoints, forward_results, recomputed_steps)."""
+    torch = _torch()
+    P = DeviceProblem(A, "fp64", use_graph=False)
+    n, ne = A.ndof, A.nelem_total
+    with torch.cuda.stream(P.stream):
+        A.set_element_log_scale(np.asarray(g, dtype=np.float64))
+        zero = torch.zeros(n, dtype=torch.float64, device=P.dev)
+        u0 = zero.clone() if U_init is None else torch.as_tensor(np.asarray(U_init, np.float64), device=P.dev)
+        um = zero.clone() if U_prev is None else torch.as_tensor(np.asarray(U_prev, np.float64), device=P.dev)
+        ckpt = {0: (um.clone(), u0.clone())}
+        states = {-1: um, 0: u0}
+        fwd = []
+        for s in range(0, nsteps, every):
+            e = min(s + every, nsteps)
+            seg = {s - 1: states[s - 1], s: states[s]}
+            fwd += _forward_steps(P, A, s, e, dt, seg, rtol_lin, traction, abs_tol)
+            states = {e - 1: seg[e - 1], e: seg[e]}
+            if e < nsteps:
+                ckpt[e] = (seg[e - 1].clone(), seg[e].clone())
+        UN = states[nsteps]
+        J = objective(UN.cpu().numpy()) if objective else None
+        # ---- backward sweep
+        drows = torch.as_tensor(A.dirichlet_rows(), device=P.dev, dtype=torch.long)
+        b = {nsteps - 1: torch.as_tensor(np.asarray(dJdU_final(UN.cpu().numpy()), np.float64),
+                                         device=P.dev).clone()}
+        grad = torch.zeros(ne, dtype=torch.float64, device=P.dev)
+        gstep = torch.empty(ne, dtype=torch.float64, device=P.dev)
+        Vj = torch.empty(A.nnz, dtype=torch.float64, device=P.dev)
+        c = torch.empty(n, dtype=torch.float64, device=P.dev)
+        recomputed = 0
+        for s in sorted(ckpt.keys(), reverse=True):
+            e = min(s + every, nsteps)
+            seg = {s - 1: ckpt[s][0], s: ckpt[s][1]}
+            _forward_steps(P, A, s, e, dt, seg, rtol_lin, traction, abs_tol)
+            recomputed += e - s
+            for k in range(e - 1, s - 1, -1):
+                bk = b.pop(k, None)
+                if bk is None:
+                    continue                      # no objective dependence reaches this step
+                bk[drows] = 0.0
+                A.set_history_device(1, seg[k].data_ptr())
+                A.set_history_device(2, seg[k - 1].data_ptr())
+                U = seg[k + 1]
+                A.tangent_device(U.data_ptr(), P.V.data_ptr(), "fp64")          # K_k
+                lam = _sym_solve(P, bk, rtol_lin)
+                lam[drows] = 0.0
+                A.adjoint_backward_device(U.data_ptr(), None, lam.data_ptr(), None, gstep.data_ptr(), "fp64")
+                grad += gstep
+                for level, tgt in ((1, k - 1), (2, k - 2)):
+                    if tgt < 0:
+                        continue
+                    A.history_jacobian_device(U.data_ptr(), Vj.data_ptr(), level, "fp64")
+                    A.adjoint_backward_device(None, Vj.data_ptr(), lam.data_ptr(), c.data_ptr(), None, "fp64")
+                    if tgt in b:
+                        b[tgt] -= c
+                    else:
+                        b[tgt] = -c
+        A.set_element_log_scale(None)
+        P.stream.synchronize()
+        return dict(J=J, grad=(-grad).cpu().numpy(), U_N=UN.cpu().numpy(), checkpoints=sorted(ckpt.keys()),
+                    forward_results=fwd, recomputed_steps=recomputed)

@@ -207,6 +207,13 @@ typedef struct {
 } igab_batch_tune_result;
 int igab_batch_autotune(igab_batch *b, const double *U_dev, int what, int reps, igab_batch_tune_result *out);
 
+/* ---- history Jacobians of the transient physics (no reference counterpart; the discrete
+ * adjoint of the time stepping needs them): CSR values (the tangent's pattern) of
+ * d R / d U_hist[level] at U and the context's history levels, level 1 (t_n) or 2 (t_{n-1});
+ * Dirichlet rows are zero (R = U - g there does not depend on the history).  The
+ * matrices are symmetric; apply their transpose with igab_adjoint_backward. */
+int igab_history_jacobian_device(igab_ctx *ctx, const double *U_dev, void *vals_dev, int prec, int level);
+
 /* ---- residual for callers that cannot have the library allocate device memory.
  * No counterpart in the reference.  Same result as igab_residual, but U and R
  * are staged in a file-scope device array (2 x 8 MiB, held by every GPU that

@@ -10,16 +10,23 @@
  * the eigenvectors of that 2x2 block makes it diagonal, so
  *   K_e = X'^T diag(s) X',   s = w_q * eigenvalues.
  * Both products run on DMMA tiles:
- *   - X' (48 rows = 4 Gauss points x 12 variables, 88 padded columns) sits in
- *     shared memory once; a warp loads its A fragments from it and forms its
- *     B fragments by scaling the same registers with s.  The 66 upper 8x8
- *     tiles of the 88x88 element matrix are spread over the 4 warps (table in
- *     igab_warp_tiles.inc), the lower triangle follows by symmetry.
- *   - Gamma (32x32 padded, 10 upper tiles) from N^T and w geo N.
- * 128 threads and ~108 KB of shared memory per block let two blocks share
- * an SM, so one block's scalar work (field, point integrand, X') overlaps the
- * other's tensor work.  Scatter: read-modify-write into the CSR values,
- * conflict-free within one of the 8 tile colours (igab_kernels.cu).
+ *   - X' (48 rows = 4 Gauss points x 12 variables, 88 padded columns) is built
+ *     in shared memory straight from the 1-D basis tables (sum factorisation of
+ *     sum_m dv'/du_{k,m} N_a^m over x, y, z; one task per (point, variable,
+ *     component, x-function), the variable warp-uniform); a warp loads its A
+ *     fragments from it and forms its B fragments by scaling the same
+ *     registers with s.  The 66 upper 8x8 tiles of the 88x88 element matrix are
+ *     spread over the 4 warps (table in igab_warp_tiles.inc), the lower
+ *     triangle follows by symmetry.
+ *   - Gamma (27 x 27, identical for the three components) in the rank-6 form
+ *     Gamma = sum_q sum_i U_qi V_qi^T with geo = [[S, T], [T^T, 0]]:
+ *       U_i = d_i N_a, V_i = w ((S grad N_a)_i + (T H_a)_i)     (i < 3)
+ *       U_i = w (T H_a)_I, V_i = d_I N_a                         (i = 3 + I)
+ *     on 10 upper 8x8 tiles of the 32-padded block, 6 k-rows per point.
+ * 128 threads and ~90 KB of shared memory per block let two blocks share an
+ * SM, so one block's scalar work (field, point integrand, X') overlaps the
+ * other's tensor work.  Scatter: fire-and-forget reductions into the CSR
+ * values, conflict-free within one of the 8 tile colours (igab_kernels.cu).
  */
 #include <cuda_runtime.h>
 #include "igab_device.cuh"
@@ -31,9 +38,9 @@ namespace {
 #define NTHR 128
 #define DQ 4            /* Gauss points per batch */
 #define DROWS (DQ * 12) /* k rows of X' per batch */
-#define GROWS (DQ * 9)  /* k rows of the geometric product per batch */
+#define GROWS (DQ * 6)  /* k rows of the geometric product per batch: U / V rows, 6 per point */
 #define XS 100          /* X' row stride (doubles): = 4 mod 16 keeps fragment loads conflict-free */
-#define GS 36           /* N^T / GN row stride: = 4 mod 16 */
+#define GS 36           /* U / V row stride: = 4 mod 16; columns a >= 27 stay zero */
 
 /* point data */
 #define PT_F 0
@@ -47,28 +54,26 @@ namespace {
 #define PT_W 56
 #define PT_N 57
 
-/* work buffer: interpolation A[972] C[864] | X'[48][100] + points[64][57] | K[88][88] */
+/* work buffer: interpolation A[972] C[864] | X'[48][100] + points[64][57] | K[88][88] + Gamma[32][32] */
 #define W_A 0
 #define W_C 972
 #define W_X 0
 #define W_PT (DROWS * XS)
 #define W_SIZE (DROWS * XS + IGAB_NQ3 * PT_N)
+#define W_GAM (88 * 88)
+#define W_ALL (W_SIZE > W_GAM + 32 * 32 ? W_SIZE : W_GAM + 32 * 32)
 
 template <int TE>
 struct dmma_smem {
     static constexpr int TC = TE + 2;
     static constexpr int NCP = TC * TC * TC;
-    double W[W_SIZE > 88 * 88 ? W_SIZE : 88 * 88];
-    double NT[GROWS][GS];     /* N^T: row 9 qb + m, column a (a >= 27 zero); Gamma[32][32] at the end */
-    double GN[GROWS][GS];     /* w geo N: row 9 qb + m, column b (b >= 27 zero) */
-    double Gv[DQ][12][27];    /* rotated dv/du_s */
-    double geo[DQ][81];
+    double W[W_ALL];
+    double UT[GROWS][GS];     /* U rows of the geometric product: row 6 qb + i, column a */
+    double VT[GROWS][GS];     /* V rows */
     double sc[DROWS];
     double U[NCP * 3];
     double tab[3][TE][IGAB_TAB1D];
     double wh[3][TE][IGAB_NQ];
-    double gcoef[12][9];
-    int gsrc[12][9];
     long rbase[81];       /* CSR row bases of the element matrix (elem_row_base) */
     int rsx[81], rsy[81];
 };
@@ -98,7 +103,7 @@ __device__ __forceinline__ void sym2_eig(double a, double b, double c, double &c
 
 template <int W>
 __device__ __forceinline__ void warp_mma(const double *__restrict__ X, const double *__restrict__ sc,
-                                         const double *__restrict__ NT, const double *__restrict__ GN, int lane,
+                                         const double *__restrict__ UT, const double *__restrict__ VT, int lane,
                                          double (&acc)[17][2], double (&gacc)[3][2])
 {
     using WT = warp_tiles<W>;
@@ -122,9 +127,9 @@ __device__ __forceinline__ void warp_mma(const double *__restrict__ X, const dou
         const int kr = 4 * kb + r4;
         double fa[WT::NGA], fb[WT::NGB];
 #pragma unroll
-        for (int b = 0; b < WT::NGA; b++) fa[b] = NT[kr * GS + 8 * WT::gablk(b) + c8];
+        for (int b = 0; b < WT::NGA; b++) fa[b] = UT[kr * GS + 8 * WT::gablk(b) + c8];
 #pragma unroll
-        for (int b = 0; b < WT::NGB; b++) fb[b] = GN[kr * GS + 8 * WT::gbblk(b) + c8];
+        for (int b = 0; b < WT::NGB; b++) fb[b] = VT[kr * GS + 8 * WT::gbblk(b) + c8];
 #pragma unroll
         for (int t = 0; t < WT::NGT; t++) dmma(gacc[t][0], gacc[t][1], fa[WT::gti(t)], fb[WT::gtj(t)]);
     }
@@ -159,6 +164,47 @@ __device__ __forceinline__ void warp_dump(double *__restrict__ K, double *__rest
     default: CALL(3); break; \
     }
 
+/* gradient of rotated variable v with respect to the 9 strain components of
+ * displacement component k (igab_ge_grad_var, then the (va, vb) rotation) */
+__device__ __forceinline__ void dm_grad_var(const double *p, int v, int k, double g[9])
+{
+#pragma unroll
+    for (int m = 0; m < 9; m++) g[m] = 0.0;
+    const double is2 = IGAB_INV_SQRT2, is3 = IGAB_INV_SQRT3, is6 = IGAB_INV_SQRT6;
+    const double F0 = p[PT_F + 3 * k], F1 = p[PT_F + 3 * k + 1], F2 = p[PT_F + 3 * k + 2];
+    const double *G = p + PT_G + 6 * k;
+    if (v == 0) {
+        g[0] = F0 * is3; g[1] = F1 * is3; g[2] = F2 * is3;
+    } else if (v <= 2) {
+        const double cs = p[PT_CS], sn = p[PT_SN];
+        const double a0 = F0 * is2, a1 = -F1 * is2;                       /* va */
+        const double b0 = F0 * is6, b1 = F1 * is6, b2 = -2.0 * F2 * is6;  /* vb */
+        if (v == 1) { g[0] = cs * a0 - sn * b0; g[1] = cs * a1 - sn * b1; g[2] = -sn * b2; }
+        else        { g[0] = sn * a0 + cs * b0; g[1] = sn * a1 + cs * b1; g[2] = cs * b2; }
+    } else if (v == 3) {
+        g[0] = 0.5 * F1; g[1] = 0.5 * F0;
+    } else if (v == 4) {
+        g[0] = 0.5 * F2; g[2] = 0.5 * F0;
+    } else if (v == 5) {
+        g[1] = 0.5 * F2; g[2] = 0.5 * F1;
+    } else if (v == 6) {   /* strain-gradient variables (idx6: xx xy xz yy yz zz) */
+        g[0] = G[0] * is2; g[1] = -G[1] * is2; g[3] = F0 * is2; g[4] = -F1 * is2;
+    } else if (v == 7) {
+        g[0] = G[1] * is2; g[1] = -G[3] * is2; g[4] = F0 * is2; g[6] = -F1 * is2;
+    } else if (v == 8) {
+        g[0] = G[2] * is2; g[1] = -G[4] * is2; g[5] = F0 * is2; g[7] = -F1 * is2;
+    } else if (v == 9) {
+        g[0] = G[0] * is6; g[1] = G[1] * is6; g[2] = -2.0 * G[2] * is6;
+        g[3] = F0 * is6; g[4] = F1 * is6; g[5] = -2.0 * F2 * is6;
+    } else if (v == 10) {
+        g[0] = G[1] * is6; g[1] = G[3] * is6; g[2] = -2.0 * G[4] * is6;
+        g[4] = F0 * is6; g[6] = F1 * is6; g[7] = -2.0 * F2 * is6;
+    } else {
+        g[0] = G[2] * is6; g[1] = G[4] * is6; g[2] = -2.0 * G[5] * is6;
+        g[5] = F0 * is6; g[7] = F1 * is6; g[8] = -2.0 * F2 * is6;
+    }
+}
+
 /* one tile: all NTHR threads of the block, uniformly */
 template <int TE>
 __device__ __forceinline__ void dmma_tile(const igab_geom &g, const tile_t &Tl, const double *__restrict__ U,
@@ -187,42 +233,10 @@ __device__ __forceinline__ void dmma_tile(const igab_geom &g, const tile_t &Tl, 
         int d = idx / (TE * IGAB_NQ), r = idx % (TE * IGAB_NQ), le = r / IGAB_NQ, q = r % IGAB_NQ;
         S.wh[d][le][q] = le < Tl.nv[d] ? g.wh[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
     }
-    /* sparse structure of dv/du_{k,m}: one source term per (v, m) (igab_ge_grad_var) */
-    if (tid < 108) {
-        const int v = tid / 9, m = tid % 9;
-        int src = -1;
-        double cf = 0.0;
-        const double is2 = IGAB_INV_SQRT2, is3 = IGAB_INV_SQRT3, is6 = IGAB_INV_SQRT6;
-        if (v == 0) { if (m < 3) { src = m; cf = is3; } }
-        else if (v == 1) { if (m == 0) { src = 0; cf = is2; } else if (m == 1) { src = 1; cf = -is2; } }
-        else if (v == 2) { if (m < 2) { src = m; cf = is6; } else if (m == 2) { src = 2; cf = -2.0 * is6; } }
-        else if (v == 3) { if (m == 0) { src = 1; cf = 0.5; } else if (m == 1) { src = 0; cf = 0.5; } }
-        else if (v == 4) { if (m == 0) { src = 2; cf = 0.5; } else if (m == 2) { src = 0; cf = 0.5; } }
-        else if (v == 5) { if (m == 1) { src = 2; cf = 0.5; } else if (m == 2) { src = 1; cf = 0.5; } }
-        else {
-            const int K = v < 9 ? v - 6 : v - 9;
-            const int q0 = igab_idx6(0, K), q1 = igab_idx6(1, K), q2 = igab_idx6(2, K);
-            if (v < 9) {
-                if (m == 0) { src = 3 + q0; cf = is2; }
-                else if (m == 1) { src = 3 + q1; cf = -is2; }
-                else if (m == 3 + q0) { src = 0; cf = is2; }
-                else if (m == 3 + q1) { src = 1; cf = -is2; }
-            } else {
-                if (m == 0) { src = 3 + q0; cf = is6; }
-                else if (m == 1) { src = 3 + q1; cf = is6; }
-                else if (m == 2) { src = 3 + q2; cf = -2.0 * is6; }
-                else if (m == 3 + q0) { src = 0; cf = is6; }
-                else if (m == 3 + q1) { src = 1; cf = is6; }
-                else if (m == 3 + q2) { src = 2; cf = -2.0 * is6; }
-            }
-        }
-        S.gsrc[v][m] = src;
-        S.gcoef[v][m] = cf;
-    }
-    /* padding (a, b >= 27) of N^T and GN stays zero */
+    /* the padding columns (a >= 27) of U / V stay zero */
     for (int idx = tid; idx < GROWS * GS; idx += NTHR) {
-        (&S.NT[0][0])[idx] = 0.0;
-        (&S.GN[0][0])[idx] = 0.0;
+        (&S.UT[0][0])[idx] = 0.0;
+        (&S.VT[0][0])[idx] = 0.0;
     }
     __syncthreads();
 
@@ -306,94 +320,88 @@ __device__ __forceinline__ void dmma_tile(const igab_geom &g, const tile_t &Tl, 
         for (int t = 0; t < 3; t++) gacc[t][0] = gacc[t][1] = 0.0;
 
         for (int q0 = 0; q0 < IGAB_NQ3; q0 += DQ) {
-            /* (a) basis products (as N^T), rotated variable gradients, scales, geometric blocks */
             if (q0 == 0)   /* the interpolation / staging data under X' is dead: padding columns back to zero */
                 for (int idx = tid; idx < DROWS * (XS - 81); idx += NTHR)
                     Xb[(idx / (XS - 81)) * XS + 81 + idx % (XS - 81)] = 0.0;
-            for (int o = tid; o < DQ * 243; o += NTHR) {
-                int m = o % 9, a = (o / 9) % 27, qb = o / 243;
-                int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
-                int al = m + 1;
-                S.NT[9 * qb + m][a] = Bx[qx * 9 + (a / 9) * 3 + a_kx(al)] * By[qy * 9 + ((a / 3) % 3) * 3 + a_ky(al)] *
-                                      Bz[qz * 9 + (a % 3) * 3 + a_kz(al)];
-            }
-            for (int o = tid; o < DQ * 12 * 27; o += NTHR) {
-                const int sidx = o % 27, v = (o / 27) % 12, qb = o / 324;
-                const int k = sidx / 9, m = sidx % 9;
-                const double *pt = PTb + (q0 + qb) * PT_N;
-                double val;
-                if (v == 1 || v == 2) {
-                    const int i1 = S.gsrc[1][m], i2 = S.gsrc[2][m];
-                    const double g1 = i1 < 0 ? 0.0 : S.gcoef[1][m] * (i1 < 3 ? pt[PT_F + 3 * k + i1] : pt[PT_G + 6 * k + i1 - 3]);
-                    const double g2 = i2 < 0 ? 0.0 : S.gcoef[2][m] * (i2 < 3 ? pt[PT_F + 3 * k + i2] : pt[PT_G + 6 * k + i2 - 3]);
-                    const double cs = pt[PT_CS], sn = pt[PT_SN];
-                    val = v == 1 ? cs * g1 - sn * g2 : sn * g1 + cs * g2;
-                } else {
-                    const int i0 = S.gsrc[v][m];
-                    val = i0 < 0 ? 0.0 : S.gcoef[v][m] * (i0 < 3 ? pt[PT_F + 3 * k + i0] : pt[PT_G + 6 * k + i0 - 3]);
-                }
-                if (sidx == 0) S.sc[qb * 12 + v] = pt[PT_W] * pt[PT_LAM + v];
-                S.Gv[qb][v][sidx] = val;
-            }
-            for (int o = tid; o < DQ * 81; o += NTHR) {
-                const int n = o % 9, m = (o / 9) % 9, qb = o / 81;
-                const double *pt = PTb + (q0 + qb) * PT_N;
-                const int lo = m < n ? m : n, hi = m < n ? n : m;
-                double gv = 0.0;
-                if (hi < 3) {
-                    gv = lo == hi ? pt[PT_SIG + lo] : 0.5 * pt[PT_D1S + (lo == 0 ? hi - 1 : 2)];
-                } else if (lo < 3) {
+            /* (a) X' rows: task (variable v, point qb, component k, x-function ax) -> 9 outputs
+             * (ay, az), X'[(qb, v)][3a + k] = sum_m dv'/du_{k,m} Bx By Bz, summed over x, y, z */
+            for (int t = tid; t < DQ * 12 * 9; t += NTHR) {
+                const int v = t / (DQ * 9), r = t % (DQ * 9);
+                const int qb = r / 9, k = (r / 3) % 3, ax = r % 3;
+                const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
+                double gv[9];
+                dm_grad_var(PTb + q * PT_N, v, k, gv);
+                const double *bxp = Bx + qx * 9 + ax * 3;
+                const double bx0 = bxp[0], bx1 = bxp[1], bx2 = bxp[2];
+                /* coefficients of By[ky] per kz: derivative m -> (kx, ky, kz) as eval_Bspline */
+                const double t00 = gv[0] * bx1 + gv[3] * bx2, t01 = gv[1] * bx0 + gv[4] * bx1, t02 = gv[6] * bx0;
+                const double t10 = gv[2] * bx0 + gv[5] * bx1, t11 = gv[7] * bx0;
+                const double t20 = gv[8] * bx0;
+                double *xr = Xb + (qb * 12 + v) * XS + k;
 #pragma unroll
-                    for (int K = 0; K < 3; K++)
-                        if (3 + igab_idx6(lo, K) == hi) gv = pt[PT_TAU + 3 * lo + K];
-                }
-                S.geo[qb][m * 9 + n] = pt[PT_W] * gv;
-            }
-            __syncthreads();
-            /* (b) X' = Gv' . N (9 outputs per task) and GN = (w geo) N */
-            for (int o = tid; o < DQ * 12 * 3 * 3; o += NTHR) {
-                const int part = o % 3, k = (o / 3) % 3, v = (o / 9) % 12, qb = o / 108;
-                double gr[9];
+                for (int ay = 0; ay < 3; ay++) {
+                    const double *byp = By + qy * 9 + ay * 3;
+                    const double cy0 = t00 * byp[0] + t01 * byp[1] + t02 * byp[2];
+                    const double cy1 = t10 * byp[0] + t11 * byp[1];
+                    const double cy2 = t20 * byp[0];
 #pragma unroll
-                for (int m = 0; m < 9; m++) gr[m] = S.Gv[qb][v][9 * k + m];
-                double *xr = Xb + (qb * 12 + v) * XS;
-                const double *nt = &S.NT[9 * qb][0];
-                if (v < 6) {
-#pragma unroll
-                    for (int j = 0; j < 9; j++) {
-                        const int a = 9 * part + j;
-                        xr[3 * a + k] = gr[0] * nt[a] + gr[1] * nt[GS + a] + gr[2] * nt[2 * GS + a];
-                    }
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 9; j++) {
-                        const int a = 9 * part + j;
-                        double t = 0.0;
-#pragma unroll
-                        for (int m = 0; m < 9; m++) t += gr[m] * nt[m * GS + a];
-                        xr[3 * a + k] = t;
+                    for (int az = 0; az < 3; az++) {
+                        const double *bzp = Bz + qz * 9 + az * 3;
+                        xr[3 * (9 * ax + 3 * ay + az)] = cy0 * bzp[0] + cy1 * bzp[1] + cy2 * bzp[2];
                     }
                 }
             }
-            for (int o = tid; o < DQ * 243; o += NTHR) {
-                const int b = o % 27, m = (o / 27) % 9, qb = o / 243;
-                const double *gr = &S.geo[qb][m * 9];
-                const double *nt = &S.NT[9 * qb][b];
-                double t = 0.0;
+            /* U / V rows of the geometric block: task (row i, point qb, ax, ay) -> 3 outputs (az) */
+            for (int t = tid; t < DQ * 6 * 9; t += NTHR) {
+                const int i = t / (DQ * 9), r = t % (DQ * 9);
+                const int qb = r / 9, ax = (r / 3) % 3, ay = r % 3;
+                const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
+                const double *p = PTb + q * PT_N;
+                const double w = p[PT_W];
+                const double bx0 = Bx[qx * 9 + ax * 3], bx1 = Bx[qx * 9 + ax * 3 + 1], bx2 = Bx[qx * 9 + ax * 3 + 2];
+                const double by0 = By[qy * 9 + ay * 3], by1 = By[qy * 9 + ay * 3 + 1], by2 = By[qy * 9 + ay * 3 + 2];
+                const int I = i < 3 ? i : i - 3;
+                const double s00 = p[PT_SIG], s11 = p[PT_SIG + 1], s22 = p[PT_SIG + 2];
+                const double s01 = 0.5 * p[PT_D1S], s02 = 0.5 * p[PT_D1S + 1], s12 = 0.5 * p[PT_D1S + 2];
+                const double tI0 = p[PT_TAU + 3 * I], tI1 = p[PT_TAU + 3 * I + 1], tI2 = p[PT_TAU + 3 * I + 2];
 #pragma unroll
-                for (int n = 0; n < 9; n++) t += gr[n] * nt[n * GS];
-                S.GN[9 * qb + m][b] = t;
+                for (int az = 0; az < 3; az++) {
+                    const double *bzp = Bz + qz * 9 + az * 3;
+                    const double bz0 = bzp[0], bz1 = bzp[1], bz2 = bzp[2];
+                    const double dx = bx1 * by0 * bz0, dy = bx0 * by1 * bz0, dz = bx0 * by0 * bz1;
+                    /* second derivatives H[idx6(I, K)], K = 0..2 */
+                    double h0, h1, h2;
+                    if (I == 0) { h0 = bx2 * by0 * bz0; h1 = bx1 * by1 * bz0; h2 = bx1 * by0 * bz1; }
+                    else if (I == 1) { h0 = bx1 * by1 * bz0; h1 = bx0 * by2 * bz0; h2 = bx0 * by1 * bz1; }
+                    else { h0 = bx1 * by0 * bz1; h1 = bx0 * by1 * bz1; h2 = bx0 * by0 * bz2; }
+                    const double th = tI0 * h0 + tI1 * h1 + tI2 * h2;   /* (T H_a)_I */
+                    const double dI = I == 0 ? dx : (I == 1 ? dy : dz);
+                    const int a = 9 * ax + 3 * ay + az, row = qb * 6 + i;
+                    if (i < 3) {
+                        const double sg = I == 0 ? s00 * dx + s01 * dy + s02 * dz
+                                        : (I == 1 ? s01 * dx + s11 * dy + s12 * dz : s02 * dx + s12 * dy + s22 * dz);
+                        S.UT[row][a] = dI;
+                        S.VT[row][a] = w * (sg + th);
+                    } else {
+                        S.UT[row][a] = w * th;
+                        S.VT[row][a] = dI;
+                    }
+                }
+            }
+            if (tid < DROWS) {
+                const double *p = PTb + (q0 + tid / 12) * PT_N;
+                S.sc[tid] = p[PT_W] * p[PT_LAM + tid % 12];
             }
             __syncthreads();
-            /* (c) tensor-core accumulation K += X'^T diag(sc) X', Gamma += N^T GN */
-#define MMA_CALL(Wn) warp_mma<Wn>(Xb, S.sc, &S.NT[0][0], &S.GN[0][0], lane, acc, gacc)
+            /* (b) tensor-core accumulation K += X'^T diag(sc) X', Gamma += U^T V */
+#define MMA_CALL(Wn) warp_mma<Wn>(Xb, S.sc, &S.UT[0][0], &S.VT[0][0], lane, acc, gacc)
             WARP_SWITCH(MMA_CALL)
 #undef MMA_CALL
             __syncthreads();
         }
         /* ---- stage K and Gamma in shared memory, then scatter the 81 x 81 element matrix */
         double *const K = S.W;
-        double *const Gam = &S.NT[0][0];
+        double *const Gam = S.W + W_GAM;
 #define DUMP_CALL(Wn) warp_dump<Wn>(K, Gam, lane, acc, gacc)
         WARP_SWITCH(DUMP_CALL)
 #undef DUMP_CALL
@@ -411,9 +419,6 @@ __device__ __forceinline__ void dmma_tile(const igab_geom &g, const tile_t &Tl, 
             if (k1 == k2) v += a1 <= a2 ? Gam[a1 * 32 + a2] : Gam[a2 * 32 + a1];
             atomicAdd(&vals[S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9], v);
         }
-        __syncthreads();
-        /* Gamma overwrote N^T: restore the zero padding of N^T */
-        for (int idx = tid; idx < GROWS * GS; idx += NTHR) (&S.NT[0][0])[idx] = 0.0;
         __syncthreads();
     }
 }

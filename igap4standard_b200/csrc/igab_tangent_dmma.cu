@@ -9,38 +9,52 @@
  * Phi'' is diagonal except for the (va, vb) pair; rotating those two rows by
  * the eigenvectors of that 2x2 block makes it diagonal, so
  *   K_e = X'^T diag(s) X',   s = w_q * eigenvalues.
- * Both products run on DMMA tiles:
- *   - X' (48 rows = 4 Gauss points x 12 variables, 88 padded columns) is built
- *     in shared memory straight from the 1-D basis tables (sum factorisation of
- *     sum_m dv'/du_{k,m} N_a^m over x, y, z; one task per (point, variable,
- *     component, x-function), the variable warp-uniform); a warp loads its A
- *     fragments from it and forms its B fragments by scaling the same
- *     registers with s.  The 66 upper 8x8 tiles of the 88x88 element matrix are
- *     spread over the 4 warps (table in igab_warp_tiles.inc), the lower
- *     triangle follows by symmetry.
- *   - Gamma (27 x 27, identical for the three components) in the rank-6 form
- *     Gamma = sum_q sum_i U_qi V_qi^T with geo = [[S, T], [T^T, 0]]:
- *       U_i = d_i N_a, V_i = w ((S grad N_a)_i + (T H_a)_i)     (i < 3)
- *       U_i = w (T H_a)_I, V_i = d_I N_a                         (i = 3 + I)
- *     on 10 upper 8x8 tiles of the 32-padded block, 6 k-rows per point.
- * 128 threads and ~90 KB of shared memory per block let two blocks share an
- * SM, so one block's scalar work (field, point integrand, X') overlaps the
- * other's tensor work.  Scatter: fire-and-forget reductions into the CSR
- * values, conflict-free within one of the 8 tile colours (igab_kernels.cu).
+ * Gamma in the rank-6 form Gamma = sum_q sum_i U_qi V_qi^T, geo = [[S, T], [T^T, 0]]:
+ *   U_i = d_i N_a, V_i = w ((S grad N_a)_i + (T H_a)_i)     (i < 3)
+ *   U_i = w (T H_a)_I, V_i = d_I N_a                         (i = 3 + I)
+ *
+ * Warp-specialised, one 512-thread block per SM, persistent over the tiles
+ * (2x2x2 elements) of one colour or of a batched work list:
+ *   - 8 builder warps compute, per element, the field at the 64 Gauss points
+ *     (sum factorisation), the point integrand, and then per batch of 4 points
+ *     the 48 rows of X' (straight from the 1-D basis tables: one task per
+ *     (point, variable, component, x-function)), the 24 U / V rows and the
+ *     scales s, into one of two shared-memory slots;
+ *   - 8 consumer warps run the DMMA products on the slot: the 66 upper 8x8
+ *     tiles of the 88x88 element matrix and the 10 upper tiles of the 32x32
+ *     Gamma block, split over the warps by igab_warp_tiles8.inc, with the
+ *     accumulators in registers for the whole element.  At the end of an
+ *     element they add Gamma to the diagonal component blocks and reduce the
+ *     81x81 matrix into the CSR values straight from the accumulators
+ *     (fire-and-forget red.global.add; the lower triangle mirrors the upper
+ *     one exactly).  Tiles of one colour touch disjoint entries and the
+ *     elements of a tile are separated by a consumer barrier, so every entry
+ *     receives its additions in a fixed order.
+ * The slots are handed over with mbarriers (full: 256 builder arrivals, empty:
+ * 256 consumer arrivals).  Every wait is bounded; a wait that gives up sets the
+ * block's abort flag and the status word, and both roles leave their loops.
  */
 #include <cuda_runtime.h>
 #include "igab_device.cuh"
+#include "igab_tc.cuh"
 
 namespace {
 
-#include "igab_warp_tiles.inc"
+#include "igab_warp_tiles8.inc"
 
-#define NTHR 128
+#define NCONS 256       /* consumer threads (warps 0-7): DMMA tiles and scatter */
+#define NBLD 256        /* builder threads (warps 8-15): field, integrand, X', U / V */
+#define NTHR (NCONS + NBLD)
+#define NSLOT 2         /* X' / U / V slots in flight */
+#define BAR_CONS 1      /* named barrier of the consumers */
+#define BAR_BLD 2       /* named barrier of the builders */
 #define DQ 4            /* Gauss points per batch */
 #define DROWS (DQ * 12) /* k rows of X' per batch */
 #define GROWS (DQ * 6)  /* k rows of the geometric product per batch: U / V rows, 6 per point */
 #define XS 100          /* X' row stride (doubles): = 4 mod 16 keeps fragment loads conflict-free */
 #define GS 36           /* U / V row stride: = 4 mod 16; columns a >= 27 stay zero */
+#define TE 2            /* tile edge (elements) */
+#define TCP (TE + 2)    /* control points per tile edge */
 
 /* point data */
 #define PT_F 0
@@ -54,28 +68,30 @@ namespace {
 #define PT_W 56
 #define PT_N 57
 
-/* work buffer: interpolation A[972] C[864] | X'[48][100] + points[64][57] | K[88][88] + Gamma[32][32] */
-#define W_A 0
-#define W_C 972
-#define W_X 0
-#define W_PT (DROWS * XS)
-#define W_SIZE (DROWS * XS + IGAB_NQ3 * PT_N)
-#define W_GAM (88 * 88)
-#define W_ALL (W_SIZE > W_GAM + 32 * 32 ? W_SIZE : W_GAM + 32 * 32)
+/* one tile of work as the builders publish it to the consumers */
+struct dws_tile {
+    igab_geom g;
+    const double *U;
+    double *vals;
+    int tile, colour, inst, pad;   /* tile < 0: no more work */
+};
 
-template <int TE>
-struct dmma_smem {
-    static constexpr int TC = TE + 2;
-    static constexpr int NCP = TC * TC * TC;
-    double W[W_ALL];
-    double UT[GROWS][GS];     /* U rows of the geometric product: row 6 qb + i, column a */
-    double VT[GROWS][GS];     /* V rows */
-    double sc[DROWS];
-    double U[NCP * 3];
+struct dws_smem {
+    double X[NSLOT][DROWS * XS];     /* X' rows (row 12 qb + v, column 3 a + k) */
+    double UT[NSLOT][GROWS * GS];    /* U rows of the geometric product (row 6 qb + i, column a) */
+    double VT[NSLOT][GROWS * GS];    /* V rows */
+    double sc[NSLOT][DROWS];         /* s of the X' rows */
+    double pt[IGAB_NQ3 * PT_N];      /* point data of the element being built */
+    double AC[972 + 864];            /* interpolation scratch */
+    double gam[32 * 32];             /* upper tiles of Gamma at the end of an element */
+    double U[TCP * TCP * TCP * 3];   /* displacements of the tile's control points */
     double tab[3][TE][IGAB_TAB1D];
     double wh[3][TE][IGAB_NQ];
-    long rbase[81];       /* CSR row bases of the element matrix (elem_row_base) */
+    long rbase[81];                  /* CSR row bases of the element matrix (elem_row_base) */
     int rsx[81], rsy[81];
+    dws_tile td[2];                  /* tile k in td[k & 1] */
+    unsigned long long full[NSLOT], empty[NSLOT];
+    int abort_flag;
 };
 
 __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
@@ -83,6 +99,11 @@ __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                  : "+d"(c0), "+d"(c1)
                  : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void red_add(double *p, double v)
+{
+    atomicAdd(p, v);   /* result unused: a fire-and-forget reduction */
 }
 
 /* eigen-rotation of [[a, b], [b, c]] (Jacobi / symmetric Schur 2x2): (cs, sn, l1, l2)
@@ -100,69 +121,6 @@ __device__ __forceinline__ void sym2_eig(double a, double b, double c, double &c
     l1 = a - t * b;
     l2 = c + t * b;
 }
-
-template <int W>
-__device__ __forceinline__ void warp_mma(const double *__restrict__ X, const double *__restrict__ sc,
-                                         const double *__restrict__ UT, const double *__restrict__ VT, int lane,
-                                         double (&acc)[17][2], double (&gacc)[3][2])
-{
-    using WT = warp_tiles<W>;
-    const int r4 = lane & 3, c8 = lane >> 2;
-#pragma unroll 2
-    for (int kb = 0; kb < DROWS / 4; kb++) {
-        const int kr = 4 * kb + r4;
-        const double s = sc[kr];
-        const double *row = X + kr * XS + c8;
-        double f[WT::NB], g[WT::NB];
-#pragma unroll
-        for (int b = 0; b < WT::NB; b++) {
-            f[b] = row[8 * WT::blk(b)];
-            g[b] = f[b] * s;
-        }
-#pragma unroll
-        for (int t = 0; t < WT::NT; t++) dmma(acc[t][0], acc[t][1], f[WT::ti(t)], g[WT::tj(t)]);
-    }
-#pragma unroll 3
-    for (int kb = 0; kb < GROWS / 4; kb++) {
-        const int kr = 4 * kb + r4;
-        double fa[WT::NGA], fb[WT::NGB];
-#pragma unroll
-        for (int b = 0; b < WT::NGA; b++) fa[b] = UT[kr * GS + 8 * WT::gablk(b) + c8];
-#pragma unroll
-        for (int b = 0; b < WT::NGB; b++) fb[b] = VT[kr * GS + 8 * WT::gbblk(b) + c8];
-#pragma unroll
-        for (int t = 0; t < WT::NGT; t++) dmma(gacc[t][0], gacc[t][1], fa[WT::gti(t)], fb[WT::gtj(t)]);
-    }
-}
-
-/* accumulator tiles -> shared K[c1][c2] (stride 88) and Gamma[a1][a2] (stride 32) */
-template <int W>
-__device__ __forceinline__ void warp_dump(double *__restrict__ K, double *__restrict__ Gam, int lane,
-                                          const double (&acc)[17][2], const double (&gacc)[3][2])
-{
-    using WT = warp_tiles<W>;
-    const int r = lane >> 2, c = 2 * (lane & 3);
-#pragma unroll
-    for (int t = 0; t < WT::NT; t++) {
-        const int c1 = 8 * WT::blk(WT::ti(t)) + r, c2 = 8 * WT::blk(WT::tj(t)) + c;
-        K[c1 * 88 + c2] = acc[t][0];
-        K[c1 * 88 + c2 + 1] = acc[t][1];
-    }
-#pragma unroll
-    for (int t = 0; t < WT::NGT; t++) {
-        const int a1 = 8 * WT::gablk(WT::gti(t)) + r, a2 = 8 * WT::gbblk(WT::gtj(t)) + c;
-        Gam[a1 * 32 + a2] = gacc[t][0];
-        Gam[a1 * 32 + a2 + 1] = gacc[t][1];
-    }
-}
-
-#define WARP_SWITCH(CALL)    \
-    switch (warp) {          \
-    case 0: CALL(0); break;  \
-    case 1: CALL(1); break;  \
-    case 2: CALL(2); break;  \
-    default: CALL(3); break; \
-    }
 
 /* gradient of rotated variable v with respect to the 9 strain components of
  * displacement component k (igab_ge_grad_var, then the (va, vb) rotation) */
@@ -205,264 +163,540 @@ __device__ __forceinline__ void dm_grad_var(const double *p, int v, int k, doubl
     }
 }
 
-/* one tile: all NTHR threads of the block, uniformly */
-template <int TE>
-__device__ __forceinline__ void dmma_tile(const igab_geom &g, const tile_t &Tl, const double *__restrict__ U,
-                                          double *__restrict__ vals, dmma_smem<TE> &S)
-{
-    constexpr int TC = TE + 2;
-    constexpr int NCP = TC * TC * TC;
-    constexpr int NEL = TE * TE * TE;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    double *const Xb = S.W + W_X;
-    double *const PTb = S.W + W_PT;
+/* ---------------------------------------------------------------- work sources */
 
-    for (int idx = tid; idx < NCP * 3; idx += NTHR) {
-        int i = idx % 3, cp = idx / 3;
-        int lz = cp % TC, ly = (cp / TC) % TC, lx = cp / (TC * TC);
-        double v = 0.0;
-        if (lx < Tl.nv[0] + 2 && ly < Tl.nv[1] + 2 && lz < Tl.nv[2] + 2)
-            v = U[3 * cp_index(g, Tl.e0[0] + lx, Tl.e0[1] + ly, Tl.e0[2] + lz) + i];
-        S.U[idx] = v;
+/* the tiles of one colour, dealt round-robin over the persistent blocks */
+struct src_colour {
+    igab_geom g;
+    const double *U;
+    double *vals;
+    int colour;
+    long ntiles;
+    int *status;
+    __device__ void fetch(int k, dws_tile &R) const
+    {
+        const long t = blockIdx.x + (long)k * gridDim.x;
+        R.tile = t < ntiles ? (int)t : -1;
+        if (R.tile < 0) return;
+        R.g = g;
+        R.U = U;
+        R.vals = vals;
+        R.colour = colour;
+        R.inst = 0;
     }
-    for (int idx = tid; idx < 3 * TE * IGAB_TAB1D; idx += NTHR) {
-        int d = idx / (TE * IGAB_TAB1D), r = idx % (TE * IGAB_TAB1D), le = r / IGAB_TAB1D, o = r % IGAB_TAB1D;
-        S.tab[d][le][o] = le < Tl.nv[d] ? g.tab[d][(long)(Tl.e0[d] + le) * IGAB_TAB1D + o] : 0.0;
+    __device__ void done(const dws_tile &) const {}
+};
+
+/* the batched work list: items (instance, colour, tile) in colour-major order;
+ * an item starts once every earlier colour of its instance is complete */
+struct src_batch {
+    igab_batch_dev B;
+    const double *U;
+    double *vals;
+    int *status;
+    __device__ void fetch(int, dws_tile &R) const
+    {
+        const int it = atomicAdd(B.counter, 1);
+        if (it >= B.nitems) {
+            R.tile = -1;
+            return;
+        }
+        const int4 w = B.items[it];
+        int *done = B.done + 8 * w.x;
+        const int *need = B.need + 8 * w.x;
+        for (int c = 0; c < w.y; c++) {
+            long spins = 0;
+            while (atomicOr(&done[c], 0) < need[c]) {
+                if (++spins > IGAB_BATCH_SPIN) {
+                    atomicOr(B.status, 2);
+                    break;
+                }
+                __nanosleep(128);
+            }
+        }
+        __threadfence();
+        R.g = B.geoms[w.x];
+        R.U = U + B.dof_off[w.x];
+        R.vals = vals + B.nnz_off[w.x];
+        R.tile = w.z;
+        R.colour = w.y;
+        R.inst = w.x;
     }
-    for (int idx = tid; idx < 3 * TE * IGAB_NQ; idx += NTHR) {
-        int d = idx / (TE * IGAB_NQ), r = idx % (TE * IGAB_NQ), le = r / IGAB_NQ, q = r % IGAB_NQ;
-        S.wh[d][le][q] = le < Tl.nv[d] ? g.wh[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
+    /* consumers, after the tile's last reduction: publish the finished tile */
+    __device__ void done(const dws_tile &R) const
+    {
+        __threadfence();
+        tc_bar_sync(BAR_CONS, NCONS);
+        if (threadIdx.x == 0) atomicAdd(&B.done[8 * R.inst + R.colour], 1);
     }
-    /* the padding columns (a >= 27) of U / V stay zero */
-    for (int idx = tid; idx < GROWS * GS; idx += NTHR) {
+};
+
+/* ---------------------------------------------------------------- builders */
+
+/* wait until slot (gb % NSLOT) is free again; uniform over the builders */
+__device__ __forceinline__ bool bld_acquire(dws_smem &S, int gb)
+{
+    const int b = gb % NSLOT, u = gb / NSLOT;
+    const volatile int *abort = &S.abort_flag;
+    bool ok = !*abort;
+    if (ok && u > 0) ok = tc_mbar_wait_abortable(&S.empty[b], (u - 1) & 1, abort);
+    return tc_bar_and(BAR_BLD, NBLD, ok);
+}
+
+/* X', U / V and s of the batch of points q0 .. q0 + 3 into slot b */
+__device__ __forceinline__ void bld_batch(dws_smem &S, int b, int q0, const double *Bx, const double *By,
+                                          const double *Bz, int tb)
+{
+    double *const Xs = S.X[b];
+    double *const UTs = S.UT[b];
+    double *const VTs = S.VT[b];
+    const double *const PTb = S.pt;
+    /* X' rows: task (variable v, point qb, component k, x-function ax) -> 9 outputs
+     * (ay, az), X'[(qb, v)][3a + k] = sum_m dv'/du_{k,m} Bx By Bz, summed over x, y, z;
+     * U / V rows: task (row i, point qb, ax, ay) -> 3 outputs (az) of U and of V */
+    for (int t = tb; t < DQ * 12 * 9 + DQ * 6 * 9; t += NBLD) {
+        if (t < DQ * 12 * 9) {
+            const int v = t / (DQ * 9), r = t % (DQ * 9);
+            const int qb = r / 9, k = (r / 3) % 3, ax = r % 3;
+            const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
+            double gv[9];
+            dm_grad_var(PTb + q * PT_N, v, k, gv);
+            const double *bxp = Bx + qx * 9 + ax * 3;
+            const double bx0 = bxp[0], bx1 = bxp[1], bx2 = bxp[2];
+            /* coefficients of By[ky] per kz: derivative m -> (kx, ky, kz) as eval_Bspline */
+            const double t00 = gv[0] * bx1 + gv[3] * bx2, t01 = gv[1] * bx0 + gv[4] * bx1, t02 = gv[6] * bx0;
+            const double t10 = gv[2] * bx0 + gv[5] * bx1, t11 = gv[7] * bx0;
+            const double t20 = gv[8] * bx0;
+            double *xr = Xs + (qb * 12 + v) * XS + k;
+#pragma unroll
+            for (int ay = 0; ay < 3; ay++) {
+                const double *byp = By + qy * 9 + ay * 3;
+                const double cy0 = t00 * byp[0] + t01 * byp[1] + t02 * byp[2];
+                const double cy1 = t10 * byp[0] + t11 * byp[1];
+                const double cy2 = t20 * byp[0];
+#pragma unroll
+                for (int az = 0; az < 3; az++) {
+                    const double *bzp = Bz + qz * 9 + az * 3;
+                    xr[3 * (9 * ax + 3 * ay + az)] = cy0 * bzp[0] + cy1 * bzp[1] + cy2 * bzp[2];
+                }
+            }
+        } else {
+            const int tg = t - DQ * 12 * 9;
+            const int i = tg / (DQ * 9), r = tg % (DQ * 9);
+            const int qb = r / 9, ax = (r / 3) % 3, ay = r % 3;
+            const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
+            const double *p = PTb + q * PT_N;
+            const double w = p[PT_W];
+            const double bx0 = Bx[qx * 9 + ax * 3], bx1 = Bx[qx * 9 + ax * 3 + 1], bx2 = Bx[qx * 9 + ax * 3 + 2];
+            const double by0 = By[qy * 9 + ay * 3], by1 = By[qy * 9 + ay * 3 + 1], by2 = By[qy * 9 + ay * 3 + 2];
+            const int I = i < 3 ? i : i - 3;
+            const double s00 = p[PT_SIG], s11 = p[PT_SIG + 1], s22 = p[PT_SIG + 2];
+            const double s01 = 0.5 * p[PT_D1S], s02 = 0.5 * p[PT_D1S + 1], s12 = 0.5 * p[PT_D1S + 2];
+            const double tI0 = p[PT_TAU + 3 * I], tI1 = p[PT_TAU + 3 * I + 1], tI2 = p[PT_TAU + 3 * I + 2];
+#pragma unroll
+            for (int az = 0; az < 3; az++) {
+                const double *bzp = Bz + qz * 9 + az * 3;
+                const double bz0 = bzp[0], bz1 = bzp[1], bz2 = bzp[2];
+                const double dx = bx1 * by0 * bz0, dy = bx0 * by1 * bz0, dz = bx0 * by0 * bz1;
+                /* second derivatives H[idx6(I, K)], K = 0..2 */
+                double h0, h1, h2;
+                if (I == 0) { h0 = bx2 * by0 * bz0; h1 = bx1 * by1 * bz0; h2 = bx1 * by0 * bz1; }
+                else if (I == 1) { h0 = bx1 * by1 * bz0; h1 = bx0 * by2 * bz0; h2 = bx0 * by1 * bz1; }
+                else { h0 = bx1 * by0 * bz1; h1 = bx0 * by1 * bz1; h2 = bx0 * by0 * bz2; }
+                const double th = tI0 * h0 + tI1 * h1 + tI2 * h2;   /* (T H_a)_I */
+                const double dI = I == 0 ? dx : (I == 1 ? dy : dz);
+                const int a = 9 * ax + 3 * ay + az, row = qb * 6 + i;
+                if (i < 3) {
+                    const double sg = I == 0 ? s00 * dx + s01 * dy + s02 * dz
+                                    : (I == 1 ? s01 * dx + s11 * dy + s12 * dz : s02 * dx + s12 * dy + s22 * dz);
+                    UTs[row * GS + a] = dI;
+                    VTs[row * GS + a] = w * (sg + th);
+                } else {
+                    UTs[row * GS + a] = w * th;
+                    VTs[row * GS + a] = dI;
+                }
+            }
+        }
+    }
+    if (tb < DROWS) {
+        const double *p = PTb + (q0 + tb / 12) * PT_N;
+        S.sc[b][tb] = p[PT_W] * p[PT_LAM + tb % 12];
+    }
+}
+
+template <class Src>
+__device__ void dws_builder(const Src &F, dws_smem &S)
+{
+    const int tb = threadIdx.x - NCONS;
+    int gb = 0;   /* batches published so far */
+    bool aborted = false;
+    for (int k = 0; !aborted; k++) {
+        dws_tile &R = S.td[k & 1];
+        if (tb == 0) F.fetch(k, R);
+        tc_bar_sync(BAR_BLD, NBLD);
+        if (R.tile < 0) {
+            /* the end of the work, published through the next slot */
+            if (!bld_acquire(S, gb)) aborted = true;
+            else tc_mbar_arrive(&S.full[gb % NSLOT]);
+            break;
+        }
+        const igab_geom &g = R.g;
+        tile_t Tl;
+        decode_tile(g, TE, R.colour, R.tile, Tl);
+        for (int idx = tb; idx < TCP * TCP * TCP * 3; idx += NBLD) {
+            int i = idx % 3, cp = idx / 3;
+            int lz = cp % TCP, ly = (cp / TCP) % TCP, lx = cp / (TCP * TCP);
+            double v = 0.0;
+            if (lx < Tl.nv[0] + 2 && ly < Tl.nv[1] + 2 && lz < Tl.nv[2] + 2)
+                v = R.U[3 * cp_index(g, Tl.e0[0] + lx, Tl.e0[1] + ly, Tl.e0[2] + lz) + i];
+            S.U[idx] = v;
+        }
+        for (int idx = tb; idx < 3 * TE * IGAB_TAB1D; idx += NBLD) {
+            int d = idx / (TE * IGAB_TAB1D), r = idx % (TE * IGAB_TAB1D), le = r / IGAB_TAB1D, o = r % IGAB_TAB1D;
+            S.tab[d][le][o] = le < Tl.nv[d] ? g.tab[d][(long)(Tl.e0[d] + le) * IGAB_TAB1D + o] : 0.0;
+        }
+        for (int idx = tb; idx < 3 * TE * IGAB_NQ; idx += NBLD) {
+            int d = idx / (TE * IGAB_NQ), r = idx % (TE * IGAB_NQ), le = r / IGAB_NQ, q = r % IGAB_NQ;
+            S.wh[d][le][q] = le < Tl.nv[d] ? g.wh[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
+        }
+        tc_bar_sync(BAR_BLD, NBLD);
+        for (int le = 0; le < TE * TE * TE && !aborted; le++) {
+            const int lex = le / (TE * TE), ley = (le / TE) % TE, lez = le % TE;
+            if (!(lex < Tl.nv[0] && ley < Tl.nv[1] && lez < Tl.nv[2])) continue;   /* uniform */
+            const double *Bx = S.tab[0][lex];
+            const double *By = S.tab[1][ley];
+            const double *Bz = S.tab[2][lez];
+            double *const A = S.AC;
+            double *const C = S.AC + 972;
+            /* ---- field at the 64 Gauss points (sum-factorised, as the residual) */
+            for (int o = tb; o < 972; o += NBLD) {
+                int i = o % 3, kz = (o / 3) % 3, ay = (o / 9) % 3, ax = (o / 27) % 3, q = o / 81;
+                const double *u0 = &S.U[(((lex + ax) * TCP + (ley + ay)) * TCP + lez) * 3 + i];
+                A[o] = Bz[q * 9 + kz] * u0[0] + Bz[q * 9 + 3 + kz] * u0[3] + Bz[q * 9 + 6 + kz] * u0[6];
+            }
+            tc_bar_sync(BAR_BLD, NBLD);
+            for (int o = tb; o < 864; o += NBLD) {
+                int i = o % 3, kk = (o / 3) % 6, ax = (o / 18) % 3, qq = o / 54;
+                int qyy = qq & 3, qzz = qq >> 2;
+                const double *a0 = &A[((qzz * 3 + ax) * 3) * 9 + kk_kz(kk) * 3 + i];
+                C[o] = By[qyy * 9 + kk_ky(kk)] * a0[0] + By[qyy * 9 + 3 + kk_ky(kk)] * a0[9] +
+                       By[qyy * 9 + 6 + kk_ky(kk)] * a0[18];
+            }
+            tc_bar_sync(BAR_BLD, NBLD);
+            /* ---- point integrand data (64 threads), point order q = 16 qz + 4 qy + qx */
+            if (tb < IGAB_NQ3) {
+                const int qx = tb & 3, qy = (tb >> 2) & 3, qz = tb >> 4, qq = qy + 4 * qz;
+                double u[30];
+#pragma unroll
+                for (int a = 0; a < 10; a++)
+#pragma unroll
+                    for (int i = 0; i < 3; i++) {
+                        double s = 0.0;
+#pragma unroll
+                        for (int ax = 0; ax < 3; ax++)
+                            s += Bx[qx * 9 + ax * 3 + a_kx(a)] * C[((qq * 3 + ax) * 6 + a_kk(a)) * 3 + i];
+                        u[10 * i + a] = s;
+                    }
+                if (g.periodic) {
+#pragma unroll
+                    for (int i = 0; i < 3; i++)
+#pragma unroll
+                        for (int J = 0; J < 3; J++) u[10 * i + 1 + J] += g.pp[3 * i + J];
+                }
+                igab_ge_point<double> P;
+                igab_ge_eval(u, g.coef, P);
+                double *pt = S.pt + tb * PT_N;
+#pragma unroll
+                for (int k2 = 0; k2 < 3; k2++)
+#pragma unroll
+                    for (int J = 0; J < 3; J++) pt[PT_F + 3 * k2 + J] = P.F[k2][J];
+#pragma unroll
+                for (int k2 = 0; k2 < 3; k2++)
+#pragma unroll
+                    for (int c = 0; c < 6; c++) pt[PT_G + 6 * k2 + c] = P.G[k2][c];
+                double cs, sn, l1, l2;
+                sym2_eig(P.d2[1], P.d2ab, P.d2[2], cs, sn, l1, l2);
+#pragma unroll
+                for (int v = 0; v < 12; v++) pt[PT_LAM + v] = v == 1 ? l1 : (v == 2 ? l2 : P.d2[v]);
+                pt[PT_CS] = cs;
+                pt[PT_SN] = sn;
+#pragma unroll
+                for (int I = 0; I < 3; I++) pt[PT_SIG + I] = P.sig[I];
+#pragma unroll
+                for (int I = 0; I < 3; I++) pt[PT_D1S + I] = P.d1[3 + I];
+#pragma unroll
+                for (int I = 0; I < 3; I++)
+#pragma unroll
+                    for (int K = 0; K < 3; K++) pt[PT_TAU + 3 * I + K] = P.tau[I][K];
+                pt[PT_W] = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz] *
+                           elem_scale(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez);
+            }
+            tc_bar_sync(BAR_BLD, NBLD);
+            /* ---- the 16 batches of this element */
+            for (int q0 = 0; q0 < IGAB_NQ3; q0 += DQ) {
+                if (!bld_acquire(S, gb)) {
+                    aborted = true;
+                    break;
+                }
+                const int b = gb % NSLOT;
+                bld_batch(S, b, q0, Bx, By, Bz, tb);
+                tc_mbar_arrive(&S.full[b]);
+                gb++;
+            }
+        }
+    }
+    if (aborted && tb == 0) {
+        S.abort_flag = 1;
+        atomicOr(F.status, 1);
+    }
+}
+
+/* ---------------------------------------------------------------- consumers */
+
+/* wait until slot (gb % NSLOT) holds batch gb; uniform over the consumers */
+__device__ __forceinline__ bool cons_acquire(dws_smem &S, int gb)
+{
+    const int b = gb % NSLOT;
+    const volatile int *abort = &S.abort_flag;
+    bool ok = !*abort;
+    if (ok) ok = tc_mbar_wait_abortable(&S.full[b], (gb / NSLOT) & 1, abort);
+    return tc_bar_and(BAR_CONS, NCONS, ok);
+}
+
+template <int W>
+struct cons_acc {
+    using WT = warp_tiles8<W>;
+    double k[WT::NT > 0 ? WT::NT : 1][2];
+    double g[WT::NGT > 0 ? WT::NGT : 1][2];
+};
+
+/* one batch of the DMMA products: K += X'^T diag(sc) X' on the warp's K tiles,
+ * Gamma += U^T V on its Gamma tiles */
+template <int W>
+__device__ __forceinline__ void warp_mma8(const double *__restrict__ X, const double *__restrict__ sc,
+                                          const double *__restrict__ UT, const double *__restrict__ VT, int lane,
+                                          cons_acc<W> &a)
+{
+    using WT = warp_tiles8<W>;
+    const int r4 = lane & 3, c8 = lane >> 2;
+    if constexpr (WT::NT > 0) {
+#pragma unroll 2
+        for (int kb = 0; kb < DROWS / 4; kb++) {
+            const int kr = 4 * kb + r4;
+            const double s = sc[kr];
+            const double *row = X + kr * XS + c8;
+            double f[WT::NB], g[WT::NB];
+#pragma unroll
+            for (int b = 0; b < WT::NB; b++) {
+                f[b] = row[8 * WT::blk(b)];
+                g[b] = f[b] * s;
+            }
+#pragma unroll
+            for (int t = 0; t < WT::NT; t++) dmma(a.k[t][0], a.k[t][1], f[WT::ti(t)], g[WT::tj(t)]);
+        }
+    }
+    if constexpr (WT::NGT > 0) {
+#pragma unroll 3
+        for (int kb = 0; kb < GROWS / 4; kb++) {
+            const int kr = 4 * kb + r4;
+            double fa[WT::NGA], fb[WT::NGB];
+#pragma unroll
+            for (int b = 0; b < WT::NGA; b++) fa[b] = UT[kr * GS + 8 * WT::gablk(b) + c8];
+#pragma unroll
+            for (int b = 0; b < WT::NGB; b++) fb[b] = VT[kr * GS + 8 * WT::gbblk(b) + c8];
+#pragma unroll
+            for (int t = 0; t < WT::NGT; t++) dmma(a.g[t][0], a.g[t][1], fa[WT::gti(t)], fb[WT::gtj(t)]);
+        }
+    }
+}
+
+__device__ __forceinline__ long csr_at(const dws_smem &S, int c1, int c2)
+{
+    return S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9;
+}
+
+/* the warp's K tiles plus Gamma on the diagonal component blocks, reduced into
+ * the CSR values; entry (c1, c2) and its mirror (c2, c1) receive the upper value */
+template <int W>
+__device__ __forceinline__ void warp_scatter8(double *__restrict__ vals, const dws_smem &S, int lane,
+                                              const cons_acc<W> &a)
+{
+    using WT = warp_tiles8<W>;
+    const int r = lane >> 2, c = 2 * (lane & 3);
+#pragma unroll
+    for (int t = 0; t < WT::NT; t++) {
+        const int bi = WT::blk(WT::ti(t)), bj = WT::blk(WT::tj(t));
+        double v2[2] = {a.k[t][0], a.k[t][1]};
+        if (bi == bj) {
+            /* diagonal tile: entry (r, c + e) below the diagonal takes (c + e, r),
+             * held by lane 4 (c + e) + r / 2, element r & 1 */
+            const double x0 = __shfl_sync(0xffffffffu, a.k[t][0], 4 * c + (r >> 1));
+            const double y0 = __shfl_sync(0xffffffffu, a.k[t][1], 4 * c + (r >> 1));
+            const double x1 = __shfl_sync(0xffffffffu, a.k[t][0], 4 * (c + 1) + (r >> 1));
+            const double y1 = __shfl_sync(0xffffffffu, a.k[t][1], 4 * (c + 1) + (r >> 1));
+            if (r > c) v2[0] = (r & 1) ? y0 : x0;
+            if (r > c + 1) v2[1] = (r & 1) ? y1 : x1;
+        }
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int c1 = 8 * bi + r, c2 = 8 * bj + c + e;
+            if (c1 < 81 && c2 < 81) {
+                const int a1 = c1 / 3, a2 = c2 / 3;
+                double v = v2[e];
+                if (c1 % 3 == c2 % 3) v += a1 <= a2 ? S.gam[a1 * 32 + a2] : S.gam[a2 * 32 + a1];
+                red_add(vals + csr_at(S, c1, c2), v);
+                if (bi != bj) red_add(vals + csr_at(S, c2, c1), v);
+            }
+        }
+    }
+}
+
+template <int W, class Src>
+__device__ void dws_consumer(const Src &F, dws_smem &S)
+{
+    using WT = warp_tiles8<W>;
+    const int tid = threadIdx.x, lane = tid & 31;
+    int gb = 0;   /* batches consumed so far */
+    bool aborted = false;
+    for (int k = 0;; k++) {
+        /* the first batch of tile k (or the end of the work) */
+        if (!cons_acquire(S, gb)) {
+            aborted = true;
+            break;
+        }
+        const dws_tile &R = S.td[k & 1];
+        if (R.tile < 0) break;
+        tile_t Tl;
+        decode_tile(R.g, TE, R.colour, R.tile, Tl);
+        bool have = true;
+        for (int le = 0; le < TE * TE * TE && !aborted; le++) {
+            const int lex = le / (TE * TE), ley = (le / TE) % TE, lez = le % TE;
+            if (!(lex < Tl.nv[0] && ley < Tl.nv[1] && lez < Tl.nv[2])) continue;   /* uniform */
+            cons_acc<W> a;
+#pragma unroll
+            for (int t = 0; t < (WT::NT > 0 ? WT::NT : 1); t++) a.k[t][0] = a.k[t][1] = 0.0;
+#pragma unroll
+            for (int t = 0; t < (WT::NGT > 0 ? WT::NGT : 1); t++) a.g[t][0] = a.g[t][1] = 0.0;
+            for (int q0 = 0; q0 < IGAB_NQ3; q0 += DQ) {
+                if (!have && !cons_acquire(S, gb)) {
+                    aborted = true;
+                    break;
+                }
+                have = false;
+                const int b = gb % NSLOT;
+                warp_mma8<W>(S.X[b], S.sc[b], S.UT[b], S.VT[b], lane, a);
+                tc_mbar_arrive(&S.empty[b]);
+                gb++;
+            }
+            if (aborted) break;
+            /* Gamma (upper tiles) and the CSR row bases of the element */
+            if constexpr (WT::NGT > 0) {
+                const int r = lane >> 2, c = 2 * (lane & 3);
+#pragma unroll
+                for (int t = 0; t < WT::NGT; t++) {
+                    const int a1 = 8 * WT::gablk(WT::gti(t)) + r, a2 = 8 * WT::gbblk(WT::gtj(t)) + c;
+                    S.gam[a1 * 32 + a2] = a.g[t][0];
+                    S.gam[a1 * 32 + a2 + 1] = a.g[t][1];
+                }
+            }
+            if (tid < 81)
+                elem_row_base(R.g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez, tid, S.rbase[tid], S.rsx[tid],
+                              S.rsy[tid]);
+            tc_bar_sync(BAR_CONS, NCONS);
+            warp_scatter8<W>(R.vals, S, lane, a);
+            tc_bar_sync(BAR_CONS, NCONS);
+        }
+        if (aborted) break;
+        F.done(R);
+    }
+    if (aborted && tid == 0) {
+        S.abort_flag = 1;
+        atomicOr(F.status, 1);
+    }
+}
+
+template <class Src>
+__device__ __forceinline__ void dws_run(const Src &F)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    dws_smem &S = *reinterpret_cast<dws_smem *>(smem_raw);
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        S.abort_flag = 0;
+        for (int b = 0; b < NSLOT; b++) {
+            tc_mbar_init(&S.full[b], NBLD);
+            tc_mbar_init(&S.empty[b], NCONS);
+        }
+        tc_fence_mbar_init();
+    }
+    /* the padding columns of X' (a >= 27) and of U / V stay zero */
+    for (int idx = tid; idx < NSLOT * DROWS * (XS - 81); idx += NTHR) {
+        const int b = idx / (DROWS * (XS - 81)), r = idx % (DROWS * (XS - 81));
+        S.X[b][(r / (XS - 81)) * XS + 81 + r % (XS - 81)] = 0.0;
+    }
+    for (int idx = tid; idx < NSLOT * GROWS * GS; idx += NTHR) {
         (&S.UT[0][0])[idx] = 0.0;
         (&S.VT[0][0])[idx] = 0.0;
     }
     __syncthreads();
-
-    for (int le = 0; le < NEL; le++) {
-        const int lex = le / (TE * TE), ley = (le / TE) % TE, lez = le % TE;
-        if (!(lex < Tl.nv[0] && ley < Tl.nv[1] && lez < Tl.nv[2])) continue;   /* block-uniform */
-        const double *Bx = S.tab[0][lex];
-        const double *By = S.tab[1][ley];
-        const double *Bz = S.tab[2][lez];
-        double *const A = S.W + W_A;
-        double *const C = S.W + W_C;
-        /* ---- field at the 64 Gauss points (sum-factorised, as the residual) */
-        for (int o = tid; o < 972; o += NTHR) {
-            int i = o % 3, kz = (o / 3) % 3, ay = (o / 9) % 3, ax = (o / 27) % 3, q = o / 81;
-            const double *u0 = &S.U[(((lex + ax) * TC + (ley + ay)) * TC + lez) * 3 + i];
-            A[o] = Bz[q * 9 + kz] * u0[0] + Bz[q * 9 + 3 + kz] * u0[3] + Bz[q * 9 + 6 + kz] * u0[6];
-        }
-        __syncthreads();
-        for (int o = tid; o < 864; o += NTHR) {
-            int i = o % 3, kk = (o / 3) % 6, ax = (o / 18) % 3, qq = o / 54;
-            int qyy = qq & 3, qzz = qq >> 2;
-            const double *a0 = &A[((qzz * 3 + ax) * 3) * 9 + kk_kz(kk) * 3 + i];
-            C[o] = By[qyy * 9 + kk_ky(kk)] * a0[0] + By[qyy * 9 + 3 + kk_ky(kk)] * a0[9] +
-                   By[qyy * 9 + 6 + kk_ky(kk)] * a0[18];
-        }
-        __syncthreads();
-        /* ---- point integrand data (64 threads), point order q = 16 qz + 4 qy + qx */
-        if (tid < IGAB_NQ3) {
-            const int qx = tid & 3, qy = (tid >> 2) & 3, qz = tid >> 4, qq = qy + 4 * qz;
-            double u[30];
-#pragma unroll
-            for (int a = 0; a < 10; a++)
-#pragma unroll
-                for (int i = 0; i < 3; i++) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int ax = 0; ax < 3; ax++)
-                        s += Bx[qx * 9 + ax * 3 + a_kx(a)] * C[((qq * 3 + ax) * 6 + a_kk(a)) * 3 + i];
-                    u[10 * i + a] = s;
-                }
-            if (g.periodic) {
-#pragma unroll
-                for (int i = 0; i < 3; i++)
-#pragma unroll
-                    for (int J = 0; J < 3; J++) u[10 * i + 1 + J] += g.pp[3 * i + J];
-            }
-            igab_ge_point<double> P;
-            igab_ge_eval(u, g.coef, P);
-            double *pt = PTb + tid * PT_N;
-#pragma unroll
-            for (int k = 0; k < 3; k++)
-#pragma unroll
-                for (int J = 0; J < 3; J++) pt[PT_F + 3 * k + J] = P.F[k][J];
-#pragma unroll
-            for (int k = 0; k < 3; k++)
-#pragma unroll
-                for (int c = 0; c < 6; c++) pt[PT_G + 6 * k + c] = P.G[k][c];
-            double cs, sn, l1, l2;
-            sym2_eig(P.d2[1], P.d2ab, P.d2[2], cs, sn, l1, l2);
-#pragma unroll
-            for (int v = 0; v < 12; v++) pt[PT_LAM + v] = v == 1 ? l1 : (v == 2 ? l2 : P.d2[v]);
-            pt[PT_CS] = cs;
-            pt[PT_SN] = sn;
-#pragma unroll
-            for (int I = 0; I < 3; I++) pt[PT_SIG + I] = P.sig[I];
-#pragma unroll
-            for (int I = 0; I < 3; I++) pt[PT_D1S + I] = P.d1[3 + I];
-#pragma unroll
-            for (int I = 0; I < 3; I++)
-#pragma unroll
-                for (int K = 0; K < 3; K++) pt[PT_TAU + 3 * I + K] = P.tau[I][K];
-            pt[PT_W] = S.wh[0][lex][qx] * S.wh[1][ley][qy] * S.wh[2][lez][qz] *
-                       elem_scale(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez);
-        }
-        __syncthreads();
-
-        double acc[17][2], gacc[3][2];
-#pragma unroll
-        for (int t = 0; t < 17; t++) acc[t][0] = acc[t][1] = 0.0;
-#pragma unroll
-        for (int t = 0; t < 3; t++) gacc[t][0] = gacc[t][1] = 0.0;
-
-        for (int q0 = 0; q0 < IGAB_NQ3; q0 += DQ) {
-            if (q0 == 0)   /* the interpolation / staging data under X' is dead: padding columns back to zero */
-                for (int idx = tid; idx < DROWS * (XS - 81); idx += NTHR)
-                    Xb[(idx / (XS - 81)) * XS + 81 + idx % (XS - 81)] = 0.0;
-            /* (a) X' rows: task (variable v, point qb, component k, x-function ax) -> 9 outputs
-             * (ay, az), X'[(qb, v)][3a + k] = sum_m dv'/du_{k,m} Bx By Bz, summed over x, y, z */
-            for (int t = tid; t < DQ * 12 * 9; t += NTHR) {
-                const int v = t / (DQ * 9), r = t % (DQ * 9);
-                const int qb = r / 9, k = (r / 3) % 3, ax = r % 3;
-                const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
-                double gv[9];
-                dm_grad_var(PTb + q * PT_N, v, k, gv);
-                const double *bxp = Bx + qx * 9 + ax * 3;
-                const double bx0 = bxp[0], bx1 = bxp[1], bx2 = bxp[2];
-                /* coefficients of By[ky] per kz: derivative m -> (kx, ky, kz) as eval_Bspline */
-                const double t00 = gv[0] * bx1 + gv[3] * bx2, t01 = gv[1] * bx0 + gv[4] * bx1, t02 = gv[6] * bx0;
-                const double t10 = gv[2] * bx0 + gv[5] * bx1, t11 = gv[7] * bx0;
-                const double t20 = gv[8] * bx0;
-                double *xr = Xb + (qb * 12 + v) * XS + k;
-#pragma unroll
-                for (int ay = 0; ay < 3; ay++) {
-                    const double *byp = By + qy * 9 + ay * 3;
-                    const double cy0 = t00 * byp[0] + t01 * byp[1] + t02 * byp[2];
-                    const double cy1 = t10 * byp[0] + t11 * byp[1];
-                    const double cy2 = t20 * byp[0];
-#pragma unroll
-                    for (int az = 0; az < 3; az++) {
-                        const double *bzp = Bz + qz * 9 + az * 3;
-                        xr[3 * (9 * ax + 3 * ay + az)] = cy0 * bzp[0] + cy1 * bzp[1] + cy2 * bzp[2];
-                    }
-                }
-            }
-            /* U / V rows of the geometric block: task (row i, point qb, ax, ay) -> 3 outputs (az) */
-            for (int t = tid; t < DQ * 6 * 9; t += NTHR) {
-                const int i = t / (DQ * 9), r = t % (DQ * 9);
-                const int qb = r / 9, ax = (r / 3) % 3, ay = r % 3;
-                const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
-                const double *p = PTb + q * PT_N;
-                const double w = p[PT_W];
-                const double bx0 = Bx[qx * 9 + ax * 3], bx1 = Bx[qx * 9 + ax * 3 + 1], bx2 = Bx[qx * 9 + ax * 3 + 2];
-                const double by0 = By[qy * 9 + ay * 3], by1 = By[qy * 9 + ay * 3 + 1], by2 = By[qy * 9 + ay * 3 + 2];
-                const int I = i < 3 ? i : i - 3;
-                const double s00 = p[PT_SIG], s11 = p[PT_SIG + 1], s22 = p[PT_SIG + 2];
-                const double s01 = 0.5 * p[PT_D1S], s02 = 0.5 * p[PT_D1S + 1], s12 = 0.5 * p[PT_D1S + 2];
-                const double tI0 = p[PT_TAU + 3 * I], tI1 = p[PT_TAU + 3 * I + 1], tI2 = p[PT_TAU + 3 * I + 2];
-#pragma unroll
-                for (int az = 0; az < 3; az++) {
-                    const double *bzp = Bz + qz * 9 + az * 3;
-                    const double bz0 = bzp[0], bz1 = bzp[1], bz2 = bzp[2];
-                    const double dx = bx1 * by0 * bz0, dy = bx0 * by1 * bz0, dz = bx0 * by0 * bz1;
-                    /* second derivatives H[idx6(I, K)], K = 0..2 */
-                    double h0, h1, h2;
-                    if (I == 0) { h0 = bx2 * by0 * bz0; h1 = bx1 * by1 * bz0; h2 = bx1 * by0 * bz1; }
-                    else if (I == 1) { h0 = bx1 * by1 * bz0; h1 = bx0 * by2 * bz0; h2 = bx0 * by1 * bz1; }
-                    else { h0 = bx1 * by0 * bz1; h1 = bx0 * by1 * bz1; h2 = bx0 * by0 * bz2; }
-                    const double th = tI0 * h0 + tI1 * h1 + tI2 * h2;   /* (T H_a)_I */
-                    const double dI = I == 0 ? dx : (I == 1 ? dy : dz);
-                    const int a = 9 * ax + 3 * ay + az, row = qb * 6 + i;
-                    if (i < 3) {
-                        const double sg = I == 0 ? s00 * dx + s01 * dy + s02 * dz
-                                        : (I == 1 ? s01 * dx + s11 * dy + s12 * dz : s02 * dx + s12 * dy + s22 * dz);
-                        S.UT[row][a] = dI;
-                        S.VT[row][a] = w * (sg + th);
-                    } else {
-                        S.UT[row][a] = w * th;
-                        S.VT[row][a] = dI;
-                    }
-                }
-            }
-            if (tid < DROWS) {
-                const double *p = PTb + (q0 + tid / 12) * PT_N;
-                S.sc[tid] = p[PT_W] * p[PT_LAM + tid % 12];
-            }
-            __syncthreads();
-            /* (b) tensor-core accumulation K += X'^T diag(sc) X', Gamma += U^T V */
-#define MMA_CALL(Wn) warp_mma<Wn>(Xb, S.sc, &S.UT[0][0], &S.VT[0][0], lane, acc, gacc)
-            WARP_SWITCH(MMA_CALL)
-#undef MMA_CALL
-            __syncthreads();
-        }
-        /* ---- stage K and Gamma in shared memory, then scatter the 81 x 81 element matrix */
-        double *const K = S.W;
-        double *const Gam = S.W + W_GAM;
-#define DUMP_CALL(Wn) warp_dump<Wn>(K, Gam, lane, acc, gacc)
-        WARP_SWITCH(DUMP_CALL)
-#undef DUMP_CALL
-        if (tid < 81)
-            elem_row_base(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez, tid, S.rbase[tid], S.rsx[tid], S.rsy[tid]);
-        __syncthreads();
-        /* added into the CSR values with fire-and-forget reductions (red.global.add):
-         * the tiles of one colour touch disjoint entries and the elements of a tile
-         * are separated by a barrier, so every entry receives its additions in a
-         * fixed order */
-        for (int idx = tid; idx < 81 * 81; idx += NTHR) {
-            const int c1 = idx / 81, c2 = idx % 81;
-            const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
-            double v = c1 <= c2 ? K[c1 * 88 + c2] : K[c2 * 88 + c1];
-            if (k1 == k2) v += a1 <= a2 ? Gam[a1 * 32 + a2] : Gam[a2 * 32 + a1];
-            atomicAdd(&vals[S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9], v);
-        }
-        __syncthreads();
+    if (tid >= NCONS) {
+        dws_builder(F, S);
+        return;
+    }
+    switch (tid >> 5) {
+    case 0: dws_consumer<0>(F, S); break;
+    case 1: dws_consumer<1>(F, S); break;
+    case 2: dws_consumer<2>(F, S); break;
+    case 3: dws_consumer<3>(F, S); break;
+    case 4: dws_consumer<4>(F, S); break;
+    case 5: dws_consumer<5>(F, S); break;
+    case 6: dws_consumer<6>(F, S); break;
+    default: dws_consumer<7>(F, S); break;
     }
 }
 
-template <int TE>
-__global__ void __launch_bounds__(NTHR, 2) k_tan_dmma(igab_geom g, const double *__restrict__ U,
-                                                      double *__restrict__ vals, int colour)
+__global__ void __launch_bounds__(NTHR, 1) k_tan_dmma(src_colour F)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    dmma_smem<TE> &S = *reinterpret_cast<dmma_smem<TE> *>(smem_raw);
-    tile_t Tl;
-    if (!decode_tile(g, TE, colour, blockIdx.x, Tl)) return;
-    dmma_tile<TE>(g, Tl, U, vals, S);
+    dws_run(F);
 }
 
 /* persistent FP64 tangent over the tiles of every instance of a batch */
-__global__ void __launch_bounds__(NTHR, 2) k_tan_dmma_batch(igab_batch_dev B, const double *__restrict__ U,
-                                                            double *__restrict__ vals)
+__global__ void __launch_bounds__(NTHR, 1) k_tan_dmma_batch(src_batch F)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    dmma_smem<2> &S = *reinterpret_cast<dmma_smem<2> *>(smem_raw);
-    __shared__ batch_slot sl;
-    while (batch_next(B, sl)) {
-        tile_t Tl;
-        decode_tile(sl.g, 2, sl.colour, sl.tile, Tl);
-        dmma_tile<2>(sl.g, Tl, U + B.dof_off[sl.inst], vals + B.nnz_off[sl.inst], S);
-        batch_done(B, sl);
+    dws_run(F);
+}
+
+int sm_count()
+{
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+            n = 148;
     }
+    return n;
 }
 
 } /* namespace */
 
 int igab_launch_tan_dmma_batch(const igab_batch_dev &B, int grid, cudaStream_t st, const double *dU, double *dv)
 {
-    const size_t sm = sizeof(dmma_smem<2>);
+    const size_t sm = sizeof(dws_smem);
     IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_dmma_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_tan_dmma_batch<<<grid, NTHR, sm, st>>>(B, dU, dv);
+    src_batch F;
+    F.B = B;
+    F.U = dU;
+    F.vals = dv;
+    F.status = B.status;
+    k_tan_dmma_batch<<<grid, NTHR, sm, st>>>(F);
     IGAB_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
 int igab_batch_occupancy_dmma(int *per_sm)
 {
-    const size_t sm = sizeof(dmma_smem<2>);
+    const size_t sm = sizeof(dws_smem);
     IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_dmma_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     IGAB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_tan_dmma_batch, NTHR, sm));
     return 0;
@@ -471,12 +705,20 @@ int igab_batch_occupancy_dmma(int *per_sm)
 int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv)
 {
     igab_geom g = c->geom();
-    size_t sm = sizeof(dmma_smem<2>);
-    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_dmma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const size_t sm = sizeof(dws_smem);
+    IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const int nsm = sm_count();
     for (int colour = 0; colour < 8; colour++) {
-        long nblk = tiles_of_colour(g, 2, colour);
-        if (nblk == 0) continue;
-        k_tan_dmma<2><<<(unsigned)nblk, NTHR, sm, c->stream>>>(g, dU, dv, colour);
+        const long nt = tiles_of_colour(g, TE, colour);
+        if (nt == 0) continue;
+        src_colour F;
+        F.g = g;
+        F.U = dU;
+        F.vals = dv;
+        F.colour = colour;
+        F.ntiles = nt;
+        F.status = c->d_status;
+        k_tan_dmma<<<(unsigned)(nt < nsm ? nt : nsm), NTHR, sm, c->stream>>>(F);
         c->last_launches++;
     }
     IGAB_CUDA_TRY(cudaGetLastError());

@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=4, help="elements per side of the CPU sample mesh")
     ap.add_argument("--no-tune", action="store_true", help="skip the schedule autotuner")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-density", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-instance batched assembly")
     ap.add_argument("--batch-instances", type=int, default=512)
     ap.add_argument("--transient", type=int, default=0, metavar="STEPS",
@@ -101,8 +102,10 @@ def _ref_sample_worker(args):
     t1 = time.perf_counter()
     C.tangent(U)
     t2 = time.perf_counter()
+    C.intdensity(13)   # iga_intdensity on U_hist level 0 (left there by the residual callback)
+    t3 = time.perf_counter()
     C.close()
-    return (t1 - t0, t2 - t1, m ** 3)
+    return (t1 - t0, t2 - t1, m ** 3, t3 - t2)
 
 
 class RefPool:
@@ -119,6 +122,7 @@ class RefPool:
         wall = time.perf_counter() - t0
         tr = np.mean([r[0] for r in res]) / res[0][2]
         tt = np.mean([r[1] for r in res]) / res[0][2]
+        self.td = np.mean([r[3] for r in res]) / res[0][2]   # intdensity per element
         return tr, tt, wall
 
     def close(self):
@@ -500,6 +504,27 @@ def run_ours(args):
                                  "K^T lambda on the FP64 CSR tangent, lambda given; the adjoint linear solve "
                                  "K^T lambda = dJ/dU is the caller's (PETSc KSP in the reference application)"}
 
+    # ---- integrated densities (src/iga_intdensity.c) of the same state: 13 ge densities
+    dens = None
+    if not args.no_density:
+        HHd = torch.empty(16, dtype=torch.float64, device=dev)
+        for _ in range(2):
+            A.intdensity_device(U.data_ptr(), HHd.data_ptr())
+        dlaunch = A.last_launch_count()
+        barrier()
+        d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        d0.record(stream)
+        for _ in range(args.steps):
+            A.intdensity_device(U.data_ptr(), HHd.data_ptr())
+        d1.record(stream)
+        barrier()
+        dms = d0.elapsed_time(d1) / args.steps
+        dens = {"ms": round(dms, 3), "densities": 13, "launches": int(dlaunch),
+                "gauss_points_per_s": round(nel * 64 / (dms * 1e-3), 1),
+                "definition": "iga_intdensity: volume integral of the 13 phys/ge densities (energy, stresses, "
+                              "volume fractions) at the 64 Gauss points of every element, minus the Neumann "
+                              "boundary work; device-resident U, CUDA events"}
+
     batch = None
     if not args.no_batch:
         batch = bench_batch(args, dev, local, barrier)
@@ -558,6 +583,7 @@ def run_ours(args):
                           "tangent_volume": round(k64[2], 3), "tangent_dirichlet": round(k64[3], 3)},
             "residual_tflops_alg": round(res_tf, 3) if res_tf else None,
             "adjoint_grads_per_s": adjoint["grads_per_s"] if adjoint else None, "adjoint": adjoint,
+            "intdensity": dens,
             "schedule": schedule, "batch_config3": batch, "transient_config2": trans,
             "transient_adjoint_config4": trans_adj,
             "clocks": clk, "gpu_launches": int(launches64), "roofline": roofline,
@@ -579,6 +605,10 @@ def run_ours(args):
                                         "sample": "%d processes x %d^3 elements (reference residual+tangent), "
                                                   "per-element time extrapolated to %d^3 (%.1f s wall)"
                                                   % (P, args.cpu_sample, n, wall)}
+                if dens is not None:
+                    dens["reference_cpu_ms"] = round(pool.td * nel / P * 1e3, 1)
+                    dens["reference_cpu_sample"] = ("reference iga_intdensity on %d processes x %d^3 elements, "
+                                                    "per-element time extrapolated to %d^3" % (P, args.cpu_sample, n))
             else:
                 line["cpu_baseline"] = None
         except Exception as e:

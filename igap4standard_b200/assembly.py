@@ -168,6 +168,23 @@ class Assembly:
             check(self.lib, "igab_dirichlet_rows", self.lib.igab_dirichlet_rows(self.h, ctypes.byref(n), _ptr(rows)))
         return rows
 
+    def ndensity(self):
+        n = ctypes.c_int()
+        check(self.lib, "igab_ndensity", self.lib.igab_ndensity(self.h, ctypes.byref(n)))
+        return n.value
+
+    def intdensity(self, U):
+        """Integrated densities (src/iga_intdensity.c): volume integral of the point
+        density at U (phys/ge) or at the history levels (phys/getime) minus the
+        Neumann boundary integrals, as in the reference's HH_ array."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        HH = np.empty(self.ndensity())
+        check(self.lib, "igab_intdensity", self.lib.igab_intdensity(self.h, _ptr(U), _ptr(HH)))
+        return HH
+
+    def intdensity_device(self, U_ptr, HH_ptr):
+        check(self.lib, "igab_intdensity_device", self.lib.igab_intdensity_device(self.h, vp(U_ptr), vp(HH_ptr)))
+
     def history_jacobian_device(self, U_ptr, vals_ptr, level, prec="fp64"):
         """CSR values of dR/dU_hist[level] (transient physics; Dirichlet rows zero)."""
         check(self.lib, "igab_history_jacobian_device",

@@ -97,6 +97,13 @@ class Case:
     def app(self):
         return self.lib.iga_case_app(self.h)
 
+    def intdensity(self, nd):
+        """This library's iga_intdensity (src/iga_intdensity.c:10) on U_hist as it
+        stands: nd integrated densities (13 for phys/ge, 2 for phys/getime)."""
+        HH = np.zeros(nd)
+        self.lib.iga_intdensity(_p(HH), vp(self.app))
+        return HH
+
 
 def gpu_case(*args, **kw):
     """A case whose callbacks are the B200 drop-in (libsnesiga_b200)."""

@@ -21,6 +21,10 @@ extern void ge_residual(double *, double *, double *) __attribute__((weak));
 extern void ge_tangent(double *, double *, double *) __attribute__((weak));
 extern void getime_residual(double *, double *, double *) __attribute__((weak));
 extern void getime_tangent(double *, double *, double *) __attribute__((weak));
+extern void ge_density(double *, double *, double *) __attribute__((weak));
+extern void ge_densityb(double *, double *, double, double *, int) __attribute__((weak));
+extern void getime_density(double *, double *, double *) __attribute__((weak));
+extern void getime_densityb(double *, double *, double, double *, int) __attribute__((weak));
 /* subset-only error latches (weak: absent under a real PETSc) */
 extern int petsc_subset_mat_error(Mat A) __attribute__((weak));
 extern int petsc_subset_vec_error(Vec v) __attribute__((weak));
@@ -77,6 +81,8 @@ iga_case *iga_case_create(int phys_kind, const int nelem[3], const double *knots
     memcpy(c->phys.par_mat, par_mat, 9 * sizeof(double));
     c->phys.residual = (phys_kind == IGA_CASE_GE) ? ge_residual : getime_residual;
     c->phys.tangent = (phys_kind == IGA_CASE_GE) ? ge_tangent : getime_tangent;
+    c->phys.density = (phys_kind == IGA_CASE_GE) ? ge_density : getime_density;
+    c->phys.densityb = (phys_kind == IGA_CASE_GE) ? ge_densityb : getime_densityb;
 
     /* ---- Nurbs, one rank */
     Nurbs *nb = &c->nurbs;

@@ -330,6 +330,7 @@ static void free_ctx(igab_ctx *c)
     cudaFree(c->d_dnz); cudaFree(c->d_combo_info); cudaFree(c->d_hist);
     cudaFree(c->d_U); cudaFree(c->d_R); cudaFree(c->d_vals);
     cudaFree(c->d_escale); cudaFree(c->d_lam); cudaFree(c->d_status);
+    cudaFree(c->d_dens_part); cudaFree(c->d_HH);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     for (int k = 0; k < 6; k++)
@@ -703,6 +704,39 @@ extern "C" int igab_history_jacobian_device(igab_ctx *ctx, const double *U_dev, 
     int rc = igab_launch_tan_getime_level(ctx, U_dev, vals_dev, prec, level);
     if (!rc) rc = igab_launch_zero_csr_rows(ctx, vals_dev, prec);
     return rc;
+}
+
+extern "C" int igab_ndensity(const igab_ctx *ctx, int *n)
+{
+    ARG_CHECK(ctx && n, "igab_ndensity: null argument");
+    *n = ctx->phys == IGAB_PHYS_GETIME ? 2 : 13;   /* phys/getime/init.c:14, phys/ge/init.c:14 */
+    return 0;
+}
+
+extern "C" int igab_intdensity_device(igab_ctx *ctx, const double *U_dev, double *HH_dev)
+{
+    ARG_CHECK(ctx && U_dev && HH_dev, "igab_intdensity_device: null argument");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    return igab_launch_density(ctx, U_dev, HH_dev);
+}
+
+extern "C" int igab_intdensity(igab_ctx *ctx, const double *U_host, double *HH_host)
+{
+    ARG_CHECK(ctx && U_host && HH_host, "igab_intdensity: null argument");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    int rc = ensure_buffers(ctx, -1);
+    if (rc) return rc;
+    if (!ctx->d_HH) IGAB_CUDA_TRY(cudaMalloc((void **)&ctx->d_HH, 16 * sizeof(double)));
+    int nd = 0;
+    igab_ndensity(ctx, &nd);
+    IGAB_CUDA_TRY(cudaMemcpyAsync(ctx->d_U, U_host, (size_t)ctx->ndof * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    rc = igab_intdensity_device(ctx, ctx->d_U, ctx->d_HH);
+    if (rc) return rc;
+    IGAB_CUDA_TRY(cudaMemcpyAsync(HH_host, ctx->d_HH, (size_t)nd * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < nd; i++)
+        if (!isfinite(HH_host[i])) { igab_set_error("igab_intdensity: non-finite density %d", i); return IGAB_ERR_NONFINITE; }
+    return 0;
 }
 
 extern "C" int igab_set_stream(igab_ctx *ctx, void *cuda_stream)

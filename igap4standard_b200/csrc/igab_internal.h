@@ -126,6 +126,11 @@ struct igab_ctx {
     bool escale_on = false;
     double *d_lam = nullptr;           /* [ndof] lambda with Dirichlet rows zeroed */
 
+    /* integrated densities: per-block partial rows, result */
+    double *d_dens_part = nullptr;
+    size_t dens_part_bytes = 0;
+    double *d_HH = nullptr;
+
     /* captured assembly graph */
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -136,6 +141,7 @@ struct igab_ctx {
 
 /* kernels / launchers (igab_kernels.cu) */
 int igab_launch_residual(igab_ctx *c, const double *dU, double *dR);
+int igab_launch_density(igab_ctx *c, const double *dU, double *dHH);   /* igab_density.cu */
 int igab_launch_tangent(igab_ctx *c, const double *dU, void *dvals, int prec);
 int igab_launch_csr_cols(igab_ctx *c, int *dcols);
 int igab_launch_check_finite(igab_ctx *c, const void *dev, long n, int prec, int *all_finite);

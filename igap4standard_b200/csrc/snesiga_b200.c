@@ -6,6 +6,7 @@
  * assembly itself happens on the GPU through the igab C ABI.
  */
 #include <stdio.h>
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
@@ -289,6 +290,35 @@ PetscErrorCode snesiga_b200_Residual(SNES snes, Vec U_, Vec Residual_, void *app
     if (rc) fprintf(stderr, "snesiga_b200: residual failed: %s\n", igab_last_error());
     return map_err(rc);
 }
+
+/* Integrated densities of app->U_hist (level 0 is the iterate the callbacks saw last;
+ * phys/getime also reads history levels 1 and 2) -- replaces src/iga_intdensity.c:10.
+ * The reference has no error return: on failure every density is NaN and the
+ * error is printed. */
+void snesiga_b200_intdensity(double HH_[], void *app_)
+{
+    IGA *app = (IGA *)app_;
+    const int nd = app && app->phys ? app->phys->ndensity : 0;
+    gpu_state *s;
+    int rc = get_state(app_, &s);
+    if (!rc) rc = sync_params(s);
+    if (!rc) rc = sync_neumann(s);
+    if (!rc) {
+        int n = 0;
+        rc = igab_ndensity(s->ctx, &n);
+        if (!rc && n != nd) {
+            fprintf(stderr, "snesiga_b200: phys declares %d densities, the GPU path computes %d\n", nd, n);
+            rc = IGAB_ERR_ARG;
+        }
+    }
+    if (!rc) rc = igab_intdensity(s->ctx, app->U_hist, HH_);
+    if (rc) {
+        fprintf(stderr, "snesiga_b200: intdensity failed: %s\n", igab_last_error());
+        for (int i = 0; i < nd; i++) HH_[i] = NAN;
+    }
+}
+
+void iga_intdensity(double HH_[], void *app_) { snesiga_b200_intdensity(HH_, app_); }
 
 /* Put the structured AIJ pattern into P the first time (as the reference's
  * first MatSetValues pass does) and check that P's CSR is exactly it. */

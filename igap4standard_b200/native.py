@@ -96,6 +96,9 @@ IGAB_API = [
     ("igab_tc_peak", ctypes.c_int, [ctypes.c_int, ctypes.c_int, c_double_p]),
     ("igab_history_jacobian_device", ctypes.c_int, [vp, vp, vp, ctypes.c_int, ctypes.c_int]),
     ("igab_dirichlet_rows", ctypes.c_int, [vp, c_long_p, vp]),
+    ("igab_ndensity", ctypes.c_int, [vp, c_int_p]),
+    ("igab_intdensity", ctypes.c_int, [vp, vp, vp]),
+    ("igab_intdensity_device", ctypes.c_int, [vp, vp, vp]),
     ("igab_batch_create", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]),
     ("igab_batch_destroy", ctypes.c_int, [vp]),
     ("igab_batch_sizes", ctypes.c_int, [vp, c_long_p, c_long_p, c_long_p, vp, vp]),
@@ -128,6 +131,8 @@ DROPIN_API = [
     ("snesiga_gpu_set_tangent_precision", ctypes.c_int, [vp, ctypes.c_int]),
     ("snesiga_gpu_context", vp, [vp]),
     ("snesiga_gpu_last_timings", ctypes.c_int, [vp, c_double_p]),
+    ("iga_intdensity", None, [vp, vp]),
+    ("snesiga_b200_intdensity", None, [vp, vp]),
 ]
 
 CASE_API = [

@@ -214,6 +214,20 @@ int igab_batch_autotune(igab_batch *b, const double *U_dev, int what, int reps, 
  * matrices are symmetric; apply their transpose with igab_adjoint_backward. */
 int igab_history_jacobian_device(igab_ctx *ctx, const double *U_dev, void *vals_dev, int prec, int level);
 
+/* ---- integrated densities (replaces src/iga_intdensity.c:10 `iga_intdensity`):
+ * HH[i] = sum over elements and Gauss points of w * density_i(u) minus the Neumann
+ * boundary integrals of the boundary density (phys/ge/density.c: 13 values -- energy,
+ * stresses, volume fractions; phys/getime/density.c: 2 values -- energy at the
+ * midpoint of history levels 1 and 2 plus kinetic energy, and the Neumann area).
+ * u is U (level 0) for phys/ge and the context's history levels for phys/getime;
+ * the traction is the context's Neumann values (igab_set_neumann_values).
+ * igab_ndensity gives the count; igab_intdensity copies HH to the host,
+ * igab_intdensity_device writes it to device memory on the context's stream.
+ * Sums are taken in a fixed order: results are bitwise repeatable. */
+int igab_ndensity(const igab_ctx *ctx, int *n);
+int igab_intdensity(igab_ctx *ctx, const double *U_host, double *HH_host);
+int igab_intdensity_device(igab_ctx *ctx, const double *U_dev, double *HH_dev);
+
 /* ---- residual for callers that cannot have the library allocate device memory.
  * No counterpart in the reference.  Same result as igab_residual, but U and R
  * are staged in a file-scope device array (2 x 8 MiB, held by every GPU that

@@ -11,6 +11,7 @@
  *   snesiga_Tangent   replaces src/snesiga_Tangent.c:13    (assembles into Pmat_,
  *                     assembles Tangent_ if it differs, :275-279)
  *   snesiga_init      replaces src/snesiga_init.c:12       (single rank)
+ *   iga_intdensity    replaces src/iga_intdensity.c:10     (integrated densities)
  * The GPU state (device buffers, pattern check, traction table) lives in a
  * registry keyed by the IGA pointer, so the IGA struct stays binary-identical.
  * It is created on the first callback (or by snesiga_gpu_init) and released
@@ -34,9 +35,14 @@ PetscErrorCode snesiga_Residual(SNES snes, Vec U_, Vec Residual_, void *app_);
 PetscErrorCode snesiga_Tangent(SNES snes, Vec U_, Mat Tangent_, Mat Pmat_, void *app_);
 void snesiga_init(void *app_, void *phys_, void *nurbs_, void *bc_, void *snesassmbl_, void *iocomm_);
 
+/* integrated densities of app->U_hist, replacing src/iga_intdensity.c:10
+ * (include/iga.h:29); NaN in every slot on failure (the reference returns void) */
+void iga_intdensity(double HH_[], void *app_);
+
 /* the same callbacks under names that cannot collide with libigap4 */
 PetscErrorCode snesiga_b200_Residual(SNES snes, Vec U_, Vec Residual_, void *app_);
 PetscErrorCode snesiga_b200_Tangent(SNES snes, Vec U_, Mat Tangent_, Mat Pmat_, void *app_);
+void snesiga_b200_intdensity(double HH_[], void *app_);
 
 /* explicit GPU state management (optional; the callbacks create it lazily) */
 PetscErrorCode snesiga_gpu_init(void *app_, int device);

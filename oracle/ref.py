@@ -6,7 +6,7 @@ case builder (same C API as igap4standard_b200.case) and the reference's
 point functions: ge_residual/ge_tangent (phys/ge), getime_residual/
 getime_tangent (phys/getime), eval_Bspline (mesh/nurbs/eval_Bspline.c),
 evalN (mesh/nurbs/evalN.c), legendre_handle (src/quadrature.c),
-iga_dirichlet (src/iga_dirichlet.c).
+iga_dirichlet (src/iga_dirichlet.c), iga_intdensity (src/iga_intdensity.c).
 """
 import ctypes
 import os
@@ -44,6 +44,8 @@ def lib():
         L.iga_dirichlet.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int,
                                     ctypes.c_int]
         L.iga_dirichlet.restype = None
+        L.iga_intdensity.argtypes = [vp, vp]
+        L.iga_intdensity.restype = None
         L.oracle_scale_install.argtypes = [vp, vp, ctypes.c_long]
         L.oracle_scale_install.restype = None
         L.oracle_scale_remove.argtypes = [vp]

@@ -105,3 +105,33 @@ def test_port_matches_reference_random(oracle_lib, port_oracle):
         rp, cc, v = port_oracle.PortCase(*args).tangent(U)
         assert np.array_equal(rp, rp_r) and np.array_equal(cc, c_r)
         assert np.all(np.abs(v - v_r) <= tangent_tolerance(rp_r, v_r))
+
+
+def test_reference_intdensity_known_answers(oracle_lib):
+    """The reference's iga_intdensity (src/iga_intdensity.c) on states with closed-form
+    integrals (unit cube): every phys/ge density vanishes at rest; for phys/getime with
+    U_hist[2] = 0 and U_hist[1] = c e_x at every control point (partition of unity:
+    a rigid shift) the midpoint energy vanishes and HH[0] = rho c^2 / (2 dt^2), and
+    HH[1] is minus the Neumann area (phys/getime/density.c:61), one unit face per
+    (face, order, dof) combination marked Neumann."""
+    from igap4standard_b200 import mesh
+    nelem = (3, 2, 4)
+    kn = mesh.knots_for(nelem, perturb=0.1, seed=2)
+    bc, pd = mesh.bc_config0()
+    pn = np.zeros(39)
+    C = oracle_lib.case("ge", nelem, kn, mesh.par_mat_from_lame(1.0, 1.0, 0.1), bc, np.zeros(9), pd, pn)
+    C.set_history(0, np.zeros(C.ndof))
+    assert np.array_equal(C.intdensity(13), np.zeros(13))
+    pm = mesh.par_mat_from_lame(1.0, 1.0, 0.1)
+    rho, dt, c = 1.7, 2e-3, 3e-3
+    pm[5], pm[7] = rho, dt
+    T = oracle_lib.case("getime", nelem, kn, pm, bc, np.zeros(9), pd, pn)
+    U1 = np.zeros(T.ndof)
+    U1[0::3] = c
+    T.set_history(0, U1)
+    T.set_history(1, U1)
+    T.set_history(2, np.zeros(T.ndof))
+    HH = T.intdensity(2)
+    n_neumann = int(np.sum(np.asarray(bc) == 1))
+    assert abs(HH[0] - rho * c * c / (2 * dt * dt)) <= 1e-12 * rho * c * c / (2 * dt * dt)
+    assert abs(HH[1] + n_neumann) <= 1e-13 * max(n_neumann, 1)

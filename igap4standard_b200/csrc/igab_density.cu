@@ -35,6 +35,7 @@ namespace {
 #define DN_MAX 13
 #define VOL_THREADS 256
 #define SURF_THREADS 128
+#define RED_THREADS 256
 
 struct dens_geom {
     igab_geom g;
@@ -255,10 +256,10 @@ __global__ void __launch_bounds__(SURF_THREADS) k_density_surface(dens_geom D, i
 }
 
 template <int ND>
-__global__ void k_density_reduce(const double *__restrict__ part, long nvol, long nsurf, double *__restrict__ HH)
+__global__ void __launch_bounds__(RED_THREADS) k_density_reduce(const double *__restrict__ part, long nvol, long nsurf, double *__restrict__ HH)
 {
-    __shared__ double red[32 * DN_MAX];
-    const int tid = threadIdx.x;   /* 1024 threads */
+    __shared__ double red[(RED_THREADS / 32) * DN_MAX];
+    const int tid = threadIdx.x;   /* RED_THREADS threads */
     double v[DN_MAX], s[DN_MAX];
 #pragma unroll
     for (int i = 0; i < DN_MAX; i++) v[i] = s[i] = 0.0;
@@ -269,8 +270,8 @@ __global__ void k_density_reduce(const double *__restrict__ part, long nvol, lon
 #pragma unroll
         for (int i = 0; i < ND; i++) s[i] += part[(nvol + b) * DN_MAX + i];
     __shared__ double rows[2][DN_MAX];
-    block_rows<1024, ND>(v, rows[0], red);
-    block_rows<1024, ND>(s, rows[1], red);
+    block_rows<RED_THREADS, ND>(v, rows[0], red);
+    block_rows<RED_THREADS, ND>(s, rows[1], red);
     if (tid < ND) HH[tid] = rows[0][tid] - rows[1][tid];
 }
 
@@ -287,7 +288,7 @@ void launch_density(igab_ctx *c, const dens_geom &D, long nvol, long nsurf, doub
             c->d_dens_part + nvol * DN_MAX);
         c->last_launches++;
     }
-    k_density_reduce<ND><<<1, 1024, 0, c->stream>>>(c->d_dens_part, nvol, nsurf, dHH);
+    k_density_reduce<ND><<<1, RED_THREADS, 0, c->stream>>>(c->d_dens_part, nvol, nsurf, dHH);
     c->last_launches++;
 }
 

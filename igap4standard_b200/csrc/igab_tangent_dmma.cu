@@ -17,9 +17,11 @@
  * (2x2x2 elements) of one colour or of a batched work list:
  *   - 8 builder warps compute, per element, the field at the 64 Gauss points
  *     (sum factorisation), the point integrand, and then per batch of 4 points
- *     the 48 rows of X' (straight from the 1-D basis tables: one task per
- *     (point, variable, component, x-function)), the 24 U / V rows and the
- *     scales s, into one of two shared-memory slots;
+ *     the 48 rows of X' (one task per (point, basis function, component): the
+ *     9 derivatives of the basis function from the 1-D tables, then all 12
+ *     variables' entries in straight-line code), the 24 U / V rows (one task
+ *     per (point, basis function)) and the scales s, into one of two
+ *     shared-memory slots;
  *   - 8 consumer warps run the DMMA products on the slot: the 66 upper 8x8
  *     tiles of the 88x88 element matrix and the 10 upper tiles of the 32x32
  *     Gamma block, split over the warps by igab_warp_tiles8.inc, with the
@@ -122,47 +124,6 @@ __device__ __forceinline__ void sym2_eig(double a, double b, double c, double &c
     l2 = c + t * b;
 }
 
-/* gradient of rotated variable v with respect to the 9 strain components of
- * displacement component k (igab_ge_grad_var, then the (va, vb) rotation) */
-__device__ __forceinline__ void dm_grad_var(const double *p, int v, int k, double g[9])
-{
-#pragma unroll
-    for (int m = 0; m < 9; m++) g[m] = 0.0;
-    const double is2 = IGAB_INV_SQRT2, is3 = IGAB_INV_SQRT3, is6 = IGAB_INV_SQRT6;
-    const double F0 = p[PT_F + 3 * k], F1 = p[PT_F + 3 * k + 1], F2 = p[PT_F + 3 * k + 2];
-    const double *G = p + PT_G + 6 * k;
-    if (v == 0) {
-        g[0] = F0 * is3; g[1] = F1 * is3; g[2] = F2 * is3;
-    } else if (v <= 2) {
-        const double cs = p[PT_CS], sn = p[PT_SN];
-        const double a0 = F0 * is2, a1 = -F1 * is2;                       /* va */
-        const double b0 = F0 * is6, b1 = F1 * is6, b2 = -2.0 * F2 * is6;  /* vb */
-        if (v == 1) { g[0] = cs * a0 - sn * b0; g[1] = cs * a1 - sn * b1; g[2] = -sn * b2; }
-        else        { g[0] = sn * a0 + cs * b0; g[1] = sn * a1 + cs * b1; g[2] = cs * b2; }
-    } else if (v == 3) {
-        g[0] = 0.5 * F1; g[1] = 0.5 * F0;
-    } else if (v == 4) {
-        g[0] = 0.5 * F2; g[2] = 0.5 * F0;
-    } else if (v == 5) {
-        g[1] = 0.5 * F2; g[2] = 0.5 * F1;
-    } else if (v == 6) {   /* strain-gradient variables (idx6: xx xy xz yy yz zz) */
-        g[0] = G[0] * is2; g[1] = -G[1] * is2; g[3] = F0 * is2; g[4] = -F1 * is2;
-    } else if (v == 7) {
-        g[0] = G[1] * is2; g[1] = -G[3] * is2; g[4] = F0 * is2; g[6] = -F1 * is2;
-    } else if (v == 8) {
-        g[0] = G[2] * is2; g[1] = -G[4] * is2; g[5] = F0 * is2; g[7] = -F1 * is2;
-    } else if (v == 9) {
-        g[0] = G[0] * is6; g[1] = G[1] * is6; g[2] = -2.0 * G[2] * is6;
-        g[3] = F0 * is6; g[4] = F1 * is6; g[5] = -2.0 * F2 * is6;
-    } else if (v == 10) {
-        g[0] = G[1] * is6; g[1] = G[3] * is6; g[2] = -2.0 * G[4] * is6;
-        g[4] = F0 * is6; g[6] = F1 * is6; g[7] = -2.0 * F2 * is6;
-    } else {
-        g[0] = G[2] * is6; g[1] = G[4] * is6; g[2] = -2.0 * G[5] * is6;
-        g[5] = F0 * is6; g[7] = F1 * is6; g[8] = -2.0 * F2 * is6;
-    }
-}
-
 /* ---------------------------------------------------------------- work sources */
 
 /* the tiles of one colour, dealt round-robin over the persistent blocks */
@@ -243,7 +204,15 @@ __device__ __forceinline__ bool bld_acquire(dws_smem &S, int gb)
     return tc_bar_and(BAR_BLD, NBLD, ok);
 }
 
-/* X', U / V and s of the batch of points q0 .. q0 + 3 into slot b */
+/* X', U / V and s of the batch of points q0 .. q0 + 3 into slot b.
+ * X' task (point qb, basis function a, component k): the 9 derivatives of N_a
+ * (dx, dy, dz, xx, xy, xz, yy, yz, zz) from the 1-D tables, then the 12 rows
+ *   X'[(qb, v)][3a + k] = sum_m dv'/du_{k,m} N_a^m
+ * with dv/du_{k,m} of igab_ge_grad_var written out per variable (F = F[k][.],
+ * G = G[k][.]; the (va, vb) pair rotated by (cs, sn)).
+ * U / V task (point qb, basis function a): the six rows of the geometric
+ * product, U_i = d_i N_a, V_i = w ((S grad N_a)_i + (T H_a)_i), U_{3+I} =
+ * w (T H_a)_I, V_{3+I} = d_I N_a, with (T H_a)_I = sum_K T[I][K] N_a^{(I,K)}. */
 __device__ __forceinline__ void bld_batch(dws_smem &S, int b, int q0, const double *Bx, const double *By,
                                           const double *Bz, int tb)
 {
@@ -251,71 +220,65 @@ __device__ __forceinline__ void bld_batch(dws_smem &S, int b, int q0, const doub
     double *const UTs = S.UT[b];
     double *const VTs = S.VT[b];
     const double *const PTb = S.pt;
-    /* X' rows: task (variable v, point qb, component k, x-function ax) -> 9 outputs
-     * (ay, az), X'[(qb, v)][3a + k] = sum_m dv'/du_{k,m} Bx By Bz, summed over x, y, z;
-     * U / V rows: task (row i, point qb, ax, ay) -> 3 outputs (az) of U and of V */
-    for (int t = tb; t < DQ * 12 * 9 + DQ * 6 * 9; t += NBLD) {
-        if (t < DQ * 12 * 9) {
-            const int v = t / (DQ * 9), r = t % (DQ * 9);
-            const int qb = r / 9, k = (r / 3) % 3, ax = r % 3;
-            const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
-            double gv[9];
-            dm_grad_var(PTb + q * PT_N, v, k, gv);
-            const double *bxp = Bx + qx * 9 + ax * 3;
-            const double bx0 = bxp[0], bx1 = bxp[1], bx2 = bxp[2];
-            /* coefficients of By[ky] per kz: derivative m -> (kx, ky, kz) as eval_Bspline */
-            const double t00 = gv[0] * bx1 + gv[3] * bx2, t01 = gv[1] * bx0 + gv[4] * bx1, t02 = gv[6] * bx0;
-            const double t10 = gv[2] * bx0 + gv[5] * bx1, t11 = gv[7] * bx0;
-            const double t20 = gv[8] * bx0;
-            double *xr = Xs + (qb * 12 + v) * XS + k;
-#pragma unroll
-            for (int ay = 0; ay < 3; ay++) {
-                const double *byp = By + qy * 9 + ay * 3;
-                const double cy0 = t00 * byp[0] + t01 * byp[1] + t02 * byp[2];
-                const double cy1 = t10 * byp[0] + t11 * byp[1];
-                const double cy2 = t20 * byp[0];
-#pragma unroll
-                for (int az = 0; az < 3; az++) {
-                    const double *bzp = Bz + qz * 9 + az * 3;
-                    xr[3 * (9 * ax + 3 * ay + az)] = cy0 * bzp[0] + cy1 * bzp[1] + cy2 * bzp[2];
-                }
-            }
+    const double is2 = IGAB_INV_SQRT2, is3 = IGAB_INV_SQRT3, is6 = IGAB_INV_SQRT6;
+    for (int t = tb; t < DQ * 81 + DQ * 27; t += NBLD) {
+        const bool xtask = t < DQ * 81;
+        const int tg = xtask ? t : t - DQ * 81;
+        const int qb = xtask ? tg / 81 : tg / 27;
+        const int a = xtask ? (tg % 81) / 3 : tg % 27;
+        const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
+        const int ax = a / 9, ay = (a / 3) % 3, az = a % 3;
+        const double *bxp = Bx + qx * 9 + ax * 3, *byp = By + qy * 9 + ay * 3, *bzp = Bz + qz * 9 + az * 3;
+        const double bx0 = bxp[0], bx1 = bxp[1], bx2 = bxp[2];
+        const double by0 = byp[0], by1 = byp[1], by2 = byp[2];
+        const double bz0 = bzp[0], bz1 = bzp[1], bz2 = bzp[2];
+        const double b00 = bx0 * by0, b10 = bx1 * by0, b01 = bx0 * by1;
+        const double dx = b10 * bz0, dy = b01 * bz0, dz = b00 * bz1;
+        const double hxx = bx2 * by0 * bz0, hxy = bx1 * by1 * bz0, hxz = b10 * bz1;
+        const double hyy = bx0 * by2 * bz0, hyz = b01 * bz1, hzz = b00 * bz2;
+        const double *p = PTb + q * PT_N;
+        if (xtask) {
+            const int k = tg % 3;
+            const double F0 = p[PT_F + 3 * k], F1 = p[PT_F + 3 * k + 1], F2 = p[PT_F + 3 * k + 2];
+            const double *G = p + PT_G + 6 * k;
+            const double G0 = G[0], G1 = G[1], G2 = G[2], G3 = G[3], G4 = G[4], G5 = G[5];
+            const double cs = p[PT_CS], sn = p[PT_SN];
+            const double e0 = F0 * dx, e1 = F1 * dy, e2 = F2 * dz;
+            const double va = (e0 - e1) * is2, vb = (e0 + e1 - 2.0 * e2) * is6;
+            double *xc = Xs + (qb * 12) * XS + 3 * a + k;
+            xc[0 * XS] = (e0 + e1 + e2) * is3;
+            xc[1 * XS] = cs * va - sn * vb;
+            xc[2 * XS] = sn * va + cs * vb;
+            xc[3 * XS] = 0.5 * (F1 * dx + F0 * dy);
+            xc[4 * XS] = 0.5 * (F2 * dx + F0 * dz);
+            xc[5 * XS] = 0.5 * (F2 * dy + F1 * dz);
+            xc[6 * XS] = (G0 * dx - G1 * dy + F0 * hxx - F1 * hxy) * is2;
+            xc[7 * XS] = (G1 * dx - G3 * dy + F0 * hxy - F1 * hyy) * is2;
+            xc[8 * XS] = (G2 * dx - G4 * dy + F0 * hxz - F1 * hyz) * is2;
+            xc[9 * XS] = (G0 * dx + G1 * dy - 2.0 * G2 * dz + F0 * hxx + F1 * hxy - 2.0 * F2 * hxz) * is6;
+            xc[10 * XS] = (G1 * dx + G3 * dy - 2.0 * G4 * dz + F0 * hxy + F1 * hyy - 2.0 * F2 * hyz) * is6;
+            xc[11 * XS] = (G2 * dx + G4 * dy - 2.0 * G5 * dz + F0 * hxz + F1 * hyz - 2.0 * F2 * hzz) * is6;
         } else {
-            const int tg = t - DQ * 12 * 9;
-            const int i = tg / (DQ * 9), r = tg % (DQ * 9);
-            const int qb = r / 9, ax = (r / 3) % 3, ay = r % 3;
-            const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
-            const double *p = PTb + q * PT_N;
             const double w = p[PT_W];
-            const double bx0 = Bx[qx * 9 + ax * 3], bx1 = Bx[qx * 9 + ax * 3 + 1], bx2 = Bx[qx * 9 + ax * 3 + 2];
-            const double by0 = By[qy * 9 + ay * 3], by1 = By[qy * 9 + ay * 3 + 1], by2 = By[qy * 9 + ay * 3 + 2];
-            const int I = i < 3 ? i : i - 3;
             const double s00 = p[PT_SIG], s11 = p[PT_SIG + 1], s22 = p[PT_SIG + 2];
             const double s01 = 0.5 * p[PT_D1S], s02 = 0.5 * p[PT_D1S + 1], s12 = 0.5 * p[PT_D1S + 2];
-            const double tI0 = p[PT_TAU + 3 * I], tI1 = p[PT_TAU + 3 * I + 1], tI2 = p[PT_TAU + 3 * I + 2];
-#pragma unroll
-            for (int az = 0; az < 3; az++) {
-                const double *bzp = Bz + qz * 9 + az * 3;
-                const double bz0 = bzp[0], bz1 = bzp[1], bz2 = bzp[2];
-                const double dx = bx1 * by0 * bz0, dy = bx0 * by1 * bz0, dz = bx0 * by0 * bz1;
-                /* second derivatives H[idx6(I, K)], K = 0..2 */
-                double h0, h1, h2;
-                if (I == 0) { h0 = bx2 * by0 * bz0; h1 = bx1 * by1 * bz0; h2 = bx1 * by0 * bz1; }
-                else if (I == 1) { h0 = bx1 * by1 * bz0; h1 = bx0 * by2 * bz0; h2 = bx0 * by1 * bz1; }
-                else { h0 = bx1 * by0 * bz1; h1 = bx0 * by1 * bz1; h2 = bx0 * by0 * bz2; }
-                const double th = tI0 * h0 + tI1 * h1 + tI2 * h2;   /* (T H_a)_I */
-                const double dI = I == 0 ? dx : (I == 1 ? dy : dz);
-                const int a = 9 * ax + 3 * ay + az, row = qb * 6 + i;
-                if (i < 3) {
-                    const double sg = I == 0 ? s00 * dx + s01 * dy + s02 * dz
-                                    : (I == 1 ? s01 * dx + s11 * dy + s12 * dz : s02 * dx + s12 * dy + s22 * dz);
-                    UTs[row * GS + a] = dI;
-                    VTs[row * GS + a] = w * (sg + th);
-                } else {
-                    UTs[row * GS + a] = w * th;
-                    VTs[row * GS + a] = dI;
-                }
-            }
+            const double *T = p + PT_TAU;
+            const double th0 = T[0] * hxx + T[1] * hxy + T[2] * hxz;
+            const double th1 = T[3] * hxy + T[4] * hyy + T[5] * hyz;
+            const double th2 = T[6] * hxz + T[7] * hyz + T[8] * hzz;
+            double *ur = UTs + (qb * 6) * GS + a, *vr = VTs + (qb * 6) * GS + a;
+            ur[0 * GS] = dx;
+            ur[1 * GS] = dy;
+            ur[2 * GS] = dz;
+            vr[0 * GS] = w * (s00 * dx + s01 * dy + s02 * dz + th0);
+            vr[1 * GS] = w * (s01 * dx + s11 * dy + s12 * dz + th1);
+            vr[2 * GS] = w * (s02 * dx + s12 * dy + s22 * dz + th2);
+            ur[3 * GS] = w * th0;
+            ur[4 * GS] = w * th1;
+            ur[5 * GS] = w * th2;
+            vr[3 * GS] = dx;
+            vr[4 * GS] = dy;
+            vr[5 * GS] = dz;
         }
     }
     if (tb < DROWS) {

@@ -168,6 +168,20 @@ class Assembly:
             check(self.lib, "igab_dirichlet_rows", self.lib.igab_dirichlet_rows(self.h, ctypes.byref(n), _ptr(rows)))
         return rows
 
+    def spmv_device(self, vals_ptr, x_ptr, y_ptr, prec="fp64"):
+        """y = K x on the tangent's pattern (device pointers, FP64 vectors)."""
+        check(self.lib, "igab_spmv_device",
+              self.lib.igab_spmv_device(self.h, vp(vals_ptr), PREC[prec], vp(x_ptr), vp(y_ptr)))
+
+    def solve_device(self, vals_ptr, b_ptr, x_ptr, prec="fp64", rtol=1e-5, atol=0.0, maxit=2000):
+        """x = K^-1 b on the device: Jacobi-preconditioned BiCGStab, x0 = 0, stop at
+        ||b - K x|| <= max(rtol ||b||, atol).  Returns (iterations, converged, residual norm)."""
+        info = native.IgabSolveInfo()
+        check(self.lib, "igab_solve_device",
+              self.lib.igab_solve_device(self.h, vp(vals_ptr), PREC[prec], vp(b_ptr), vp(x_ptr), float(rtol),
+                                         float(atol), int(maxit), ctypes.byref(info)))
+        return info.iterations, bool(info.converged), info.residual_norm
+
     def ndensity(self):
         n = ctypes.c_int()
         check(self.lib, "igab_ndensity", self.lib.igab_ndensity(self.h, ctypes.byref(n)))

@@ -331,6 +331,7 @@ static void free_ctx(igab_ctx *c)
     cudaFree(c->d_U); cudaFree(c->d_R); cudaFree(c->d_vals);
     cudaFree(c->d_escale); cudaFree(c->d_lam); cudaFree(c->d_status);
     cudaFree(c->d_dens_part); cudaFree(c->d_HH);
+    igab_krylov_release(c);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     for (int k = 0; k < 6; k++)
@@ -736,6 +737,36 @@ extern "C" int igab_intdensity(igab_ctx *ctx, const double *U_host, double *HH_h
     IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     for (int i = 0; i < nd; i++)
         if (!isfinite(HH_host[i])) { igab_set_error("igab_intdensity: non-finite density %d", i); return IGAB_ERR_NONFINITE; }
+    return 0;
+}
+
+extern "C" int igab_spmv_device(igab_ctx *ctx, const void *vals_dev, int prec, const double *x_dev, double *y_dev)
+{
+    ARG_CHECK(ctx && vals_dev && x_dev && y_dev, "igab_spmv_device: null argument");
+    ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_spmv_device: bad precision");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    ctx->last_launches = 0;
+    return igab_launch_spmv(ctx, vals_dev, prec, x_dev, y_dev);
+}
+
+extern "C" int igab_solve_device(igab_ctx *ctx, const void *vals_dev, int prec, const double *b_dev, double *x_dev,
+                                 double rtol, double atol, int maxit, igab_solve_info *info)
+{
+    ARG_CHECK(ctx && vals_dev && b_dev && x_dev, "igab_solve_device: null argument");
+    ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_solve_device: bad precision");
+    ARG_CHECK(maxit >= 1 && rtol >= 0.0 && atol >= 0.0, "igab_solve_device: bad tolerances");
+    ARG_CHECK(ctx->stream != nullptr, "igab_solve_device: needs a non-default stream (igab_set_stream)");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    int its = 0, conv = 0;
+    double rn = 0.0, bn = 0.0;
+    int rc = igab_krylov_solve(ctx, vals_dev, prec, b_dev, x_dev, rtol, atol, maxit, &its, &conv, &rn, &bn);
+    if (rc) return rc;
+    if (info) {
+        info->iterations = its;
+        info->converged = conv;
+        info->residual_norm = rn;
+        info->rhs_norm = bn;
+    }
     return 0;
 }
 

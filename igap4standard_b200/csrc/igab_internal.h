@@ -142,6 +142,11 @@ struct igab_ctx {
 /* kernels / launchers (igab_kernels.cu) */
 int igab_launch_residual(igab_ctx *c, const double *dU, double *dR);
 int igab_launch_density(igab_ctx *c, const double *dU, double *dHH);   /* igab_density.cu */
+/* igab_krylov.cu: K x on the structured pattern, Jacobi-BiCGStab on the device */
+int igab_launch_spmv(igab_ctx *c, const void *dvals, int prec, const double *dx, double *dy);
+int igab_krylov_solve(igab_ctx *c, const void *dvals, int prec, const double *db, double *dx, double rtol,
+                      double atol, int maxit, int *iterations, int *converged, double *rnorm, double *bnorm);
+void igab_krylov_release(igab_ctx *c);
 int igab_launch_tangent(igab_ctx *c, const double *dU, void *dvals, int prec);
 int igab_launch_csr_cols(igab_ctx *c, int *dcols);
 int igab_launch_check_finite(igab_ctx *c, const void *dev, long n, int prec, int *all_finite);

@@ -35,6 +35,12 @@ class IgabTuneResult(ctypes.Structure):
                 ("tangent_fp64_ms", ctypes.c_double), ("tangent_fp32_ms", ctypes.c_double)]
 
 
+class IgabSolveInfo(ctypes.Structure):
+    """igab_solve_info of include/igab.h"""
+    _fields_ = [("iterations", ctypes.c_int), ("converged", ctypes.c_int), ("residual_norm", ctypes.c_double),
+                ("rhs_norm", ctypes.c_double)]
+
+
 class IgabBatchTuneResult(ctypes.Structure):
     """igab_batch_tune_result of include/igab.h"""
     _fields_ = [("ctas_res", ctypes.c_int), ("ctas_tan64", ctypes.c_int), ("ctas_tan32", ctypes.c_int),
@@ -99,6 +105,9 @@ IGAB_API = [
     ("igab_ndensity", ctypes.c_int, [vp, c_int_p]),
     ("igab_intdensity", ctypes.c_int, [vp, vp, vp]),
     ("igab_intdensity_device", ctypes.c_int, [vp, vp, vp]),
+    ("igab_spmv_device", ctypes.c_int, [vp, vp, ctypes.c_int, vp, vp]),
+    ("igab_solve_device", ctypes.c_int, [vp, vp, ctypes.c_int, vp, vp, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_int, ctypes.POINTER(IgabSolveInfo)]),
     ("igab_batch_create", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]),
     ("igab_batch_destroy", ctypes.c_int, [vp]),
     ("igab_batch_sizes", ctypes.c_int, [vp, c_long_p, c_long_p, c_long_p, vp, vp]),

@@ -13,10 +13,10 @@ for k = torder..1 (:55).  This module does the same on the GPU:
     updated in place, which replays pick up;
   - the line search is newton.backtrack (Dennis & Schnabel A6.3.1, as PETSc's
     SNESLINESEARCHBT), on device tensors;
-  - the linear solve is Jacobi-preconditioned BiCGStab (van der Vorst, SIAM J.
-    Sci. Stat. Comput. 13 (1992) 631-644) whose operator is the library's own
-    structured K^T x kernel (K is symmetric after the symmetric Dirichlet
-    elimination, so K^T x = K x).  The reference solves with PETSc GMRES + ASM
+  - the linear solve is the library's device BiCGStab (igab_solve_device:
+    Jacobi-preconditioned, van der Vorst, SIAM J. Sci. Stat. Comput. 13 (1992)
+    631-644; scalars and the stop test on the device, iterations replayed as a
+    CUDA graph).  The reference solves with PETSc GMRES + ASM
     (src/snes_init.c:24-39), which is outside the assembly path; this solver is
     the driver's stand-in for it.
 
@@ -86,58 +86,23 @@ class DeviceProblem:
         return out
 
     def matvec(self, x, y=None):
+        """K x on the device (igab_spmv_device)."""
         torch = _torch()
         x = x.contiguous()
         y = torch.empty_like(x) if y is None else y
-        self.A.adjoint_backward_device(None, self.V.data_ptr(), x.data_ptr(), y.data_ptr(), None, self.prec)
+        self.A.spmv_device(self.V.data_ptr(), x.data_ptr(), y.data_ptr(), self.prec)
         return y
+
+    def solve(self, b, rtol, maxit=2000):
+        """K^-1 b by the library's device BiCGStab (Jacobi); returns (x, iterations, converged)."""
+        torch = _torch()
+        b = b.contiguous()
+        x = torch.empty_like(b)
+        its, ok, _ = self.A.solve_device(self.V.data_ptr(), b.data_ptr(), x.data_ptr(), self.prec, rtol, 0.0, maxit)
+        return x, its, ok
 
     def diagonal(self):
         return self.V[self.diag_pos].to(_torch().float64)
-
-
-def bicgstab(matvec, b, dinv, rtol=1e-5, atol=0.0, maxit=2000):
-    """Right-preconditioned BiCGStab (M = diag); returns (x, iterations, converged).
-    Stops when ||b - A x|| <= max(rtol ||b||, atol)."""
-    torch = _torch()
-    x = torch.zeros_like(b)
-    r = b.clone()
-    bnorm = float(b.norm())
-    if bnorm == 0.0:
-        return x, 0, True
-    tol = max(rtol * bnorm, atol)
-    rhat = r.clone()
-    rho = alpha = omega = 1.0
-    v = torch.zeros_like(b)
-    p = torch.zeros_like(b)
-    for it in range(1, maxit + 1):
-        rho_new = float(torch.dot(rhat, r))
-        if rho_new == 0.0:
-            return x, it, False
-        beta = (rho_new / rho) * (alpha / omega) if it > 1 else 0.0
-        p = r + beta * (p - omega * v) if it > 1 else r.clone()
-        phat = dinv * p
-        v = matvec(phat)
-        den = float(torch.dot(rhat, v))
-        if den == 0.0:
-            return x, it, False
-        alpha = rho_new / den
-        s = r - alpha * v
-        if float(s.norm()) <= tol:
-            x += alpha * phat
-            return x, it, True
-        shat = dinv * s
-        t = matvec(shat)
-        tt = float(torch.dot(t, t))
-        omega = float(torch.dot(t, s)) / tt if tt > 0 else 0.0
-        x += alpha * phat + omega * shat
-        r = s - omega * t
-        rho = rho_new
-        if float(r.norm()) <= tol:
-            return x, it, True
-        if omega == 0.0:
-            return x, it, False
-    return x, maxit, False
 
 
 def newton_device(P, rtol_lin=1e-5, max_subiter=newton.MAX_SUBITER, abs_tol=newton.ABS_TOL):
@@ -156,9 +121,7 @@ def newton_device(P, rtol_lin=1e-5, max_subiter=newton.MAX_SUBITER, abs_tol=newt
             reason = newton.CONVERGED_FNORM_ABS
         else:
             ttol = fnorm * newton.REL_TOL
-            d = P.diagonal()
-            dinv = torch.where(d != 0, 1.0 / d, torch.ones_like(d))
-            Y, its, _ = bicgstab(P.matvec, F, dinv, rtol=rtol_lin)
+            Y, its, _ = P.solve(F, rtol_lin)
             P.krylov_its.append(its)
             JY = P.matvec(Y)
             xnorm = float(P.X.norm())
@@ -251,10 +214,8 @@ def _run(P, A, nsteps, dt, rtol_lin, traction, U_init, U_prev, callback, abs_tol
 
 
 def _sym_solve(P, b, rtol):
-    torch = _torch()
-    d = P.diagonal()
-    dinv = torch.where(d != 0, 1.0 / d, torch.ones_like(d))
-    x, its, ok = bicgstab(P.matvec, b, dinv, rtol=rtol)
+    """K^T x = b for the symmetric tangent (Dirichlet rows and columns eliminated)."""
+    x, its, ok = P.solve(b, rtol)
     return x
 
 

@@ -228,6 +228,24 @@ int igab_ndensity(const igab_ctx *ctx, int *n);
 int igab_intdensity(igab_ctx *ctx, const double *U_host, double *HH_host);
 int igab_intdensity_device(igab_ctx *ctx, const double *U_dev, double *HH_dev);
 
+/* ---- device-resident linear algebra on the tangent (no tangent leaves the GPU; stands in
+ * for the PETSc KSP solve of the reference's Newton iteration, src/snes_init.c).
+ * igab_spmv_device: y = K x on the context's CSR pattern (vals FP64 or FP32, x, y FP64).
+ * igab_solve_device: x = K^-1 b by right-preconditioned BiCGStab, Jacobi preconditioner
+ * diag(K) (1 where a diagonal entry is 0), x0 = 0, stopping when ||b - K x|| <=
+ * max(rtol ||b||, atol) or after maxit iterations; all scalars stay on the device and
+ * iterations run as CUDA-graph replays of 8 (the context needs a non-default stream).
+ * Repeated solves give bitwise equal results. */
+typedef struct {
+    int iterations;        /* iterations run (0 when b = 0) */
+    int converged;         /* 1 when the tolerance was met */
+    double residual_norm;  /* ||b - K x|| of the recurrence at exit */
+    double rhs_norm;       /* ||b|| */
+} igab_solve_info;
+int igab_spmv_device(igab_ctx *ctx, const void *vals_dev, int prec, const double *x_dev, double *y_dev);
+int igab_solve_device(igab_ctx *ctx, const void *vals_dev, int prec, const double *b_dev, double *x_dev,
+                      double rtol, double atol, int maxit, igab_solve_info *info);
+
 /* ---- residual for callers that cannot have the library allocate device memory.
  * No counterpart in the reference.  Same result as igab_residual, but U and R
  * are staged in a file-scope device array (2 x 8 MiB, held by every GPU that

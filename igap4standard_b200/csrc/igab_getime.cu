@@ -30,9 +30,10 @@
 
 namespace {
 
+#include "igab_warp_tiles8.inc"
+
 #define GQ 2          /* Gauss points per batch */
 #define GNV 24        /* rows per Gauss point: 12 variables x (G0, G1) */
-#define GOWN 13       /* owned upper-triangle entries per thread */
 
 /* point data */
 #define GP_F0 0
@@ -48,7 +49,10 @@ namespace {
 #define GP_MASS 122
 #define GP_N 123
 
-template <typename T, int TE>
+#define GXS 100        /* X / Y row stride (doubles): = 4 mod 16, columns 81..99 stay zero */
+#define GROWS (GQ * GNV)
+
+template <int TE>
 struct gt_smem {
     static constexpr int TC = TE + 2;
     static constexpr int NCP = TC * TC * TC;
@@ -59,39 +63,143 @@ struct gt_smem {
     double A[972];
     double C[864];
     double pt[IGAB_NQ3][GP_N];
-    T N[GQ][27][10];          /* N_a^{alpha}, alpha = value, 9 derivatives */
-    T Gv[GQ][GNV][27];
-    T X[GQ][GNV][81];
-    T Y[GQ][GNV][81];
-    T GN[GQ][10][27];         /* effective geo x N (+ mass x N on the value row) */
+    double N[GQ][27][10];          /* N_a^{alpha}, alpha = value, 9 derivatives (geometric block) */
+    double GN[GQ][10][27];         /* effective geo x N (+ mass x N on the value row) */
+    double X[GROWS][GXS];          /* X rows (row 24 qb + 2 v + order, column 3 a + k) */
+    double Y[GROWS][GXS];          /* Y = w M X */
+    double gam[27 * 27];
+    long rbase[81];
+    int rsx[81], rsy[81];
 };
 
-/* dv/du_{k,m}: one source term per (v, m) from (F, G) of one Taylor order;
- * with_identity adds the unit diagonal of F (order 0 only) -- F passed already includes it */
-template <typename T>
-__device__ __forceinline__ void grad_row(const double *F, const double *G, int v, T g[9])
+__device__ __forceinline__ void gt_dmma(double &c0, double &c1, double a, double b)
 {
-    const double is2 = IGAB_INV_SQRT2, is3 = IGAB_INV_SQRT3, is6 = IGAB_INV_SQRT6;
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+/* one batch of K += X^T Y on the warp's upper 8x8 tiles (A fragments from X, B from Y) */
+template <int W>
+__device__ __forceinline__ void gt_warp_mma(const double (*X)[GXS], const double (*Y)[GXS], int lane,
+                                            double (&acc)[9][2])
+{
+    using WT = warp_tiles8<W>;
+    const int r4 = lane & 3, c8 = lane >> 2;
+#pragma unroll 2
+    for (int kb = 0; kb < GROWS / 4; kb++) {
+        const int kr = 4 * kb + r4;
+        double f[WT::NB], g[WT::NB];
 #pragma unroll
-    for (int m = 0; m < 9; m++) g[m] = T(0);
-    switch (v) {
-    case 0: g[0] = T(F[0] * is3); g[1] = T(F[1] * is3); g[2] = T(F[2] * is3); break;
-    case 1: g[0] = T(F[0] * is2); g[1] = T(-F[1] * is2); break;
-    case 2: g[0] = T(F[0] * is6); g[1] = T(F[1] * is6); g[2] = T(-2.0 * F[2] * is6); break;
-    case 3: g[0] = T(0.5 * F[1]); g[1] = T(0.5 * F[0]); break;
-    case 4: g[0] = T(0.5 * F[2]); g[2] = T(0.5 * F[0]); break;
-    case 5: g[1] = T(0.5 * F[2]); g[2] = T(0.5 * F[1]); break;
-    default:
-        if (v < 9) {
-            const int K = v - 6, q0 = igab_idx6(0, K), q1 = igab_idx6(1, K);
-            g[0] = T(G[q0] * is2); g[1] = T(-G[q1] * is2);
-            g[3 + q0] = T(F[0] * is2); g[3 + q1] = T(-F[1] * is2);
-        } else {
-            const int K = v - 9, q0 = igab_idx6(0, K), q1 = igab_idx6(1, K), q2 = igab_idx6(2, K);
-            g[0] = T(G[q0] * is6); g[1] = T(G[q1] * is6); g[2] = T(-2.0 * G[q2] * is6);
-            g[3 + q0] = T(F[0] * is6); g[3 + q1] = T(F[1] * is6); g[3 + q2] = T(-2.0 * F[2] * is6);
+        for (int b = 0; b < WT::NB; b++) {
+            f[b] = X[kr][8 * WT::blk(b) + c8];
+            g[b] = Y[kr][8 * WT::blk(b) + c8];
+        }
+#pragma unroll
+        for (int t = 0; t < WT::NT; t++) gt_dmma(acc[t][0], acc[t][1], f[WT::ti(t)], g[WT::tj(t)]);
+    }
+}
+
+/* the warp's tiles plus Gamma on the diagonal component blocks, added into the CSR
+ * values; entry (c1, c2) and its mirror (c2, c1) receive the upper value */
+template <int W, typename T>
+__device__ __forceinline__ void gt_warp_scatter(T *__restrict__ vals, const long *rbase, const int *rsx,
+                                                const int *rsy, const double *gam, int lane,
+                                                const double (&acc)[9][2])
+{
+    using WT = warp_tiles8<W>;
+    const int r = lane >> 2, c = 2 * (lane & 3);
+#pragma unroll
+    for (int t = 0; t < WT::NT; t++) {
+        const int bi = WT::blk(WT::ti(t)), bj = WT::blk(WT::tj(t));
+        double v2[2] = {acc[t][0], acc[t][1]};
+        if (bi == bj) {
+            /* diagonal tile: entry (r, c + e) below the diagonal takes (c + e, r),
+             * held by lane 4 (c + e) + r / 2, element r & 1 */
+            const double x0 = __shfl_sync(0xffffffffu, acc[t][0], 4 * c + (r >> 1));
+            const double y0 = __shfl_sync(0xffffffffu, acc[t][1], 4 * c + (r >> 1));
+            const double x1 = __shfl_sync(0xffffffffu, acc[t][0], 4 * (c + 1) + (r >> 1));
+            const double y1 = __shfl_sync(0xffffffffu, acc[t][1], 4 * (c + 1) + (r >> 1));
+            if (r > c) v2[0] = (r & 1) ? y0 : x0;
+            if (r > c + 1) v2[1] = (r & 1) ? y1 : x1;
+        }
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int c1 = 8 * bi + r, c2 = 8 * bj + c + e;
+            if (c1 < 81 && c2 < 81) {
+                const int a1 = c1 / 3, a2 = c2 / 3;
+                double v = v2[e];
+                if (c1 % 3 == c2 % 3) v += gam[a1 * 27 + a2];
+                atomicAdd(vals + rbase[c1] + (c2 / 27) * rsx[c1] + ((c2 / 9) % 3) * rsy[c1] + c2 % 9, T(v));
+                if (bi != bj)
+                    atomicAdd(vals + rbase[c2] + (c1 / 27) * rsx[c2] + ((c1 / 9) % 3) * rsy[c2] + c1 % 9, T(v));
+            }
         }
     }
+}
+
+#define GT_WARP_SWITCH(CALL)  \
+    switch (warp) {           \
+    case 0: CALL(0); break;   \
+    case 1: CALL(1); break;   \
+    case 2: CALL(2); break;   \
+    case 3: CALL(3); break;   \
+    case 4: CALL(4); break;   \
+    case 5: CALL(5); break;   \
+    case 6: CALL(6); break;   \
+    default: CALL(7); break;  \
+    }
+
+/* X and Y rows of one (point, basis function, component): the 12 variables' gradients
+ * (phys/ge variables, unrotated) for both Taylor orders a = 0, 1 (F_a, G_a of the
+ * point), contracted with the 9 derivatives of the basis function, then
+ * Y_{(v,a)} = w sum_c M[(v,a),(v',c)] X_{(v',c)} (2 x 2 per variable, 4 x 4 for (va, vb)) */
+__device__ __forceinline__ void gt_xy_task(const double *p, const double *bxp, const double *byp,
+                                           const double *bzp, int k, double *xc, double *yc)
+{
+    const double is2 = IGAB_INV_SQRT2, is3 = IGAB_INV_SQRT3, is6 = IGAB_INV_SQRT6;
+    const double bx0 = bxp[0], bx1 = bxp[1], bx2 = bxp[2];
+    const double by0 = byp[0], by1 = byp[1], by2 = byp[2];
+    const double bz0 = bzp[0], bz1 = bzp[1], bz2 = bzp[2];
+    const double b00 = bx0 * by0, b10 = bx1 * by0, b01 = bx0 * by1;
+    const double dx = b10 * bz0, dy = b01 * bz0, dz = b00 * bz1;
+    const double hxx = bx2 * by0 * bz0, hxy = bx1 * by1 * bz0, hxz = b10 * bz1;
+    const double hyy = bx0 * by2 * bz0, hyz = b01 * bz1, hzz = b00 * bz2;
+    double x[24];
+#pragma unroll
+    for (int a = 0; a < 2; a++) {
+        const double *F = p + (a ? GP_F1 : GP_F0) + 3 * k;
+        const double *G = p + (a ? GP_G1 : GP_G0) + 6 * k;
+        const double F0 = F[0], F1 = F[1], F2 = F[2];
+        const double G0 = G[0], G1 = G[1], G2 = G[2], G3 = G[3], G4 = G[4], G5 = G[5];
+        const double e0 = F0 * dx, e1 = F1 * dy, e2 = F2 * dz;
+        x[0 + a] = (e0 + e1 + e2) * is3;
+        x[2 + a] = (e0 - e1) * is2;
+        x[4 + a] = (e0 + e1 - 2.0 * e2) * is6;
+        x[6 + a] = 0.5 * (F1 * dx + F0 * dy);
+        x[8 + a] = 0.5 * (F2 * dx + F0 * dz);
+        x[10 + a] = 0.5 * (F2 * dy + F1 * dz);
+        x[12 + a] = (G0 * dx - G1 * dy + F0 * hxx - F1 * hxy) * is2;
+        x[14 + a] = (G1 * dx - G3 * dy + F0 * hxy - F1 * hyy) * is2;
+        x[16 + a] = (G2 * dx - G4 * dy + F0 * hxz - F1 * hyz) * is2;
+        x[18 + a] = (G0 * dx + G1 * dy - 2.0 * G2 * dz + F0 * hxx + F1 * hxy - 2.0 * F2 * hxz) * is6;
+        x[20 + a] = (G1 * dx + G3 * dy - 2.0 * G4 * dz + F0 * hxy + F1 * hyy - 2.0 * F2 * hyz) * is6;
+        x[22 + a] = (G2 * dx + G4 * dy - 2.0 * G5 * dz + F0 * hxz + F1 * hyz - 2.0 * F2 * hzz) * is6;
+    }
+    const double w = p[GP_W];
+#pragma unroll
+    for (int r = 0; r < 24; r++) xc[r * GXS] = x[r];
+#pragma unroll
+    for (int v = 0; v < 12; v++) {
+        if (v == 1 || v == 2) continue;
+        const double m00 = p[GP_MD + 3 * v], m01 = p[GP_MD + 3 * v + 1], m11 = p[GP_MD + 3 * v + 2];
+        yc[(2 * v) * GXS] = w * (m00 * x[2 * v] + m01 * x[2 * v + 1]);
+        yc[(2 * v + 1) * GXS] = w * (m01 * x[2 * v] + m11 * x[2 * v + 1]);
+    }
+    const double *M = p + GP_M12;
+#pragma unroll
+    for (int rr = 0; rr < 4; rr++)
+        yc[(2 + rr) * GXS] = w * (M[4 * rr] * x[2] + M[4 * rr + 1] * x[3] + M[4 * rr + 2] * x[4] + M[4 * rr + 3] * x[5]);
 }
 
 template <typename T, int TE>
@@ -99,22 +207,14 @@ __global__ void __launch_bounds__(256) k_tan_getime(igab_geom g, const double *_
                                                     T *__restrict__ vals, int colour)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    gt_smem<T, TE> &S = *reinterpret_cast<gt_smem<T, TE> *>(smem_raw);
+    gt_smem<TE> &S = *reinterpret_cast<gt_smem<TE> *>(smem_raw);
     constexpr int TC = TE + 2;
     constexpr int NCP = TC * TC * TC;
     constexpr int NEL = TE * TE * TE;
     tile_t Tl;
     if (!decode_tile(g, TE, colour, blockIdx.x, Tl)) return;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    int own[GOWN];
-#pragma unroll
-    for (int j = 0; j < GOWN; j++) {
-        int idx = tid + 256 * j;
-        int c1 = 0, rem = idx;
-        while (c1 < 81 && rem >= 81 - c1) { rem -= 81 - c1; c1++; }
-        own[j] = c1 < 81 ? (c1 << 8) | (c1 + rem) : -1;
-    }
     int gown[2];
 #pragma unroll
     for (int j = 0; j < 2; j++) {
@@ -142,6 +242,12 @@ __global__ void __launch_bounds__(256) k_tan_getime(igab_geom g, const double *_
         bool ok = le < Tl.nv[d];
         S.wh[d][le][q] = ok ? g.wh[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
         S.xq[d][le][q] = ok ? g.xq[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
+    }
+    /* the padding columns (81..99) of X and Y stay zero */
+    for (int idx = tid; idx < GROWS * (GXS - 81); idx += 256) {
+        const int r = idx / (GXS - 81), cc = 81 + idx % (GXS - 81);
+        S.X[r][cc] = 0.0;
+        S.Y[r][cc] = 0.0;
     }
     __syncthreads();
 
@@ -245,131 +351,84 @@ __global__ void __launch_bounds__(256) k_tan_getime(igab_geom g, const double *_
         }
         __syncthreads();
 
-        T acc[GOWN];
+        double acc[9][2];
 #pragma unroll
-        for (int j = 0; j < GOWN; j++) acc[j] = T(0);
-        T gacc[2] = {T(0), T(0)};
+        for (int t = 0; t < 9; t++) acc[t][0] = acc[t][1] = 0.0;
+        double gacc[2] = {0.0, 0.0};
 
         for (int q0 = 0; q0 < IGAB_NQ3; q0 += GQ) {
-            /* (a) basis values and gradient rows */
+            /* (a) basis values for the geometric block; X and Y rows per (point, function, component) */
             for (int o = tid; o < GQ * 270; o += 256) {
                 int al = o % 10, a = (o / 10) % 27, qb = o / 270;
                 int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
-                S.N[qb][a][al] = T(Bx[qx * 9 + (a / 9) * 3 + a_kx(al)] * By[qy * 9 + ((a / 3) % 3) * 3 + a_ky(al)] *
-                                   Bz[qz * 9 + (a % 3) * 3 + a_kz(al)]);
+                S.N[qb][a][al] = Bx[qx * 9 + (a / 9) * 3 + a_kx(al)] * By[qy * 9 + ((a / 3) % 3) * 3 + a_ky(al)] *
+                                 Bz[qz * 9 + (a % 3) * 3 + a_kz(al)];
             }
-            for (int o = tid; o < GQ * GNV * 3; o += 256) {
-                const int k = o % 3, r = (o / 3) % GNV, qb = o / (3 * GNV);
-                const double *pt = S.pt[q0 + qb];
-                const int v = r >> 1, a = r & 1;
-                T gg[9];
-                grad_row<T>(pt + (a ? GP_F1 : GP_F0) + 3 * k, pt + (a ? GP_G1 : GP_G0) + 6 * k, v, gg);
-#pragma unroll
-                for (int m = 0; m < 9; m++) S.Gv[qb][r][9 * k + m] = gg[m];
+            for (int t = tid; t < GQ * 81; t += 256) {
+                const int qb = t / 81, c = t % 81, a = c / 3, k = c % 3;
+                const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
+                gt_xy_task(S.pt[q], Bx + qx * 9 + (a / 9) * 3, By + qy * 9 + ((a / 3) % 3) * 3,
+                           Bz + qz * 9 + (a % 3) * 3, k, &S.X[qb * GNV][c], &S.Y[qb * GNV][c]);
             }
             __syncthreads();
-            /* (b) X = G N and the effective geometric block x N */
-            for (int o = tid; o < GQ * GNV * 81; o += 256) {
-                const int c = o % 81, r = (o / 81) % GNV, qb = o / (81 * GNV);
-                const int a = c / 3, k = c % 3;
-                T s = T(0);
-#pragma unroll
-                for (int m = 0; m < 9; m++) s += S.Gv[qb][r][9 * k + m] * S.N[qb][a][m + 1];
-                S.X[qb][r][c] = s;
-            }
+            /* (b) the effective geometric block x N */
             for (int o = tid; o < GQ * 10 * 27; o += 256) {
                 const int b = o % 27, m = (o / 27) % 10, qb = o / 270;
                 const double *pt = S.pt[q0 + qb];
-                const T *Nb = &S.N[qb][b][1];
-                T s = T(0);
+                const double *Nb = &S.N[qb][b][1];
+                double s = 0.0;
                 if (m == 9) {
-                    s = T(pt[GP_MASS]) * S.N[qb][b][0];
+                    s = pt[GP_MASS] * S.N[qb][b][0];
                 } else if (m < 3) {
                     const double *sig = pt + GP_SIG, *d1s = pt + GP_D1S, *tau = pt + GP_TAU;
                     const int o1 = (m + 1) % 3, o2 = (m + 2) % 3;
                     const int p1 = (m == 0 || o1 == 0) ? ((m + o1 == 1) ? 0 : 1) : 2;
                     const int p2 = (m == 0 || o2 == 0) ? ((m + o2 == 1) ? 0 : 1) : 2;
-                    s = T(sig[m]) * Nb[m] + T(0.5 * d1s[p1]) * Nb[o1] + T(0.5 * d1s[p2]) * Nb[o2];
-                    for (int K = 0; K < 3; K++) s += T(tau[3 * m + K]) * Nb[3 + igab_idx6(m, K)];
+                    s = sig[m] * Nb[m] + (0.5 * d1s[p1]) * Nb[o1] + (0.5 * d1s[p2]) * Nb[o2];
+                    for (int K = 0; K < 3; K++) s += tau[3 * m + K] * Nb[3 + igab_idx6(m, K)];
                 } else {
                     const double *tau = pt + GP_TAU;
                     const int c = m - 3;
                     for (int I = 0; I < 3; I++)
                         for (int K = 0; K < 3; K++)
-                            if (igab_idx6(I, K) == c) s += T(tau[3 * I + K]) * Nb[I];
+                            if (igab_idx6(I, K) == c) s += tau[3 * I + K] * Nb[I];
                 }
                 S.GN[qb][m][b] = s;
             }
             __syncthreads();
-            /* (c) Y = w M X */
-            for (int o = tid; o < GQ * GNV * 81; o += 256) {
-                const int c = o % 81, r = (o / 81) % GNV, qb = o / (81 * GNV);
-                const double *pt = S.pt[q0 + qb];
-                const int v = r >> 1, a = r & 1;
-                T s;
-                if (v == 1 || v == 2) {
-                    const int rr = 2 * (v - 1) + a;
-                    s = T(pt[GP_M12 + 4 * rr + 0]) * S.X[qb][2][c] + T(pt[GP_M12 + 4 * rr + 1]) * S.X[qb][3][c] +
-                        T(pt[GP_M12 + 4 * rr + 2]) * S.X[qb][4][c] + T(pt[GP_M12 + 4 * rr + 3]) * S.X[qb][5][c];
-                } else {
-                    const double m0 = a == 0 ? pt[GP_MD + 3 * v] : pt[GP_MD + 3 * v + 1];
-                    const double m1 = a == 0 ? pt[GP_MD + 3 * v + 1] : pt[GP_MD + 3 * v + 2];
-                    s = T(m0) * S.X[qb][2 * v][c] + T(m1) * S.X[qb][2 * v + 1][c];
-                }
-                S.Y[qb][r][c] = T(pt[GP_W]) * s;
-            }
-            __syncthreads();
-            /* (d) owned entries */
-#pragma unroll
-            for (int j = 0; j < GOWN; j++) {
-                if (own[j] < 0) continue;
-                int c1 = own[j] >> 8, c2 = own[j] & 255;
-                T s = acc[j];
-                for (int qb = 0; qb < GQ; qb++)
-#pragma unroll 8
-                    for (int r = 0; r < GNV; r++) s += S.X[qb][r][c1] * S.Y[qb][r][c2];
-                acc[j] = s;
-            }
+            /* (c) K += X^T Y on the DMMA tiles; Gamma entries on the FMA pipe */
+#define GT_MMA(Wn) gt_warp_mma<Wn>(S.X, S.Y, lane, acc)
+            GT_WARP_SWITCH(GT_MMA)
+#undef GT_MMA
 #pragma unroll
             for (int j = 0; j < 2; j++) {
                 if (gown[j] < 0) continue;
                 int a1 = gown[j] >> 8, a2 = gown[j] & 255;
-                T s = gacc[j];
+                double s = gacc[j];
                 for (int qb = 0; qb < GQ; qb++) {
-                    T t = S.N[qb][a1][0] * S.GN[qb][9][a2];
+                    double t = S.N[qb][a1][0] * S.GN[qb][9][a2];
 #pragma unroll
                     for (int m = 0; m < 9; m++) t += S.N[qb][a1][m + 1] * S.GN[qb][m][a2];
-                    s += T(S.pt[q0 + qb][GP_W]) * t;
+                    s += S.pt[q0 + qb][GP_W] * t;
                 }
                 gacc[j] = s;
             }
             __syncthreads();
         }
-        T *Gam = &S.X[0][0][0];
 #pragma unroll
         for (int j = 0; j < 2; j++) {
             if (gown[j] < 0) continue;
             int a1 = gown[j] >> 8, a2 = gown[j] & 255;
-            Gam[a1 * 27 + a2] = gacc[j];
-            Gam[a2 * 27 + a1] = gacc[j];
+            S.gam[a1 * 27 + a2] = gacc[j];
+            S.gam[a2 * 27 + a1] = gacc[j];
         }
+        if (tid < 81)
+            elem_row_base(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez, tid, S.rbase[tid], S.rsx[tid],
+                          S.rsy[tid]);
         __syncthreads();
-#pragma unroll
-        for (int j = 0; j < GOWN; j++) {
-            if (own[j] < 0) continue;
-            int c1 = own[j] >> 8, c2 = own[j] & 255;
-            int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
-            T val = acc[j];
-            if (k1 == k2) val += Gam[a1 * 27 + a2];
-            int x1 = Tl.e0[0] + lex + a1 / 9, y1 = Tl.e0[1] + ley + (a1 / 3) % 3, z1 = Tl.e0[2] + lez + a1 % 3;
-            int x2 = Tl.e0[0] + lex + a2 / 9, y2 = Tl.e0[1] + ley + (a2 / 3) % 3, z2 = Tl.e0[2] + lez + a2 % 3;
-            long r1 = 3 * cp_index(g, x1, y1, z1) + k1;
-            vals[g.rowptr[r1] + csr_pos(g, x1, y1, z1, x2, y2, z2, k2)] += val;
-            if (c1 != c2) {
-                long r2 = 3 * cp_index(g, x2, y2, z2) + k2;
-                vals[g.rowptr[r2] + csr_pos(g, x2, y2, z2, x1, y1, z1, k1)] += val;
-            }
-        }
+#define GT_SCATTER(Wn) gt_warp_scatter<Wn, T>(vals, S.rbase, S.rsx, S.rsy, S.gam, lane, acc)
+        GT_WARP_SWITCH(GT_SCATTER)
+#undef GT_SCATTER
         __syncthreads();
     }
 }
@@ -387,7 +446,7 @@ int launch_t(igab_ctx *c, const double *dU, T *dv, int level)
         for (int j = 0; j < 4; j++) g.tw[j] = w[j];
         g.tmass = g.rho / (g.dt * g.dt) - g.cii / (2.0 * g.dt);
     }
-    size_t sm = sizeof(gt_smem<T, 2>);
+    size_t sm = sizeof(gt_smem<2>);
     IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_getime<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     for (int colour = 0; colour < 8; colour++) {
         long nblk = tiles_of_colour(g, 2, colour);

@@ -51,6 +51,8 @@ namespace {
 
 #define GXS 100        /* X / Y row stride (doubles): = 4 mod 16, columns 81..99 stay zero */
 #define GROWS (GQ * GNV)
+#define GGR 16         /* geometric rows per batch: 7 per point (6 + mass), padded */
+#define GGS 36         /* U / V row stride: = 4 mod 16, columns 27..35 stay zero */
 
 template <int TE>
 struct gt_smem {
@@ -63,11 +65,11 @@ struct gt_smem {
     double A[972];
     double C[864];
     double pt[IGAB_NQ3][GP_N];
-    double N[GQ][27][10];          /* N_a^{alpha}, alpha = value, 9 derivatives (geometric block) */
-    double GN[GQ][10][27];         /* effective geo x N (+ mass x N on the value row) */
     double X[GROWS][GXS];          /* X rows (row 24 qb + 2 v + order, column 3 a + k) */
     double Y[GROWS][GXS];          /* Y = w M X */
-    double gam[27 * 27];
+    double UT[GGR][GGS];           /* U rows of the geometric block (row 7 qb + i, column a) */
+    double VT[GGR][GGS];           /* V rows */
+    double gam[32 * 32];           /* upper tiles of Gamma */
     long rbase[81];
     int rsx[81], rsy[81];
 };
@@ -79,10 +81,12 @@ __device__ __forceinline__ void gt_dmma(double &c0, double &c1, double a, double
                  : "d"(a), "d"(b));
 }
 
-/* one batch of K += X^T Y on the warp's upper 8x8 tiles (A fragments from X, B from Y) */
+/* one batch of K += X^T Y on the warp's upper 8x8 tiles (A fragments from X, B from Y)
+ * and Gamma += U^T V on its Gamma tiles */
 template <int W>
-__device__ __forceinline__ void gt_warp_mma(const double (*X)[GXS], const double (*Y)[GXS], int lane,
-                                            double (&acc)[9][2])
+__device__ __forceinline__ void gt_warp_mma(const double (*X)[GXS], const double (*Y)[GXS],
+                                            const double (*UT)[GGS], const double (*VT)[GGS], int lane,
+                                            double (&acc)[9][2], double (&gacc)[10][2])
 {
     using WT = warp_tiles8<W>;
     const int r4 = lane & 3, c8 = lane >> 2;
@@ -97,6 +101,33 @@ __device__ __forceinline__ void gt_warp_mma(const double (*X)[GXS], const double
         }
 #pragma unroll
         for (int t = 0; t < WT::NT; t++) gt_dmma(acc[t][0], acc[t][1], f[WT::ti(t)], g[WT::tj(t)]);
+    }
+    if constexpr (WT::NGT > 0) {
+#pragma unroll
+        for (int kb = 0; kb < GGR / 4; kb++) {
+            const int kr = 4 * kb + r4;
+            double fa[WT::NGA], fb[WT::NGB];
+#pragma unroll
+            for (int b = 0; b < WT::NGA; b++) fa[b] = UT[kr][8 * WT::gablk(b) + c8];
+#pragma unroll
+            for (int b = 0; b < WT::NGB; b++) fb[b] = VT[kr][8 * WT::gbblk(b) + c8];
+#pragma unroll
+            for (int t = 0; t < WT::NGT; t++) gt_dmma(gacc[t][0], gacc[t][1], fa[WT::gti(t)], fb[WT::gtj(t)]);
+        }
+    }
+}
+
+/* the warp's Gamma tiles into gam (upper tiles, stride 32) */
+template <int W>
+__device__ __forceinline__ void gt_warp_gamma(double *gam, int lane, const double (&gacc)[10][2])
+{
+    using WT = warp_tiles8<W>;
+    const int r = lane >> 2, c = 2 * (lane & 3);
+#pragma unroll
+    for (int t = 0; t < WT::NGT; t++) {
+        const int a1 = 8 * WT::gablk(WT::gti(t)) + r, a2 = 8 * WT::gbblk(WT::gtj(t)) + c;
+        gam[a1 * 32 + a2] = gacc[t][0];
+        gam[a1 * 32 + a2 + 1] = gacc[t][1];
     }
 }
 
@@ -129,7 +160,7 @@ __device__ __forceinline__ void gt_warp_scatter(T *__restrict__ vals, const long
             if (c1 < 81 && c2 < 81) {
                 const int a1 = c1 / 3, a2 = c2 / 3;
                 double v = v2[e];
-                if (c1 % 3 == c2 % 3) v += gam[a1 * 27 + a2];
+                if (c1 % 3 == c2 % 3) v += a1 <= a2 ? gam[a1 * 32 + a2] : gam[a2 * 32 + a1];
                 atomicAdd(vals + rbase[c1] + (c2 / 27) * rsx[c1] + ((c2 / 9) % 3) * rsy[c1] + c2 % 9, T(v));
                 if (bi != bj)
                     atomicAdd(vals + rbase[c2] + (c1 / 27) * rsx[c2] + ((c1 / 9) % 3) * rsy[c2] + c1 % 9, T(v));
@@ -154,6 +185,7 @@ __device__ __forceinline__ void gt_warp_scatter(T *__restrict__ vals, const long
  * (phys/ge variables, unrotated) for both Taylor orders a = 0, 1 (F_a, G_a of the
  * point), contracted with the 9 derivatives of the basis function, then
  * Y_{(v,a)} = w sum_c M[(v,a),(v',c)] X_{(v',c)} (2 x 2 per variable, 4 x 4 for (va, vb)) */
+template <int HALF>
 __device__ __forceinline__ void gt_xy_task(const double *p, const double *bxp, const double *byp,
                                            const double *bzp, int k, double *xc, double *yc)
 {
@@ -165,41 +197,88 @@ __device__ __forceinline__ void gt_xy_task(const double *p, const double *bxp, c
     const double dx = b10 * bz0, dy = b01 * bz0, dz = b00 * bz1;
     const double hxx = bx2 * by0 * bz0, hxy = bx1 * by1 * bz0, hxz = b10 * bz1;
     const double hyy = bx0 * by2 * bz0, hyz = b01 * bz1, hzz = b00 * bz2;
-    double x[24];
+    /* x[2 (v - 6 HALF) + a]: the variables of this half (0..5, or 6..11) */
+    double x[12];
 #pragma unroll
     for (int a = 0; a < 2; a++) {
         const double *F = p + (a ? GP_F1 : GP_F0) + 3 * k;
-        const double *G = p + (a ? GP_G1 : GP_G0) + 6 * k;
         const double F0 = F[0], F1 = F[1], F2 = F[2];
-        const double G0 = G[0], G1 = G[1], G2 = G[2], G3 = G[3], G4 = G[4], G5 = G[5];
-        const double e0 = F0 * dx, e1 = F1 * dy, e2 = F2 * dz;
-        x[0 + a] = (e0 + e1 + e2) * is3;
-        x[2 + a] = (e0 - e1) * is2;
-        x[4 + a] = (e0 + e1 - 2.0 * e2) * is6;
-        x[6 + a] = 0.5 * (F1 * dx + F0 * dy);
-        x[8 + a] = 0.5 * (F2 * dx + F0 * dz);
-        x[10 + a] = 0.5 * (F2 * dy + F1 * dz);
-        x[12 + a] = (G0 * dx - G1 * dy + F0 * hxx - F1 * hxy) * is2;
-        x[14 + a] = (G1 * dx - G3 * dy + F0 * hxy - F1 * hyy) * is2;
-        x[16 + a] = (G2 * dx - G4 * dy + F0 * hxz - F1 * hyz) * is2;
-        x[18 + a] = (G0 * dx + G1 * dy - 2.0 * G2 * dz + F0 * hxx + F1 * hxy - 2.0 * F2 * hxz) * is6;
-        x[20 + a] = (G1 * dx + G3 * dy - 2.0 * G4 * dz + F0 * hxy + F1 * hyy - 2.0 * F2 * hyz) * is6;
-        x[22 + a] = (G2 * dx + G4 * dy - 2.0 * G5 * dz + F0 * hxz + F1 * hyz - 2.0 * F2 * hzz) * is6;
+        if (HALF == 0) {
+            const double e0 = F0 * dx, e1 = F1 * dy, e2 = F2 * dz;
+            x[0 + a] = (e0 + e1 + e2) * is3;
+            x[2 + a] = (e0 - e1) * is2;
+            x[4 + a] = (e0 + e1 - 2.0 * e2) * is6;
+            x[6 + a] = 0.5 * (F1 * dx + F0 * dy);
+            x[8 + a] = 0.5 * (F2 * dx + F0 * dz);
+            x[10 + a] = 0.5 * (F2 * dy + F1 * dz);
+        } else {
+            const double *G = p + (a ? GP_G1 : GP_G0) + 6 * k;
+            const double G0 = G[0], G1 = G[1], G2 = G[2], G3 = G[3], G4 = G[4], G5 = G[5];
+            x[0 + a] = (G0 * dx - G1 * dy + F0 * hxx - F1 * hxy) * is2;
+            x[2 + a] = (G1 * dx - G3 * dy + F0 * hxy - F1 * hyy) * is2;
+            x[4 + a] = (G2 * dx - G4 * dy + F0 * hxz - F1 * hyz) * is2;
+            x[6 + a] = (G0 * dx + G1 * dy - 2.0 * G2 * dz + F0 * hxx + F1 * hxy - 2.0 * F2 * hxz) * is6;
+            x[8 + a] = (G1 * dx + G3 * dy - 2.0 * G4 * dz + F0 * hxy + F1 * hyy - 2.0 * F2 * hyz) * is6;
+            x[10 + a] = (G2 * dx + G4 * dy - 2.0 * G5 * dz + F0 * hxz + F1 * hyz - 2.0 * F2 * hzz) * is6;
+        }
     }
     const double w = p[GP_W];
+    const int r0 = 12 * HALF;   /* first row of this half */
 #pragma unroll
-    for (int r = 0; r < 24; r++) xc[r * GXS] = x[r];
+    for (int r = 0; r < 12; r++) xc[(r0 + r) * GXS] = x[r];
 #pragma unroll
-    for (int v = 0; v < 12; v++) {
+    for (int j = 0; j < 6; j++) {
+        const int v = 6 * HALF + j;
         if (v == 1 || v == 2) continue;
         const double m00 = p[GP_MD + 3 * v], m01 = p[GP_MD + 3 * v + 1], m11 = p[GP_MD + 3 * v + 2];
-        yc[(2 * v) * GXS] = w * (m00 * x[2 * v] + m01 * x[2 * v + 1]);
-        yc[(2 * v + 1) * GXS] = w * (m01 * x[2 * v] + m11 * x[2 * v + 1]);
+        yc[(r0 + 2 * j) * GXS] = w * (m00 * x[2 * j] + m01 * x[2 * j + 1]);
+        yc[(r0 + 2 * j + 1) * GXS] = w * (m01 * x[2 * j] + m11 * x[2 * j + 1]);
     }
-    const double *M = p + GP_M12;
+    if (HALF == 0) {
+        const double *M = p + GP_M12;
 #pragma unroll
-    for (int rr = 0; rr < 4; rr++)
-        yc[(2 + rr) * GXS] = w * (M[4 * rr] * x[2] + M[4 * rr + 1] * x[3] + M[4 * rr + 2] * x[4] + M[4 * rr + 3] * x[5]);
+        for (int rr = 0; rr < 4; rr++)
+            yc[(2 + rr) * GXS] =
+                w * (M[4 * rr] * x[2] + M[4 * rr + 1] * x[3] + M[4 * rr + 2] * x[4] + M[4 * rr + 3] * x[5]);
+    }
+}
+
+/* U / V rows of the geometric block for (point, basis function): U_i = d_i N_a,
+ * V_i = w ((S grad N_a)_i + (T H_a)_i), U_{3+I} = w (T H_a)_I, V_{3+I} = d_I N_a
+ * (effective S = sig / d1s, T = tau of the point) and the inertia / damping row
+ * U_6 = N_a, V_6 = w mass N_a */
+__device__ __forceinline__ void gt_uv_task(const double *p, const double *bxp, const double *byp,
+                                           const double *bzp, double *ur, double *vr)
+{
+    const double bx0 = bxp[0], bx1 = bxp[1], bx2 = bxp[2];
+    const double by0 = byp[0], by1 = byp[1], by2 = byp[2];
+    const double bz0 = bzp[0], bz1 = bzp[1], bz2 = bzp[2];
+    const double b00 = bx0 * by0, b10 = bx1 * by0, b01 = bx0 * by1;
+    const double dx = b10 * bz0, dy = b01 * bz0, dz = b00 * bz1;
+    const double hxx = bx2 * by0 * bz0, hxy = bx1 * by1 * bz0, hxz = b10 * bz1;
+    const double hyy = bx0 * by2 * bz0, hyz = b01 * bz1, hzz = b00 * bz2;
+    const double w = p[GP_W];
+    const double s00 = p[GP_SIG], s11 = p[GP_SIG + 1], s22 = p[GP_SIG + 2];
+    const double s01 = 0.5 * p[GP_D1S], s02 = 0.5 * p[GP_D1S + 1], s12 = 0.5 * p[GP_D1S + 2];
+    const double *T = p + GP_TAU;
+    const double th0 = T[0] * hxx + T[1] * hxy + T[2] * hxz;
+    const double th1 = T[3] * hxy + T[4] * hyy + T[5] * hyz;
+    const double th2 = T[6] * hxz + T[7] * hyz + T[8] * hzz;
+    ur[0 * GGS] = dx;
+    ur[1 * GGS] = dy;
+    ur[2 * GGS] = dz;
+    vr[0 * GGS] = w * (s00 * dx + s01 * dy + s02 * dz + th0);
+    vr[1 * GGS] = w * (s01 * dx + s11 * dy + s12 * dz + th1);
+    vr[2 * GGS] = w * (s02 * dx + s12 * dy + s22 * dz + th2);
+    ur[3 * GGS] = w * th0;
+    ur[4 * GGS] = w * th1;
+    ur[5 * GGS] = w * th2;
+    vr[3 * GGS] = dx;
+    vr[4 * GGS] = dy;
+    vr[5 * GGS] = dz;
+    const double n0 = b00 * bz0;
+    ur[6 * GGS] = n0;
+    vr[6 * GGS] = w * p[GP_MASS] * n0;
 }
 
 template <typename T, int TE>
@@ -214,15 +293,6 @@ __global__ void __launch_bounds__(256) k_tan_getime(igab_geom g, const double *_
     tile_t Tl;
     if (!decode_tile(g, TE, colour, blockIdx.x, Tl)) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-
-    int gown[2];
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-        int idx = tid + 256 * j;
-        int a1 = 0, rem = idx;
-        while (a1 < 27 && rem >= 27 - a1) { rem -= 27 - a1; a1++; }
-        gown[j] = a1 < 27 ? (a1 << 8) | (a1 + rem) : -1;
-    }
 
     for (int idx = tid; idx < NCP * 3; idx += 256) {
         int i = idx % 3, cp = idx / 3;
@@ -243,11 +313,15 @@ __global__ void __launch_bounds__(256) k_tan_getime(igab_geom g, const double *_
         S.wh[d][le][q] = ok ? g.wh[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
         S.xq[d][le][q] = ok ? g.xq[d][(long)(Tl.e0[d] + le) * IGAB_NQ + q] : 0.0;
     }
-    /* the padding columns (81..99) of X and Y stay zero */
+    /* the padding columns (81..99) of X and Y, and the padding rows and columns of U / V, stay zero */
     for (int idx = tid; idx < GROWS * (GXS - 81); idx += 256) {
         const int r = idx / (GXS - 81), cc = 81 + idx % (GXS - 81);
         S.X[r][cc] = 0.0;
         S.Y[r][cc] = 0.0;
+    }
+    for (int idx = tid; idx < GGR * GGS; idx += 256) {
+        (&S.UT[0][0])[idx] = 0.0;
+        (&S.VT[0][0])[idx] = 0.0;
     }
     __syncthreads();
 
@@ -351,77 +425,42 @@ __global__ void __launch_bounds__(256) k_tan_getime(igab_geom g, const double *_
         }
         __syncthreads();
 
-        double acc[9][2];
+        double acc[9][2], gacc[10][2];
 #pragma unroll
         for (int t = 0; t < 9; t++) acc[t][0] = acc[t][1] = 0.0;
-        double gacc[2] = {0.0, 0.0};
+#pragma unroll
+        for (int t = 0; t < 10; t++) gacc[t][0] = gacc[t][1] = 0.0;
 
         for (int q0 = 0; q0 < IGAB_NQ3; q0 += GQ) {
-            /* (a) basis values for the geometric block; X and Y rows per (point, function, component) */
-            for (int o = tid; o < GQ * 270; o += 256) {
-                int al = o % 10, a = (o / 10) % 27, qb = o / 270;
-                int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
-                S.N[qb][a][al] = Bx[qx * 9 + (a / 9) * 3 + a_kx(al)] * By[qy * 9 + ((a / 3) % 3) * 3 + a_ky(al)] *
-                                 Bz[qz * 9 + (a % 3) * 3 + a_kz(al)];
-            }
-            for (int t = tid; t < GQ * 81; t += 256) {
-                const int qb = t / 81, c = t % 81, a = c / 3, k = c % 3;
-                const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
-                gt_xy_task(S.pt[q], Bx + qx * 9 + (a / 9) * 3, By + qy * 9 + ((a / 3) % 3) * 3,
-                           Bz + qz * 9 + (a % 3) * 3, k, &S.X[qb * GNV][c], &S.Y[qb * GNV][c]);
-            }
-            __syncthreads();
-            /* (b) the effective geometric block x N */
-            for (int o = tid; o < GQ * 10 * 27; o += 256) {
-                const int b = o % 27, m = (o / 27) % 10, qb = o / 270;
-                const double *pt = S.pt[q0 + qb];
-                const double *Nb = &S.N[qb][b][1];
-                double s = 0.0;
-                if (m == 9) {
-                    s = pt[GP_MASS] * S.N[qb][b][0];
-                } else if (m < 3) {
-                    const double *sig = pt + GP_SIG, *d1s = pt + GP_D1S, *tau = pt + GP_TAU;
-                    const int o1 = (m + 1) % 3, o2 = (m + 2) % 3;
-                    const int p1 = (m == 0 || o1 == 0) ? ((m + o1 == 1) ? 0 : 1) : 2;
-                    const int p2 = (m == 0 || o2 == 0) ? ((m + o2 == 1) ? 0 : 1) : 2;
-                    s = sig[m] * Nb[m] + (0.5 * d1s[p1]) * Nb[o1] + (0.5 * d1s[p2]) * Nb[o2];
-                    for (int K = 0; K < 3; K++) s += tau[3 * m + K] * Nb[3 + igab_idx6(m, K)];
+            /* (a) X and Y rows: tasks (point, half of the variables, basis function, component);
+             * U / V rows: tasks (point, basis function) */
+            for (int t = tid; t < GQ * 162 + GQ * 27; t += 256) {
+                if (t < GQ * 162) {
+                    const int qb = t / 162, half = (t / 81) & 1, c = t % 81, a = c / 3, k = c % 3;
+                    const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
+                    const double *bxp = Bx + qx * 9 + (a / 9) * 3, *byp = By + qy * 9 + ((a / 3) % 3) * 3,
+                                 *bzp = Bz + qz * 9 + (a % 3) * 3;
+                    if (half == 0)
+                        gt_xy_task<0>(S.pt[q], bxp, byp, bzp, k, &S.X[qb * GNV][c], &S.Y[qb * GNV][c]);
+                    else
+                        gt_xy_task<1>(S.pt[q], bxp, byp, bzp, k, &S.X[qb * GNV][c], &S.Y[qb * GNV][c]);
                 } else {
-                    const double *tau = pt + GP_TAU;
-                    const int c = m - 3;
-                    for (int I = 0; I < 3; I++)
-                        for (int K = 0; K < 3; K++)
-                            if (igab_idx6(I, K) == c) s += tau[3 * I + K] * Nb[I];
+                    const int tg = t - GQ * 162, qb = tg / 27, a = tg % 27;
+                    const int q = q0 + qb, qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
+                    gt_uv_task(S.pt[q], Bx + qx * 9 + (a / 9) * 3, By + qy * 9 + ((a / 3) % 3) * 3,
+                               Bz + qz * 9 + (a % 3) * 3, &S.UT[7 * qb][a], &S.VT[7 * qb][a]);
                 }
-                S.GN[qb][m][b] = s;
             }
             __syncthreads();
-            /* (c) K += X^T Y on the DMMA tiles; Gamma entries on the FMA pipe */
-#define GT_MMA(Wn) gt_warp_mma<Wn>(S.X, S.Y, lane, acc)
+            /* (b) K += X^T Y and Gamma += U^T V on the DMMA tiles */
+#define GT_MMA(Wn) gt_warp_mma<Wn>(S.X, S.Y, S.UT, S.VT, lane, acc, gacc)
             GT_WARP_SWITCH(GT_MMA)
 #undef GT_MMA
-#pragma unroll
-            for (int j = 0; j < 2; j++) {
-                if (gown[j] < 0) continue;
-                int a1 = gown[j] >> 8, a2 = gown[j] & 255;
-                double s = gacc[j];
-                for (int qb = 0; qb < GQ; qb++) {
-                    double t = S.N[qb][a1][0] * S.GN[qb][9][a2];
-#pragma unroll
-                    for (int m = 0; m < 9; m++) t += S.N[qb][a1][m + 1] * S.GN[qb][m][a2];
-                    s += S.pt[q0 + qb][GP_W] * t;
-                }
-                gacc[j] = s;
-            }
             __syncthreads();
         }
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            if (gown[j] < 0) continue;
-            int a1 = gown[j] >> 8, a2 = gown[j] & 255;
-            S.gam[a1 * 27 + a2] = gacc[j];
-            S.gam[a2 * 27 + a1] = gacc[j];
-        }
+#define GT_GAM(Wn) gt_warp_gamma<Wn>(S.gam, lane, gacc)
+        GT_WARP_SWITCH(GT_GAM)
+#undef GT_GAM
         if (tid < 81)
             elem_row_base(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez, tid, S.rbase[tid], S.rsx[tid],
                           S.rsy[tid]);

@@ -16,10 +16,12 @@
  * can be replayed until the host sees the flag (one read of the state per
  * replay) and the result equals a solve tested after every iteration.
  *
- * K x: one warp per row of the structured CSR pattern; the row's entries are
- * nxb * nyb runs of 3 nzb values whose columns are consecutive (z fastest,
- * then the component), so a lane's column is the run's first column plus its
- * offset.  The warp sums its lanes in a fixed shuffle order.
+ * K x: one warp per control point, i.e. its three rows, which share their
+ * columns: nxb * nyb (<= 25) runs of L = 3 nzb values whose columns are
+ * consecutive (z fastest, then the component).  Lane j holds the first column of
+ * run j; an entry's run is p / L by a multiply-shift reciprocal and its column is
+ * fetched from that lane by a shuffle; one gathered x value serves the three
+ * rows.  The warp sums its lanes in a fixed shuffle order per row.
  */
 #include <cuda_runtime.h>
 #include <vector>
@@ -66,22 +68,41 @@ __global__ void __launch_bounds__(KV_THREADS) k_spmv(igab_geom g, const T *__res
                                                      const bcg_state *S, int skip_half)
 {
     if (S && (skip_half ? halted_or_half(S) : halted(S))) return;
-    const long r = (long)blockIdx.x * (KV_THREADS / 32) + (threadIdx.x >> 5);
+    const long cp = (long)blockIdx.x * (KV_THREADS / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
-    if (r >= g.ndof) return;
+    if (3 * cp >= g.ndof) return;   /* warp-uniform */
     int x0, y0, z0, nxb, nyb, nzb, x1, y1, z1, k1;
-    row_window(g, r, x0, y0, z0, nxb, nyb, nzb, x1, y1, z1, k1);
-    const int L = 3 * nzb, total = nxb * nyb * L;
-    const T *vr = vals + g.rowptr[r];
-    double acc = 0.0;
-    for (int p = lane; p < total; p += 32) {
-        const int run = p / L, j = p - run * L;
-        const long col = 3 * cp_index(g, x0 + run / nyb, y0 + run % nyb, z0) + j;
-        acc += double(vr[p]) * x[col];
+    row_window(g, 3 * cp, x0, y0, z0, nxb, nyb, nzb, x1, y1, z1, k1);
+    const int L = 3 * nzb, total = nxb * nyb * L;   /* L in {9, 12, 15}, total <= 375 */
+    /* lane j < nxb * nyb (<= 25) holds the first column of run j */
+    const long base_own = lane < nxb * nyb ? 3 * cp_index(g, x0 + lane / nyb, y0 + lane % nyb, z0) : 0;
+    /* run = p / L as (p * ceil(2^16 / L)) >> 16, exact for L in {9, 12, 15} and p < 375 */
+    const unsigned invL = (65536u + (unsigned)L - 1u) / (unsigned)L;
+    /* the three rows of the control point share the columns; row k starts k * total later */
+    const T *v0 = vals + g.rowptr[3 * cp], *v1 = v0 + total, *v2 = v1 + total;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int p0 = 0; p0 < total; p0 += 32) {
+        const int p = p0 + lane;
+        const int run = (int)(((unsigned)(p < total ? p : 0) * invL) >> 16);
+        const long base = __shfl_sync(0xffffffffu, base_own, run);
+        if (p < total) {
+            const double xv = x[base + (p - run * L)];
+            a0 += double(v0[p]) * xv;
+            a1 += double(v1[p]) * xv;
+            a2 += double(v2[p]) * xv;
+        }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) y[r] = acc;
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if (lane == 0) {
+        y[3 * cp] = a0;
+        y[3 * cp + 1] = a1;
+        y[3 * cp + 2] = a2;
+    }
 }
 
 /* dinv = 1 / K_ii (1 where K_ii = 0) */
@@ -351,7 +372,7 @@ void launch_iteration(igab_ctx *c, const igab_geom &g, bcg_work &w, const T *val
     const long n = w.n;
     double *r = w.vec, *rh = w.vec + n, *p = w.vec + 2 * n, *ph = w.vec + 3 * n, *v = w.vec + 4 * n;
     double *s = w.vec + 5 * n, *sh = w.vec + 6 * n, *t = w.vec + 7 * n, *x = w.vec + 8 * n, *dinv = w.vec + 9 * n;
-    const unsigned rows_blocks = (unsigned)((n + KV_THREADS / 32 - 1) / (KV_THREADS / 32));
+    const unsigned rows_blocks = (unsigned)((n / 3 + KV_THREADS / 32 - 1) / (KV_THREADS / 32));
     cudaStream_t st = c->stream;
     k_bcg_p<<<KV_BLOCKS, KV_THREADS, 0, st>>>(n, r, p, v, dinv, ph, w.S);
     k_spmv<T><<<rows_blocks, KV_THREADS, 0, st>>>(g, vals, ph, v, w.S, 0);
@@ -397,7 +418,7 @@ void igab_krylov_release(igab_ctx *c)
 int igab_launch_spmv(igab_ctx *c, const void *dvals, int prec, const double *dx, double *dy)
 {
     igab_geom g = c->geom();
-    const unsigned rows_blocks = (unsigned)((c->ndof + KV_THREADS / 32 - 1) / (KV_THREADS / 32));
+    const unsigned rows_blocks = (unsigned)((c->ndof / 3 + KV_THREADS / 32 - 1) / (KV_THREADS / 32));
     if (prec == IGAB_PREC_FP64)
         k_spmv<double><<<rows_blocks, KV_THREADS, 0, c->stream>>>(g, (const double *)dvals, dx, dy, nullptr, 0);
     else

@@ -525,6 +525,42 @@ def run_ours(args):
                               "volume fractions) at the 64 Gauss points of every element, minus the Neumann "
                               "boundary work; device-resident U, CUDA events"}
 
+    # ---- knot-insertion refinement (mesh/nurbs/nurbs_knotinsert.c) of a 32^3 field to 64^3,
+    # host array in place (the reference's interface), and the reference's own routine
+    knot = None
+    if not args.no_density and rank == 0:
+        import ctypes
+        lib = A.lib
+        kn_nel = np.array([n, n, n], dtype=np.int32)
+        per = np.zeros(3, dtype=np.int32)
+        base = np.zeros((n + 2) ** 3 * 3)
+        nc = (n // 2 + 2) ** 3 * 3
+        base[:nc] = np.random.default_rng(6).uniform(-1e-3, 1e-3, nc)
+        vp_ = ctypes.c_void_p
+        Ut = base.copy()
+        lib.igab_knot_insert(Ut.ctypes.data_as(vp_), kn_nel.ctypes.data_as(vp_), 1, 2, 3, per.ctypes.data_as(vp_), local)
+        reps = 5
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            Ut[:] = base
+            lib.igab_knot_insert(Ut.ctypes.data_as(vp_), kn_nel.ctypes.data_as(vp_), 1, 2, 3, per.ctypes.data_as(vp_), local)
+        kms = (time.perf_counter() - t0) * 1e3 / reps
+        knot = {"ms": round(kms, 3), "from": [n // 2] * 3, "to": [n] * 3, "dofs": 3 * (n + 2) ** 3,
+                "definition": "igab_knot_insert (one level of mid-span knot insertion, host array in place, "
+                              "host<->device copies included), wall clock"}
+        if not args.no_cpu:
+            try:
+                from oracle import ref
+                if ref.available():
+                    Ur = base.copy()
+                    t0 = time.perf_counter()
+                    ref.lib().nurbs_knotinsert(Ur.ctypes.data_as(vp_), kn_nel.ctypes.data_as(vp_), 1, 2, 3, 3,
+                                               per.ctypes.data_as(vp_))
+                    knot["reference_cpu_ms"] = round((time.perf_counter() - t0) * 1e3, 3)
+                    knot["reference_cpu_cores"] = 1
+            except Exception as e:
+                knot["reference_cpu_error"] = str(e)
+
     batch = None
     if not args.no_batch:
         batch = bench_batch(args, dev, local, barrier)
@@ -583,7 +619,7 @@ def run_ours(args):
                           "tangent_volume": round(k64[2], 3), "tangent_dirichlet": round(k64[3], 3)},
             "residual_tflops_alg": round(res_tf, 3) if res_tf else None,
             "adjoint_grads_per_s": adjoint["grads_per_s"] if adjoint else None, "adjoint": adjoint,
-            "intdensity": dens,
+            "intdensity": dens, "knot_insert": knot,
             "schedule": schedule, "batch_config3": batch, "transient_config2": trans,
             "transient_adjoint_config4": trans_adj,
             "clocks": clk, "gpu_launches": int(launches64), "roofline": roofline,

@@ -255,4 +255,5 @@ int iga_case_tangent_csr(const iga_case *c, int *rowptr, int *cols, double *vals
 }
 
 void *iga_case_app(iga_case *c) { return &c->app; }
+void *iga_case_iocomm(iga_case *c) { return &c->io; }
 void *iga_case_snesassmbl(iga_case *c) { return &c->sa; }

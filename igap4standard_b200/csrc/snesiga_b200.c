@@ -320,6 +320,57 @@ void snesiga_b200_intdensity(double HH_[], void *app_)
 
 void iga_intdensity(double HH_[], void *app_) { snesiga_b200_intdensity(HH_, app_); }
 
+/* Knot-insertion refinement of a solution -- replaces mesh/nurbs/nurbs_knotinsert.c:7
+ * (same signature, ndim = 3, porder = 2); runs on GPU 0.  The reference asserts on a
+ * bad argument: here the error is printed and the array is left unchanged. */
+void nurbs_knotinsert(double *U_universal, const int nelem[], int nref, int porder, int ndim, int ndof,
+                      int bc_periodic[])
+{
+    if (ndim != 3) {
+        fprintf(stderr, "snesiga_b200: nurbs_knotinsert needs ndim = 3\n");
+        return;
+    }
+    if (igab_knot_insert(U_universal, nelem, nref, porder, ndof, bc_periodic, 0))
+        fprintf(stderr, "snesiga_b200: nurbs_knotinsert failed: %s\n", igab_last_error());
+}
+
+/* Solution files -- replace src/ioutil.c:89 and :126 on one rank: levels ihist0 ..
+ * ihist1 - 1 of U_hist (iocomm->nDof values each) in universal order
+ * (iocomm->universalIdx), raw doubles, level after level. */
+void write_solution(const char *fname, double *U_hist, void *iocomm_, int ihist0, int ihist1)
+{
+    IOcomm *io = (IOcomm *)iocomm_;
+    const long n = io->nDof, nl = ihist1 - ihist0;
+    double *buf = (double *)malloc((size_t)(nl > 0 ? nl : 1) * (size_t)(io->nDof_global > 0 ? io->nDof_global : 1) * sizeof(double));
+    if (!buf) {
+        fprintf(stderr, "snesiga_b200: write_solution: out of memory\n");
+        return;
+    }
+    for (long l = 0; l < nl; l++)
+        for (long i = 0; i < n; i++) buf[l * io->nDof_global + io->universalIdx[i]] = U_hist[(ihist0 + l) * n + i];
+    if (igab_write_solution(fname, buf, io->nDof_global, 0, (int)nl))
+        fprintf(stderr, "snesiga_b200: write_solution failed: %s\n", igab_last_error());
+    free(buf);
+}
+
+void read_solution(const char *fname, double *U_hist, void *iocomm_, int ihist0, int ihist1)
+{
+    IOcomm *io = (IOcomm *)iocomm_;
+    const long n = io->nDof, nl = ihist1 - ihist0;
+    double *buf = (double *)malloc((size_t)(nl > 0 ? nl : 1) * (size_t)(io->nDof_global > 0 ? io->nDof_global : 1) * sizeof(double));
+    if (!buf) {
+        fprintf(stderr, "snesiga_b200: read_solution: out of memory\n");
+        return;
+    }
+    if (igab_read_solution(fname, buf, io->nDof_global, 0, (int)nl)) {
+        fprintf(stderr, "snesiga_b200: read_solution failed: %s\n", igab_last_error());
+    } else {
+        for (long l = 0; l < nl; l++)
+            for (long i = 0; i < n; i++) U_hist[(ihist0 + l) * n + i] = buf[l * io->nDof_global + io->universalIdx[i]];
+    }
+    free(buf);
+}
+
 /* Put the structured AIJ pattern into P the first time (as the reference's
  * first MatSetValues pass does) and check that P's CSR is exactly it. */
 static int ensure_pattern(gpu_state *s, Mat P)

@@ -106,6 +106,9 @@ IGAB_API = [
     ("igab_intdensity", ctypes.c_int, [vp, vp, vp]),
     ("igab_intdensity_device", ctypes.c_int, [vp, vp, vp]),
     ("igab_spmv_device", ctypes.c_int, [vp, vp, ctypes.c_int, vp, vp]),
+    ("igab_knot_insert", ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int]),
+    ("igab_write_solution", ctypes.c_int, [ctypes.c_char_p, vp, ctypes.c_long, ctypes.c_int, ctypes.c_int]),
+    ("igab_read_solution", ctypes.c_int, [ctypes.c_char_p, vp, ctypes.c_long, ctypes.c_int, ctypes.c_int]),
     ("igab_solve_device", ctypes.c_int, [vp, vp, ctypes.c_int, vp, vp, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_int, ctypes.POINTER(IgabSolveInfo)]),
     ("igab_batch_create", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]),
@@ -142,6 +145,9 @@ DROPIN_API = [
     ("snesiga_gpu_last_timings", ctypes.c_int, [vp, c_double_p]),
     ("iga_intdensity", None, [vp, vp]),
     ("snesiga_b200_intdensity", None, [vp, vp]),
+    ("nurbs_knotinsert", None, [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]),
+    ("write_solution", None, [ctypes.c_char_p, vp, vp, ctypes.c_int, ctypes.c_int]),
+    ("read_solution", None, [ctypes.c_char_p, vp, vp, ctypes.c_int, ctypes.c_int]),
 ]
 
 CASE_API = [
@@ -158,6 +164,7 @@ CASE_API = [
     ("iga_case_tangent_nnz", ctypes.c_long, [vp]),
     ("iga_case_tangent_csr", ctypes.c_int, [vp, vp, vp, vp]),
     ("iga_case_app", vp, [vp]),
+    ("iga_case_iocomm", vp, [vp]),
     ("iga_case_snesassmbl", vp, [vp]),
     ("iga_case_neumann", None, [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]),
 ]

@@ -54,6 +54,8 @@ int  iga_case_tangent_csr(const iga_case *c, int *rowptr, int *cols, double *val
 
 /* opaque handles for code that wants to call further library functions */
 void *iga_case_app(iga_case *c);
+/* the IOcomm the case's snesiga_init filled (write_solution / read_solution, src/ioutil.c:89) */
+void *iga_case_iocomm(iga_case *c);
 void *iga_case_snesassmbl(iga_case *c);
 
 /* the default app hook: neumann_ = par_neumann[6*face+3*order+idof]

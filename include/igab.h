@@ -246,6 +246,20 @@ int igab_spmv_device(igab_ctx *ctx, const void *vals_dev, int prec, const double
 int igab_solve_device(igab_ctx *ctx, const void *vals_dev, int prec, const double *b_dev, double *x_dev,
                       double rtol, double atol, int maxit, igab_solve_info *info);
 
+/* ---- mesh refinement and solution files (mesh/nurbs/nurbs_knotinsert.c:7, src/ioutil.c:89, :126).
+ * igab_knot_insert: refine the p = 2 control points of a field, in place in host memory
+ * (U_universal[ndof * cp + dof], cp = (x nb1 + y) nb2 + z with nb = nelem + 2, or nelem
+ * along a periodic direction), from nelem / 2^nref to nelem elements per direction by
+ * inserting the mid-point of every knot span nref times; the array must hold the refined
+ * size.  porder must be 2; nelem a positive multiple of 2^nref.  Runs on the given GPU.
+ * igab_write_solution / igab_read_solution: history levels ihist0 .. ihist1 - 1 of U_hist
+ * (ndof doubles each) to / from a raw file, level after level, in the universal dof order
+ * of one rank (the reference's format). */
+int igab_knot_insert(double *U_universal, const int nelem[3], int nref, int porder, int ndof,
+                     const int bc_periodic[3], int device);
+int igab_write_solution(const char *fname, const double *U_hist, long ndof, int ihist0, int ihist1);
+int igab_read_solution(const char *fname, double *U_hist, long ndof, int ihist0, int ihist1);
+
 /* ---- residual for callers that cannot have the library allocate device memory.
  * No counterpart in the reference.  Same result as igab_residual, but U and R
  * are staged in a file-scope device array (2 x 8 MiB, held by every GPU that

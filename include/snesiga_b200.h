@@ -38,6 +38,12 @@ void snesiga_init(void *app_, void *phys_, void *nurbs_, void *bc_, void *snesas
 /* integrated densities of app->U_hist, replacing src/iga_intdensity.c:10
  * (include/iga.h:29); NaN in every slot on failure (the reference returns void) */
 void iga_intdensity(double HH_[], void *app_);
+/* knot-insertion refinement (mesh/nurbs/nurbs_knotinsert.c:7) and solution files
+ * (src/ioutil.c:89, :126), same signatures; errors are printed (the reference asserts) */
+void nurbs_knotinsert(double *U_universal, const int nelem[], int nref, int porder, int ndim, int ndof,
+                      int bc_periodic[]);
+void write_solution(const char *fname, double *U_hist, void *iocomm_, int ihist0, int ihist1);
+void read_solution(const char *fname, double *U_hist, void *iocomm_, int ihist0, int ihist1);
 
 /* the same callbacks under names that cannot collide with libigap4 */
 PetscErrorCode snesiga_b200_Residual(SNES snes, Vec U_, Vec Residual_, void *app_);

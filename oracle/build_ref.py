@@ -16,8 +16,8 @@ sources compiled (paths inside the reference project):
 
   src/snesiga_Residual.c  src/snesiga_Tangent.c  src/snesiga_init.c
   src/iga_dirichlet.c     src/quadrature.c       src/mathutil.c
-  src/iga_intdensity.c
-  mesh/nurbs/eval_Bspline.c  mesh/nurbs/evalN.c
+  src/iga_intdensity.c     src/ioutil.c
+  mesh/nurbs/eval_Bspline.c  mesh/nurbs/evalN.c  mesh/nurbs/nurbs_knotinsert.c
   phys/ge/{init,assert_par_mat,residual,tangent,density,field}.c
   phys/getime/{init,assert_par_mat,residual,tangent,density,field}.c
 
@@ -53,8 +53,8 @@ LIB = os.path.join(OUT_DIR, "libref_iga.so")
 
 REF_SOURCES = [
     "src/snesiga_Residual.c", "src/snesiga_Tangent.c", "src/snesiga_init.c",
-    "src/iga_dirichlet.c", "src/quadrature.c", "src/mathutil.c", "src/iga_intdensity.c",
-    "mesh/nurbs/eval_Bspline.c", "mesh/nurbs/evalN.c",
+    "src/iga_dirichlet.c", "src/quadrature.c", "src/mathutil.c", "src/iga_intdensity.c", "src/ioutil.c",
+    "mesh/nurbs/eval_Bspline.c", "mesh/nurbs/evalN.c", "mesh/nurbs/nurbs_knotinsert.c",
     "phys/ge/init.c", "phys/ge/assert_par_mat.c", "phys/ge/residual.c", "phys/ge/tangent.c",
     "phys/ge/density.c", "phys/ge/field.c",
     "phys/getime/init.c", "phys/getime/assert_par_mat.c", "phys/getime/residual.c",

@@ -6,7 +6,9 @@ case builder (same C API as igap4standard_b200.case) and the reference's
 point functions: ge_residual/ge_tangent (phys/ge), getime_residual/
 getime_tangent (phys/getime), eval_Bspline (mesh/nurbs/eval_Bspline.c),
 evalN (mesh/nurbs/evalN.c), legendre_handle (src/quadrature.c),
-iga_dirichlet (src/iga_dirichlet.c), iga_intdensity (src/iga_intdensity.c).
+iga_dirichlet (src/iga_dirichlet.c), iga_intdensity (src/iga_intdensity.c),
+nurbs_knotinsert (mesh/nurbs/nurbs_knotinsert.c), write_solution / read_solution
+(src/ioutil.c).
 """
 import ctypes
 import os
@@ -46,6 +48,12 @@ def lib():
         L.iga_dirichlet.restype = None
         L.iga_intdensity.argtypes = [vp, vp]
         L.iga_intdensity.restype = None
+        L.nurbs_knotinsert.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
+        L.nurbs_knotinsert.restype = None
+        L.write_solution.argtypes = [ctypes.c_char_p, vp, vp, ctypes.c_int, ctypes.c_int]
+        L.write_solution.restype = None
+        L.read_solution.argtypes = [ctypes.c_char_p, vp, vp, ctypes.c_int, ctypes.c_int]
+        L.read_solution.restype = None
         L.oracle_scale_install.argtypes = [vp, vp, ctypes.c_long]
         L.oracle_scale_install.restype = None
         L.oracle_scale_remove.argtypes = [vp]

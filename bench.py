@@ -41,6 +41,8 @@ RES_ALG_FLOPS = 64 * (2 * (27 * 30 + 27 * 30) + 270)
 # flops the tangent kernel executes per element on the tensor path: 66 upper 8x8 tiles
 # x 12 variables per point, plus 10 upper 8x8 tiles of the geometric block x 6 U / V rows per point
 TAN_EXEC_FLOPS = 64 * 2 * (66 * 64 * 12 + 10 * 64 * 6)
+# DRAM bytes per element of the FP64 tangent kernel (ncu, 32^3 colour launch: 243.12 MB / 4,096)
+TAN64_DRAM_BYTES_PER_ELEMENT = 243.12e6 / 4096
 
 
 def parse():
@@ -572,19 +574,15 @@ def run_ours(args):
     nlaunch = max(k64[5], 1)
     achieved = nel * TAN_ALG_FLOPS / (tan_ms * 1e-3) / 1e12
     executed = nel * TAN_EXEC_FLOPS / (tan_ms * 1e-3) / 1e12
-    traffic = None
-    tp = os.path.join(REPO, "profiles", "tangent_volume_traffic.json")
-    if os.path.exists(tp):
-        try:
-            with open(tp) as f:
-                traffic = json.load(f).get("bytes_per_element")
-            if traffic is not None:
-                traffic = traffic * nel / nlaunch
-        except Exception:
-            traffic = None
+    # DRAM traffic of the FP64 tangent kernel from one ncu capture of a 32^3 colour launch
+    # (dram__bytes_read.sum + dram__bytes_write.sum = 151.08 MB + 92.04 MB for 4,096
+    # elements), scaled to a launch of this mesh by its elements (the traffic is the CSR
+    # read-modify-write of each element matrix, so it grows with the element count)
+    traffic = round(TAN64_DRAM_BYTES_PER_ELEMENT * nel / nlaunch)
     roofline = {"bound": "tensor", "pipe": "FP64 tensor (mma.sync m8n8k4 f64) + FP64 FMA", "achieved": round(achieved, 3),
                 "peak": round(peak64, 3),
                 "unit": "TFLOP/s", "frac": round(achieved / peak64, 4), "traffic": traffic,
+                "traffic_source": "ncu dram bytes of one 32^3 colour launch (4,096 elements), scaled per element",
                 "kernel": "k_tan_dmma", "avg_launch_ms": round(tan_ms / nlaunch, 3),
                 "flops_per_launch": nel * TAN_ALG_FLOPS / nlaunch,
                 "flops_definition": "algorithmic B^T D B per element = 64*2*(30*81*10+81*81*10) (effective: the "

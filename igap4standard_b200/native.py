@@ -107,6 +107,7 @@ IGAB_API = [
     ("igab_intdensity_device", ctypes.c_int, [vp, vp, vp]),
     ("igab_spmv_device", ctypes.c_int, [vp, vp, ctypes.c_int, vp, vp]),
     ("igab_knot_insert", ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int]),
+    ("igab_knot_release", ctypes.c_int, [ctypes.c_int]),
     ("igab_write_solution", ctypes.c_int, [ctypes.c_char_p, vp, ctypes.c_long, ctypes.c_int, ctypes.c_int]),
     ("igab_read_solution", ctypes.c_int, [ctypes.c_char_p, vp, ctypes.c_long, ctypes.c_int, ctypes.c_int]),
     ("igab_solve_device", ctypes.c_int, [vp, vp, ctypes.c_int, vp, vp, ctypes.c_double, ctypes.c_double,

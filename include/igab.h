@@ -251,12 +251,17 @@ int igab_solve_device(igab_ctx *ctx, const void *vals_dev, int prec, const doubl
  * (U_universal[ndof * cp + dof], cp = (x nb1 + y) nb2 + z with nb = nelem + 2, or nelem
  * along a periodic direction), from nelem / 2^nref to nelem elements per direction by
  * inserting the mid-point of every knot span nref times; the array must hold the refined
- * size.  porder must be 2; nelem a positive multiple of 2^nref.  Runs on the given GPU.
+ * size.  porder must be 2; nelem a positive multiple of 2^nref.  Runs on the given GPU;
+ * its two device buffers stay allocated between calls (grown to the largest refined
+ * field seen on that device) and calls in one process are serialised.
+ * igab_knot_release: frees those buffers on the given device (no counterpart in the
+ * reference); the next igab_knot_insert allocates them again.
  * igab_write_solution / igab_read_solution: history levels ihist0 .. ihist1 - 1 of U_hist
  * (ndof doubles each) to / from a raw file, level after level, in the universal dof order
  * of one rank (the reference's format). */
 int igab_knot_insert(double *U_universal, const int nelem[3], int nref, int porder, int ndof,
                      const int bc_periodic[3], int device);
+int igab_knot_release(int device);
 int igab_write_solution(const char *fname, const double *U_hist, long ndof, int ihist0, int ihist1);
 int igab_read_solution(const char *fname, double *U_hist, long ndof, int ihist0, int ihist1);
 

@@ -57,3 +57,25 @@ def test_knot_insert_rejects_bad_sizes(built):
     U = np.zeros(8 * 6 * 6 * 3)
     assert lib.igab_knot_insert(_p(U), _p(nel), 2, 2, 3, _p(pb), 0) != 0     # 6 is not a multiple of 4
     assert lib.igab_knot_insert(_p(U), _p(nel), 1, 3, 3, _p(pb), 0) != 0     # porder 3
+    assert lib.igab_knot_insert(_p(U), _p(nel), 1, 2, 3, _p(pb), -1) != 0    # no device -1
+    assert lib.igab_knot_release(-1) != 0
+
+
+def test_knot_insert_buffers_kept_and_released(built, oracle_lib):
+    """The device buffers kept between calls: a large field, then smaller ones in
+    the larger buffers (nothing of the previous call leaks into the result), then
+    after igab_knot_release, allocated again."""
+    from igap4standard_b200 import native
+    lib = native.lib_cuda()
+    for k, (nelem, nref, per) in enumerate([((16, 16, 8), 1, (0, 0, 0)), ((4, 6, 8), 1, (1, 0, 1)),
+                                            ((8, 4, 4), 2, (0, 0, 0)), (None, 0, 0), ((4, 6, 8), 1, (1, 0, 1))]):
+        if nelem is None:
+            assert lib.igab_knot_release(0) == 0
+            assert lib.igab_knot_release(0) == 0        # nothing held: no-op
+            continue
+        nel, pb, U, nfine = _arrays(nelem, nref, per, 3, 11 + k)
+        U_ref, U_gpu = U.copy(), U.copy()
+        oracle_lib.lib().nurbs_knotinsert(_p(U_ref), _p(nel), nref, 2, 3, 3, _p(pb))
+        assert lib.igab_knot_insert(_p(U_gpu), _p(nel), nref, 2, 3, _p(pb), 0) == 0
+        a, b = U_ref[:nfine], U_gpu[:nfine]
+        assert np.abs(a - b).max() <= 1e-15 * np.abs(a).max()

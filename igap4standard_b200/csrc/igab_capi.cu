@@ -336,6 +336,9 @@ static void free_ctx(igab_ctx *c)
     if (c->graph) cudaGraphDestroy(c->graph);
     for (int k = 0; k < 6; k++)
         if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+    for (int k = 0; k < IGAB_MAX_SLABS; k++)
+        if (c->slab_ev[k]) cudaEventDestroy(c->slab_ev[k]);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -661,14 +664,30 @@ extern "C" int igab_tangent(igab_ctx *ctx, const double *U_host, void *vals_host
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     int rc = ensure_buffers(ctx, prec);
     if (rc) return rc;
+    if (!ctx->copy_stream) IGAB_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
     IGAB_CUDA_TRY(cudaMemcpyAsync(ctx->d_U, U_host, (size_t)ctx->ndof * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    rc = igab_tangent_device(ctx, ctx->d_U, ctx->d_vals, prec);
+    /* x-slab by x-slab: the rows a slab finishes are downloaded on the copy stream while
+     * the next slabs are assembled (the values are the same as one whole-mesh pass) */
+    long row_end[IGAB_MAX_SLABS];
+    int nslab = 0;
+    rc = igab_launch_tangent_slabs(ctx, ctx->d_U, ctx->d_vals, prec, row_end, &nslab);
     if (rc) return rc;
+    const size_t es = prec == IGAB_PREC_FP64 ? sizeof(double) : sizeof(float);
+    const int *rp = ctx->rowptr_h.data();
+    long r0 = 0;
+    for (int i = 0; i < nslab; i++) {
+        IGAB_CUDA_TRY(cudaStreamWaitEvent(ctx->copy_stream, ctx->slab_ev[i], 0));
+        const size_t off = (size_t)rp[r0] * es, len = (size_t)(rp[row_end[i]] - rp[r0]) * es;
+        if (len)
+            IGAB_CUDA_TRY(cudaMemcpyAsync((char *)vals_host + off, (const char *)ctx->d_vals + off, len,
+                                          cudaMemcpyDeviceToHost, ctx->copy_stream));
+        r0 = row_end[i];
+    }
     int fin = 1;
     rc = igab_launch_check_finite(ctx, ctx->d_vals, ctx->nnz, prec, &fin);
+    const cudaError_t ce = cudaStreamSynchronize(ctx->copy_stream);
     if (rc) return rc;
-    size_t es = prec == IGAB_PREC_FP64 ? sizeof(double) : sizeof(float);
-    IGAB_CUDA_TRY(cudaMemcpyAsync(vals_host, ctx->d_vals, (size_t)ctx->nnz * es, cudaMemcpyDeviceToHost, ctx->stream));
+    IGAB_CUDA_TRY(ce);
     IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     rc = check_status(ctx);
     if (rc) return rc;

@@ -39,9 +39,16 @@ struct tile_t {
     int nv[3];  /* valid elements per direction */
 };
 
+/* Colour = 4 px + 2 py + pz, p the parities of the tile coordinates; tile ids of a
+ * colour run with x slowest.  With the x parity most significant, the tiles of
+ * one colour inside an x-range of tiles are a contiguous range of ids, and
+ * launching the colours slab by slab along x, each slab starting on an odd tile,
+ * adds into every CSR entry in the same order as launching each colour over the
+ * whole mesh: an entry is touched by at most two x-tiles t, t+1, and across a slab
+ * boundary t is even (colours 0-3, first in either order). */
 __device__ __forceinline__ bool decode_tile(const igab_geom &g, int TE, int colour, int bid, tile_t &T)
 {
-    int c[3] = {colour & 1, (colour >> 1) & 1, (colour >> 2) & 1};
+    int c[3] = {(colour >> 2) & 1, (colour >> 1) & 1, colour & 1};
     int nc[3];
     for (int d = 0; d < 3; d++) {
         int nt = (g.ne[d] + TE - 1) / TE;
@@ -156,11 +163,31 @@ long tiles_of_colour(const igab_geom &g, int TE, int colour)
 {
     long n = 1;
     for (int d = 0; d < 3; d++) {
-        int c = (colour >> d) & 1;
+        int c = (colour >> (2 - d)) & 1;
         int nt = (g.ne[d] + TE - 1) / TE;
         n *= nt > c ? (nt - c + 1) / 2 : 0;
     }
     return n;
+}
+
+/* the tiles of a colour whose x tile coordinate lies in [tx0, tx1): ids
+ * *first .. *first + return value - 1 (decode_tile numbering) */
+long tiles_of_colour_in(const igab_geom &g, int TE, int colour, int tx0, int tx1, long *first)
+{
+    const int cx = (colour >> 2) & 1;
+    long plane = 1;
+    for (int d = 1; d < 3; d++) {
+        int c = (colour >> (2 - d)) & 1;
+        int nt = (g.ne[d] + TE - 1) / TE;
+        plane *= nt > c ? (nt - c + 1) / 2 : 0;
+    }
+    const int ntx = (g.ne[0] + TE - 1) / TE;
+    const int ncx = ntx > cx ? (ntx - cx + 1) / 2 : 0;
+    int i0 = (tx0 - cx + 1) / 2, i1 = (tx1 - cx + 1) / 2;   /* tx = 2 i + cx in [tx0, tx1) */
+    if (i0 < 0) i0 = 0;
+    if (i1 > ncx) i1 = ncx;
+    *first = (long)i0 * plane;
+    return i1 > i0 ? (long)(i1 - i0) * plane : 0;
 }
 
 } /* namespace */

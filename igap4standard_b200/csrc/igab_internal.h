@@ -59,6 +59,8 @@ struct igab_batch_dev {
     int *status;           /* bit 1: a dependency wait gave up */
 };
 
+#define IGAB_MAX_SLABS 32   /* x-slabs of the host-pointer tangent */
+
 struct igab_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -131,6 +133,10 @@ struct igab_ctx {
     size_t dens_part_bytes = 0;
     double *d_HH = nullptr;
 
+    /* host-pointer tangent: download stream, and one event per x-slab whose rows are final */
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t slab_ev[IGAB_MAX_SLABS] = {};
+
     /* captured assembly graph */
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -148,12 +154,16 @@ int igab_krylov_solve(igab_ctx *c, const void *dvals, int prec, const double *db
                       double atol, int maxit, int *iterations, int *converged, double *rnorm, double *bnorm);
 void igab_krylov_release(igab_ctx *c);
 int igab_launch_tangent(igab_ctx *c, const double *dU, void *dvals, int prec);
+/* the same, slab by slab along x: after slab i, rows [0, row_end[i]) are final and
+ * c->slab_ev[i] is recorded on c->stream (one slab when the kernels have no x-range) */
+int igab_launch_tangent_slabs(igab_ctx *c, const double *dU, void *dvals, int prec, long *row_end, int *nslab);
 int igab_launch_csr_cols(igab_ctx *c, int *dcols);
 int igab_launch_check_finite(igab_ctx *c, const void *dev, long n, int prec, int *all_finite);
 int igab_launch_basis_tables(igab_ctx *c, int d, const double *dkv, const double *dgx, const double *dgw);
 int igab_launch_fma_peak(int prec, double *tflops);
-int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv);
-int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv);
+/* tangent volume kernels over the tiles with x tile coordinate in [tx0, tx1) (tiles of 2 elements) */
+int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv, int tx0, int tx1);
+int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv, int tx0, int tx1);
 /* persistent batched launches (igab_batch.cu builds the work list) */
 int igab_launch_res_batch(const igab_batch_dev &B, int grid, cudaStream_t s, const double *dU, double *dR);
 int igab_launch_tan_dmma_batch(const igab_batch_dev &B, int grid, cudaStream_t s, const double *dU, double *dv);

@@ -658,9 +658,11 @@ __global__ void __launch_bounds__(256) k_tan_volume(igab_geom g, const double *_
 }
 
 /* MatZeroRowsColumns(P, rows, 1.0) on the structured pattern (src/snesiga_Tangent.c:270):
- * one thread per (Dirichlet row, entry of that row). */
+ * one thread per (Dirichlet row, entry of that row); only entries in rows [r0, r1) are
+ * written (every write to an entry writes the same value, so the rows may be done in parts). */
 template <typename T>
-__device__ __forceinline__ void tan_dirichlet_entry(const igab_geom &g, int r, int s, T *__restrict__ vals)
+__device__ __forceinline__ void tan_dirichlet_entry(const igab_geom &g, int r, int s, T *__restrict__ vals,
+                                                    long r0 = 0, long r1 = 0x7fffffffffffffffL)
 {
     int cp = r / 3;
     int z = cp % g.nb[2], y = (cp / g.nb[2]) % g.nb[1], x = cp / (g.nb[2] * g.nb[1]);
@@ -673,18 +675,19 @@ __device__ __forceinline__ void tan_dirichlet_entry(const igab_geom &g, int r, i
     int k2 = s % 3, q = s / 3;
     int cz = z0 + q % nzb, cy = y0 + (q / nzb) % nyb, cx = x0 + q / (nzb * nyb);
     long c = 3 * cp_index(g, cx, cy, cz) + k2;
-    vals[g.rowptr[r] + s] = (c == r) ? T(1) : T(0);
-    if (c != r) vals[g.rowptr[c] + csr_pos(g, cx, cy, cz, x, y, z, r % 3)] = T(0);
+    if (r >= r0 && r < r1) vals[g.rowptr[r] + s] = (c == r) ? T(1) : T(0);
+    if (c != r && c >= r0 && c < r1) vals[g.rowptr[c] + csr_pos(g, cx, cy, cz, x, y, z, r % 3)] = T(0);
 }
 
 template <typename T>
-__global__ void k_tan_dirichlet(igab_geom g, long nd, const int *__restrict__ drow, T *__restrict__ vals)
+__global__ void k_tan_dirichlet(igab_geom g, long nd, const int *__restrict__ drow, T *__restrict__ vals, long r0,
+                                long r1)
 {
     long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     long j = t / 375;
     int s = (int)(t % 375);
     if (j >= nd) return;
-    tan_dirichlet_entry<T>(g, drow[j], s, vals);
+    tan_dirichlet_entry<T>(g, drow[j], s, vals, r0, r1);
 }
 
 /* zero the Dirichlet rows of a CSR matrix (no column change, no diagonal): one thread per
@@ -859,6 +862,29 @@ int launch_tan_volume(igab_ctx *c, const igab_geom &g, const double *dU, T *dv)
     return 0;
 }
 
+/* the selected tangent volume kernels, over the x tiles [tx0, tx1) (tiles of 2 elements)
+ * where the kernel takes a range, else over the whole mesh */
+template <typename T>
+int launch_tan_volume_x(igab_ctx *c, const igab_geom &g, const double *dU, T *dv, int tx0, int tx1)
+{
+    if (c->phys == IGAB_PHYS_GETIME)
+        return igab_launch_tan_getime(c, dU, dv, sizeof(T) == 8 ? IGAB_PREC_FP64 : IGAB_PREC_FP32);
+    if (sizeof(T) == 8 && c->tan_kernel == 1) return igab_launch_tan_dmma(c, dU, (double *)dv, tx0, tx1);
+    if (sizeof(T) == 4 && c->tan32_kernel == 1) return igab_launch_tan_tc32(c, dU, (float *)dv, tx0, tx1);
+    return launch_tan_volume<T, 2>(c, g, dU, dv);
+}
+
+template <typename T>
+int launch_tan_dirichlet(igab_ctx *c, const igab_geom &g, T *dv, long r0, long r1)
+{
+    if (c->nd == 0) return 0;
+    long n = c->nd * 375;
+    k_tan_dirichlet<T><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(g, c->nd, c->d_drow, dv, r0, r1);
+    c->last_launches++;
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
 template <typename T>
 int launch_tangent_t(igab_ctx *c, const double *dU, T *dv)
 {
@@ -866,26 +892,73 @@ int launch_tangent_t(igab_ctx *c, const double *dU, T *dv)
     IGAB_CUDA_TRY(cudaMemsetAsync(dv, 0, (size_t)c->nnz * sizeof(T), c->stream));
     igab_mark(c, 3);
     int l0 = c->last_launches;
-    int e;
-    if (c->phys == IGAB_PHYS_GETIME)
-        e = igab_launch_tan_getime(c, dU, dv, sizeof(T) == 8 ? IGAB_PREC_FP64 : IGAB_PREC_FP32);
-    else if (sizeof(T) == 8 && c->tan_kernel == 1)
-        e = igab_launch_tan_dmma(c, dU, (double *)dv);
-    else if (sizeof(T) == 4 && c->tan32_kernel == 1)
-        e = igab_launch_tan_tc32(c, dU, (float *)dv);
-    else
-        e = launch_tan_volume<T, 2>(c, g, dU, dv);
+    int e = launch_tan_volume_x<T>(c, g, dU, dv, 0, (c->ne[0] + 1) / 2);
     if (e) return e;
     c->nvol_tan = c->last_launches - l0;
     igab_mark(c, 4);
-    if (c->nd > 0) {
-        long n = c->nd * 375;
-        k_tan_dirichlet<T><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(g, c->nd, c->d_drow, dv);
-        c->last_launches++;
-        IGAB_CUDA_TRY(cudaGetLastError());
-    }
+    if ((e = launch_tan_dirichlet<T>(c, g, dv, 0, c->ndof))) return e;
     igab_mark(c, 5);
     c->ev_tan = c->profiling;
+    return 0;
+}
+
+/* x-slab boundaries (odd tile coordinates, increasing) of the host-pointer tangent:
+ * slabs of 8 tiles, then 4, 2, 2 and 1 (or 2) tiles at the end, so that the rows
+ * finished last, whose download cannot overlap any compute, are few.  None below
+ * 12 tiles. */
+int slab_bounds(int ntx, int *b)
+{
+    if (ntx < 12) return 0;
+    int tmp[IGAB_MAX_SLABS], n = 0;
+    int x = (ntx - 1) % 2 == 1 ? ntx - 1 : ntx - 2;
+    tmp[n++] = x;
+    const int tail[3] = {2, 2, 4};
+    for (int i = 0; i < 3; i++) {
+        if (x - tail[i] < 8) break;
+        x -= tail[i];
+        tmp[n++] = x;
+    }
+    while (x - 8 >= 8 && n < IGAB_MAX_SLABS - 1) {
+        x -= 8;
+        tmp[n++] = x;
+    }
+    for (int i = 0; i < n; i++) b[i] = tmp[n - 1 - i];
+    return n;
+}
+
+template <typename T>
+int launch_tangent_slabs_t(igab_ctx *c, const double *dU, T *dv, long *row_end, int *nslab)
+{
+    igab_geom g = c->geom();
+    const int ntx = (c->ne[0] + 1) / 2;
+    int b[IGAB_MAX_SLABS];
+    const bool ranged = c->phys != IGAB_PHYS_GETIME && (sizeof(T) == 8 ? c->tan_kernel == 1 : c->tan32_kernel == 1);
+    const int nb = ranged ? slab_bounds(ntx, b) : 0;
+    for (int i = 0; i <= nb; i++)
+        if (!c->slab_ev[i]) IGAB_CUDA_TRY(cudaEventCreateWithFlags(&c->slab_ev[i], cudaEventDisableTiming));
+    IGAB_CUDA_TRY(cudaMemsetAsync(dv, 0, (size_t)c->nnz * sizeof(T), c->stream));
+    igab_mark(c, 3);
+    int nvol = 0;
+    const long plane = 3L * c->nb[1] * c->nb[2];   /* rows per control-point layer in x */
+    long r0 = 0;
+    for (int i = 0; i <= nb; i++) {
+        const int tx0 = i ? b[i - 1] : 0, tx1 = i < nb ? b[i] : ntx;
+        const int lv = c->last_launches;
+        int e = launch_tan_volume_x<T>(c, g, dU, dv, tx0, tx1);
+        if (e) return e;
+        nvol += c->last_launches - lv;
+        if (i == nb) igab_mark(c, 4);
+        /* control points below x = 2 tx1 are touched by no element of a later slab */
+        const long r1 = i < nb ? 2L * tx1 * plane : c->ndof;
+        if ((e = launch_tan_dirichlet<T>(c, g, dv, r0, r1))) return e;
+        IGAB_CUDA_TRY(cudaEventRecord(c->slab_ev[i], c->stream));
+        row_end[i] = r1;
+        r0 = r1;
+    }
+    c->nvol_tan = nvol;
+    igab_mark(c, 5);
+    c->ev_tan = c->profiling;
+    *nslab = nb + 1;
     return 0;
 }
 
@@ -926,6 +999,14 @@ int igab_launch_tangent(igab_ctx *c, const double *dU, void *dvals, int prec)
     c->last_launches = 0;
     if (prec == IGAB_PREC_FP64) return launch_tangent_t<double>(c, dU, (double *)dvals);
     if (prec == IGAB_PREC_FP32) return launch_tangent_t<float>(c, dU, (float *)dvals);
+    return IGAB_ERR_ARG;
+}
+
+int igab_launch_tangent_slabs(igab_ctx *c, const double *dU, void *dvals, int prec, long *row_end, int *nslab)
+{
+    c->last_launches = 0;
+    if (prec == IGAB_PREC_FP64) return launch_tangent_slabs_t<double>(c, dU, (double *)dvals, row_end, nslab);
+    if (prec == IGAB_PREC_FP32) return launch_tangent_slabs_t<float>(c, dU, (float *)dvals, row_end, nslab);
     return IGAB_ERR_ARG;
 }
 

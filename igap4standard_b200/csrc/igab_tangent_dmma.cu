@@ -132,12 +132,13 @@ struct src_colour {
     const double *U;
     double *vals;
     int colour;
+    long tile0;    /* first tile id (an x-slab of the colour) */
     long ntiles;
     int *status;
     __device__ void fetch(int k, dws_tile &R) const
     {
         const long t = blockIdx.x + (long)k * gridDim.x;
-        R.tile = t < ntiles ? (int)t : -1;
+        R.tile = t < ntiles ? (int)(tile0 + t) : -1;
         if (R.tile < 0) return;
         R.g = g;
         R.U = U;
@@ -665,20 +666,22 @@ int igab_batch_occupancy_dmma(int *per_sm)
     return 0;
 }
 
-int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv)
+int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv, int tx0, int tx1)
 {
     igab_geom g = c->geom();
     const size_t sm = sizeof(dws_smem);
     IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const int nsm = sm_count();
     for (int colour = 0; colour < 8; colour++) {
-        const long nt = tiles_of_colour(g, TE, colour);
+        long first = 0;
+        const long nt = tiles_of_colour_in(g, TE, colour, tx0, tx1, &first);
         if (nt == 0) continue;
         src_colour F;
         F.g = g;
         F.U = dU;
         F.vals = dv;
         F.colour = colour;
+        F.tile0 = first;
         F.ntiles = nt;
         F.status = c->d_status;
         k_tan_dmma<<<(unsigned)(nt < nsm ? nt : nsm), NTHR, sm, c->stream>>>(F);

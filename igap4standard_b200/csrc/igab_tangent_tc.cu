@@ -693,12 +693,13 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
 
 template <int TE>
 __global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32(igab_geom g, const double *__restrict__ U,
-                                                         float *__restrict__ vals, int colour, int *status)
+                                                         float *__restrict__ vals, int colour, int tile0,
+                                                         int *status)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     tc_smem<TE> &S = *reinterpret_cast<tc_smem<TE> *>(smem_raw);
     tile_t Tl;
-    if (!decode_tile(g, TE, colour, blockIdx.x, Tl)) return;   /* block-uniform, before any barrier */
+    if (!decode_tile(g, TE, colour, tile0 + (int)blockIdx.x, Tl)) return;   /* block-uniform, before any barrier */
     tc_state Q;
     tc_setup<TE>(S, Q);
     if (threadIdx.x < TCN_BLD) tc_tile<TE>(g, Tl, U, vals, S, Q);
@@ -890,7 +891,7 @@ extern "C" int igab_tc_peak(int device, int n_cols, double *tflops)
     }
 }
 
-int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv)
+int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv, int tx0, int tx1)
 {
     igab_geom g = c->geom();
     const size_t sm = sizeof(tc_smem<2>);
@@ -904,9 +905,10 @@ int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv)
         return IGAB_ERR_UNSUPPORTED;
     }
     for (int colour = 0; colour < 8; colour++) {
-        long nblk = tiles_of_colour(g, 2, colour);
+        long first = 0;
+        const long nblk = tiles_of_colour_in(g, 2, colour, tx0, tx1, &first);
         if (nblk == 0) continue;
-        k_tan_tc32<2><<<(unsigned)nblk, TCN_THR, sm, c->stream>>>(g, dU, dv, colour, c->d_status);
+        k_tan_tc32<2><<<(unsigned)nblk, TCN_THR, sm, c->stream>>>(g, dU, dv, colour, (int)first, c->d_status);
         c->last_launches++;
     }
     IGAB_CUDA_TRY(cudaGetLastError());

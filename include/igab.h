@@ -89,7 +89,10 @@ int igab_set_history(igab_ctx *ctx, int level, const double *U, int on_device);
  * context stream; the host variants copy U in and the result out. */
 int igab_residual(igab_ctx *ctx, const double *U_host, double *R_host);
 int igab_residual_device(igab_ctx *ctx, const double *U_dev, double *R_dev);
-/* vals: nnz doubles (IGAB_PREC_FP64) or floats (IGAB_PREC_FP32) */
+/* vals: nnz doubles (IGAB_PREC_FP64) or floats (IGAB_PREC_FP32).  igab_tangent
+ * assembles meshes of 23 or more elements along x slab by slab along x and downloads
+ * the rows each slab finishes on a second stream while the next slabs are assembled
+ * (pinned vals_host overlaps fully); the values are bitwise those of igab_tangent_device. */
 int igab_tangent(igab_ctx *ctx, const double *U_host, void *vals_host, int prec);
 int igab_tangent_device(igab_ctx *ctx, const double *U_dev, void *vals_dev, int prec);
 

@@ -354,16 +354,17 @@ __device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2][
     }
 }
 
-/* Pre-pass of an element-matrix chunk (threads 0-95, one (slot, component)
- * each): the row's coefficients r * d v'/d u_{k,m} (m = 0..8) and its point,
- * so that the 288 build tasks read them instead of each evaluating the
- * variable gradient (which branches on the variable). */
+/* Pre-pass of an element-matrix chunk (every third builder thread, one (slot,
+ * component) each, so that the 96 items spread over the 9 builder warps): the
+ * row's coefficients r * d v'/d u_{k,m} (m = 0..8) and its point, so that the 288
+ * build tasks read them instead of each evaluating the variable gradient (which
+ * branches on the variable). */
 template <int TE>
 __device__ __forceinline__ void tc_prepass(tc_smem<TE> &S, int par, int bucket, int base, int cntb)
 {
     const int t = threadIdx.x;
-    if (t >= 3 * TC_KC) return;
-    const int j = t / 3, k = t % 3, slot = base + j;
+    if (t % 3 != 0 || t >= 9 * TC_KC) return;
+    const int it = t / 3, j = it / 3, k = it % 3, slot = base + j;
     float *gout = S.gk[par][j][k];
     if (slot < cntb) {
         const int id = S.map[bucket][slot], q = id / 12, v = id % 12;
@@ -529,10 +530,12 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         for (int ch = 0; ch < nch; ch++) {
             const int b = gc & 1;
             unsigned char *st = S.stage[b];
-            /* stage b holds chunk gc-2: wait for its MMAs; the barrier also publishes the pre-pass */
+            /* stage b holds chunk gc-2: one thread waits for its MMAs (their operand reads
+             * are complete once the commit arrives); the barrier passes that on to the
+             * other builders and also publishes the pre-pass */
             bool ok = true;
             if (pend[b]) {
-                ok = tc_mbar_wait_abortable(&S.done[b], ph[b], abort);
+                if (tid == 0) ok = tc_mbar_wait_abortable(&S.done[b], ph[b], abort);
                 ph[b] ^= 1u;
                 pend[b] = false;
             }
@@ -640,7 +643,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         for (int k = 0; k < 2 && !aborted; k++) {
             const int b = (gc + k) & 1;   /* chunk gc-2, then gc-1 */
             if (!pend[b]) continue;
-            const bool ok = tc_mbar_wait_abortable(&S.done[b], ph[b], abort);
+            const bool ok = tid == 0 ? tc_mbar_wait_abortable(&S.done[b], ph[b], abort) : true;
             ph[b] ^= 1u;
             pend[b] = false;
             if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) aborted = true;

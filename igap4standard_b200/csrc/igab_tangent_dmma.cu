@@ -201,7 +201,8 @@ __device__ __forceinline__ bool bld_acquire(dws_smem &S, int gb)
     const int b = gb % NSLOT, u = gb / NSLOT;
     const volatile int *abort = &S.abort_flag;
     bool ok = !*abort;
-    if (ok && u > 0) ok = tc_mbar_wait_abortable(&S.empty[b], (u - 1) & 1, abort);
+    /* one builder waits; the named barrier orders the others' slot writes after it */
+    if (ok && u > 0 && threadIdx.x == NCONS) ok = tc_mbar_wait_abortable(&S.empty[b], (u - 1) & 1, abort);
     return tc_bar_and(BAR_BLD, NBLD, ok);
 }
 
@@ -423,7 +424,8 @@ __device__ __forceinline__ bool cons_acquire(dws_smem &S, int gb)
     const int b = gb % NSLOT;
     const volatile int *abort = &S.abort_flag;
     bool ok = !*abort;
-    if (ok) ok = tc_mbar_wait_abortable(&S.full[b], (gb / NSLOT) & 1, abort);
+    /* one consumer waits; the named barrier orders the others' slot reads after it */
+    if (ok && threadIdx.x == 0) ok = tc_mbar_wait_abortable(&S.full[b], (gb / NSLOT) & 1, abort);
     return tc_bar_and(BAR_CONS, NCONS, ok);
 }
 

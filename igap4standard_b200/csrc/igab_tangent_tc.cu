@@ -669,13 +669,20 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         /* ---- symmetric part + Gamma on the k1 = k2 blocks, added into the CSR values
          * with fire-and-forget reductions (red.global.add): the tiles of one colour
          * touch disjoint entries and the elements of a tile are separated by a
-         * barrier, so every entry still receives its additions in a fixed order */
-        for (int idx = tid; idx < 81 * 81; idx += TCN_BLD) {
-            const int c1 = idx / 81, c2 = idx % 81;
-            const int a1 = c1 / 3, k1 = c1 % 3, a2 = c2 / 3, k2 = c2 % 3;
-            float v = 0.5f * (E[c1 * 81 + c2] + E[c2 * 81 + c1]);
-            if (k1 == k2) v += 0.5f * (Gm[a1 * 27 + a2] + Gm[a2 * 27 + a1]);
-            atomicAdd(&vals[S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9], v);
+         * barrier, so every entry still receives its additions in a fixed order.
+         * Thread (k1, c2), 243 of them, walks the rows c1 = 3 a1 + k1: the column's
+         * position terms and the Gamma test are per-thread constants. */
+        if (tid < 243) {
+            const int k1 = tid / 81, c2 = tid % 81, a2 = c2 / 3;
+            const bool gam = k1 == c2 % 3;
+            const int o2 = c2 / 27, p2 = (c2 / 9) % 3, z2 = c2 % 9;
+#pragma unroll 3
+            for (int a1 = 0; a1 < 27; a1++) {
+                const int c1 = 3 * a1 + k1;
+                float v = 0.5f * (E[c1 * 81 + c2] + E[c2 * 81 + c1]);
+                if (gam) v += 0.5f * (Gm[a1 * 27 + a2] + Gm[a2 * 27 + a1]);
+                atomicAdd(&vals[S.rbase[c1] + o2 * S.rsx[c1] + p2 * S.rsy[c1] + z2], v);
+            }
         }
         tc_bar_sync(TC_BAR_BLD, TCN_BLD);
     }

@@ -27,7 +27,9 @@
  * points (FP64), the point integrand (FP64, 64 threads) and sign buckets of
  * the 768 (point, variable) rows, then build chunks of 32 rows into a double-
  * buffered shared-memory stage (TF32 hi/lo in the K-major layout of
- * igab_tc.cuh) and hand each to the issuer through an mbarrier.  The issuer
+ * igab_tc.cuh; element-matrix column c sits at operand row tc_pos(c), so that a
+ * builder thread's 9 outputs are 1024 bytes apart) and hand each to the issuer
+ * through an mbarrier.  The issuer
  * runs 4 k-steps x 2 MMAs (M 128, N 96; negate-A for negative-curvature rows)
  * or x 3 (M 128, N 32, Gamma rows) per chunk and commits to the stage's
  * mbarrier, which frees the stage for the chunk after next.  An element
@@ -156,6 +158,14 @@ __device__ __forceinline__ void tc_grad_var(const float *p, int v, int k, float 
         g[0] = G[2] * is6; g[1] = G[4] * is6; g[2] = -2.f * G[5] * is6;
         g[5] = F0 * is6; g[7] = F1 * is6; g[8] = -2.f * F2 * is6;
     }
+}
+
+/* operand row of element-matrix column c = 3 a + k, a = 9 ax + g: 8 g + 3 k + ax, or
+ * 72 + g for k = ax = 2 (a bijection of 0..80 onto 0..80) */
+__device__ __forceinline__ int tc_pos(int c)
+{
+    const int a = c / 3, cb = 3 * (c % 3) + a / 9, g = a % 9;
+    return cb < 8 ? 8 * g + cb : 72 + g;
 }
 
 __device__ __forceinline__ void st_pair(unsigned char *hi_base, unsigned char *lo_base, uint32_t off, float y,
@@ -541,9 +551,16 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
             }
             if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) { aborted = true; break; }
             if (ch < cpos + cneg) {
-                /* main rows: task (slot j, component k, ax) -> 9 outputs (ay, az) */
+                /* main rows: task (slot j, component k, ax) -> 9 outputs (ay, az), column
+                 * c = 3 (9 ax + 3 ay + az) + k at operand row tc_pos(c): row 8 g + 3 k + ax
+                 * for g = 3 ay + az, or 72 + g for k = ax = 2, so the 9 stores sit at
+                 * off0 + g * step (+ adj at g = 8) */
                 const int par = ch & 1;
-                const int j = tid / 9, k = (tid / 3) % 3, ax = tid % 3;
+                const int j = tid / 9, k = (tid / 3) % 3, ax = tid % 3, cb = 3 * k + ax;
+                const uint32_t off0 = (uint32_t)((j >> 2) * TC_LBO + (j & 3) * 4) +
+                                      (cb < 8 ? (uint32_t)cb * 16u : 9u * TC_SBO);
+                const uint32_t step = cb < 8 ? (uint32_t)TC_SBO : 16u;
+                const uint32_t adj8 = cb < 8 ? 0u : (uint32_t)(TC_SBO - 128);
                 unsigned char *hi = st, *lo = st + TC_MAIN_LO;
                 const int q = S.qs[par][j];
                 if (q >= 0) {
@@ -568,19 +585,17 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
 #pragma unroll
                         for (int az = 0; az < 3; az++) {
                             const float y = cy0 * bz[3 * az] + cy1 * bz[3 * az + 1] + cy2 * bz[3 * az + 2];
-                            const int c = 3 * (9 * ax + 3 * ay + az) + k;
-                            st_pair(hi, lo, tc_off(c, j), y, 2.f);
+                            const int gg = 3 * ay + az;
+                            st_pair(hi, lo, off0 + (uint32_t)gg * step + (gg == 8 ? adj8 : 0u), y, 2.f);
                         }
                     }
                 } else {
 #pragma unroll
-                    for (int ay = 0; ay < 3; ay++)
-#pragma unroll
-                        for (int az = 0; az < 3; az++) {
-                            const uint32_t off = tc_off(3 * (9 * ax + 3 * ay + az) + k, j);
-                            *reinterpret_cast<float *>(hi + off) = 0.f;
-                            *reinterpret_cast<float *>(lo + off) = 0.f;
-                        }
+                    for (int gg = 0; gg < 9; gg++) {
+                        const uint32_t off = off0 + (uint32_t)gg * step + (gg == 8 ? adj8 : 0u);
+                        *reinterpret_cast<float *>(hi + off) = 0.f;
+                        *reinterpret_cast<float *>(lo + off) = 0.f;
+                    }
                 }
             } else {
                 /* Gamma rows: task (slot j, ax, ay) -> 3 outputs (az) of U and V */
@@ -671,17 +686,23 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
          * touch disjoint entries and the elements of a tile are separated by a
          * barrier, so every entry still receives its additions in a fixed order.
          * Thread (k1, c2), 243 of them, walks the rows c1 = 3 a1 + k1: the column's
-         * position terms and the Gamma test are per-thread constants. */
+         * position terms and the Gamma test are per-thread constants.  E is indexed by
+         * operand rows (tc_pos). */
         if (tid < 243) {
             const int k1 = tid / 81, c2 = tid % 81, a2 = c2 / 3;
+            const int q2 = tc_pos(c2);
             const bool gam = k1 == c2 % 3;
             const int o2 = c2 / 27, p2 = (c2 / 9) % 3, z2 = c2 % 9;
+#pragma unroll 1
+            for (int ax1 = 0; ax1 < 3; ax1++) {
+                const int cb = 3 * k1 + ax1, pb = cb < 8 ? cb : 72, ps = cb < 8 ? 8 : 1;
 #pragma unroll 3
-            for (int a1 = 0; a1 < 27; a1++) {
-                const int c1 = 3 * a1 + k1;
-                float v = 0.5f * (E[c1 * 81 + c2] + E[c2 * 81 + c1]);
-                if (gam) v += 0.5f * (Gm[a1 * 27 + a2] + Gm[a2 * 27 + a1]);
-                atomicAdd(&vals[S.rbase[c1] + o2 * S.rsx[c1] + p2 * S.rsy[c1] + z2], v);
+                for (int g1 = 0; g1 < 9; g1++) {
+                    const int a1 = 9 * ax1 + g1, c1 = 3 * a1 + k1, q1 = pb + ps * g1;
+                    float v = 0.5f * (E[q1 * 81 + q2] + E[q2 * 81 + q1]);
+                    if (gam) v += 0.5f * (Gm[a1 * 27 + a2] + Gm[a2 * 27 + a1]);
+                    atomicAdd(&vals[S.rbase[c1] + o2 * S.rsx[c1] + p2 * S.rsy[c1] + z2], v);
+                }
             }
         }
         tc_bar_sync(TC_BAR_BLD, TCN_BLD);

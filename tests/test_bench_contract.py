@@ -1,0 +1,44 @@
+"""The one-line JSON contract of bench.py's reference arm (`--impl reference`): the
+reference's own CPU assembly timed on a small sample and extrapolated, with the keys a
+driver reads (metric, value, unit, cpu_baseline, e2e with zero host copies).  Runs on
+CPU; the GPU arm is exercised by the GPU runs themselves."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_json_line(built):
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference library not built")
+    out = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0", "--cpu-sample", "2"], cwd=REPO, capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.strip().startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    for k in ("metric", "value", "unit", "steps", "warmup", "higher_is_better", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["unit"] == "ms" and d["higher_is_better"] is False and d["value"] > 0
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    e = d["e2e"]
+    assert e["value"] == d["value"] and e["unit"] == d["unit"]
+    assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+    assert d["config"]["nelem"] == [64, 64, 64]
+
+
+def test_reference_arm_other_ranks_exit_quietly(built):
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    out = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0", "--cpu-sample", "2"], cwd=REPO, capture_output=True, text=True,
+                         timeout=600, env=env)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert not [l for l in out.stdout.splitlines() if l.strip().startswith("{")]

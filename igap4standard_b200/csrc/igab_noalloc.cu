@@ -16,38 +16,31 @@
  *    holds the 16 MiB array until the process exits.
  *  - all calls share the one array; calls that overlap on the GPU (several
  *    host threads, or several contexts on one device at once) race.
- *  - the first call on a device looks up the array's device address
- *    (cudaGetSymbolAddress) and caches it; that first call should come
- *    before any stream capture.
+ *  - in host code the array's name only stands for it: its device address
+ *    belongs to the CUDA context that loaded this module, so every call looks
+ *    it up with cudaGetSymbolAddress on the context's device (a lookup, not an
+ *    allocation) instead of keeping it from an earlier call, which would go
+ *    stale after cudaDeviceReset or under another context.
  */
 #include <cuda_runtime.h>
 #include <math.h>
 #include "igab_internal.h"
 
 #define IGAB_NOALLOC_MAX_DOF (1L << 20)
-#define IGAB_NOALLOC_MAX_DEVICES 64
-
 /* staging: [0, MAX) holds U, [MAX, 2 MAX) holds R */
 static __device__ __align__(256) double g_noalloc_stage[2 * IGAB_NOALLOC_MAX_DOF];
 
-static double *g_stage_addr[IGAB_NOALLOC_MAX_DEVICES];
-
-static int stage_address(int device, double **out)
+/* device address of the staging array in the current context (the caller has
+ * made the context's device current) */
+static int stage_address(double **out)
 {
-    if (device < 0 || device >= IGAB_NOALLOC_MAX_DEVICES) {
-        igab_set_error("igab_residual_noalloc: device index %d out of range", device);
-        return IGAB_ERR_ARG;
+    double *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_stage);
+    if (e != cudaSuccess || !p) {
+        igab_set_error("igab_residual_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        return IGAB_ERR_CUDA;
     }
-    if (!g_stage_addr[device]) {
-        double *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_stage);
-        if (e != cudaSuccess) {
-            igab_set_error("igab_residual_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-            return IGAB_ERR_CUDA;
-        }
-        g_stage_addr[device] = p;
-    }
-    *out = g_stage_addr[device];
+    *out = p;
     return 0;
 }
 
@@ -68,7 +61,7 @@ extern "C" int igab_residual_noalloc(igab_ctx *ctx, const double *U_host, double
     }
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     double *stage = nullptr;
-    int rc = stage_address(ctx->device, &stage);
+    int rc = stage_address(&stage);
     if (rc) return rc;
     double *dU = stage;
     double *dR = stage + IGAB_NOALLOC_MAX_DOF;

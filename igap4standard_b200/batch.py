@@ -117,6 +117,12 @@ class Batch:
     def sync(self):
         check(self.lib, "igab_batch_sync", self.lib.igab_batch_sync(self.h))
 
+    def set_wait_limit(self, polls=0, unreachable=False):
+        """Poll limit of the colour-dependency wait (0 = default); unreachable=True makes
+        the waits on colour 0 of instance 0 run out (test switch of the give-up path)."""
+        check(self.lib, "igab_batch_set_wait_limit",
+              self.lib.igab_batch_set_wait_limit(self.h, int(polls), 1 if unreachable else 0))
+
     def last_launch_count(self):
         n = ctypes.c_int()
         check(self.lib, "igab_batch_last_launch_count", self.lib.igab_batch_last_launch_count(self.h, ctypes.byref(n)))

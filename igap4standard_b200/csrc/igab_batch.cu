@@ -48,6 +48,9 @@ struct igab_batch {
     /* schedule: CTAs per SM of the persistent kernels (0 = as many as fit), instance order */
     int ctas[3] = {0, 0, 0};
     int order = 0;
+    /* colour-dependency wait: poll limit, and the test switch that makes it run out */
+    long spin_limit = IGAB_BATCH_SPIN;
+    int hold = 0;
     int last_launches = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -150,6 +153,8 @@ igab_batch_dev dev_view(const igab_batch *b)
     B.dof_off = b->d_dof_off;
     B.nnz_off = b->d_nnz_off;
     B.status = b->d_status;
+    B.spin_limit = b->spin_limit;
+    B.hold = b->hold;
     return B;
 }
 
@@ -397,6 +402,14 @@ extern "C" int igab_batch_sync(igab_batch *b)
     IGAB_CUDA_TRY(cudaSetDevice(b->device));
     IGAB_CUDA_TRY(cudaStreamSynchronize(b->stream));
     return check_batch_status(b);
+}
+
+extern "C" int igab_batch_set_wait_limit(igab_batch *b, long polls, int unreachable)
+{
+    BATCH_CHECK(b && polls >= 0, "igab_batch_set_wait_limit: bad argument");
+    b->spin_limit = polls > 0 ? polls : IGAB_BATCH_SPIN;
+    b->hold = unreachable ? 1 : 0;
+    return 0;
 }
 
 extern "C" int igab_batch_last_launch_count(const igab_batch *b, int *n)

@@ -109,6 +109,28 @@ __device__ __forceinline__ double elem_scale(const igab_geom &g, int ex, int ey,
 /* ---- persistent batched launches: one work item (a tile of one instance) at a time */
 #define IGAB_BATCH_SPIN (1L << 22)   /* polls (with a 128 ns sleep) before a dependency wait gives up */
 
+/* one thread: wait until every colour before `colour` of instance `inst` is
+ * complete.  Each wait polls at most B.spin_limit times (128 ns sleep between
+ * polls), then sets bit 2 of the status word and moves on; B.hold raises the
+ * count that colour 0 of instance 0 must reach, so that the waits on it cannot
+ * finish (a host-set test switch that exercises the give-up path). */
+__device__ __forceinline__ void batch_wait_colours(const igab_batch_dev &B, int inst, int colour)
+{
+    int *done = B.done + 8 * inst;
+    const int *need = B.need + 8 * inst;
+    for (int c = 0; c < colour; c++) {
+        const int target = need[c] + (inst == 0 && c == 0 ? B.hold : 0);
+        long spins = 0;
+        while (atomicOr(&done[c], 0) < target) {
+            if (++spins > B.spin_limit) {
+                atomicOr(B.status, 2);
+                break;
+            }
+            __nanosleep(128);
+        }
+    }
+}
+
 struct batch_slot {
     igab_geom g;      /* geometry of the current item's instance */
     int item, inst, colour, tile;
@@ -127,18 +149,7 @@ __device__ __forceinline__ bool batch_next(const igab_batch_dev &B, batch_slot &
             sl.inst = w.x;
             sl.colour = w.y;
             sl.tile = w.z;
-            int *done = B.done + 8 * w.x;
-            const int *need = B.need + 8 * w.x;
-            for (int c = 0; c < w.y; c++) {
-                long spins = 0;
-                while (atomicOr(&done[c], 0) < need[c]) {
-                    if (++spins > IGAB_BATCH_SPIN) {
-                        atomicOr(B.status, 2);
-                        break;
-                    }
-                    __nanosleep(128);
-                }
-            }
+            batch_wait_colours(B, w.x, w.y);
             __threadfence();
         }
     }

@@ -104,3 +104,66 @@ def test_batch_config3_shapes(built):
     d0, d1 = B.dof_offsets[i], B.dof_offsets[i + 1]
     R1, _ = _single(dict(inst[i], par_periodic=np.zeros(9)), U[d0:d1], "fp64")
     assert np.array_equal(R[d0:d1], R1)
+
+
+@pytest.mark.parametrize("op", ["residual", "fp64", "fp32"])
+def test_batch_wait_gives_up_and_recovers(built, op):
+    """A colour-dependency wait that cannot finish (its target count is raised past
+    what the tiles publish) gives up after its poll limit: the launch ends,
+    igab_batch_sync reports status 2, and the next launch is correct again."""
+    import torch
+    from igap4standard_b200 import Batch
+    inst = _instances()[2:5]              # (4,4,4), (3,1,2), (6,5,7): several tiles per colour
+    B = Batch(inst)
+    U = np.random.default_rng(9).uniform(-1e-3, 1e-3, B.ndof)
+    ref = B.residual(U) if op == "residual" else B.tangent(U, op)
+    Ud = torch.as_tensor(U).cuda()
+    out = torch.zeros(ref.size, dtype=torch.float32 if op == "fp32" else torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    B.set_wait_limit(64, unreachable=True)
+    if op == "residual":
+        B.residual_device(Ud.data_ptr(), out.data_ptr())
+    else:
+        B.tangent_device(Ud.data_ptr(), out.data_ptr(), op)
+    rc = B.lib.igab_batch_sync(B.h)
+    assert rc == 2, "the unreachable wait did not report"
+    assert b"status 2" in B.lib.igab_last_error()
+    B.set_wait_limit(0, unreachable=False)
+    again = B.residual(U) if op == "residual" else B.tangent(U, op)
+    assert np.array_equal(again, ref)
+    B.close()
+
+
+@pytest.mark.slow
+def test_batch_config3_against_reference(built, checker):
+    """Batched results at the 512-instance workload's sizes (n^3, n in 6..24, each
+    instance with its own lambda, mu, l) against the reference's own CPU assembly:
+    the residual of every instance of an 8-instance draw, and the FP64 (entrywise
+    1e-12) and FP32 (rowwise 1e-5) tangents of its two 6^3 instances."""
+    from cases import residual_tolerance, tangent_tolerance
+    from igap4standard_b200 import Batch
+    inst = mesh.batch_config3(n_instances=8, seed=3)
+    B = Batch(inst)
+    U = np.random.default_rng(3).uniform(-1e-3, 1e-3, B.ndof)
+    R = B.residual(U)
+    V = B.tangent(U, "fp64")
+    W = B.tangent(U, "fp32").astype(np.float64)
+    small = [i for i, c in enumerate(inst) if c["nelem"][0] == 6]
+    assert len(small) == 2
+    for i, c in enumerate(inst):
+        d0, d1 = B.dof_offsets[i], B.dof_offsets[i + 1]
+        ref = checker("ge", c["nelem"], c["knots"], c["par_mat"], c["bc_type"], np.zeros(9),
+                      c["par_dirichlet"], np.zeros(39))
+        R_ref = ref.residual(U[d0:d1])
+        assert np.all(np.abs(R[d0:d1] - R_ref) <= residual_tolerance(R_ref)), "instance %d residual" % i
+        if i not in small:
+            continue
+        rp, cols, v_ref = ref.tangent(U[d0:d1])
+        z0, z1 = B.nnz_offsets[i], B.nnz_offsets[i + 1]
+        rp_b, cols_b = B.pattern(i)
+        assert np.array_equal(rp_b, rp) and np.array_equal(cols_b, cols)
+        assert np.all(np.abs(V[z0:z1] - v_ref) <= tangent_tolerance(rp, v_ref)), "instance %d FP64 tangent" % i
+        rowmax = np.maximum.reduceat(np.abs(v_ref), rp[:-1])
+        err = np.maximum.reduceat(np.abs(W[z0:z1] - v_ref), rp[:-1])
+        assert np.max(err / rowmax) <= 1e-5, "instance %d FP32 tangent" % i
+    B.close()

@@ -182,6 +182,31 @@ class Assembly:
                                          float(atol), int(maxit), ctypes.byref(info)))
         return info.iterations, bool(info.converged), info.residual_norm
 
+    def newton_solve_device(self, U_ptr, prec="fp64", ksp_rtol=1e-5, ksp_maxit=100000, abstol=1e-10,
+                            max_subiter=10000, verbose=False, history_cap=64):
+        """Device Newton solve (igab_newton_solve) from the state at U_ptr (device, FP64,
+        overwritten with the result).  Returns a dict of the solve info plus the ||F|| and
+        Krylov-iteration history of each subiteration."""
+        o = native.IgabNewtonOpts()
+        self.lib.igab_newton_defaults(ctypes.byref(o))
+        o.prec = PREC[prec]
+        o.ksp_rtol = float(ksp_rtol)
+        o.ksp_maxit = int(ksp_maxit)
+        o.abstol = float(abstol)
+        o.max_subiter = int(max_subiter)
+        o.verbose = 1 if verbose else 0
+        info = native.IgabNewtonInfo()
+        fh = np.zeros(history_cap)
+        kh = np.zeros(history_cap, dtype=np.int32)
+        check(self.lib, "igab_newton_solve",
+              self.lib.igab_newton_solve(self.h, vp(U_ptr), ctypes.byref(o), ctypes.byref(info), _ptr(fh), _ptr(kh),
+                                         int(history_cap)))
+        out = {f: getattr(info, f) for f, _ in native.IgabNewtonInfo._fields_}
+        m = min(out["iterations"] + 1, history_cap)
+        out["fnorms"] = fh[:m].tolist()
+        out["krylov"] = kh[:m].tolist()
+        return out
+
     def ndensity(self):
         n = ctypes.c_int()
         check(self.lib, "igab_ndensity", self.lib.igab_ndensity(self.h, ctypes.byref(n)))

@@ -11,6 +11,7 @@ than its sources.  ``python -m igap4standard_b200.build [--force]``.
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(PKG)
@@ -25,7 +26,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
 
 CUDA_SOURCES = ["igab_kernels.cu", "igab_tangent_dmma.cu", "igab_tangent_tc.cu", "igab_getime.cu", "igab_capi.cu",
                 "igab_batch.cu", "igab_autotune.cu", "igab_noalloc.cu", "igab_density.cu", "igab_krylov.cu",
-                "igab_refine.cu"]
+                "igab_refine.cu", "igab_newton.cu"]
 CUDA_HEADERS = ["igab_internal.h", "igab_math.cuh", "igab_device.cuh", "igab_warp_tiles8.inc", "igab_tc.cuh"]
 
 LIB_CUDA = os.path.join(LIBDIR, "libigap4_b200.so")
@@ -53,11 +54,9 @@ def build(force=False, verbose=False):
     # ---- CUDA library
     srcs = [os.path.join(CSRC, s) for s in CUDA_SOURCES]
     if force or _stale(LIB_CUDA, srcs + hdrs + [__file__]):
-        objs = []
-        for s in srcs:
-            o = os.path.join(LIBDIR, os.path.basename(s) + ".o")
-            _run([NVCC] + NVCC_FLAGS + ["-c", s, "-o", o])
-            objs.append(o)
+        objs = [os.path.join(LIBDIR, os.path.basename(s) + ".o") for s in srcs]
+        with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 4))) as ex:
+            list(ex.map(lambda so: _run([NVCC] + NVCC_FLAGS + ["-c", so[0], "-o", so[1]]), zip(srcs, objs)))
         _run([NVCC] + ARCH + ["-shared", "-o", LIB_CUDA] + objs)
         for o in objs:
             os.remove(o)

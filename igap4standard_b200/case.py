@@ -93,6 +93,14 @@ class Case:
         a = np.ascontiguousarray(pm, dtype=np.float64)
         self.lib.iga_case_set_par_mat(self.h, _p(a))
 
+    def solve(self, U0):
+        """The linked library's snes_solve from U0; returns (converged, U)."""
+        U = np.array(U0, dtype=np.float64, copy=True)
+        rc = self.lib.iga_case_solve(self.h, _p(U))
+        if rc < 0:
+            raise RuntimeError("no snes_solve in this library")
+        return rc == 0, U
+
     @property
     def app(self):
         return self.lib.iga_case_app(self.h)

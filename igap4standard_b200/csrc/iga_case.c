@@ -25,6 +25,8 @@ extern void ge_density(double *, double *, double *) __attribute__((weak));
 extern void ge_densityb(double *, double *, double, double *, int) __attribute__((weak));
 extern void getime_density(double *, double *, double *) __attribute__((weak));
 extern void getime_densityb(double *, double *, double, double *, int) __attribute__((weak));
+/* the solver loop (present in libsnesiga_b200: the device Newton solve) */
+extern void snes_solve(void *snesassmbl_) __attribute__((weak));
 /* subset-only error latches (weak: absent under a real PETSc) */
 extern int petsc_subset_mat_error(Mat A) __attribute__((weak));
 extern int petsc_subset_vec_error(Vec v) __attribute__((weak));
@@ -257,3 +259,18 @@ int iga_case_tangent_csr(const iga_case *c, int *rowptr, int *cols, double *vals
 void *iga_case_app(iga_case *c) { return &c->app; }
 void *iga_case_iocomm(iga_case *c) { return &c->io; }
 void *iga_case_snesassmbl(iga_case *c) { return &c->sa; }
+
+int iga_case_solve(iga_case *c, double *U)
+{
+    if (!snes_solve) return -1;
+    PetscScalar *u;
+    VecGetArray(c->sa.U, &u);
+    memcpy(u, U, (size_t)c->ndof * sizeof(double));
+    VecRestoreArray(c->sa.U, &u);
+    c->sa.converged = 0;
+    snes_solve(&c->sa);
+    VecGetArray(c->sa.U, &u);
+    memcpy(U, u, (size_t)c->ndof * sizeof(double));
+    VecRestoreArray(c->sa.U, &u);
+    return c->sa.converged ? 0 : 1;
+}

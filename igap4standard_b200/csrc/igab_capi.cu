@@ -332,6 +332,7 @@ static void free_ctx(igab_ctx *c)
     cudaFree(c->d_escale); cudaFree(c->d_lam); cudaFree(c->d_status);
     cudaFree(c->d_dens_part); cudaFree(c->d_HH);
     igab_krylov_release(c);
+    igab_newton_release(c);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     for (int k = 0; k < 6; k++)
@@ -350,6 +351,9 @@ extern "C" int igab_create(const igab_mesh_desc *desc, int device, igab_ctx **ou
     ARG_CHECK(desc->phys == IGAB_PHYS_GE || desc->phys == IGAB_PHYS_GETIME, "igab_create: unknown physics");
     ARG_CHECK(desc->knots, "igab_create: knots missing");
     for (int d = 0; d < 3; d++) ARG_CHECK(desc->nelem[d] >= 1, "igab_create: nelem must be >= 1");
+    /* the reference reads bc_type as 0 (Dirichlet) or 1 (Neumann) only (include/bc.h:6) */
+    for (int i = 0; i < 36; i++)
+        ARG_CHECK(desc->bc_type[i] == 0 || desc->bc_type[i] == 1, "igab_create: bc_type entries must be 0 or 1");
     long ncp = 1;
     for (int d = 0; d < 3; d++) ncp *= desc->nelem[d] + 2;
     ARG_CHECK(3 * ncp < 2147483647L, "igab_create: dof count exceeds int32");
@@ -623,6 +627,35 @@ extern "C" int igab_device_buffers(igab_ctx *ctx, double **U_dev, double **R_dev
     if (U_dev) *U_dev = ctx->d_U;
     if (R_dev) *R_dev = ctx->d_R;
     if (vals_dev) *vals_dev = ctx->d_vals;
+    return 0;
+}
+
+extern "C" int igab_upload(igab_ctx *ctx, const double *host, double *dev, long n)
+{
+    ARG_CHECK(ctx && host && dev && n >= 0, "igab_upload: bad argument");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    IGAB_CUDA_TRY(cudaMemcpyAsync(dev, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+extern "C" int igab_download(igab_ctx *ctx, const double *dev, double *host, long n)
+{
+    ARG_CHECK(ctx && host && dev && n >= 0, "igab_download: bad argument");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    IGAB_CUDA_TRY(cudaMemcpyAsync(host, dev, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+extern "C" int igab_staging_bytes(const igab_ctx *ctx, size_t *bytes)
+{
+    ARG_CHECK(ctx && bytes, "igab_staging_bytes: null argument");
+    size_t b = 0;
+    if (ctx->d_U) b += (size_t)ctx->ndof * sizeof(double);
+    if (ctx->d_R) b += (size_t)ctx->ndof * sizeof(double);
+    if (ctx->d_vals) b += (size_t)ctx->nnz * (ctx->vals_prec == IGAB_PREC_FP64 ? sizeof(double) : sizeof(float));
+    *bytes = b;
     return 0;
 }
 

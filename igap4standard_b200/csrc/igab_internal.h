@@ -57,6 +57,8 @@ struct igab_batch_dev {
     const long *dof_off;   /* [n] offsets of the instances in U / R */
     const long *nnz_off;   /* [n] offsets in the CSR values */
     int *status;           /* bit 1: a dependency wait gave up */
+    long spin_limit;       /* polls before a dependency wait gives up */
+    int hold;              /* added to need[0] of instance 0 (test switch; 0 in normal use) */
 };
 
 #define IGAB_MAX_SLABS 32   /* x-slabs of the host-pointer tangent */
@@ -137,6 +139,12 @@ struct igab_ctx {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t slab_ev[IGAB_MAX_SLABS] = {};
 
+    /* device Newton solve (igab_newton.cu): F, G, Y, J Y, W and reduction scratch; tangent values */
+    double *d_nl = nullptr;
+    double *h_nl = nullptr;            /* pinned, 2 doubles */
+    void *d_nl_vals = nullptr;
+    size_t nl_vals_bytes = 0;
+
     /* captured assembly graph */
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -153,6 +161,7 @@ int igab_launch_spmv(igab_ctx *c, const void *dvals, int prec, const double *dx,
 int igab_krylov_solve(igab_ctx *c, const void *dvals, int prec, const double *db, double *dx, double rtol,
                       double atol, int maxit, int *iterations, int *converged, double *rnorm, double *bnorm);
 void igab_krylov_release(igab_ctx *c);
+void igab_newton_release(igab_ctx *c);   /* igab_newton.cu */
 int igab_launch_tangent(igab_ctx *c, const double *dU, void *dvals, int prec);
 /* the same, slab by slab along x: after slab i, rows [0, row_end[i]) are final and
  * c->slab_ev[i] is recorded on c->stream (one slab when the kernels have no x-range) */

@@ -1,0 +1,402 @@
+/*
+ * Newton solve on the device: the reference application's solver loop
+ * (src/snes_solve.c:10-36) with the SNES configuration of src/snes_init.c:8-47,
+ * driving the GPU assembly without moving a residual or a tangent to the host.
+ *
+ * The loop repeats one-step Newton solves (SNESSetTolerances(abstol 1e-10,
+ * rtol 1e-20, stol 1e-20, max_it 1), src/snes_init.c:18) until the reason is
+ * not "max iterations"; it also stops when ||F|| stagnates, |F_old - F_new| /
+ * F_old < 1e-6 with F_old = 999 before the first pass (src/snes_solve.c:28-32).
+ * One step (SNESNEWTONLS, src/snes_init.c:19):
+ *   F = R(X); stop if ||F|| < abstol; J = K(X) (Dirichlet rows and columns
+ *   zeroed, unit diagonal, as the tangent callback leaves it); J Y = F by the
+ *   device Krylov solve (igab_krylov_solve, stands in for PETSc's KSP);
+ *   backtracking line search of cubic order along X - lambda Y
+ *   (SNESLINESEARCHBT, src/snes_init.c:21-22).
+ * The line search is the algorithm of Dennis and Schnabel, "Numerical Methods
+ * for Unconstrained Optimization and Nonlinear Equations" (1983), A6.3.1: a
+ * full step, then a quadratic backtrack, then cubic ones, each new lambda held
+ * in [0.1, 0.5] of the previous one, sufficient decrease with alpha = 1e-4,
+ * minimum lambda 1e-12, steps longer than 1e8 scaled down, the initial slope
+ * -(F, J Y) forced negative.
+ *
+ * Vectors live on the device; every norm and dot product is a fixed-order
+ * two-pass reduction (per-block partial sums over a fixed grid, then one block),
+ * so a solve is bitwise repeatable.  The host holds only the scalars of the
+ * line search and the convergence tests.
+ */
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cuda_runtime.h>
+#include "igab_internal.h"
+
+namespace {
+
+#define NL_THREADS 256
+#define NL_BLOCKS 296   /* 2 x 148 SMs */
+
+constexpr double NL_F_OLD0 = 999.0;   /* src/snes_solve.c:22 */
+
+/* partial sums of (a0, b0) [and (a1, b1)] per block, fixed order */
+__global__ void __launch_bounds__(NL_THREADS) k_nl_dot(long n, const double *__restrict__ a0,
+                                                       const double *__restrict__ b0, const double *__restrict__ a1,
+                                                       const double *__restrict__ b1, double *part)
+{
+    double s0 = 0.0, s1 = 0.0;
+    for (long i = blockIdx.x * (long)NL_THREADS + threadIdx.x; i < n; i += (long)NL_BLOCKS * NL_THREADS) {
+        s0 += a0[i] * b0[i];
+        if (a1) s1 += a1[i] * b1[i];
+    }
+    __shared__ double red[2][NL_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    }
+    if (lane == 0) {
+        red[0][warp] = s0;
+        red[1][warp] = s1;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double s = 0.0;
+        for (int w = 0; w < NL_THREADS / 32; w++) s += red[threadIdx.x][w];
+        part[threadIdx.x * NL_BLOCKS + blockIdx.x] = s;
+    }
+}
+
+/* one block: out[k] = sum of part[k][0..NL_BLOCKS) in a fixed order */
+__global__ void __launch_bounds__(NL_THREADS) k_nl_finish(const double *part, double *out)
+{
+    __shared__ double red[2][NL_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < 2; k++) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < NL_BLOCKS; b += NL_THREADS) s += part[k * NL_BLOCKS + b];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) red[k][warp] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double s = 0.0;
+        for (int w = 0; w < NL_THREADS / 32; w++) s += red[threadIdx.x][w];
+        out[threadIdx.x] = s;
+    }
+}
+
+/* W = X - lam Y */
+__global__ void k_nl_step(long n, const double *__restrict__ X, const double *__restrict__ Y, double lam,
+                          double *__restrict__ W)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        W[i] = X[i] - lam * Y[i];
+}
+
+/* Y *= s */
+__global__ void k_nl_scale(long n, double *__restrict__ Y, double s)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) Y[i] *= s;
+}
+
+struct nl_work {
+    igab_ctx *c;
+    long n;
+    double *F, *G, *Y, *JY, *W;   /* residual at X, at the trial point, step, J Y, trial point */
+    double *part, *dots;          /* reduction scratch (device) */
+    double *h_dots;               /* pinned host copy of dots[2] */
+    void *vals;
+    int prec;
+    int launches;
+
+    /* (a0, b0) [and (a1, b1)] on the device, both results on the host */
+    int dot(const double *a0, const double *b0, const double *a1, const double *b1, double out[2])
+    {
+        k_nl_dot<<<NL_BLOCKS, NL_THREADS, 0, c->stream>>>(n, a0, b0, a1, b1, part);
+        k_nl_finish<<<1, NL_THREADS, 0, c->stream>>>(part, dots);
+        launches += 2;
+        IGAB_CUDA_TRY(cudaGetLastError());
+        IGAB_CUDA_TRY(cudaMemcpyAsync(h_dots, dots, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        IGAB_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        out[0] = h_dots[0];
+        out[1] = h_dots[1];
+        return 0;
+    }
+    int norm(const double *a, double *out)
+    {
+        double d[2];
+        int rc = dot(a, a, nullptr, nullptr, d);
+        *out = std::sqrt(d[0]);
+        return rc;
+    }
+    void step(const double *X, double lam, double *Wout)
+    {
+        k_nl_step<<<NL_BLOCKS, NL_THREADS, 0, c->stream>>>(n, X, Y, lam, Wout);
+        launches++;
+    }
+};
+
+using clk = std::chrono::steady_clock;
+double ms_since(clk::time_point t0)
+{
+    return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+}
+
+struct nl_counters {
+    int nres = 0, ntan = 0;
+    long kits = 0;
+    double ms_res = 0.0, ms_tan = 0.0, ms_ksp = 0.0;
+};
+
+/* F = R(X) and ||F|| */
+int eval_residual(nl_work &w, const double *X, double *F, double *fnorm, nl_counters &k)
+{
+    const auto t0 = clk::now();
+    int rc = igab_launch_residual(w.c, X, F);
+    w.launches += w.c->last_launches;
+    if (!rc) rc = w.norm(F, fnorm);
+    k.nres++;
+    k.ms_res += ms_since(t0);
+    return rc;
+}
+
+/* backtracking line search along X - lambda Y (the caller has J Y in w.JY).
+ * On return w.W holds the accepted point and w.G its residual. */
+int line_search(nl_work &w, const double *X, double fnorm, double &gnorm, double &lam, bool &ok, nl_counters &k)
+{
+    const double alpha = 1e-4, minlambda = 1e-12, maxstep = 1e8;
+    const int max_its = 40;
+    double d[2];
+    int rc = w.norm(w.Y, &d[0]);
+    if (rc) return rc;
+    const double ynorm = d[0];
+    if (ynorm > maxstep) {
+        k_nl_scale<<<NL_BLOCKS, NL_THREADS, 0, w.c->stream>>>(w.n, w.Y, maxstep / ynorm);
+        k_nl_scale<<<NL_BLOCKS, NL_THREADS, 0, w.c->stream>>>(w.n, w.JY, maxstep / ynorm);
+        w.launches += 2;
+    }
+    if ((rc = w.dot(w.F, w.JY, nullptr, nullptr, d))) return rc;
+    double initslope = d[0];
+    if (initslope > 0.0) initslope = -initslope;
+    if (initslope == 0.0) initslope = -1.0;
+    const double f2 = fnorm * fnorm;
+    auto accept = [&](double gn, double l) { return std::isfinite(gn) && 0.5 * gn * gn <= 0.5 * f2 + l * alpha * initslope; };
+    lam = 1.0;
+    w.step(X, lam, w.W);
+    if ((rc = eval_residual(w, w.W, w.G, &gnorm, k))) return rc;
+    if (!std::isfinite(gnorm)) {
+        ok = false;
+        return 0;
+    }
+    if (accept(gnorm, lam)) {
+        ok = true;
+        return 0;
+    }
+    /* quadratic first backtrack */
+    double lamtemp = -initslope / (gnorm * gnorm - f2 - 2.0 * lam * initslope);
+    lamtemp = std::min(lamtemp, 0.5 * lam);
+    lam = lamtemp <= 0.1 * lam ? 0.1 * lam : lamtemp;
+    w.step(X, lam, w.W);
+    double gprev = gnorm, lamprev = 1.0;
+    if ((rc = eval_residual(w, w.W, w.G, &gnorm, k))) return rc;
+    if (accept(gnorm, lam)) {
+        ok = true;
+        return 0;
+    }
+    /* cubic backtracks */
+    for (int it = 0; it < max_its; it++) {
+        if (lam <= minlambda) break;
+        const double t1 = 0.5 * (gnorm * gnorm - f2) - lam * initslope;
+        const double t2 = 0.5 * (gprev * gprev - f2) - lamprev * initslope;
+        const double a = (t1 / (lam * lam) - t2 / (lamprev * lamprev)) / (lam - lamprev);
+        const double b = (-lamprev * t1 / (lam * lam) + lam * t2 / (lamprev * lamprev)) / (lam - lamprev);
+        const double disc = std::max(b * b - 3.0 * a * initslope, 0.0);
+        lamtemp = a == 0.0 ? -initslope / (2.0 * b) : (-b + std::sqrt(disc)) / (3.0 * a);
+        lamprev = lam;
+        gprev = gnorm;
+        lamtemp = std::min(lamtemp, 0.5 * lam);
+        lam = lamtemp <= 0.1 * lam ? 0.1 * lam : lamtemp;
+        w.step(X, lam, w.W);
+        if ((rc = eval_residual(w, w.W, w.G, &gnorm, k))) return rc;
+        if (accept(gnorm, lam)) {
+            ok = true;
+            return 0;
+        }
+    }
+    ok = false;
+    return 0;
+}
+
+} /* namespace */
+
+void igab_newton_release(igab_ctx *c)
+{
+    cudaFree(c->d_nl);
+    cudaFree(c->d_nl_vals);
+    cudaFreeHost(c->h_nl);
+    c->d_nl = nullptr;
+    c->d_nl_vals = nullptr;
+    c->h_nl = nullptr;
+    c->nl_vals_bytes = 0;
+}
+
+extern "C" void igab_newton_defaults(igab_newton_opts *o)
+{
+    if (!o) return;
+    o->prec = IGAB_PREC_FP64;
+    o->abstol = 1e-10;
+    o->rtol = 1e-20;
+    o->stol = 1e-20;
+    o->stagnation = 1e-6;
+    o->max_subiter = 10000;
+    o->ksp_rtol = 1e-5;
+    o->ksp_maxit = 100000;
+    o->verbose = 0;
+}
+
+extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton_opts *opts, igab_newton_info *info,
+                                 double *fnorm_history, int *krylov_history, int history_cap)
+{
+    if (!ctx || !U_dev || !opts || !info) {
+        igab_set_error("igab_newton_solve: null argument");
+        return IGAB_ERR_ARG;
+    }
+    if ((opts->prec != IGAB_PREC_FP64 && opts->prec != IGAB_PREC_FP32) || opts->max_subiter < 1 ||
+        opts->ksp_maxit < 1 || !(opts->ksp_rtol >= 0.0) || !(opts->abstol >= 0.0)) {
+        igab_set_error("igab_newton_solve: bad options");
+        return IGAB_ERR_ARG;
+    }
+    if (history_cap < 0 || (history_cap > 0 && !fnorm_history && !krylov_history)) {
+        igab_set_error("igab_newton_solve: bad history buffers");
+        return IGAB_ERR_ARG;
+    }
+    if (!ctx->stream) {
+        igab_set_error("igab_newton_solve: needs a non-default stream (igab_set_stream)");
+        return IGAB_ERR_ARG;
+    }
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    const auto t_start = clk::now();
+    const long n = ctx->ndof;
+    const size_t es = opts->prec == IGAB_PREC_FP64 ? sizeof(double) : sizeof(float);
+    if (!ctx->d_nl) IGAB_CUDA_TRY(cudaMalloc((void **)&ctx->d_nl, ((size_t)5 * n + 2 * NL_BLOCKS + 2) * sizeof(double)));
+    if (!ctx->h_nl) IGAB_CUDA_TRY(cudaMallocHost((void **)&ctx->h_nl, 2 * sizeof(double)));
+    if (ctx->nl_vals_bytes < (size_t)ctx->nnz * es) {
+        cudaFree(ctx->d_nl_vals);
+        ctx->d_nl_vals = nullptr;
+        ctx->nl_vals_bytes = 0;
+        IGAB_CUDA_TRY(cudaMalloc(&ctx->d_nl_vals, (size_t)ctx->nnz * es));
+        ctx->nl_vals_bytes = (size_t)ctx->nnz * es;
+    }
+    nl_work w;
+    w.c = ctx;
+    w.n = n;
+    w.F = ctx->d_nl;
+    w.G = w.F + n;
+    w.Y = w.G + n;
+    w.JY = w.Y + n;
+    w.W = w.JY + n;
+    w.part = w.W + n;
+    w.dots = w.part + 2 * NL_BLOCKS;
+    w.h_dots = ctx->h_nl;
+    w.vals = ctx->d_nl_vals;
+    w.prec = opts->prec;
+    w.launches = 0;
+
+    nl_counters k;
+    double *X = U_dev;
+    double f_old = NL_F_OLD0, fnorm = 0.0;
+    int reason = IGAB_SNES_DIVERGED_MAX_IT, its = 0, rc = 0;
+    for (int sub = 0; sub < opts->max_subiter; sub++) {
+        /* one SNESSolve with max_it = 1 */
+        int kits = 0;
+        if ((rc = eval_residual(w, X, w.F, &fnorm, k))) return rc;
+        if (!std::isfinite(fnorm)) {
+            reason = IGAB_SNES_DIVERGED_FNORM_NAN;
+        } else if (fnorm < opts->abstol) {
+            reason = IGAB_SNES_CONVERGED_FNORM_ABS;
+        } else {
+            const double ttol = fnorm * opts->rtol;
+            auto t0 = clk::now();
+            rc = igab_launch_tangent(ctx, X, w.vals, w.prec);
+            w.launches += ctx->last_launches;
+            if (!rc) {
+                cudaError_t e = cudaStreamSynchronize(ctx->stream);
+                if (e != cudaSuccess) {
+                    igab_set_error("igab_newton_solve: tangent: %s", cudaGetErrorString(e));
+                    return IGAB_ERR_CUDA;
+                }
+            }
+            if (rc) return rc;
+            k.ntan++;
+            k.ms_tan += ms_since(t0);
+            t0 = clk::now();
+            int conv = 0;
+            double rn = 0.0, bn = 0.0;
+            rc = igab_krylov_solve(ctx, w.vals, w.prec, w.F, w.Y, opts->ksp_rtol, 0.0, opts->ksp_maxit, &kits, &conv,
+                                   &rn, &bn);
+            w.launches += ctx->last_launches;
+            if (rc) return rc;
+            k.kits += kits;
+            k.ms_ksp += ms_since(t0);
+            /* J Y with the Jacobian of the solve (line-search slope) */
+            if ((rc = igab_launch_spmv(ctx, w.vals, w.prec, w.Y, w.JY))) return rc;
+            w.launches++;
+            double xn = 0.0;
+            if ((rc = w.norm(X, &xn))) return rc;
+            double gnorm = 0.0, lam = 1.0;
+            bool ok = false;
+            if ((rc = line_search(w, X, fnorm, gnorm, lam, ok, k))) return rc;
+            /* the accepted (or last tried) point becomes the iterate, as in SNESNEWTONLS */
+            IGAB_CUDA_TRY(cudaMemcpyAsync(X, w.W, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+            double *t = w.F;
+            w.F = w.G;
+            w.G = t;
+            fnorm = gnorm;
+            its++;
+            double yn = 0.0;
+            if ((rc = w.norm(w.Y, &yn))) return rc;
+            const double snorm = lam * yn;
+            if (!ok)
+                reason = IGAB_SNES_DIVERGED_LINE_SEARCH;
+            else if (!std::isfinite(fnorm))
+                reason = IGAB_SNES_DIVERGED_FNORM_NAN;
+            else if (fnorm < opts->abstol)
+                reason = IGAB_SNES_CONVERGED_FNORM_ABS;
+            else if (fnorm <= ttol)
+                reason = IGAB_SNES_CONVERGED_FNORM_RELATIVE;
+            else if (snorm < opts->stol * xn)
+                reason = IGAB_SNES_CONVERGED_SNORM_RELATIVE;
+            else
+                reason = IGAB_SNES_DIVERGED_MAX_IT;
+        }
+        /* src/snes_solve.c:28-32: stagnation ends the loop */
+        if (std::fabs(f_old - fnorm) / f_old < opts->stagnation) reason = IGAB_SNES_DIVERGED_LINE_SEARCH;
+        f_old = fnorm;
+        if (sub < history_cap) {
+            if (fnorm_history) fnorm_history[sub] = fnorm;
+            if (krylov_history) krylov_history[sub] = kits;
+        }
+        if (opts->verbose) {
+            printf("%6d: Fnorm = %e, #lin.ite.= %6d, (%08.2f[min])\n", sub + 1, fnorm, kits,
+                   ms_since(t_start) / 60000.0);
+            fflush(stdout);
+        }
+        if (reason != IGAB_SNES_DIVERGED_MAX_IT) break;
+    }
+    IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    info->iterations = its;
+    info->reason = reason;
+    info->converged = reason > 0;
+    info->krylov_iterations = k.kits;
+    info->n_residual = k.nres;
+    info->n_tangent = k.ntan;
+    info->fnorm = fnorm;
+    info->ms_residual = k.ms_res;
+    info->ms_tangent = k.ms_tan;
+    info->ms_krylov = k.ms_ksp;
+    info->ms_total = ms_since(t_start);
+    info->launches = w.launches;
+    return 0;
+}

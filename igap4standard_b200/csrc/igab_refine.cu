@@ -248,6 +248,14 @@ extern "C" int igab_read_solution(const char *fname, double *U_hist, long ndof, 
         return IGAB_ERR_ARG;
     }
     const size_t n = (size_t)(ihist1 - ihist0) * (size_t)ndof;
+    /* a short file is an error before anything is read: the caller's array stays as it was */
+    long bytes = -1;
+    if (fseek(f, 0, SEEK_END) == 0) bytes = ftell(f);
+    if (bytes < 0 || (size_t)bytes < n * sizeof(double) || fseek(f, 0, SEEK_SET) != 0) {
+        fclose(f);
+        igab_set_error("igab_read_solution: %s holds fewer than %zu values", fname, n);
+        return IGAB_ERR_ARG;
+    }
     const size_t r = fread(U_hist + (size_t)ihist0 * ndof, sizeof(double), n, f);
     fclose(f);
     if (r != n) {

@@ -86,6 +86,8 @@ struct dws_smem {
     double pt[IGAB_NQ3 * PT_N];      /* point data of the element being built */
     double AC[972 + 864];            /* interpolation scratch */
     double gam[32 * 32];             /* upper tiles of Gamma at the end of an element */
+    double kst[66 * 64];             /* the element matrix staged for the deferred scatter: upper 8x8
+                                        tiles of the 88x88 matrix, tile (bi, bj) at kst_tile(bi, bj) */
     double U[TCP * TCP * TCP * 3];   /* displacements of the tile's control points */
     double tab[3][TE][IGAB_TAB1D];
     double wh[3][TE][IGAB_NQ];
@@ -147,6 +149,7 @@ struct src_colour {
         R.inst = 0;
     }
     __device__ void done(const dws_tile &) const {}
+    static constexpr bool publishes_tiles = false;   /* tiles of one colour: disjoint entries */
 };
 
 /* the batched work list: items (instance, colour, tile) in colour-major order;
@@ -164,18 +167,7 @@ struct src_batch {
             return;
         }
         const int4 w = B.items[it];
-        int *done = B.done + 8 * w.x;
-        const int *need = B.need + 8 * w.x;
-        for (int c = 0; c < w.y; c++) {
-            long spins = 0;
-            while (atomicOr(&done[c], 0) < need[c]) {
-                if (++spins > IGAB_BATCH_SPIN) {
-                    atomicOr(B.status, 2);
-                    break;
-                }
-                __nanosleep(128);
-            }
-        }
+        batch_wait_colours(B, w.x, w.y);
         __threadfence();
         R.g = B.geoms[w.x];
         R.U = U + B.dof_off[w.x];
@@ -191,6 +183,7 @@ struct src_batch {
         tc_bar_sync(BAR_CONS, NCONS);
         if (threadIdx.x == 0) atomicAdd(&B.done[8 * R.inst + R.colour], 1);
     }
+    static constexpr bool publishes_tiles = true;    /* later colours wait on the finished count */
 };
 
 /* ---------------------------------------------------------------- builders */
@@ -481,42 +474,52 @@ __device__ __forceinline__ long csr_at(const dws_smem &S, int c1, int c2)
     return S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9;
 }
 
-/* the warp's K tiles plus Gamma on the diagonal component blocks, reduced into
- * the CSR values; entry (c1, c2) and its mirror (c2, c1) receive the upper value */
+/* index of upper tile (bi, bj), bi <= bj < 11, in the staged element matrix */
+__device__ __forceinline__ int kst_tile(int bi, int bj)
+{
+    return bi * 11 - (bi * (bi - 1)) / 2 + (bj - bi);
+}
+
+/* the warp's K tiles into the staging buffer (Gamma goes to S.gam separately) */
 template <int W>
-__device__ __forceinline__ void warp_scatter8(double *__restrict__ vals, const dws_smem &S, int lane,
-                                              const cons_acc<W> &a)
+__device__ __forceinline__ void warp_stage8(dws_smem &S, int lane, const cons_acc<W> &a)
 {
     using WT = warp_tiles8<W>;
     const int r = lane >> 2, c = 2 * (lane & 3);
 #pragma unroll
     for (int t = 0; t < WT::NT; t++) {
-        const int bi = WT::blk(WT::ti(t)), bj = WT::blk(WT::tj(t));
-        double v2[2] = {a.k[t][0], a.k[t][1]};
-        if (bi == bj) {
-            /* diagonal tile: entry (r, c + e) below the diagonal takes (c + e, r),
-             * held by lane 4 (c + e) + r / 2, element r & 1 */
-            const double x0 = __shfl_sync(0xffffffffu, a.k[t][0], 4 * c + (r >> 1));
-            const double y0 = __shfl_sync(0xffffffffu, a.k[t][1], 4 * c + (r >> 1));
-            const double x1 = __shfl_sync(0xffffffffu, a.k[t][0], 4 * (c + 1) + (r >> 1));
-            const double y1 = __shfl_sync(0xffffffffu, a.k[t][1], 4 * (c + 1) + (r >> 1));
-            if (r > c) v2[0] = (r & 1) ? y0 : x0;
-            if (r > c + 1) v2[1] = (r & 1) ? y1 : x1;
-        }
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-            const int c1 = 8 * bi + r, c2 = 8 * bj + c + e;
-            if (c1 < 81 && c2 < 81) {
-                const int a1 = c1 / 3, a2 = c2 / 3;
-                double v = v2[e];
-                if (c1 % 3 == c2 % 3) v += a1 <= a2 ? S.gam[a1 * 32 + a2] : S.gam[a2 * 32 + a1];
-                red_add(vals + csr_at(S, c1, c2), v);
-                if (bi != bj) red_add(vals + csr_at(S, c2, c1), v);
-            }
-        }
+        double *d = S.kst + kst_tile(WT::blk(WT::ti(t)), WT::blk(WT::tj(t))) * 64 + r * 8 + c;
+        d[0] = a.k[t][0];
+        d[1] = a.k[t][1];
     }
 }
 
+#define KST_ENTRIES (81 * 81)
+#define KST_PARTS ((KST_ENTRIES + NCONS - 1) / NCONS)   /* 26 parts of NCONS entries */
+
+/* part p of the staged element's scatter: entries i = p NCONS + tid of the 81 x 81
+ * matrix, (c1, c2) = (i / 81, i % 81), each taking the upper value K(min, max), plus
+ * Gamma(min, max) on the diagonal component blocks (c1 = c2 mod 3), reduced into the
+ * CSR values.  Every entry of the element receives exactly one reduction. */
+__device__ __forceinline__ void kst_scatter_part(double *__restrict__ vals, const dws_smem &S, int p, int tid)
+{
+    const int i = p * NCONS + tid;
+    if (i >= KST_ENTRIES) return;
+    const int c1 = i / 81, c2 = i % 81;
+    const int lo = c1 < c2 ? c1 : c2, hi = c1 < c2 ? c2 : c1;
+    double v = S.kst[kst_tile(lo >> 3, hi >> 3) * 64 + (lo & 7) * 8 + (hi & 7)];
+    if (c1 % 3 == c2 % 3) v += S.gam[(lo / 3) * 32 + hi / 3];
+    red_add(vals + csr_at(S, c1, c2), v);
+}
+
+/* The consumers.  Per element: the 16 batches of DMMA products with the accumulators in
+ * registers; then (after a consumer barrier) the accumulators, Gamma and the element's
+ * CSR row bases are staged in shared memory, and the element is reduced into the CSR
+ * values during the next element's batches (two parts of 256 entries after each batch),
+ * so the reductions overlap the DMMAs.  The barrier before staging also orders every
+ * reduction of an element before any of the next one: per-entry order stays fixed.
+ * The staged element is flushed at the end of the work, and at the end of every tile
+ * when the work source publishes finished tiles (batched work lists). */
 template <int W, class Src>
 __device__ void dws_consumer(const Src &F, dws_smem &S)
 {
@@ -524,6 +527,7 @@ __device__ void dws_consumer(const Src &F, dws_smem &S)
     const int tid = threadIdx.x, lane = tid & 31;
     int gb = 0;   /* batches consumed so far */
     bool aborted = false;
+    double *pvals = nullptr;   /* CSR values of the staged element (nullptr: nothing staged) */
     for (int k = 0;; k++) {
         /* the first batch of tile k (or the end of the work) */
         if (!cons_acquire(S, gb)) {
@@ -543,7 +547,7 @@ __device__ void dws_consumer(const Src &F, dws_smem &S)
             for (int t = 0; t < (WT::NT > 0 ? WT::NT : 1); t++) a.k[t][0] = a.k[t][1] = 0.0;
 #pragma unroll
             for (int t = 0; t < (WT::NGT > 0 ? WT::NGT : 1); t++) a.g[t][0] = a.g[t][1] = 0.0;
-            for (int q0 = 0; q0 < IGAB_NQ3; q0 += DQ) {
+            for (int q0 = 0, bt = 0; q0 < IGAB_NQ3; q0 += DQ, bt++) {
                 if (!have && !cons_acquire(S, gb)) {
                     aborted = true;
                     break;
@@ -553,9 +557,15 @@ __device__ void dws_consumer(const Src &F, dws_smem &S)
                 warp_mma8<W>(S.X[b], S.sc[b], S.UT[b], S.VT[b], lane, a);
                 tc_mbar_arrive(&S.empty[b]);
                 gb++;
+                if (pvals) {
+                    kst_scatter_part(pvals, S, 2 * bt, tid);
+                    kst_scatter_part(pvals, S, 2 * bt + 1, tid);
+                }
             }
             if (aborted) break;
-            /* Gamma (upper tiles) and the CSR row bases of the element */
+            /* every reduction of the staged element is issued: stage this one */
+            tc_bar_sync(BAR_CONS, NCONS);
+            warp_stage8<W>(S, lane, a);
             if constexpr (WT::NGT > 0) {
                 const int r = lane >> 2, c = 2 * (lane & 3);
 #pragma unroll
@@ -568,12 +578,20 @@ __device__ void dws_consumer(const Src &F, dws_smem &S)
             if (tid < 81)
                 elem_row_base(R.g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez, tid, S.rbase[tid], S.rsx[tid],
                               S.rsy[tid]);
-            tc_bar_sync(BAR_CONS, NCONS);
-            warp_scatter8<W>(R.vals, S, lane, a);
-            tc_bar_sync(BAR_CONS, NCONS);
+            pvals = R.vals;
+            /* the next cons_acquire (a consumer barrier) publishes the stage before its use */
         }
         if (aborted) break;
+        if (Src::publishes_tiles && pvals) {
+            tc_bar_sync(BAR_CONS, NCONS);
+            for (int p = 0; p < KST_PARTS; p++) kst_scatter_part(pvals, S, p, tid);
+            pvals = nullptr;
+        }
         F.done(R);
+    }
+    if (!aborted && pvals) {
+        tc_bar_sync(BAR_CONS, NCONS);
+        for (int p = 0; p < KST_PARTS; p++) kst_scatter_part(pvals, S, p, tid);
     }
     if (aborted && tid == 0) {
         S.abort_flag = 1;

@@ -89,7 +89,7 @@ struct tc_smem {
     float gk[2][TC_KC][3][9];           /* per chunk parity: r * d v'/d u_{k,m} of each slot (pre-pass) */
     int qs[2][TC_KC];                   /* point of each slot, -1 for padding rows */
     int cnt[2];
-    int part[2][2];                     /* per-warp bucket counts for the scan */
+    int vcnt[12][2][2];                 /* rows per (variable, point warp, sign) */
     long rbase[81];                     /* CSR row bases of the element matrix (elem_row_base) */
     int rsx[81], rsy[81];
     unsigned long long full[2];         /* stage b written (288 builder arrivals) */
@@ -364,17 +364,17 @@ __device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2][
     }
 }
 
-/* Pre-pass of an element-matrix chunk (every third builder thread, one (slot,
- * component) each, so that the 96 items spread over the 9 builder warps): the
- * row's coefficients r * d v'/d u_{k,m} (m = 0..8) and its point, so that the 288
- * build tasks read them instead of each evaluating the variable gradient (which
- * branches on the variable). */
+/* Pre-pass of an element-matrix chunk (builder threads 0-95, one (slot, component)
+ * each): the row's coefficients r * d v'/d u_{k,m} (m = 0..8) and its point, so that
+ * the 288 build tasks read them instead of each evaluating the variable gradient
+ * (which branches on the variable; the variable-major slot order makes the branch
+ * mostly uniform across a warp). */
 template <int TE>
 __device__ __forceinline__ void tc_prepass(tc_smem<TE> &S, int par, int bucket, int base, int cntb)
 {
     const int t = threadIdx.x;
-    if (t % 3 != 0 || t >= 9 * TC_KC) return;
-    const int it = t / 3, j = it / 3, k = it % 3, slot = base + j;
+    if (t >= 3 * TC_KC) return;
+    const int j = t / 3, k = t % 3, slot = base + j;
     float *gout = S.gk[par][j][k];
     if (slot < cntb) {
         const int id = S.map[bucket][slot], q = id / 12, v = id % 12;
@@ -505,27 +505,39 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
 #pragma unroll
                 for (int K = 0; K < 3; K++) pt[TP_T + 3 * I + K] = (float)(w * P.tau[I][K]);
         }
-        /* ---- sign buckets: exclusive scan of the per-point counts over the 64 points */
-        int pinc = __popc(pmask), ninc = __popc(nmask);
+        /* ---- sign buckets in variable-major order: the slot of row (q, v) counts the
+         * bucket's rows of smaller variables, then the points before q with the same
+         * sign for v (ballot ranks over the two point warps).  Consecutive slots then
+         * share their variable, so the pre-pass branches alike across a warp. */
         if (tid < IGAB_NQ3) {
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int tp = __shfl_up_sync(0xffffffffu, pinc, o), tn = __shfl_up_sync(0xffffffffu, ninc, o);
-                if (lane >= o) { pinc += tp; ninc += tn; }
+#pragma unroll 1
+            for (int v = 0; v < 12; v++) {
+                const unsigned pb = __ballot_sync(0xffffffffu, (pmask >> v) & 1u);
+                const unsigned nb = __ballot_sync(0xffffffffu, (nmask >> v) & 1u);
+                if (lane == 0) {
+                    S.vcnt[v][warp][0] = __popc(pb);
+                    S.vcnt[v][warp][1] = __popc(nb);
+                }
             }
-            if (lane == 31) { S.part[warp][0] = pinc; S.part[warp][1] = ninc; }
         }
         tc_bar_sync(TC_BAR_BLD, TCN_BLD);
         if (tid < IGAB_NQ3) {
-            int po = pinc - __popc(pmask) + (warp ? S.part[0][0] : 0);
-            int no = ninc - __popc(nmask) + (warp ? S.part[0][1] : 0);
+            const unsigned lt = (1u << lane) - 1u;
+            int po = 0, no = 0;   /* rows of the smaller variables */
+#pragma unroll 1
             for (int v = 0; v < 12; v++) {
-                if (pmask & (1u << v)) S.map[0][po++] = (unsigned short)(12 * tid + v);
-                if (nmask & (1u << v)) S.map[1][no++] = (unsigned short)(12 * tid + v);
+                const unsigned pb = __ballot_sync(0xffffffffu, (pmask >> v) & 1u);
+                const unsigned nb = __ballot_sync(0xffffffffu, (nmask >> v) & 1u);
+                if ((pmask >> v) & 1u)
+                    S.map[0][po + (warp ? S.vcnt[v][0][0] : 0) + __popc(pb & lt)] = (unsigned short)(12 * tid + v);
+                if ((nmask >> v) & 1u)
+                    S.map[1][no + (warp ? S.vcnt[v][0][1] : 0) + __popc(nb & lt)] = (unsigned short)(12 * tid + v);
+                po += S.vcnt[v][0][0] + S.vcnt[v][1][0];
+                no += S.vcnt[v][0][1] + S.vcnt[v][1][1];
             }
             if (tid == 0) {
-                S.cnt[0] = S.part[0][0] + S.part[1][0];
-                S.cnt[1] = S.part[0][1] + S.part[1][1];
+                S.cnt[0] = po;
+                S.cnt[1] = no;
             }
         }
         tc_bar_sync(TC_BAR_BLD, TCN_BLD);

@@ -46,8 +46,38 @@ typedef struct gpu_state {
     int prec;
     double *vals32; /* host widening buffer for the FP32 mode (floats) */
     double ms[4];
+    double ksp_rtol;                 /* device Newton solve: Krylov tolerance (0: PETSc's default 1e-5) */
+    int ksp_maxit;
+    igab_newton_info last_solve;
     struct gpu_state *next;
 } gpu_state;
+
+/* which SNESAssmbl belongs to which IGA (recorded by snesiga_init; the reference's
+ * snes_solve(void *snesassmbl) has no application argument) */
+typedef struct sa_link {
+    void *sa, *app;
+    struct sa_link *next;
+} sa_link;
+static sa_link *g_links = NULL;
+
+static void link_snesassmbl(void *sa, void *app)
+{
+    for (sa_link *l = g_links; l; l = l->next)
+        if (l->sa == sa) { l->app = app; return; }
+    sa_link *l = (sa_link *)malloc(sizeof(sa_link));
+    if (!l) return;
+    l->sa = sa;
+    l->app = app;
+    l->next = g_links;
+    g_links = l;
+}
+
+static void *app_of_snesassmbl(void *sa)
+{
+    for (sa_link *l = g_links; l; l = l->next)
+        if (l->sa == sa) return l->app;
+    return NULL;
+}
 
 static gpu_state *g_states = NULL;
 
@@ -531,4 +561,93 @@ void snesiga_init(void *app_, void *phys_, void *nurbs_, void *bc_, void *snesas
     MatSetOption(sa->Tangent_, MAT_SUBSET_OFF_PROC_ENTRIES, PETSC_TRUE);
     sa->snes_Residual = snesiga_b200_Residual;
     sa->snes_Tangent = snesiga_b200_Tangent;
+    link_snesassmbl(snesassmbl_, app_);
 }
+
+int snesiga_gpu_set_ksp(void *app_, double rtol, int maxit)
+{
+    gpu_state *s;
+    int rc = get_state(app_, &s);
+    if (rc) return rc;
+    if (rtol < 0.0 || maxit < 0) return PETSC_ERR_SUP;
+    s->ksp_rtol = rtol;
+    s->ksp_maxit = maxit;
+    return 0;
+}
+
+int snesiga_gpu_last_solve(void *app_, igab_newton_info *info)
+{
+    gpu_state *s = find_state(app_);
+    if (!s || !info) return PETSC_ERR_SUP;
+    *info = s->last_solve;
+    return 0;
+}
+
+static const char *reason_name(int r)
+{
+    switch (r) {
+    case IGAB_SNES_DIVERGED_FNORM_NAN: return "DIVERGED_FNORM_NAN";
+    case IGAB_SNES_DIVERGED_MAX_IT: return "DIVERGED_MAX_IT";
+    case IGAB_SNES_DIVERGED_LINE_SEARCH: return "DIVERGED_LINE_SEARCH";
+    default: return "DIVERGED";
+    }
+}
+
+/* The reference application's solver loop on the GPU -- replaces src/snes_solve.c:10
+ * (snes_solve), run with the SNES settings of src/snes_init.c:8-47.  The initial guess
+ * is snesassmbl->U, the solution goes back there; app->U_hist[0..nselfIdx) holds it
+ * afterwards and snesassmbl->Residual_ the residual at it, as after the reference's
+ * loop.  Every residual, tangent and Krylov solve stays on the device
+ * (igab_newton_solve): no tangent is copied to the host AIJ matrix.  Prints the
+ * reference's line per subiteration; sets snesassmbl->converged. */
+void snesiga_b200_solve(void *snesassmbl_)
+{
+    SNESAssmbl *sa = (SNESAssmbl *)snesassmbl_;
+    void *app_ = app_of_snesassmbl(snesassmbl_);
+    gpu_state *s = NULL;
+    int rc = app_ ? get_state(app_, &s) : IGAB_ERR_ARG;
+    if (!app_) fprintf(stderr, "snesiga_b200: snes_solve: this SNESAssmbl was not set up by snesiga_init\n");
+    if (!rc) rc = sync_params(s);
+    if (!rc) rc = sync_neumann(s);
+    double *dU = NULL;
+    if (!rc) rc = igab_device_buffers(s->ctx, &dU, NULL, NULL, IGAB_PREC_FP64);
+    PetscScalar *u = NULL;
+    if (!rc) {
+        VecGetArray(sa->U, &u);
+        rc = igab_upload(s->ctx, u, dU, s->ndof);
+    }
+    if (!rc) {
+        igab_newton_opts o;
+        igab_newton_defaults(&o);
+        o.prec = s->prec;
+        if (s->ksp_rtol > 0.0) o.ksp_rtol = s->ksp_rtol;
+        if (s->ksp_maxit > 0) o.ksp_maxit = s->ksp_maxit;
+        o.verbose = 1;
+        memset(&s->last_solve, 0, sizeof(s->last_solve));
+        rc = igab_newton_solve(s->ctx, dU, &o, &s->last_solve, NULL, NULL, 0);
+    }
+    if (!rc) rc = igab_download(s->ctx, dU, u, s->ndof);
+    if (u) {
+        if (!rc) keep_history(s->app, u);
+        VecRestoreArray(sa->U, &u);
+    }
+    if (!rc) {
+        /* the residual at the solution in Residual_, as SNES leaves its function vector */
+        const PetscScalar *uc;
+        PetscScalar *r;
+        VecGetArrayRead(sa->U, &uc);
+        VecGetArray(sa->Residual_, &r);
+        rc = igab_residual(s->ctx, uc, r);
+        VecRestoreArray(sa->Residual_, &r);
+        VecRestoreArrayRead(sa->U, &uc);
+    }
+    if (rc) {
+        fprintf(stderr, "snesiga_b200: snes_solve failed: %s\n", igab_last_error());
+        sa->converged = 0;
+        return;
+    }
+    if (!s->last_solve.converged) printf("%s.\n", reason_name(s->last_solve.reason));
+    sa->converged = s->last_solve.converged ? 1 : 0;
+}
+
+void snes_solve(void *snesassmbl_) { snesiga_b200_solve(snesassmbl_); }

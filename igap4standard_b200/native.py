@@ -41,6 +41,21 @@ class IgabSolveInfo(ctypes.Structure):
                 ("rhs_norm", ctypes.c_double)]
 
 
+class IgabNewtonOpts(ctypes.Structure):
+    """igab_newton_opts of include/igab.h"""
+    _fields_ = [("prec", ctypes.c_int), ("abstol", ctypes.c_double), ("rtol", ctypes.c_double),
+                ("stol", ctypes.c_double), ("stagnation", ctypes.c_double), ("max_subiter", ctypes.c_int),
+                ("ksp_rtol", ctypes.c_double), ("ksp_maxit", ctypes.c_int), ("verbose", ctypes.c_int)]
+
+
+class IgabNewtonInfo(ctypes.Structure):
+    """igab_newton_info of include/igab.h"""
+    _fields_ = [("iterations", ctypes.c_int), ("reason", ctypes.c_int), ("converged", ctypes.c_int),
+                ("n_residual", ctypes.c_int), ("n_tangent", ctypes.c_int), ("krylov_iterations", ctypes.c_long),
+                ("fnorm", ctypes.c_double), ("ms_residual", ctypes.c_double), ("ms_tangent", ctypes.c_double),
+                ("ms_krylov", ctypes.c_double), ("ms_total", ctypes.c_double), ("launches", ctypes.c_long)]
+
+
 class IgabBatchTuneResult(ctypes.Structure):
     """igab_batch_tune_result of include/igab.h"""
     _fields_ = [("ctas_res", ctypes.c_int), ("ctas_tan64", ctypes.c_int), ("ctas_tan32", ctypes.c_int),
@@ -90,6 +105,11 @@ IGAB_API = [
     ("igab_last_kernel_ms", ctypes.c_int, [vp, c_double_p]),
     ("igab_fma_peak", ctypes.c_int, [ctypes.c_int, ctypes.c_int, c_double_p]),
     ("igab_residual_noalloc", ctypes.c_int, [vp, vp, vp]),
+    ("igab_staging_bytes", ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_size_t)]),
+    ("igab_newton_defaults", None, [vp]),
+    ("igab_upload", ctypes.c_int, [vp, vp, vp, ctypes.c_long]),
+    ("igab_download", ctypes.c_int, [vp, vp, vp, ctypes.c_long]),
+    ("igab_newton_solve", ctypes.c_int, [vp, vp, vp, vp, vp, vp, ctypes.c_int]),
     ("igab_set_option", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
     ("igab_graph_capture", ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int, ctypes.c_int]),
     ("igab_graph_launch", ctypes.c_int, [vp]),
@@ -123,6 +143,7 @@ IGAB_API = [
     ("igab_batch_residual_device", ctypes.c_int, [vp, vp, vp]),
     ("igab_batch_tangent_device", ctypes.c_int, [vp, vp, vp, ctypes.c_int]),
     ("igab_batch_sync", ctypes.c_int, [vp]),
+    ("igab_batch_set_wait_limit", ctypes.c_int, [vp, ctypes.c_long, ctypes.c_int]),
     ("igab_batch_last_launch_count", ctypes.c_int, [vp, c_int_p]),
     ("igab_batch_graph_capture", ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int]),
     ("igab_batch_graph_launch", ctypes.c_int, [vp]),
@@ -144,6 +165,10 @@ DROPIN_API = [
     ("snesiga_gpu_set_tangent_precision", ctypes.c_int, [vp, ctypes.c_int]),
     ("snesiga_gpu_context", vp, [vp]),
     ("snesiga_gpu_last_timings", ctypes.c_int, [vp, c_double_p]),
+    ("snesiga_gpu_set_ksp", ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
+    ("snesiga_gpu_last_solve", ctypes.c_int, [vp, vp]),
+    ("snesiga_b200_solve", None, [vp]),
+    ("snes_solve", None, [vp]),
     ("iga_intdensity", None, [vp, vp]),
     ("snesiga_b200_intdensity", None, [vp, vp]),
     ("nurbs_knotinsert", None, [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]),
@@ -167,6 +192,7 @@ CASE_API = [
     ("iga_case_app", vp, [vp]),
     ("iga_case_iocomm", vp, [vp]),
     ("iga_case_snesassmbl", vp, [vp]),
+    ("iga_case_solve", ctypes.c_int, [vp, vp]),
     ("iga_case_neumann", None, [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]),
 ]
 

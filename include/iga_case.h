@@ -52,6 +52,11 @@ int  iga_case_tangent(iga_case *c, const double *U);
 long iga_case_tangent_nnz(const iga_case *c);
 int  iga_case_tangent_csr(const iga_case *c, int *rowptr, int *cols, double *vals);
 
+/* the library's solver loop (snes_solve, src/snes_solve.c:10) from the initial guess U;
+ * U receives the solution.  0 converged, 1 not converged, -1 no snes_solve linked
+ * (the oracle build has none: the reference's needs PETSc's SNES). */
+int  iga_case_solve(iga_case *c, double *U);
+
 /* opaque handles for code that wants to call further library functions */
 void *iga_case_app(iga_case *c);
 /* the IOcomm the case's snesiga_init filled (write_solution / read_solution, src/ioutil.c:89) */

@@ -101,6 +101,10 @@ int igab_set_stream(igab_ctx *ctx, void *cuda_stream);
 int igab_sync(igab_ctx *ctx);
 /* device buffers owned by the context, sized ndof / nnz, for callers without an allocator */
 int igab_device_buffers(igab_ctx *ctx, double **U_dev, double **R_dev, void **vals_dev, int prec);
+/* n doubles host -> device / device -> host on the context's stream, synchronously
+ * (for C callers that do not link the CUDA runtime; no reference counterpart) */
+int igab_upload(igab_ctx *ctx, const double *host, double *dev, long n);
+int igab_download(igab_ctx *ctx, const double *dev, double *host, long n);
 /* check a device vector for NaN/Inf (1 = all finite) */
 int igab_check_finite(igab_ctx *ctx, const void *dev, long n, int prec, int *all_finite);
 
@@ -194,9 +198,19 @@ int igab_batch_refresh(igab_batch *b);
 int igab_batch_set_stream(igab_batch *b, void *cuda_stream);
 int igab_batch_set_schedule(igab_batch *b, int ctas_res, int ctas_tan64, int ctas_tan32, int order);
 int igab_batch_get_schedule(const igab_batch *b, int *ctas_res, int *ctas_tan64, int *ctas_tan32, int *order);
+/* The launches below return once enqueued.  A tile of colour c waits (bounded) for the
+ * earlier colours of its instance; a wait that gives up sets a status word and the
+ * launch still ends, with that instance's R or values incomplete.  igab_batch_sync
+ * (after igab_batch_residual_device, igab_batch_tangent_device or
+ * igab_batch_graph_launch) reports it as IGAB_ERR_CUDA and clears it: check its
+ * return before using the results. */
 int igab_batch_residual_device(igab_batch *b, const double *U_dev, double *R_dev);
 int igab_batch_tangent_device(igab_batch *b, const double *U_dev, void *vals_dev, int prec);
 int igab_batch_sync(igab_batch *b);
+/* colour-dependency wait: polls (128 ns apart) before a wait gives up, 0 = the default
+ * 4,194,304; unreachable = 1 makes every wait on colour 0 of instance 0 run out (a test
+ * switch for the give-up path; results are then incomplete).  No reference counterpart. */
+int igab_batch_set_wait_limit(igab_batch *b, long polls, int unreachable);
 int igab_batch_last_launch_count(const igab_batch *b, int *n);
 /* one Newton iteration's assembly (residual then tangent) captured in a CUDA graph */
 int igab_batch_graph_capture(igab_batch *b, const double *U_dev, double *R_dev, void *vals_dev, int prec);
@@ -249,6 +263,48 @@ int igab_spmv_device(igab_ctx *ctx, const void *vals_dev, int prec, const double
 int igab_solve_device(igab_ctx *ctx, const void *vals_dev, int prec, const double *b_dev, double *x_dev,
                       double rtol, double atol, int maxit, igab_solve_info *info);
 
+/* ---- Newton solve on the device (replaces the reference application's solver loop,
+ * src/snes_solve.c:10-36, run with the SNES configuration of src/snes_init.c:8-47):
+ * one-step Newton solves (NEWTONLS, backtracking line search of cubic order; abstol on
+ * ||F||_2, rtol, stol) repeated until a step ends with a reason other than "maximum
+ * iterations", or until ||F|| stagnates (|F_old - F_new| / F_old < stagnation, F_old =
+ * 999 at the start; reported as DIVERGED_LINE_SEARCH, as the reference does).  The linear
+ * solve of each step is the Jacobi BiCGStab of igab_solve_device (stand-in for PETSc's
+ * GMRES + ASM) to ksp_rtol, on the tangent assembled in opts.prec; no residual or tangent
+ * leaves the GPU.  U_dev holds the initial guess and receives the solution; the context's
+ * Neumann values and history levels are used as set.  fnorm_history / krylov_history
+ * (either may be NULL) receive ||F|| and the Krylov iteration count of the first
+ * history_cap subiterations.  verbose = 1 prints the reference's line per subiteration. */
+enum igab_snes_reason {
+    IGAB_SNES_CONVERGED_FNORM_ABS = 2, IGAB_SNES_CONVERGED_FNORM_RELATIVE = 3,
+    IGAB_SNES_CONVERGED_SNORM_RELATIVE = 4, IGAB_SNES_DIVERGED_FNORM_NAN = -4,
+    IGAB_SNES_DIVERGED_MAX_IT = -5, IGAB_SNES_DIVERGED_LINE_SEARCH = -6
+};   /* PETSc's SNESConvergedReason numbering */
+typedef struct {
+    int prec;              /* tangent precision: IGAB_PREC_FP64, or IGAB_PREC_FP32 (inexact Newton) */
+    double abstol;         /* 1e-10   SNESSetTolerances, src/snes_init.c:18 */
+    double rtol;           /* 1e-20 */
+    double stol;           /* 1e-20 */
+    double stagnation;     /* 1e-6    src/snes_solve.c:29 */
+    int max_subiter;       /* 10000   src/snes_solve.c:24 */
+    double ksp_rtol;       /* 1e-5    PETSc's default KSP relative tolerance */
+    int ksp_maxit;         /* 100000  iterations per linear solve */
+    int verbose;           /* 0 */
+} igab_newton_opts;
+typedef struct {
+    int iterations;          /* Newton steps taken */
+    int reason;              /* igab_snes_reason of the last subiteration */
+    int converged;           /* reason > 0 */
+    int n_residual, n_tangent;
+    long krylov_iterations;  /* over all linear solves */
+    double fnorm;            /* ||F||_2 at exit */
+    double ms_residual, ms_tangent, ms_krylov, ms_total;   /* wall time by phase */
+    long launches;           /* kernels launched */
+} igab_newton_info;
+void igab_newton_defaults(igab_newton_opts *opts);
+int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton_opts *opts, igab_newton_info *info,
+                      double *fnorm_history, int *krylov_history, int history_cap);
+
 /* ---- mesh refinement and solution files (mesh/nurbs/nurbs_knotinsert.c:7, src/ioutil.c:89, :126).
  * igab_knot_insert: refine the p = 2 control points of a field, in place in host memory
  * (U_universal[ndof * cp + dof], cp = (x nb1 + y) nb2 + z with nb = nelem + 2, or nelem
@@ -274,9 +330,14 @@ int igab_read_solution(const char *fname, double *U_hist, long ndof, int ihist0,
  * loads the library) instead of context buffers obtained with cudaMalloc; a
  * call allocates nothing.  Meshes above 1,048,576 dofs are rejected
  * (IGAB_ERR_ARG).  All calls share the array: calls that overlap on the GPU
- * race.  The first call on a device looks up the array's address and should
- * come before any stream capture. */
+ * race.  Each call looks up the array's address in the current CUDA context
+ * (cudaGetSymbolAddress, which allocates nothing). */
 int igab_residual_noalloc(igab_ctx *ctx, const double *U_host, double *R_host);
+/* device bytes the context holds for the host-pointer entry points (the U, R and
+ * tangent-value staging that igab_residual, igab_tangent and igab_device_buffers
+ * allocate on first use; 0 before then).  No counterpart in the reference; lets a
+ * caller check that igab_residual_noalloc left the context without staging. */
+int igab_staging_bytes(const igab_ctx *ctx, size_t *bytes);
 
 #ifdef __cplusplus
 }

@@ -26,6 +26,7 @@
 #define SNESIGA_B200_H
 
 #include "igap4_structs.h"
+#include "igab.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -67,6 +68,21 @@ void *snesiga_gpu_context(void *app_);
 /* milliseconds of the last callback: [0] residual total, [1] tangent total,
  * [2] residual kernels, [3] tangent kernels */
 int snesiga_gpu_last_timings(void *app_, double ms[4]);
+
+/* The solver loop on the GPU, replacing src/snes_solve.c:10 (same signature): the
+ * Newton iteration of src/snes_init.c:8-47 / src/snes_solve.c:10-36 with every
+ * residual, tangent and Krylov solve on the device (igab_newton_solve; the tangent
+ * never reaches the host AIJ matrix).  Initial guess and solution in
+ * snesassmbl->U; afterwards app->U_hist[0..nselfIdx) holds the solution and
+ * snesassmbl->Residual_ the residual there; snesassmbl->converged is set.  Prints
+ * the reference's line per subiteration.  The SNESAssmbl must come from this
+ * library's snesiga_init.  Tangent precision: snesiga_gpu_set_tangent_precision. */
+void snes_solve(void *snesassmbl_);
+void snesiga_b200_solve(void *snesassmbl_);
+/* Krylov tolerance and iteration limit of the device solve (0: defaults 1e-5, 100000) */
+int snesiga_gpu_set_ksp(void *app_, double rtol, int maxit);
+/* iteration counts, norms and phase times of the last snes_solve on this application */
+int snesiga_gpu_last_solve(void *app_, igab_newton_info *info);
 
 #ifdef __cplusplus
 }

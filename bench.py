@@ -35,9 +35,12 @@ METRIC = "Newton-step assembly ms & adjoint grads/s at 64^3, mixed vs FP64, 1xB2
 
 # Algorithmic flops per element (4^3 Gauss points):
 #  tangent  64 * 2 * (30*81*10 + 81*81*10) = B^T D B with the dof-block-sparse B
-#  residual 64 * 2 * (27*30 + 27*30) + 64 * 270 (interpolation, test contraction, basis)
+#  residual 64 * (2 * (27*30 + 27*30) + 270 + 758): interpolation, test contraction, basis
+#           products and the point integrand, whose 758 operations per call are counted in
+#           the reference's phys/ge/residual.c by oracle/count_integrand_flops.py
+GE_RESIDUAL_INTEGRAND_FLOPS = 758
 TAN_ALG_FLOPS = 64 * 2 * (30 * 81 * 10 + 81 * 81 * 10)
-RES_ALG_FLOPS = 64 * (2 * (27 * 30 + 27 * 30) + 270)
+RES_ALG_FLOPS = 64 * (2 * (27 * 30 + 27 * 30) + 270 + GE_RESIDUAL_INTEGRAND_FLOPS)
 # flops the tangent kernel executes per element on the tensor path: 66 upper 8x8 tiles
 # x 12 variables per point, plus 10 upper 8x8 tiles of the geometric block x 6 U / V rows per point
 TAN_EXEC_FLOPS = 64 * 2 * (66 * 64 * 12 + 10 * 64 * 6)
@@ -54,16 +57,21 @@ def parse():
     ap.add_argument("--n", type=int, default=64, help="elements per side")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-sample", type=int, default=4, help="elements per side of the CPU sample mesh")
     ap.add_argument("--no-tune", action="store_true", help="skip the schedule autotuner")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-density", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-instance batched assembly")
     ap.add_argument("--batch-instances", type=int, default=512)
-    ap.add_argument("--transient", type=int, default=0, metavar="STEPS",
-                    help="also time STEPS steps of the transient workload (phys/getime, 32^3, dt 1e-3)")
-    ap.add_argument("--transient-adjoint", type=int, default=0, metavar="STEPS",
-                    help="also time one checkpointed transient adjoint gradient over STEPS steps (32^3, every 10)")
+    ap.add_argument("--transient", type=int, default=200, metavar="STEPS",
+                    help="time STEPS steps of the transient workload (phys/getime, 32^3, dt 1e-3); 0 skips")
+    ap.add_argument("--transient-adjoint", type=int, default=50, metavar="STEPS",
+                    help="time one checkpointed transient adjoint gradient over STEPS steps (32^3, every 10); "
+                         "0 skips")
+    ap.add_argument("--no-newton", action="store_true", help="skip the FP64 / mixed Newton solves at n^3")
+    ap.add_argument("--newton-ksp-rtol", type=float, default=1e-5,
+                    help="Krylov tolerance of the Newton solves (PETSc's default KSP rtol)")
+    ap.add_argument("--no-adjoint-static", action="store_true",
+                    help="skip the end-to-end static adjoint gradient at 32^3")
     return ap.parse_args()
 
 
@@ -88,44 +96,70 @@ def config_dict(n, ndof, nnz):
 # ------------------------------------------------------------------ CPU side
 
 def _ref_sample_worker(args):
-    """One process: the reference's residual + tangent on an m^3 sample mesh."""
-    m, seed = args
+    """One process: the reference's residual (then iga_intdensity) on an x-y slab of the
+    n^3 workload, and its tangent on a slab of the 8x8x16 sub-block, each on its own
+    single-rank mesh with the workload's knot perturbation, material and BCs."""
+    res_shape, tan_shape, seed = args
     sys.path.insert(0, REPO)
     from oracle import ref
     from igap4standard_b200 import mesh
-    nelem = (m, m, m)
-    kn = mesh.knots_for(nelem, perturb=0.1, seed=1)
     pm = mesh.par_mat_from_lame(1.0, 1.0, 0.1)
     bc, pd = mesh.bc_config0()
-    C = ref.case("ge", nelem, kn, pm, bc, np.zeros(9), pd, np.zeros(39))
-    U = np.random.default_rng(seed).uniform(-1e-3, 1e-3, C.ndof)
-    t0 = time.perf_counter()
-    C.residual(U)
-    t1 = time.perf_counter()
-    C.tangent(U)
-    t2 = time.perf_counter()
-    C.intdensity(13)   # iga_intdensity on U_hist level 0 (left there by the residual callback)
-    t3 = time.perf_counter()
-    C.close()
-    return (t1 - t0, t2 - t1, m ** 3, t3 - t2)
+    out = []
+    for shape, what in ((res_shape, "res"), (tan_shape, "tan")):
+        C = ref.case("ge", shape, mesh.knots_for(shape, perturb=0.1, seed=1), pm, bc, np.zeros(9), pd, np.zeros(39))
+        U = np.random.default_rng(seed).uniform(-1e-3, 1e-3, C.ndof)
+        t0 = time.perf_counter()
+        if what == "res":
+            C.residual(U)
+            t1 = time.perf_counter()
+            C.intdensity(13)   # iga_intdensity on U_hist level 0 (left there by the residual callback)
+            t2 = time.perf_counter()
+            out += [t1 - t0, t2 - t1]
+        else:
+            C.tangent(U)
+            out.append(time.perf_counter() - t0)
+        C.close()
+    return out
 
 
 class RefPool:
-    """Host-core pool running the reference's CPU assembly (spawned processes)."""
+    """Host-core pool running the reference's CPU assembly (spawned processes, one mesh each).
+
+    A sample covers the n^3 workload's element count for the residual: P processes, each on
+    an n x n x ceil(n/P) slab, run at once; and 1,024 elements for the tangent: the 8x8x16
+    sub-block as P slabs of 8 x 8 x ceil(16/P).  Times are per element, from each process's
+    own clock around the reference callback."""
 
     def __init__(self, procs):
         import multiprocessing as mp
         self.procs = procs
         self.pool = mp.get_context("spawn").Pool(procs)
 
-    def sample(self, m):
+    def shapes(self, n):
+        P = self.procs
+        return (n, n, max(1, -(-n // P))), (8, 8, max(1, -(-16 // P)))
+
+    def sample(self, n):
+        rs, ts = self.shapes(n)
         t0 = time.perf_counter()
-        res = self.pool.map(_ref_sample_worker, [(m, i) for i in range(self.procs)])
+        res = self.pool.map(_ref_sample_worker, [(rs, ts, i) for i in range(self.procs)])
         wall = time.perf_counter() - t0
-        tr = np.mean([r[0] for r in res]) / res[0][2]
-        tt = np.mean([r[1] for r in res]) / res[0][2]
-        self.td = np.mean([r[3] for r in res]) / res[0][2]   # intdensity per element
+        ne_r, ne_t = rs[0] * rs[1] * rs[2], ts[0] * ts[1] * ts[2]
+        tr = float(np.mean([r[0] for r in res])) / ne_r
+        self.td = float(np.mean([r[1] for r in res])) / ne_r   # intdensity per element
+        tt = float(np.mean([r[2] for r in res])) / ne_t
+        self.res_elements = ne_r * self.procs
+        self.tan_elements = ne_t * self.procs
         return tr, tt, wall
+
+    def describe(self, n):
+        rs, ts = self.shapes(n)
+        return ("%d processes at once (throughput mode, no MPI), reference code: residual on %d x %d x %d slabs "
+                "(%d elements per sample, the %d^3 workload's count), tangent on %d x %d x %d slabs of the 8x8x16 "
+                "sub-block (%d elements per sample, time per element extrapolated to %d^3)"
+                % (self.procs, rs[0], rs[1], rs[2], rs[0] * rs[1] * rs[2] * self.procs, n, ts[0], ts[1], ts[2],
+                   ts[0] * ts[1] * ts[2] * self.procs, n))
 
     def close(self):
         self.pool.close()
@@ -157,13 +191,12 @@ def run_reference(args):
     nel = n ** 3
     P = cpu_procs()
     pool = RefPool(P)
-    m = args.cpu_sample
     for _ in range(max(args.warmup, 0)):
-        pool.sample(m)
+        pool.sample(n)
     per = []
     walls = []
     for _ in range(args.steps):
-        tr, tt, wall = pool.sample(m)
+        tr, tt, wall = pool.sample(n)
         per.append((tr, tt))
         walls.append(wall)
     pool.close()
@@ -171,14 +204,14 @@ def run_reference(args):
     tt = float(np.mean([p[1] for p in per]))
     ms = (tr + tt) * nel / P * 1e3
     ndof, nnz = mesh.n_dof((n, n, n)), mesh.nnz_of((n, n, n))
-    sample = ("%d processes x %d^3-element mesh per step (residual+tangent, reference code), per-element time "
-              "extrapolated to %d^3 elements with %d processes in parallel (throughput mode, no MPI)" % (P, m, n, P))
+    sample = pool.describe(n) + "; value = (residual + tangent per element) x %d^3 / %d processes" % (n, P)
     line = {"impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_dict(n, ndof, nnz),
             "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": P, "kind": "reference", "sample": sample,
-                             "residual_us_per_element": tr * 1e6, "tangent_ms_per_element": tt * 1e3},
+                             "residual_us_per_element": tr * 1e6, "tangent_ms_per_element": tt * 1e3,
+                             "residual": "measured on the full element count", "tangent": "extrapolated"},
             "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "sample_wall_s": float(np.mean(walls))}
     print(json.dumps(line))
@@ -364,6 +397,112 @@ def bench_transient_adjoint(args, device):
            "timing": "host wall clock: forward solve + backward sweep with segment recomputation"}
     A.close()
     return res
+
+
+def bench_newton_config1(args, device):
+    """The config-1 problem solved: FP64 and FP32-tangent Newton from U = 0 to ||F||_2 <
+    1e-10 at n^3 with the reference application's solver loop (src/snes_solve.c:10-36,
+    SNES settings of src/snes_init.c:8-47) run on the device by igab_newton_solve: every
+    residual, tangent and Jacobi-BiCGStab solve (PETSc's default KSP rtol 1e-5) on the GPU."""
+    import torch
+    from igap4standard_b200 import Assembly
+    n = args.n
+    nelem, kn, pm, bc, pd = workload(n)
+    A = Assembly(nelem, kn, pm, bc, pd, device=device)
+    out, sol = {}, {}
+    for prec in ("fp64", "fp32"):
+        U = torch.zeros(A.ndof, dtype=torch.float64, device=torch.device("cuda", device))
+        torch.cuda.synchronize()
+        info = A.newton_solve_device(U.data_ptr(), prec, ksp_rtol=args.newton_ksp_rtol)
+        sol[prec] = U
+        its = max(info["iterations"], 1)
+        out[prec] = {"newton_iterations": info["iterations"], "converged": bool(info["converged"]),
+                     "reason": info["reason"], "final_fnorm": info["fnorm"], "fnorms": info["fnorms"],
+                     "krylov_iterations": info["krylov_iterations"], "krylov_per_newton": info["krylov"],
+                     "residual_evaluations": info["n_residual"], "tangent_evaluations": info["n_tangent"],
+                     "wall_s": round(info["ms_total"] / 1e3, 3),
+                     "ms_per_newton_step": round(info["ms_total"] / its, 3),
+                     "assembly_ms_per_newton_step": round((info["ms_residual"] + info["ms_tangent"]) / its, 3),
+                     "krylov_ms_per_newton_step": round(info["ms_krylov"] / its, 3),
+                     "launches": info["launches"]}
+    u64, u32 = sol["fp64"], sol["fp32"]
+    scale = float(u64.abs().max())
+    out["u_mixed_vs_fp64_rel_inf"] = float((u32 - u64).abs().max()) / max(scale, 1e-300)
+    out["extra_iterations_mixed"] = out["fp32"]["newton_iterations"] - out["fp64"]["newton_iterations"]
+    out["workload"] = ("config 1: %d^3, knots perturbed +-0.1h (seed 1), lambda=mu=1, l=0.1, BCs of config 0, "
+                       "from U = 0 to ||F||_2 < 1e-10 (absolute, the reference's SNES tolerance)" % n)
+    out["linear_solver"] = ("Jacobi-preconditioned BiCGStab on the device (stands in for PETSc's GMRES + ASM), "
+                            "rtol %g" % args.newton_ksp_rtol)
+    out["timing"] = "host wall clock of igab_newton_solve (phases synchronised)"
+    A.close()
+    del u64, u32, sol
+    torch.cuda.empty_cache()
+    return out
+
+
+def bench_adjoint_static(args, device):
+    """Config 4 (static) end to end at 32^3: per-element stiffness scales s_e = exp(g_e),
+    g ~ N(0, 0.3^2) (32,768 parameters, seed 4); J = 1/2 sum over the control points of face
+    x = 1 of |U - U*|^2 with U* the solution at g* (seed 5).  One gradient = the forward
+    Newton solve at g (device), the tangent at the solution, the adjoint solve K^T lam =
+    dJ/dU (device BiCGStab; K is symmetric), then dJ/dg = -lam . dR/dg (igab_adjoint_backward)."""
+    import torch
+    from igap4standard_b200 import Assembly, mesh
+    n = 32
+    nelem = (n, n, n)
+    kn = mesh.knots_for(nelem, perturb=0.1, seed=1)
+    pm = mesh.par_mat_from_lame(1.0, 1.0, 0.1)
+    bc, pd = mesh.bc_config0()
+    A = Assembly(nelem, kn, pm, bc, pd, device=device)
+    dev = torch.device("cuda", device)
+    st = torch.cuda.Stream(device=dev)
+    A.set_stream(st.cuda_stream)
+    nb = n + 2
+    mask = torch.zeros((nb, nb, nb, 3), dtype=torch.float64)
+    mask[-1] = 1.0
+    mask = mask.reshape(-1).to(dev)
+    ne = A.nelem_total
+    gstar = np.random.default_rng(5).normal(0.0, 0.3, ne)
+    g = np.random.default_rng(4).normal(0.0, 0.3, ne)
+    V = torch.empty(A.nnz, dtype=torch.float64, device=dev)
+    with torch.cuda.stream(st):
+        Ustar = torch.zeros(A.ndof, dtype=torch.float64, device=dev)
+        A.set_element_log_scale(gstar)
+        A.newton_solve_device(Ustar.data_ptr(), "fp64", ksp_rtol=1e-10)
+
+        def gradient(g):
+            t0 = time.perf_counter()
+            A.set_element_log_scale(g)
+            U = torch.zeros(A.ndof, dtype=torch.float64, device=dev)
+            fwd = A.newton_solve_device(U.data_ptr(), "fp64", ksp_rtol=1e-10)
+            t1 = time.perf_counter()
+            A.tangent_device(U.data_ptr(), V.data_ptr(), "fp64")
+            b = mask * (U - Ustar)
+            lam = torch.zeros_like(U)
+            its, ok, _ = A.solve_device(V.data_ptr(), b.data_ptr(), lam.data_ptr(), "fp64", 1e-10, 0.0, 200000)
+            grad = torch.empty(ne, dtype=torch.float64, device=dev)
+            A.adjoint_backward_device(U.data_ptr(), None, lam.data_ptr(), None, grad.data_ptr())
+            grad = -grad
+            st.synchronize()
+            t2 = time.perf_counter()
+            J = 0.5 * float((b * b).sum())
+            return grad, J, fwd, its, ok, t1 - t0, t2 - t1
+
+        gradient(g)                       # warm-up (graph captures, workspaces)
+        grad, J, fwd, its, ok, tf, tb = gradient(g)
+    A.set_element_log_scale(None)
+    out = {"parameters": ne, "grads_per_s": round(1.0 / (tf + tb), 4), "forward_s": round(tf, 3),
+           "adjoint_s": round(tb, 3), "forward_newton_iterations": fwd["iterations"],
+           "forward_krylov_iterations": fwd["krylov_iterations"], "forward_fnorm": fwd["fnorm"],
+           "adjoint_krylov_iterations": its, "adjoint_converged": bool(ok), "J": J,
+           "grad_norm": float(grad.norm()),
+           "definition": "one gradient end to end: device Newton solve at g (FP64, KSP rtol 1e-10), tangent at "
+                         "the solution, adjoint solve K^T lam = dJ/dU (device BiCGStab, rtol 1e-10), "
+                         "dJ/dg = -lam . dR/dg; host wall clock"}
+    A.close()
+    del V
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_ours(args):
@@ -609,6 +748,8 @@ def run_ours(args):
         batch = bench_batch(args, dev, local, barrier)
     trans = bench_transient(args, local) if args.transient > 0 else None
     trans_adj = bench_transient_adjoint(args, local) if args.transient_adjoint > 0 else None
+    newton1 = None if args.no_newton else bench_newton_config1(args, local)
+    adj_static = None if args.no_adjoint_static else bench_adjoint_static(args, local)
 
     # ---- roofline of the dominant kernel (tangent volume, 8 colour launches per step)
     tan_ms = k64[2]
@@ -660,7 +801,7 @@ def run_ours(args):
             "adjoint_grads_per_s": adjoint["grads_per_s"] if adjoint else None, "adjoint": adjoint,
             "intdensity": dens, "knot_insert": knot,
             "schedule": schedule, "batch_config3": batch, "transient_config2": trans,
-            "transient_adjoint_config4": trans_adj,
+            "transient_adjoint_config4": trans_adj, "newton_config1": newton1, "adjoint_config4_e2e": adj_static,
             "clocks": clk, "gpu_launches": int(launches64), "roofline": roofline,
             "roofline_mixed": roofline_mixed,
             "peaks_measured": {"fp64_tflops": round(peak64, 2), "fp32_tflops": round(peak32, 2),
@@ -673,17 +814,18 @@ def run_ours(args):
             if ref.available():
                 P = min(cpu_procs(), 64)
                 pool = RefPool(P)
-                tr, tt, wall = pool.sample(args.cpu_sample)
+                tr, tt, wall = pool.sample(n)
                 pool.close()
                 ms = (tr + tt) * nel / P * 1e3
                 line["cpu_baseline"] = {"value": round(ms, 1), "unit": "ms", "cores": P, "kind": "reference",
-                                        "sample": "%d processes x %d^3 elements (reference residual+tangent), "
-                                                  "per-element time extrapolated to %d^3 (%.1f s wall)"
-                                                  % (P, args.cpu_sample, n, wall)}
+                                        "sample": pool.describe(n) + " (%.1f s wall)" % wall,
+                                        "residual_us_per_element": round(tr * 1e6, 3),
+                                        "tangent_ms_per_element": round(tt * 1e3, 4),
+                                        "residual": "measured on the full element count", "tangent": "extrapolated"}
                 if dens is not None:
                     dens["reference_cpu_ms"] = round(pool.td * nel / P * 1e3, 1)
-                    dens["reference_cpu_sample"] = ("reference iga_intdensity on %d processes x %d^3 elements, "
-                                                    "per-element time extrapolated to %d^3" % (P, args.cpu_sample, n))
+                    dens["reference_cpu_sample"] = ("reference iga_intdensity on the residual sample's slabs "
+                                                    "(%d elements), %d processes" % (pool.res_elements, P))
             else:
                 line["cpu_baseline"] = None
         except Exception as e:

@@ -76,7 +76,10 @@ def obj_name(rel):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("IGAP4_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("IGAP4_REFERENCE", os.path.join(os.path.dirname(REPO),
+                                                                                        "reference")),
+                    help="the reference tree (default: $IGAP4_REFERENCE, else a directory named "
+                         "'reference' beside this repository)")
     ap.add_argument("--force", action="store_true")
     args = ap.parse_args()
     ref = args.reference

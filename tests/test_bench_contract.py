@@ -17,7 +17,7 @@ def test_reference_arm_json_line(built):
     if not ref.available():
         pytest.skip("reference library not built")
     out = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--steps", "1",
-                          "--warmup", "0", "--cpu-sample", "2"], cwd=REPO, capture_output=True, text=True,
+                          "--warmup", "0", "--n", "16"], cwd=REPO, capture_output=True, text=True,
                          timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.strip().startswith("{")]
@@ -32,13 +32,14 @@ def test_reference_arm_json_line(built):
     e = d["e2e"]
     assert e["value"] == d["value"] and e["unit"] == d["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
-    assert d["config"]["nelem"] == [64, 64, 64]
+    assert d["config"]["nelem"] == [16, 16, 16]
+    assert cb["residual"] == "measured on the full element count" and cb["tangent"] == "extrapolated"
 
 
 def test_reference_arm_other_ranks_exit_quietly(built):
     env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
     out = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--steps", "1",
-                          "--warmup", "0", "--cpu-sample", "2"], cwd=REPO, capture_output=True, text=True,
+                          "--warmup", "0", "--n", "16"], cwd=REPO, capture_output=True, text=True,
                          timeout=600, env=env)
     assert out.returncode == 0, out.stderr[-2000:]
     assert not [l for l in out.stdout.splitlines() if l.strip().startswith("{")]

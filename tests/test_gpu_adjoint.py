@@ -186,3 +186,57 @@ def test_adjoint_gradient_matches_central_differences(built, oracle_lib):
         print("direction %2d (%s): adjoint %.10e  central difference %.10e  rel %.2e"
               % (k, "gpu" if k % 2 == 0 else "ref", ad, fd, err))
     assert worst <= 1e-6
+
+
+def test_adjoint_gradient_config4_8cubed(built, oracle_lib):
+    """Config-4 objective on an 8^3 mesh: s_e = exp(g_e), g ~ N(0, 0.3^2) (512 parameters),
+    J = 1/2 sum over the face x = 1 control points of |U - U*|^2 with U* the solution at a
+    second draw g*; dJ/dg by the adjoint against central differences (h = 1e-6, 16
+    directions) of the B200 solve and of the reference's own scaled residual, 1e-6."""
+    from igap4standard_b200 import mesh, newton
+    nelem = (8, 8, 8)
+    kn = mesh.knots_for(nelem, perturb=0.1, seed=1)
+    pm = mesh.par_mat_from_lame(1.0, 1.0, 0.1)
+    bc, pd = mesh.bc_config0()
+    c = dict(phys="ge", nelem=nelem, knots=kn, par_mat=pm, bc_type=bc, par_dirichlet=pd, par_periodic=np.zeros(9),
+             par_neumann=np.zeros(39))
+    A = _assembly(c)
+    n_el = 512
+    mask = _face_x1_mask(nelem)
+    r_gpu, j_gpu = newton.assembly_problem(A, "fp64")
+    base = _ref_case(oracle_lib, c)
+
+    def solve_gpu(g, U0):
+        A.set_element_log_scale(g)
+        return _newton_tight(r_gpu, j_gpu, U0)
+
+    def solve_ref(g, U0):
+        ref = oracle_lib.ScaledCase(base, g)
+        A.set_element_log_scale(g)
+        U = _newton_tight(ref.residual, j_gpu, U0)
+        ref.close()
+        return U
+
+    Ustar = solve_gpu(np.random.default_rng(5).normal(0.0, 0.3, n_el), np.zeros(A.ndof))
+    g0 = np.random.default_rng(4).normal(0.0, 0.3, n_el)
+
+    def J(U):
+        return 0.5 * np.sum(mask * (U - Ustar) ** 2)
+
+    U = solve_gpu(g0, np.zeros(A.ndof))
+    A.set_element_log_scale(g0)
+    lam = newton.direct_solve(j_gpu(U).T.tocsr(), mask * (U - Ustar))
+    grad = -A.dRdg(U, lam)
+    rng = np.random.default_rng(6)
+    h = 1e-6
+    worst = 0.0
+    for k in range(16):
+        d = rng.normal(size=n_el)
+        ad = grad @ d
+        solver = solve_gpu if k % 2 == 0 else solve_ref
+        fd = (J(solver(g0 + h * d, U)) - J(solver(g0 - h * d, U))) / (2 * h)
+        err = abs(fd - ad) / max(abs(ad), 1e-3 * np.linalg.norm(grad) * np.linalg.norm(d))
+        worst = max(worst, err)
+        print("8^3 direction %2d (%s): adjoint %.10e  central difference %.10e  rel %.2e"
+              % (k, "gpu" if k % 2 == 0 else "ref", ad, fd, err))
+    assert worst <= 1e-6

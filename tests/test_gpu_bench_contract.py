@@ -17,7 +17,7 @@ def test_bench_line_small_mesh(built):
     n = 16
     out = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--n", str(n), "--steps", "3",
                           "--warmup", "3", "--no-batch", "--no-adjoint", "--no-density", "--no-tune",
-                          "--cpu-sample", "2"], cwd=REPO, capture_output=True, text=True, timeout=900)
+                          "--transient", "0", "--transient-adjoint", "0", "--no-adjoint-static"], cwd=REPO, capture_output=True, text=True, timeout=900)
     assert out.returncode == 0, out.stderr[-3000:]
     lines = [l for l in out.stdout.splitlines() if l.strip().startswith("{")]
     assert len(lines) == 1
@@ -42,3 +42,7 @@ def test_bench_line_small_mesh(built):
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["value"] > 0 and cb["cores"] >= 1
     assert "sm_mhz" in d["clocks"] and "reasons" in d["clocks"]
+    nw = d["newton_config1"]
+    for prec in ("fp64", "fp32"):
+        assert nw[prec]["converged"] and nw[prec]["final_fnorm"] < 1e-10 and nw[prec]["newton_iterations"] >= 1
+    assert nw["extra_iterations_mixed"] <= 1 and nw["u_mixed_vs_fp64_rel_inf"] < 1e-6

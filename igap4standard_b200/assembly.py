@@ -182,8 +182,19 @@ class Assembly:
                                          float(atol), int(maxit), ctypes.byref(info)))
         return info.iterations, bool(info.converged), info.residual_norm
 
+    def solve_mg_device(self, vals_ptr, b_ptr, x_ptr, prec="fp64", rtol=1e-5, atol=0.0, maxit=1000):
+        """x = K^-1 b by multigrid-preconditioned CG on the device (igab_solve_mg_device).
+        Returns (iterations, converged, residual norm, multigrid levels)."""
+        info = native.IgabSolveInfo()
+        check(self.lib, "igab_solve_mg_device",
+              self.lib.igab_solve_mg_device(self.h, vp(vals_ptr), PREC[prec], vp(b_ptr), vp(x_ptr), float(rtol),
+                                            float(atol), int(maxit), ctypes.byref(info)))
+        lev = ctypes.c_int()
+        check(self.lib, "igab_solve_mg_levels", self.lib.igab_solve_mg_levels(self.h, ctypes.byref(lev)))
+        return info.iterations, bool(info.converged), info.residual_norm, lev.value
+
     def newton_solve_device(self, U_ptr, prec="fp64", ksp_rtol=1e-5, ksp_maxit=100000, abstol=1e-10,
-                            max_subiter=10000, verbose=False, history_cap=64):
+                            max_subiter=10000, verbose=False, history_cap=64, ksp="mg"):
         """Device Newton solve (igab_newton_solve) from the state at U_ptr (device, FP64,
         overwritten with the result).  Returns a dict of the solve info plus the ||F|| and
         Krylov-iteration history of each subiteration."""
@@ -194,6 +205,7 @@ class Assembly:
         o.ksp_maxit = int(ksp_maxit)
         o.abstol = float(abstol)
         o.max_subiter = int(max_subiter)
+        o.ksp = {"mg": 1, "bicgstab": 0}[ksp]
         o.verbose = 1 if verbose else 0
         info = native.IgabNewtonInfo()
         fh = np.zeros(history_cap)

@@ -333,6 +333,7 @@ static void free_ctx(igab_ctx *c)
     cudaFree(c->d_dens_part); cudaFree(c->d_HH);
     igab_krylov_release(c);
     igab_newton_release(c);
+    igab_mg_release(c);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     for (int k = 0; k < 6; k++)
@@ -517,6 +518,7 @@ extern "C" long igab_csr_offset(const igab_ctx *ctx, long row, long col)
 extern "C" int igab_set_par_mat(igab_ctx *ctx, const double par_mat[9])
 {
     ARG_CHECK(ctx && par_mat, "igab_set_par_mat: null argument");
+    if (memcmp(ctx->par_mat, par_mat, sizeof(ctx->par_mat)) != 0) ctx->param_version++;
     memcpy(ctx->par_mat, par_mat, sizeof(ctx->par_mat));
     return 0;
 }
@@ -536,6 +538,7 @@ extern "C" int igab_set_par_dirichlet(igab_ctx *ctx, const double par_dirichlet[
 extern "C" int igab_set_par_periodic(igab_ctx *ctx, const double par_periodic[9])
 {
     ARG_CHECK(ctx && par_periodic, "igab_set_par_periodic: null argument");
+    if (memcmp(ctx->par_periodic, par_periodic, sizeof(ctx->par_periodic)) != 0) ctx->param_version++;
     memcpy(ctx->par_periodic, par_periodic, sizeof(ctx->par_periodic));
     return 0;
 }
@@ -822,6 +825,37 @@ extern "C" int igab_solve_device(igab_ctx *ctx, const void *vals_dev, int prec, 
     return 0;
 }
 
+extern "C" int igab_solve_mg_device(igab_ctx *ctx, const void *vals_dev, int prec, const double *b_dev, double *x_dev,
+                                    double rtol, double atol, int maxit, igab_solve_info *info)
+{
+    ARG_CHECK(ctx && vals_dev && b_dev && x_dev, "igab_solve_mg_device: null argument");
+    ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_solve_mg_device: bad precision");
+    ARG_CHECK(maxit >= 1 && rtol >= 0.0 && atol >= 0.0, "igab_solve_mg_device: bad tolerances");
+    ARG_CHECK(ctx->stream != nullptr, "igab_solve_mg_device: needs a non-default stream (igab_set_stream)");
+    IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    int its = 0, conv = 0, brk = 0;
+    double rn = 0.0, bn = 0.0;
+    int rc = igab_mg_solve(ctx, vals_dev, prec, b_dev, x_dev, rtol, atol, maxit, &its, &conv, &rn, &bn, &brk);
+    if (rc) return rc;
+    if (info) {
+        info->iterations = its;
+        info->converged = conv;
+        info->residual_norm = rn;
+        info->rhs_norm = bn;
+    }
+    if (brk) {
+        igab_set_error("igab_solve_mg_device: CG breakdown (the tangent is not positive definite)");
+        return IGAB_ERR_UNSUPPORTED;
+    }
+    return 0;
+}
+
+extern "C" int igab_solve_mg_levels(igab_ctx *ctx, int *levels)
+{
+    ARG_CHECK(ctx && levels, "igab_solve_mg_levels: null argument");
+    return igab_mg_levels(ctx, levels);
+}
+
 extern "C" int igab_set_stream(igab_ctx *ctx, void *cuda_stream)
 {
     ARG_CHECK(ctx, "igab_set_stream: null context");
@@ -1024,6 +1058,7 @@ extern "C" int igab_set_element_log_scale(igab_ctx *ctx, const double *g, int on
 {
     ARG_CHECK(ctx, "igab_set_element_log_scale: null context");
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    ctx->param_version++;
     if (!g) {
         ctx->escale_on = false;
         return 0;

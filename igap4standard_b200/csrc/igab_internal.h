@@ -145,6 +145,10 @@ struct igab_ctx {
     void *d_nl_vals = nullptr;
     size_t nl_vals_bytes = 0;
 
+    /* multigrid hierarchy of the Krylov solve (igab_mg.cu), rebuilt when param_version changes */
+    struct igab_mg *mg = nullptr;
+    long param_version = 0;            /* bumped by every change of par_mat, par_periodic, element scales */
+
     /* captured assembly graph */
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -162,6 +166,11 @@ int igab_krylov_solve(igab_ctx *c, const void *dvals, int prec, const double *db
                       double atol, int maxit, int *iterations, int *converged, double *rnorm, double *bnorm);
 void igab_krylov_release(igab_ctx *c);
 void igab_newton_release(igab_ctx *c);   /* igab_newton.cu */
+/* igab_mg.cu: multigrid-preconditioned CG on the context's tangent (breakdown: p.Kp <= 0) */
+int igab_mg_solve(igab_ctx *c, const void *vals, int prec, const double *b, double *x, double rtol, double atol,
+                  int maxit, int *iterations, int *converged, double *rnorm, double *bnorm, int *breakdown);
+int igab_mg_levels(igab_ctx *c, int *levels);
+void igab_mg_release(igab_ctx *c);
 int igab_launch_tangent(igab_ctx *c, const double *dU, void *dvals, int prec);
 /* the same, slab by slab along x: after slab i, rows [0, row_end[i]) are final and
  * c->slab_ev[i] is recorded on c->stream (one slab when the kernels have no x-range) */

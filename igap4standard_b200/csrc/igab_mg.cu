@@ -1,0 +1,754 @@
+/*
+ * Geometric multigrid on nested spline spaces, as the preconditioner of a conjugate
+ * gradient solve with the assembled tangent (no reference counterpart: it stands in
+ * for the PETSc KSP of the reference application, src/snes_init.c:24-39, which is
+ * outside the assembly path).
+ *
+ * Why: the phys/ge tangent is a fourth-order operator (the strain-gradient term
+ * le^2 |grad grad u|^2), so its condition number grows like h^-4; Jacobi-preconditioned
+ * Krylov iterations stall at 32^3 and 64^3.  Multigrid keeps the iteration count flat.
+ *
+ * Hierarchy.  Level 0 is the caller's mesh.  Level l+1 removes every other interior
+ * knot of level l in each direction (n elements -> n / 2), so its spline space is a
+ * subspace of level l's: the prolongation is knot insertion of the removed knots
+ * (Boehm's algorithm for p = 2, built on the host as three 1-D matrices, applied on
+ * the device as their tensor product), the restriction its transpose.  Coarsening stops
+ * at about a thousand dofs, or where a direction has an odd element count.  Coarse
+ * operators are rediscretised: each coarse level is an igab context with the same
+ * material, boundary tables and (averaged) element scales, whose tangent is assembled
+ * at the zero state by the library's own kernels (a preconditioner, so the state it is
+ * linearised at only affects the convergence rate).  The coarsest level is solved
+ * directly (dense LU with partial pivoting on the host).  Dirichlet rows, identity rows
+ * of every level's tangent, are masked out of the restricted residuals and of the
+ * prolonged corrections, which keeps the V-cycle symmetric.
+ *
+ * Smoother: Chebyshev polynomial of degree 3 in D^-1 K on [lmax / 10, 1.1 lmax], lmax
+ * estimated by power iteration; the same polynomial before and after the coarse
+ * correction, so the V-cycle is a symmetric preconditioner and CG applies.
+ *
+ * The coarse levels are rebuilt when the material, the boundary tables' values or
+ * the element scales change (the context's parameter version); the fine level's
+ * diagonal and lmax are recomputed at every solve (the tangent changes per Newton step).
+ * Every dot product is a fixed-order reduction: solves are bitwise repeatable.
+ */
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include <cuda_runtime.h>
+#include "igab_internal.h"
+#include "igab_reduce.cuh"
+
+namespace {
+
+#define MG_THREADS 256
+#define MG_BLOCKS 296
+#define MG_MAX_LEVELS 8
+#define MG_DEGREE 3            /* Chebyshev degree per smoothing */
+#define MG_POWER_ITERS 12      /* power iterations for lmax of D^-1 K */
+#define MG_COARSE_DOF 1200     /* the coarsest level is solved directly below this size */
+
+/* 1-D prolongation along one direction: fine coefficient i = sum_a w[i][a] coarse idx[i][a]
+ * (kp entries per fine point), restriction coarse j = sum_b rw[j][b] fine ridx[j][b] */
+struct mg_dir {
+    int nf = 0, nc = 0, kp = 0, kr = 0;
+    int *p_idx = nullptr;
+    double *p_w = nullptr;
+    int *r_idx = nullptr;
+    double *r_w = nullptr;
+};
+
+struct mg_level {
+    igab_ctx *ctx = nullptr;       /* level 0: the caller's; coarser: owned */
+    long n = 0;
+    const void *vals = nullptr;    /* the level's tangent values */
+    int prec = IGAB_PREC_FP64;
+    double *own_vals = nullptr;    /* coarse levels: FP64 tangent at the zero state */
+    double *dinv = nullptr;
+    double lmax = 0.0;
+    double *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *t = nullptr;
+    mg_dir dir[3];                 /* transfer between this level (coarse) and the one above */
+};
+
+__global__ void k_mg_diag_inv(igab_geom g, const void *__restrict__ vals, int prec, double *__restrict__ dinv)
+{
+    const long r = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (r >= g.ndof) return;
+    const long cp = r / 3;
+    const int k1 = (int)(r % 3);
+    const int z1 = (int)(cp % g.nb[2]), y1 = (int)((cp / g.nb[2]) % g.nb[1]), x1 = (int)(cp / ((long)g.nb[2] * g.nb[1]));
+    const int x0 = x1 > 2 ? x1 - 2 : 0, y0 = y1 > 2 ? y1 - 2 : 0, z0 = z1 > 2 ? z1 - 2 : 0;
+    const int ye = y1 + 2 < g.nb[1] - 1 ? y1 + 2 : g.nb[1] - 1;
+    const int ze = z1 + 2 < g.nb[2] - 1 ? z1 + 2 : g.nb[2] - 1;
+    const int nyb = ye - y0 + 1, nzb = ze - z0 + 1;
+    const long pos = g.rowptr[r] + (((long)(x1 - x0) * nyb + (y1 - y0)) * nzb + (z1 - z0)) * 3 + k1;
+    const double dv = prec == IGAB_PREC_FP64 ? ((const double *)vals)[pos] : (double)((const float *)vals)[pos];
+    dinv[r] = dv != 0.0 ? 1.0 / dv : 1.0;
+}
+
+#define MG_LOOP(i, n) for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < (n); i += (long)gridDim.x * blockDim.x)
+
+/* d = s * dinv * r */
+__global__ void k_mg_jac(long n, const double *__restrict__ dinv, const double *__restrict__ r, double s,
+                         double *__restrict__ d)
+{
+    MG_LOOP(i, n) d[i] = s * dinv[i] * r[i];
+}
+
+/* x += d, (x was zero when first) */
+__global__ void k_mg_add(long n, const double *__restrict__ d, double *__restrict__ x, int first)
+{
+    MG_LOOP(i, n) x[i] = first ? d[i] : x[i] + d[i];
+}
+
+/* r -= t; d = a d + c dinv r */
+__global__ void k_mg_cheb(long n, const double *__restrict__ t, const double *__restrict__ dinv, double a, double c,
+                          double *__restrict__ r, double *__restrict__ d, int update_d)
+{
+    MG_LOOP(i, n)
+    {
+        const double ri = r[i] - t[i];
+        r[i] = ri;
+        if (update_d) d[i] = a * d[i] + c * dinv[i] * ri;
+    }
+}
+
+/* r = b - t */
+__global__ void k_mg_sub(long n, const double *__restrict__ b, const double *__restrict__ t, double *__restrict__ r)
+{
+    MG_LOOP(i, n) r[i] = b[i] - t[i];
+}
+
+/* y = a x + b y */
+__global__ void k_mg_axpby(long n, double a, const double *__restrict__ x, double b, double *__restrict__ y)
+{
+    MG_LOOP(i, n) y[i] = a * x[i] + b * y[i];
+}
+
+__global__ void k_mg_copy(long n, const double *__restrict__ x, double *__restrict__ y)
+{
+    MG_LOOP(i, n) y[i] = x[i];
+}
+
+__global__ void k_mg_zero_rows(long nd, const int *__restrict__ rows, double *__restrict__ v)
+{
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t < nd) v[rows[t]] = 0.0;
+}
+
+struct mg_dirs_dev {
+    const int *p_idx[3];
+    const double *p_w[3];
+    const int *r_idx[3];
+    const double *r_w[3];
+    int kp[3], kr[3];
+    int nbf[3], nbc[3];
+};
+
+/* xf += P xc (tensor product of the three 1-D prolongations, per displacement component) */
+__global__ void k_mg_prolong(mg_dirs_dev D, const double *__restrict__ xc, double *__restrict__ xf)
+{
+    const long nf = (long)D.nbf[0] * D.nbf[1] * D.nbf[2];
+    MG_LOOP(f, nf)
+    {
+        const int iz = (int)(f % D.nbf[2]), iy = (int)((f / D.nbf[2]) % D.nbf[1]), ix = (int)(f / ((long)D.nbf[2] * D.nbf[1]));
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (int a = 0; a < D.kp[0]; a++) {
+            const double wa = D.p_w[0][ix * D.kp[0] + a];
+            const int ja = D.p_idx[0][ix * D.kp[0] + a];
+            for (int b = 0; b < D.kp[1]; b++) {
+                const double wab = wa * D.p_w[1][iy * D.kp[1] + b];
+                const long jab = ((long)ja * D.nbc[1] + D.p_idx[1][iy * D.kp[1] + b]) * D.nbc[2];
+                for (int c = 0; c < D.kp[2]; c++) {
+                    const double w = wab * D.p_w[2][iz * D.kp[2] + c];
+                    const double *u = xc + 3 * (jab + D.p_idx[2][iz * D.kp[2] + c]);
+                    s0 += w * u[0];
+                    s1 += w * u[1];
+                    s2 += w * u[2];
+                }
+            }
+        }
+        xf[3 * f] += s0;
+        xf[3 * f + 1] += s1;
+        xf[3 * f + 2] += s2;
+    }
+}
+
+/* rc = P^T rf */
+__global__ void k_mg_restrict(mg_dirs_dev D, const double *__restrict__ rf, double *__restrict__ rc)
+{
+    const long nc = (long)D.nbc[0] * D.nbc[1] * D.nbc[2];
+    MG_LOOP(j, nc)
+    {
+        const int jz = (int)(j % D.nbc[2]), jy = (int)((j / D.nbc[2]) % D.nbc[1]), jx = (int)(j / ((long)D.nbc[2] * D.nbc[1]));
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (int a = 0; a < D.kr[0]; a++) {
+            const double wa = D.r_w[0][jx * D.kr[0] + a];
+            const int ia = D.r_idx[0][jx * D.kr[0] + a];
+            for (int b = 0; b < D.kr[1]; b++) {
+                const double wab = wa * D.r_w[1][jy * D.kr[1] + b];
+                const long iab = ((long)ia * D.nbf[1] + D.r_idx[1][jy * D.kr[1] + b]) * D.nbf[2];
+                for (int c = 0; c < D.kr[2]; c++) {
+                    const double w = wab * D.r_w[2][jz * D.kr[2] + c];
+                    const double *u = rf + 3 * (iab + D.r_idx[2][jz * D.kr[2] + c]);
+                    s0 += w * u[0];
+                    s1 += w * u[1];
+                    s2 += w * u[2];
+                }
+            }
+        }
+        rc[3 * j] = s0;
+        rc[3 * j + 1] = s1;
+        rc[3 * j + 2] = s2;
+    }
+}
+
+} /* namespace */
+
+/* 1-D prolongation by knot insertion (Boehm, p = 2): the coarse knot vector kc (open)
+ * refined by the knots `ins` (ascending, inside the open interval) into the fine one.
+ * P[i][j] (nb_f x nb_c, row-major) maps coarse spline coefficients to fine ones. */
+static void igab_mg_knot_prolongation(const std::vector<double> &kc, const std::vector<double> &ins,
+                                      std::vector<double> &P, int &nbf, int &nbc)
+{
+    std::vector<double> kv = kc;
+    nbc = (int)kc.size() - 3;
+    std::vector<std::vector<double>> M(nbc, std::vector<double>(nbc, 0.0));
+    for (int j = 0; j < nbc; j++) M[j][j] = 1.0;
+    for (double t : ins) {
+        const int nk = (int)kv.size(), nb = nk - 3;
+        int k = 2;
+        while (k + 1 < nk - 3 && !(kv[k] <= t && t < kv[k + 1])) k++;
+        std::vector<std::vector<double>> Q(nb + 1, std::vector<double>(nbc, 0.0));
+        for (int i = 0; i <= nb; i++) {
+            if (i <= k - 2) Q[i] = M[i];
+            else if (i >= k + 1) Q[i] = M[i - 1];
+            else {
+                const double a = (t - kv[i]) / (kv[i + 2] - kv[i]);
+                for (int j = 0; j < nbc; j++) Q[i][j] = a * M[i][j] + (1.0 - a) * M[i - 1][j];
+            }
+        }
+        M.swap(Q);
+        kv.insert(kv.begin() + k + 1, t);
+    }
+    nbf = (int)M.size();
+    P.assign((size_t)nbf * nbc, 0.0);
+    for (int i = 0; i < nbf; i++)
+        for (int j = 0; j < nbc; j++) P[(size_t)i * nbc + j] = M[i][j];
+}
+
+struct igab_mg {
+    int nlev = 0;
+    mg_level L[MG_MAX_LEVELS];
+    long version = -1;
+    bool direct = false;            /* coarsest level solved by dense LU */
+    int nd = 0;                     /* its size */
+    std::vector<double> lu;
+    std::vector<int> piv;
+    double *h_vec = nullptr;        /* pinned nd doubles */
+    double *part = nullptr, *dots = nullptr, *h_dots = nullptr;
+    double *zero = nullptr;         /* coarse zero state */
+    double *cg = nullptr;           /* CG vectors r, z, p, q of the caller's mesh */
+    long cg_n = 0;
+    int launches = 0;
+};
+
+namespace {
+
+int mg_free_level(mg_level &L, bool own)
+{
+    if (own && L.ctx) igab_destroy(L.ctx);
+    cudaFree(L.own_vals);
+    cudaFree(L.dinv);
+    cudaFree(L.x);
+    for (int d = 0; d < 3; d++) {
+        cudaFree(L.dir[d].p_idx);
+        cudaFree(L.dir[d].p_w);
+        cudaFree(L.dir[d].r_idx);
+        cudaFree(L.dir[d].r_w);
+    }
+    L = mg_level();
+    return 0;
+}
+
+void mg_free(igab_mg *m)
+{
+    if (!m) return;
+    for (int l = 0; l < m->nlev; l++) mg_free_level(m->L[l], l > 0);
+    cudaFree(m->part);
+    cudaFree(m->zero);
+    cudaFree(m->cg);
+    cudaFreeHost(m->h_vec);
+    cudaFreeHost(m->h_dots);
+    delete m;
+}
+
+int mg_vectors(mg_level &L)
+{
+    const size_t bytes = (size_t)L.n * sizeof(double);
+    IGAB_CUDA_TRY(cudaMalloc((void **)&L.x, 5 * bytes));
+    L.b = L.x + L.n;
+    L.r = L.b + L.n;
+    L.d = L.r + L.n;
+    L.t = L.d + L.n;
+    IGAB_CUDA_TRY(cudaMalloc((void **)&L.dinv, bytes));
+    return 0;
+}
+
+int mg_upload_dir(mg_dir &D, const std::vector<double> &P, int nbf, int nbc)
+{
+    std::vector<std::vector<std::pair<int, double>>> rows(nbf), cols(nbc);
+    for (int i = 0; i < nbf; i++)
+        for (int j = 0; j < nbc; j++) {
+            const double w = P[(size_t)i * nbc + j];
+            if (w != 0.0) {
+                rows[i].push_back({j, w});
+                cols[j].push_back({i, w});
+            }
+        }
+    int kp = 1, kr = 1;
+    for (auto &r : rows) kp = std::max(kp, (int)r.size());
+    for (auto &c : cols) kr = std::max(kr, (int)c.size());
+    std::vector<int> pi((size_t)nbf * kp, 0), ri((size_t)nbc * kr, 0);
+    std::vector<double> pw((size_t)nbf * kp, 0.0), rw((size_t)nbc * kr, 0.0);
+    for (int i = 0; i < nbf; i++)
+        for (size_t a = 0; a < rows[i].size(); a++) {
+            pi[(size_t)i * kp + a] = rows[i][a].first;
+            pw[(size_t)i * kp + a] = rows[i][a].second;
+        }
+    for (int j = 0; j < nbc; j++)
+        for (size_t b = 0; b < cols[j].size(); b++) {
+            ri[(size_t)j * kr + b] = cols[j][b].first;
+            rw[(size_t)j * kr + b] = cols[j][b].second;
+        }
+    D.nf = nbf;
+    D.nc = nbc;
+    D.kp = kp;
+    D.kr = kr;
+    IGAB_CUDA_TRY(cudaMalloc((void **)&D.p_idx, pi.size() * sizeof(int)));
+    IGAB_CUDA_TRY(cudaMalloc((void **)&D.p_w, pw.size() * sizeof(double)));
+    IGAB_CUDA_TRY(cudaMalloc((void **)&D.r_idx, ri.size() * sizeof(int)));
+    IGAB_CUDA_TRY(cudaMalloc((void **)&D.r_w, rw.size() * sizeof(double)));
+    IGAB_CUDA_TRY(cudaMemcpy(D.p_idx, pi.data(), pi.size() * sizeof(int), cudaMemcpyHostToDevice));
+    IGAB_CUDA_TRY(cudaMemcpy(D.p_w, pw.data(), pw.size() * sizeof(double), cudaMemcpyHostToDevice));
+    IGAB_CUDA_TRY(cudaMemcpy(D.r_idx, ri.data(), ri.size() * sizeof(int), cudaMemcpyHostToDevice));
+    IGAB_CUDA_TRY(cudaMemcpy(D.r_w, rw.data(), rw.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+mg_dirs_dev dirs_view(const mg_level &C)
+{
+    mg_dirs_dev D;
+    for (int d = 0; d < 3; d++) {
+        D.p_idx[d] = C.dir[d].p_idx;
+        D.p_w[d] = C.dir[d].p_w;
+        D.r_idx[d] = C.dir[d].r_idx;
+        D.r_w[d] = C.dir[d].r_w;
+        D.kp[d] = C.dir[d].kp;
+        D.kr[d] = C.dir[d].kr;
+        D.nbf[d] = C.dir[d].nf;
+        D.nbc[d] = C.dir[d].nc;
+    }
+    return D;
+}
+
+/* dense LU with partial pivoting (column-major n x n in a), in place */
+bool lu_factor(int n, std::vector<double> &a, std::vector<int> &piv)
+{
+    piv.resize(n);
+    for (int k = 0; k < n; k++) {
+        int p = k;
+        double mx = std::fabs(a[(size_t)k * n + k]);
+        for (int i = k + 1; i < n; i++)
+            if (std::fabs(a[(size_t)k * n + i]) > mx) { mx = std::fabs(a[(size_t)k * n + i]); p = i; }
+        if (mx == 0.0) return false;
+        piv[k] = p;
+        if (p != k)
+            for (int j = 0; j < n; j++) std::swap(a[(size_t)j * n + k], a[(size_t)j * n + p]);
+        const double inv = 1.0 / a[(size_t)k * n + k];
+        for (int i = k + 1; i < n; i++) a[(size_t)k * n + i] *= inv;
+        for (int j = k + 1; j < n; j++) {
+            const double akj = a[(size_t)j * n + k];
+            if (akj != 0.0)
+                for (int i = k + 1; i < n; i++) a[(size_t)j * n + i] -= a[(size_t)k * n + i] * akj;
+        }
+    }
+    return true;
+}
+
+void lu_solve(int n, const std::vector<double> &a, const std::vector<int> &piv, double *x)
+{
+    for (int k = 0; k < n; k++) std::swap(x[k], x[piv[k]]);
+    for (int j = 0; j < n; j++)
+        for (int i = j + 1; i < n; i++) x[i] -= a[(size_t)j * n + i] * x[j];
+    for (int j = n - 1; j >= 0; j--) {
+        x[j] /= a[(size_t)j * n + j];
+        for (int i = 0; i < j; i++) x[i] -= a[(size_t)j * n + i] * x[j];
+    }
+}
+
+int spmv(igab_mg *m, mg_level &L, const double *x, double *y)
+{
+    const int rc = igab_launch_spmv(L.ctx, L.vals, L.prec, x, y);
+    m->launches++;
+    return rc;
+}
+
+/* lmax of D^-1 K by power iteration from a fixed start vector */
+int estimate_lmax(igab_mg *m, mg_level &L)
+{
+    cudaStream_t st = L.ctx->stream;
+    const long n = L.n;
+    std::vector<double> v0((size_t)n);
+    unsigned s = 12345u;
+    for (long i = 0; i < n; i++) {
+        s = s * 1664525u + 1013904223u;
+        v0[(size_t)i] = 0.5 + (double)(s >> 8) / (double)(1u << 24);
+    }
+    IGAB_CUDA_TRY(cudaMemcpyAsync(L.d, v0.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st));
+    double lam = 0.0, dd[2];
+    for (int it = 0; it < MG_POWER_ITERS; it++) {
+        int rc = spmv(m, L, L.d, L.t);
+        if (rc) return rc;
+        k_mg_jac<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, L.dinv, L.t, 1.0, L.r);   /* r = D^-1 K d */
+        IGAB_CUDA_TRY(rd_dot2(st, n, L.r, L.r, L.d, L.d, m->part, m->dots, m->h_dots, dd));
+        const double nr = std::sqrt(dd[0]);
+        lam = dd[1] > 0.0 ? nr / std::sqrt(dd[1]) : 0.0;
+        if (nr == 0.0) break;
+        k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, 1.0 / nr, L.r, 0.0, L.d);   /* d = r / ||r|| */
+        m->launches += 4;
+    }
+    L.lmax = lam > 0.0 ? lam : 1.0;
+    return 0;
+}
+
+/* Chebyshev smoothing of K x = b on level L from the current (x, r = b - K x);
+ * first: x is zero (x and r written from scratch: r = b on entry) */
+int chebyshev(igab_mg *m, mg_level &L, bool first)
+{
+    cudaStream_t st = L.ctx->stream;
+    const long n = L.n;
+    const double hi = 1.1 * L.lmax, lo = hi / 10.0;
+    const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    k_mg_jac<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, L.dinv, L.r, 1.0 / theta, L.d);
+    for (int i = 0; i < MG_DEGREE; i++) {
+        k_mg_add<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, L.d, L.x, first && i == 0);
+        int rc = spmv(m, L, L.d, L.t);
+        if (rc) return rc;
+        const double rn = 1.0 / (2.0 * sigma - rho);
+        k_mg_cheb<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, L.t, L.dinv, rn * rho, 2.0 * rn / delta, L.r, L.d,
+                                                     i + 1 < MG_DEGREE);
+        rho = rn;
+        m->launches += 2;
+    }
+    m->launches++;
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+void zero_dirichlet(igab_mg *m, mg_level &L, double *v)
+{
+    if (L.ctx->nd > 0) {
+        k_mg_zero_rows<<<(unsigned)((L.ctx->nd + 255) / 256), 256, 0, L.ctx->stream>>>(L.ctx->nd, L.ctx->d_drow, v);
+        m->launches++;
+    }
+}
+
+/* x_l = V-cycle approximation of K_l^-1 b_l (b in L.b, result in L.x) */
+int vcycle(igab_mg *m, int l)
+{
+    mg_level &L = m->L[l];
+    cudaStream_t st = L.ctx->stream;
+    if (l == m->nlev - 1) {
+        if (m->direct) {
+            IGAB_CUDA_TRY(cudaMemcpyAsync(m->h_vec, L.b, (size_t)L.n * sizeof(double), cudaMemcpyDeviceToHost, st));
+            IGAB_CUDA_TRY(cudaStreamSynchronize(st));
+            lu_solve(m->nd, m->lu, m->piv, m->h_vec);
+            IGAB_CUDA_TRY(cudaMemcpyAsync(L.x, m->h_vec, (size_t)L.n * sizeof(double), cudaMemcpyHostToDevice, st));
+        } else {
+            k_mg_jac<<<MG_BLOCKS, MG_THREADS, 0, st>>>(L.n, L.dinv, L.b, 1.0, L.x);
+            m->launches++;
+        }
+        return 0;
+    }
+    mg_level &C = m->L[l + 1];
+    k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(L.n, L.b, L.r);
+    m->launches++;
+    int rc = chebyshev(m, L, true);
+    if (rc) return rc;
+    /* coarse correction with the Dirichlet rows of both levels masked (symmetric) */
+    zero_dirichlet(m, L, L.r);
+    const mg_dirs_dev D = dirs_view(C);
+    k_mg_restrict<<<MG_BLOCKS, MG_THREADS, 0, st>>>(D, L.r, C.b);
+    m->launches++;
+    zero_dirichlet(m, C, C.b);
+    if ((rc = vcycle(m, l + 1))) return rc;
+    zero_dirichlet(m, C, C.x);
+    IGAB_CUDA_TRY(cudaMemsetAsync(L.t, 0, (size_t)L.n * sizeof(double), st));
+    k_mg_prolong<<<MG_BLOCKS, MG_THREADS, 0, st>>>(D, C.x, L.t);
+    m->launches++;
+    zero_dirichlet(m, L, L.t);
+    k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(L.n, 1.0, L.t, 1.0, L.x);
+    /* r = b - K x, then the same smoother again */
+    if ((rc = spmv(m, L, L.x, L.t))) return rc;
+    k_mg_sub<<<MG_BLOCKS, MG_THREADS, 0, st>>>(L.n, L.b, L.t, L.r);
+    m->launches += 2;
+    if ((rc = chebyshev(m, L, false))) return rc;
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+/* the coarse levels for the context's current parameters */
+int mg_build(igab_ctx *c, igab_mg *m)
+{
+    for (int l = 1; l < m->nlev; l++) mg_free_level(m->L[l], true);
+    m->nlev = 1;
+    m->direct = false;
+    mg_level &F = m->L[0];
+    F.ctx = c;
+    F.n = c->ndof;
+    if (!F.x) {
+        int rc = mg_vectors(F);
+        if (rc) return rc;
+    }
+    /* element log-scales of the caller's context (averaged per coarse element below) */
+    std::vector<double> s_f;
+    if (c->escale_on) {
+        s_f.resize((size_t)c->nel);
+        IGAB_CUDA_TRY(cudaMemcpy(s_f.data(), c->d_escale, (size_t)c->nel * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    size_t zero_n = 0;
+    while (m->nlev < MG_MAX_LEVELS) {
+        igab_ctx *f = m->L[m->nlev - 1].ctx;
+        if (f->ndof <= MG_COARSE_DOF) break;
+        bool ok = true;
+        for (int d = 0; d < 3; d++) ok = ok && f->ne[d] % 2 == 0 && f->ne[d] >= 4;
+        if (!ok) break;
+        igab_mesh_desc desc;
+        memset(&desc, 0, sizeof(desc));
+        desc.phys = f->phys;
+        std::vector<double> kn;
+        std::vector<double> knc[3], ins[3];
+        for (int d = 0; d < 3; d++) {
+            const std::vector<double> &kf = f->knots[d];
+            const int n = f->ne[d];
+            desc.nelem[d] = n / 2;
+            knc[d].assign(kf.begin(), kf.begin() + 3);
+            for (int i = 1; i < n; i++) {   /* interior knot i sits at kf[2 + i] */
+                if (i % 2 == 0) knc[d].push_back(kf[2 + i]);
+                else ins[d].push_back(kf[2 + i]);
+            }
+            knc[d].insert(knc[d].end(), kf.end() - 3, kf.end());
+            kn.insert(kn.end(), knc[d].begin(), knc[d].end());
+        }
+        desc.knots = kn.data();
+        memcpy(desc.par_mat, f->par_mat, sizeof(desc.par_mat));
+        memcpy(desc.bc_type, f->bc_type, sizeof(desc.bc_type));
+        memcpy(desc.par_periodic, f->par_periodic, sizeof(desc.par_periodic));
+        memcpy(desc.par_dirichlet, f->par_dirichlet, sizeof(desc.par_dirichlet));
+        igab_ctx *cc = nullptr;
+        int rc = igab_create(&desc, f->device, &cc);
+        if (rc) return rc;
+        mg_level &C = m->L[m->nlev];
+        C.ctx = cc;
+        m->nlev++;
+        if ((rc = igab_set_stream(cc, c->stream))) return rc;
+        C.n = cc->ndof;
+        C.prec = IGAB_PREC_FP64;
+        for (int d = 0; d < 3; d++) {
+            std::vector<double> P;
+            int nbf = 0, nbc = 0;
+            igab_mg_knot_prolongation(knc[d], ins[d], P, nbf, nbc);
+            if (nbf != f->nb[d] || nbc != cc->nb[d]) {
+                igab_set_error("multigrid: prolongation size %d x %d, expected %d x %d", nbf, nbc, f->nb[d], cc->nb[d]);
+                return IGAB_ERR_ARG;
+            }
+            if ((rc = mg_upload_dir(C.dir[d], P, nbf, nbc))) return rc;
+        }
+        if ((rc = mg_vectors(C))) return rc;
+        /* element scales: the mean of the eight fine elements of each coarse element */
+        if (!s_f.empty()) {
+            const int *nf = f->ne, *nc = cc->ne;
+            std::vector<double> gc((size_t)cc->nel);
+            for (int ex = 0; ex < nc[0]; ex++)
+                for (int ey = 0; ey < nc[1]; ey++)
+                    for (int ez = 0; ez < nc[2]; ez++) {
+                        double sum = 0.0;
+                        for (int k = 0; k < 8; k++) {
+                            const long fe = ((long)(2 * ex + (k >> 2)) * nf[1] + 2 * ey + ((k >> 1) & 1)) * nf[2] +
+                                            2 * ez + (k & 1);
+                            sum += s_f[(size_t)fe];
+                        }
+                        gc[((size_t)ex * nc[1] + ey) * nc[2] + ez] = std::log(sum / 8.0);
+                    }
+            std::vector<double> sc((size_t)cc->nel);
+            for (size_t e = 0; e < sc.size(); e++) sc[e] = std::exp(gc[e]);
+            s_f.swap(sc);
+            if ((rc = igab_set_element_log_scale(cc, gc.data(), 0))) return rc;
+        }
+        /* the coarse tangent at the zero state */
+        if ((size_t)C.n > zero_n) {
+            cudaFree(m->zero);
+            m->zero = nullptr;
+            IGAB_CUDA_TRY(cudaMalloc((void **)&m->zero, (size_t)C.n * sizeof(double)));
+            IGAB_CUDA_TRY(cudaMemset(m->zero, 0, (size_t)C.n * sizeof(double)));
+            zero_n = (size_t)C.n;
+        }
+        IGAB_CUDA_TRY(cudaMalloc((void **)&C.own_vals, (size_t)cc->nnz * sizeof(double)));
+        if ((rc = igab_launch_tangent(cc, m->zero, C.own_vals, IGAB_PREC_FP64))) return rc;
+        C.vals = C.own_vals;
+        k_mg_diag_inv<<<(unsigned)((C.n + 255) / 256), 256, 0, c->stream>>>(cc->geom(), C.vals, C.prec, C.dinv);
+        IGAB_CUDA_TRY(cudaGetLastError());
+        if ((rc = estimate_lmax(m, C))) return rc;
+    }
+    /* the coarsest level directly, when small */
+    mg_level &B = m->L[m->nlev - 1];
+    if (m->nlev > 1 && B.n <= MG_COARSE_DOF) {
+        igab_ctx *cc = B.ctx;
+        const int n = (int)B.n;
+        std::vector<int> cols((size_t)cc->nnz);
+        int rc = igab_csr_pattern(cc, nullptr, cols.data());
+        if (rc) return rc;
+        std::vector<double> v((size_t)cc->nnz);
+        IGAB_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        IGAB_CUDA_TRY(cudaMemcpy(v.data(), B.vals, (size_t)cc->nnz * sizeof(double), cudaMemcpyDeviceToHost));
+        m->lu.assign((size_t)n * n, 0.0);
+        for (int r = 0; r < n; r++)
+            for (int k = cc->rowptr_h[r]; k < cc->rowptr_h[r + 1]; k++) m->lu[(size_t)cols[k] * n + r] = v[k];
+        if (!lu_factor(n, m->lu, m->piv)) {
+            igab_set_error("multigrid: the coarsest tangent is singular");
+            return IGAB_ERR_NONFINITE;
+        }
+        m->direct = true;
+        m->nd = n;
+        cudaFreeHost(m->h_vec);
+        m->h_vec = nullptr;
+        IGAB_CUDA_TRY(cudaMallocHost((void **)&m->h_vec, (size_t)n * sizeof(double)));
+    }
+    m->version = c->param_version;
+    return 0;
+}
+
+} /* namespace */
+
+void igab_mg_release(igab_ctx *c)
+{
+    mg_free(c->mg);
+    c->mg = nullptr;
+}
+
+int igab_mg_levels(igab_ctx *c, int *levels)
+{
+    *levels = c->mg ? c->mg->nlev : 0;
+    return 0;
+}
+
+int igab_mg_solve(igab_ctx *c, const void *vals, int prec, const double *b, double *x, double rtol, double atol,
+                  int maxit, int *iterations, int *converged, double *rnorm, double *bnorm, int *breakdown)
+{
+    if (!c->mg) {
+        c->mg = new igab_mg();
+        IGAB_CUDA_TRY(cudaMalloc((void **)&c->mg->part, (2 * RD_BLOCKS + 2) * sizeof(double)));
+        c->mg->dots = c->mg->part + 2 * RD_BLOCKS;
+        IGAB_CUDA_TRY(cudaMallocHost((void **)&c->mg->h_dots, 2 * sizeof(double)));
+    }
+    igab_mg *m = c->mg;
+    m->launches = 0;
+    int rc = 0;
+    if (m->version != c->param_version || m->nlev == 0)
+        if ((rc = mg_build(c, m))) return rc;
+    mg_level &F = m->L[0];
+    F.vals = vals;
+    F.prec = prec;
+    cudaStream_t st = c->stream;
+    const long n = F.n;
+    k_mg_diag_inv<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(c->geom(), vals, prec, F.dinv);
+    IGAB_CUDA_TRY(cudaGetLastError());
+    if ((rc = estimate_lmax(m, F))) return rc;
+    /* preconditioned CG: x = 0, r = b; the fine level's work vectors belong to the V-cycle,
+     * so CG keeps r, z, p, q in x's companions below */
+    if (m->cg_n != n) {
+        cudaFree(m->cg);
+        m->cg = nullptr;
+        m->cg_n = 0;
+        IGAB_CUDA_TRY(cudaMalloc((void **)&m->cg, (size_t)4 * n * sizeof(double)));
+        m->cg_n = n;
+    }
+    double *r = m->cg, *z = r + n, *p = z + n, *q = p + n;
+    auto cleanup = [&]() {};
+    k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, b, r);
+    k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, 0.0, r, 0.0, x);
+    double d2[2];
+    cudaError_t e = rd_dot2(st, n, b, b, nullptr, nullptr, m->part, m->dots, m->h_dots, d2);
+    if (e != cudaSuccess) { cleanup(); IGAB_CUDA_TRY(e); }
+    const double bn = std::sqrt(d2[0]);
+    const double tol = std::max(rtol * bn, atol);
+    *bnorm = bn;
+    *rnorm = bn;
+    *iterations = 0;
+    *converged = bn <= tol ? 1 : 0;
+    *breakdown = 0;
+    if (*converged) { cleanup(); return 0; }
+    auto precond = [&](const double *rin, double *zout) -> int {
+        k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, rin, F.b);
+        int rc2 = vcycle(m, 0);
+        if (rc2) return rc2;
+        k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, F.x, zout);
+        m->launches += 2;
+        return 0;
+    };
+    if ((rc = precond(r, z))) { cleanup(); return rc; }
+    k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, z, p);
+    e = rd_dot2(st, n, r, z, nullptr, nullptr, m->part, m->dots, m->h_dots, d2);
+    if (e != cudaSuccess) { cleanup(); IGAB_CUDA_TRY(e); }
+    double rz = d2[0];
+    for (int it = 1; it <= maxit; it++) {
+        if ((rc = igab_launch_spmv(c, vals, prec, p, q))) { cleanup(); return rc; }
+        e = rd_dot2(st, n, p, q, nullptr, nullptr, m->part, m->dots, m->h_dots, d2);
+        if (e != cudaSuccess) { cleanup(); IGAB_CUDA_TRY(e); }
+        const double pq = d2[0];
+        if (!(pq > 0.0) || !(rz > 0.0)) { *breakdown = 1; break; }
+        const double alpha = rz / pq;
+        k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, alpha, p, 1.0, x);
+        k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, -alpha, q, 1.0, r);
+        e = rd_dot2(st, n, r, r, nullptr, nullptr, m->part, m->dots, m->h_dots, d2);
+        if (e != cudaSuccess) { cleanup(); IGAB_CUDA_TRY(e); }
+        *iterations = it;
+        *rnorm = std::sqrt(d2[0]);
+        if (*rnorm <= tol) { *converged = 1; break; }
+        if ((rc = precond(r, z))) { cleanup(); return rc; }
+        e = rd_dot2(st, n, r, z, nullptr, nullptr, m->part, m->dots, m->h_dots, d2);
+        if (e != cudaSuccess) { cleanup(); IGAB_CUDA_TRY(e); }
+        const double beta = d2[0] / rz;
+        rz = d2[0];
+        k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, 1.0, z, beta, p);
+        m->launches += 10;
+    }
+    cleanup();
+    IGAB_CUDA_TRY(cudaGetLastError());
+    IGAB_CUDA_TRY(cudaStreamSynchronize(st));
+    c->last_launches = m->launches;
+    return 0;
+}
+
+extern "C" int igab_mg_prolongation_1d(const double *coarse_knots, int n_coarse_elements, const double *inserted,
+                                       int n_inserted, double *P)
+{
+    if (!coarse_knots || !P || n_coarse_elements < 1 || n_inserted < 0 || (n_inserted > 0 && !inserted)) {
+        igab_set_error("igab_mg_prolongation_1d: bad argument");
+        return IGAB_ERR_ARG;
+    }
+    std::vector<double> kc(coarse_knots, coarse_knots + n_coarse_elements + 5);
+    std::vector<double> ins(inserted, inserted + n_inserted);
+    for (int i = 0; i < n_inserted; i++)
+        if (!(ins[i] > kc[2] && ins[i] < kc[kc.size() - 3]) || (i > 0 && ins[i] < ins[i - 1])) {
+            igab_set_error("igab_mg_prolongation_1d: inserted knots must be ascending and interior");
+            return IGAB_ERR_ARG;
+        }
+    std::vector<double> M;
+    int nbf = 0, nbc = 0;
+    igab_mg_knot_prolongation(kc, ins, M, nbf, nbc);
+    memcpy(P, M.data(), M.size() * sizeof(double));
+    return 0;
+}

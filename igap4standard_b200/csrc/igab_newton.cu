@@ -30,62 +30,14 @@
 #include <cstdio>
 #include <cuda_runtime.h>
 #include "igab_internal.h"
+#include "igab_reduce.cuh"
 
 namespace {
 
 #define NL_THREADS 256
-#define NL_BLOCKS 296   /* 2 x 148 SMs */
+#define NL_BLOCKS RD_BLOCKS
 
 constexpr double NL_F_OLD0 = 999.0;   /* src/snes_solve.c:22 */
-
-/* partial sums of (a0, b0) [and (a1, b1)] per block, fixed order */
-__global__ void __launch_bounds__(NL_THREADS) k_nl_dot(long n, const double *__restrict__ a0,
-                                                       const double *__restrict__ b0, const double *__restrict__ a1,
-                                                       const double *__restrict__ b1, double *part)
-{
-    double s0 = 0.0, s1 = 0.0;
-    for (long i = blockIdx.x * (long)NL_THREADS + threadIdx.x; i < n; i += (long)NL_BLOCKS * NL_THREADS) {
-        s0 += a0[i] * b0[i];
-        if (a1) s1 += a1[i] * b1[i];
-    }
-    __shared__ double red[2][NL_THREADS / 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-    }
-    if (lane == 0) {
-        red[0][warp] = s0;
-        red[1][warp] = s1;
-    }
-    __syncthreads();
-    if (threadIdx.x < 2) {
-        double s = 0.0;
-        for (int w = 0; w < NL_THREADS / 32; w++) s += red[threadIdx.x][w];
-        part[threadIdx.x * NL_BLOCKS + blockIdx.x] = s;
-    }
-}
-
-/* one block: out[k] = sum of part[k][0..NL_BLOCKS) in a fixed order */
-__global__ void __launch_bounds__(NL_THREADS) k_nl_finish(const double *part, double *out)
-{
-    __shared__ double red[2][NL_THREADS / 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = 0; k < 2; k++) {
-        double s = 0.0;
-        for (int b = threadIdx.x; b < NL_BLOCKS; b += NL_THREADS) s += part[k * NL_BLOCKS + b];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) red[k][warp] = s;
-    }
-    __syncthreads();
-    if (threadIdx.x < 2) {
-        double s = 0.0;
-        for (int w = 0; w < NL_THREADS / 32; w++) s += red[threadIdx.x][w];
-        out[threadIdx.x] = s;
-    }
-}
 
 /* W = X - lam Y */
 __global__ void k_nl_step(long n, const double *__restrict__ X, const double *__restrict__ Y, double lam,
@@ -114,14 +66,8 @@ struct nl_work {
     /* (a0, b0) [and (a1, b1)] on the device, both results on the host */
     int dot(const double *a0, const double *b0, const double *a1, const double *b1, double out[2])
     {
-        k_nl_dot<<<NL_BLOCKS, NL_THREADS, 0, c->stream>>>(n, a0, b0, a1, b1, part);
-        k_nl_finish<<<1, NL_THREADS, 0, c->stream>>>(part, dots);
         launches += 2;
-        IGAB_CUDA_TRY(cudaGetLastError());
-        IGAB_CUDA_TRY(cudaMemcpyAsync(h_dots, dots, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        IGAB_CUDA_TRY(cudaStreamSynchronize(c->stream));
-        out[0] = h_dots[0];
-        out[1] = h_dots[1];
+        IGAB_CUDA_TRY(rd_dot2(c->stream, n, a0, b0, a1, b1, part, dots, h_dots, out));
         return 0;
     }
     int norm(const double *a, double *out)
@@ -253,6 +199,7 @@ extern "C" void igab_newton_defaults(igab_newton_opts *o)
     o->max_subiter = 10000;
     o->ksp_rtol = 1e-5;
     o->ksp_maxit = 100000;
+    o->ksp = IGAB_KSP_MG_CG;
     o->verbose = 0;
 }
 
@@ -264,6 +211,7 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
         return IGAB_ERR_ARG;
     }
     if ((opts->prec != IGAB_PREC_FP64 && opts->prec != IGAB_PREC_FP32) || opts->max_subiter < 1 ||
+        (opts->ksp != IGAB_KSP_BICGSTAB && opts->ksp != IGAB_KSP_MG_CG) ||
         opts->ksp_maxit < 1 || !(opts->ksp_rtol >= 0.0) || !(opts->abstol >= 0.0)) {
         igab_set_error("igab_newton_solve: bad options");
         return IGAB_ERR_ARG;
@@ -332,12 +280,22 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
             k.ntan++;
             k.ms_tan += ms_since(t0);
             t0 = clk::now();
-            int conv = 0;
+            int conv = 0, brk = 1;
             double rn = 0.0, bn = 0.0;
-            rc = igab_krylov_solve(ctx, w.vals, w.prec, w.F, w.Y, opts->ksp_rtol, 0.0, opts->ksp_maxit, &kits, &conv,
-                                   &rn, &bn);
-            w.launches += ctx->last_launches;
-            if (rc) return rc;
+            if (opts->ksp == IGAB_KSP_MG_CG && ctx->phys == IGAB_PHYS_GE) {
+                rc = igab_mg_solve(ctx, w.vals, w.prec, w.F, w.Y, opts->ksp_rtol, 0.0, opts->ksp_maxit, &kits, &conv,
+                                   &rn, &bn, &brk);
+                w.launches += ctx->last_launches;
+                if (rc) return rc;
+            }
+            if (brk) {   /* BiCGStab: requested, transient physics, or CG met non-positive curvature */
+                int k2 = 0;
+                rc = igab_krylov_solve(ctx, w.vals, w.prec, w.F, w.Y, opts->ksp_rtol, 0.0, opts->ksp_maxit, &k2, &conv,
+                                       &rn, &bn);
+                w.launches += ctx->last_launches;
+                if (rc) return rc;
+                kits += k2;
+            }
             k.kits += kits;
             k.ms_ksp += ms_since(t0);
             /* J Y with the Jacobian of the solve (line-search slope) */

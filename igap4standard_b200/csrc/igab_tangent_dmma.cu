@@ -26,12 +26,14 @@
  *     tiles of the 88x88 element matrix and the 10 upper tiles of the 32x32
  *     Gamma block, split over the warps by igab_warp_tiles8.inc, with the
  *     accumulators in registers for the whole element.  At the end of an
- *     element they add Gamma to the diagonal component blocks and reduce the
- *     81x81 matrix into the CSR values straight from the accumulators
- *     (fire-and-forget red.global.add; the lower triangle mirrors the upper
- *     one exactly).  Tiles of one colour touch disjoint entries and the
- *     elements of a tile are separated by a consumer barrier, so every entry
- *     receives its additions in a fixed order.
+ *     element they stage the 81x81 matrix (both triangles from the upper
+ *     value, exact symmetry) and Gamma in shared memory and reduce it into
+ *     the CSR values (fire-and-forget red.global.add, Gamma added on the
+ *     diagonal component blocks) while they run the next element's DMMA
+ *     batches.  Tiles of one colour touch disjoint entries and every
+ *     reduction of an element is issued before a consumer barrier that
+ *     precedes the next element's, so every entry receives its additions in
+ *     a fixed order.
  * The slots are handed over with mbarriers (full: 256 builder arrivals, empty:
  * 256 consumer arrivals).  Every wait is bounded; a wait that gives up sets the
  * block's abort flag and the status word, and both roles leave their loops.
@@ -86,8 +88,8 @@ struct dws_smem {
     double pt[IGAB_NQ3 * PT_N];      /* point data of the element being built */
     double AC[972 + 864];            /* interpolation scratch */
     double gam[32 * 32];             /* upper tiles of Gamma at the end of an element */
-    double kst[66 * 64];             /* the element matrix staged for the deferred scatter: upper 8x8
-                                        tiles of the 88x88 matrix, tile (bi, bj) at kst_tile(bi, bj) */
+    double kst[81 * 81];             /* the element matrix staged for the deferred scatter, row-major;
+                                        both triangles hold the upper (accumulated) value */
     double U[TCP * TCP * TCP * 3];   /* displacements of the tile's control points */
     double tab[3][TE][IGAB_TAB1D];
     double wh[3][TE][IGAB_NQ];
@@ -474,13 +476,10 @@ __device__ __forceinline__ long csr_at(const dws_smem &S, int c1, int c2)
     return S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9;
 }
 
-/* index of upper tile (bi, bj), bi <= bj < 11, in the staged element matrix */
-__device__ __forceinline__ int kst_tile(int bi, int bj)
-{
-    return bi * 11 - (bi * (bi - 1)) / 2 + (bj - bi);
-}
-
-/* the warp's K tiles into the staging buffer (Gamma goes to S.gam separately) */
+/* the warp's K tiles into the staging buffer, both triangles from the upper value
+ * (Gamma goes to S.gam separately).  Every entry is written once: an off-diagonal tile
+ * writes its entries and their mirrors; a diagonal tile writes its upper entries
+ * (c1 <= c2) and the mirrors of those strictly above the diagonal. */
 template <int W>
 __device__ __forceinline__ void warp_stage8(dws_smem &S, int lane, const cons_acc<W> &a)
 {
@@ -488,34 +487,47 @@ __device__ __forceinline__ void warp_stage8(dws_smem &S, int lane, const cons_ac
     const int r = lane >> 2, c = 2 * (lane & 3);
 #pragma unroll
     for (int t = 0; t < WT::NT; t++) {
-        double *d = S.kst + kst_tile(WT::blk(WT::ti(t)), WT::blk(WT::tj(t))) * 64 + r * 8 + c;
-        d[0] = a.k[t][0];
-        d[1] = a.k[t][1];
+        const int bi = WT::blk(WT::ti(t)), bj = WT::blk(WT::tj(t));
+        const int c1 = 8 * bi + r;
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int c2 = 8 * bj + c + e;
+            if (c1 < 81 && c2 < 81) {
+                const double v = a.k[t][e];
+                if (bi != bj || c1 <= c2) S.kst[c1 * 81 + c2] = v;
+                if (bi != bj || c1 < c2) S.kst[c2 * 81 + c1] = v;
+            }
+        }
     }
 }
 
-#define KST_ENTRIES (81 * 81)
-#define KST_PARTS ((KST_ENTRIES + NCONS - 1) / NCONS)   /* 26 parts of NCONS entries */
+#define KST_ROWS 27   /* rows c1 = 3 a1 + k1 per scatter thread */
 
-/* part p of the staged element's scatter: entries i = p NCONS + tid of the 81 x 81
- * matrix, (c1, c2) = (i / 81, i % 81), each taking the upper value K(min, max), plus
- * Gamma(min, max) on the diagonal component blocks (c1 = c2 mod 3), reduced into the
- * CSR values.  Every entry of the element receives exactly one reduction. */
-__device__ __forceinline__ void kst_scatter_part(double *__restrict__ vals, const dws_smem &S, int p, int tid)
+/* rows a1 in [a0, a1e) of the staged element's scatter.  Thread t < 243 owns element-
+ * matrix column c2 = t mod 81 within component rows k1 = t / 81 and walks the rows c1 =
+ * 3 a1 + k1: the column's CSR offset terms and its Gamma test are per-thread constants.
+ * Each entry receives K (upper value) plus Gamma(min, max) on the diagonal component
+ * blocks (k1 = c2 mod 3), reduced into the CSR values once. */
+__device__ __forceinline__ void kst_scatter_rows(double *__restrict__ vals, const dws_smem &S, int a0, int a1e,
+                                                 int tid)
 {
-    const int i = p * NCONS + tid;
-    if (i >= KST_ENTRIES) return;
-    const int c1 = i / 81, c2 = i % 81;
-    const int lo = c1 < c2 ? c1 : c2, hi = c1 < c2 ? c2 : c1;
-    double v = S.kst[kst_tile(lo >> 3, hi >> 3) * 64 + (lo & 7) * 8 + (hi & 7)];
-    if (c1 % 3 == c2 % 3) v += S.gam[(lo / 3) * 32 + hi / 3];
-    red_add(vals + csr_at(S, c1, c2), v);
+    if (tid >= 243) return;
+    const int k1 = tid / 81, c2 = tid - 81 * k1, a2 = c2 / 3;
+    const int o2 = c2 / 27, p2 = (c2 / 9) % 3, z2 = c2 % 9;
+    const bool gam = k1 == c2 - 3 * a2;
+    for (int a1 = a0; a1 < a1e; a1++) {
+        const int c1 = 3 * a1 + k1;
+        double v = S.kst[c1 * 81 + c2];
+        if (gam) v += a1 <= a2 ? S.gam[a1 * 32 + a2] : S.gam[a2 * 32 + a1];
+        red_add(vals + S.rbase[c1] + o2 * S.rsx[c1] + p2 * S.rsy[c1] + z2, v);
+    }
 }
 
 /* The consumers.  Per element: the 16 batches of DMMA products with the accumulators in
  * registers; then (after a consumer barrier) the accumulators, Gamma and the element's
  * CSR row bases are staged in shared memory, and the element is reduced into the CSR
- * values during the next element's batches (two parts of 256 entries after each batch),
+ * values during the next element's batches (two of its 27 basis-function rows after each
+ * batch, one thread per (component, column)),
  * so the reductions overlap the DMMAs.  The barrier before staging also orders every
  * reduction of an element before any of the next one: per-entry order stays fixed.
  * The staged element is flushed at the end of the work, and at the end of every tile
@@ -557,10 +569,8 @@ __device__ void dws_consumer(const Src &F, dws_smem &S)
                 warp_mma8<W>(S.X[b], S.sc[b], S.UT[b], S.VT[b], lane, a);
                 tc_mbar_arrive(&S.empty[b]);
                 gb++;
-                if (pvals) {
-                    kst_scatter_part(pvals, S, 2 * bt, tid);
-                    kst_scatter_part(pvals, S, 2 * bt + 1, tid);
-                }
+                if (pvals && 2 * bt < KST_ROWS)
+                    kst_scatter_rows(pvals, S, 2 * bt, 2 * bt + 2 < KST_ROWS ? 2 * bt + 2 : KST_ROWS, tid);
             }
             if (aborted) break;
             /* every reduction of the staged element is issued: stage this one */
@@ -584,14 +594,14 @@ __device__ void dws_consumer(const Src &F, dws_smem &S)
         if (aborted) break;
         if (Src::publishes_tiles && pvals) {
             tc_bar_sync(BAR_CONS, NCONS);
-            for (int p = 0; p < KST_PARTS; p++) kst_scatter_part(pvals, S, p, tid);
+            kst_scatter_rows(pvals, S, 0, KST_ROWS, tid);
             pvals = nullptr;
         }
         F.done(R);
     }
     if (!aborted && pvals) {
         tc_bar_sync(BAR_CONS, NCONS);
-        for (int p = 0; p < KST_PARTS; p++) kst_scatter_part(pvals, S, p, tid);
+        kst_scatter_rows(pvals, S, 0, KST_ROWS, tid);
     }
     if (aborted && tid == 0) {
         S.abort_flag = 1;

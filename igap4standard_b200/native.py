@@ -45,7 +45,8 @@ class IgabNewtonOpts(ctypes.Structure):
     """igab_newton_opts of include/igab.h"""
     _fields_ = [("prec", ctypes.c_int), ("abstol", ctypes.c_double), ("rtol", ctypes.c_double),
                 ("stol", ctypes.c_double), ("stagnation", ctypes.c_double), ("max_subiter", ctypes.c_int),
-                ("ksp_rtol", ctypes.c_double), ("ksp_maxit", ctypes.c_int), ("verbose", ctypes.c_int)]
+                ("ksp_rtol", ctypes.c_double), ("ksp_maxit", ctypes.c_int), ("ksp", ctypes.c_int),
+                ("verbose", ctypes.c_int)]
 
 
 class IgabNewtonInfo(ctypes.Structure):
@@ -107,6 +108,10 @@ IGAB_API = [
     ("igab_residual_noalloc", ctypes.c_int, [vp, vp, vp]),
     ("igab_staging_bytes", ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_size_t)]),
     ("igab_newton_defaults", None, [vp]),
+    ("igab_solve_mg_device", ctypes.c_int, [vp, vp, ctypes.c_int, vp, vp, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_int, vp]),
+    ("igab_solve_mg_levels", ctypes.c_int, [vp, c_int_p]),
+    ("igab_mg_prolongation_1d", ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int, vp]),
     ("igab_upload", ctypes.c_int, [vp, vp, vp, ctypes.c_long]),
     ("igab_download", ctypes.c_int, [vp, vp, vp, ctypes.c_long]),
     ("igab_newton_solve", ctypes.c_int, [vp, vp, vp, vp, vp, vp, ctypes.c_int]),

@@ -101,7 +101,7 @@ def test_dropin_snes_solve_keeps_tangent_on_device(built, name):
     info = native.IgabNewtonInfo()
     assert lib.snesiga_gpu_last_solve(D.app, ctypes.byref(info)) == 0
     ms = np.zeros(4)
-    assert lib.snesiga_gpu_last_timings(D.app, ms.ctypes.data_as(ctypes.c_void_p)) == 0
+    assert lib.snesiga_gpu_last_timings(D.app, ms.ctypes.data_as(native.c_double_p)) == 0
     print(name, "host AIJ", host.iterations, host.fnorms, "device", info.iterations, info.fnorm,
           info.krylov_iterations)
     assert ok and info.converged

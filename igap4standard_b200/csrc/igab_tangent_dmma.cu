@@ -26,14 +26,12 @@
  *     tiles of the 88x88 element matrix and the 10 upper tiles of the 32x32
  *     Gamma block, split over the warps by igab_warp_tiles8.inc, with the
  *     accumulators in registers for the whole element.  At the end of an
- *     element they stage the 81x81 matrix (both triangles from the upper
- *     value, exact symmetry) and Gamma in shared memory and reduce it into
- *     the CSR values (fire-and-forget red.global.add, Gamma added on the
- *     diagonal component blocks) while they run the next element's DMMA
- *     batches.  Tiles of one colour touch disjoint entries and every
- *     reduction of an element is issued before a consumer barrier that
- *     precedes the next element's, so every entry receives its additions in
- *     a fixed order.
+ *     element they add Gamma to the diagonal component blocks and reduce the
+ *     81x81 matrix into the CSR values straight from the accumulators
+ *     (fire-and-forget red.global.add; the lower triangle mirrors the upper
+ *     one exactly).  Tiles of one colour touch disjoint entries and the
+ *     elements of a tile are separated by a consumer barrier, so every entry
+ *     receives its additions in a fixed order.
  * The slots are handed over with mbarriers (full: 256 builder arrivals, empty:
  * 256 consumer arrivals).  Every wait is bounded; a wait that gives up sets the
  * block's abort flag and the status word, and both roles leave their loops.
@@ -88,8 +86,6 @@ struct dws_smem {
     double pt[IGAB_NQ3 * PT_N];      /* point data of the element being built */
     double AC[972 + 864];            /* interpolation scratch */
     double gam[32 * 32];             /* upper tiles of Gamma at the end of an element */
-    double kst[81 * 81];             /* the element matrix staged for the deferred scatter, row-major;
-                                        both triangles hold the upper (accumulated) value */
     double U[TCP * TCP * TCP * 3];   /* displacements of the tile's control points */
     double tab[3][TE][IGAB_TAB1D];
     double wh[3][TE][IGAB_NQ];
@@ -151,7 +147,6 @@ struct src_colour {
         R.inst = 0;
     }
     __device__ void done(const dws_tile &) const {}
-    static constexpr bool publishes_tiles = false;   /* tiles of one colour: disjoint entries */
 };
 
 /* the batched work list: items (instance, colour, tile) in colour-major order;
@@ -185,7 +180,6 @@ struct src_batch {
         tc_bar_sync(BAR_CONS, NCONS);
         if (threadIdx.x == 0) atomicAdd(&B.done[8 * R.inst + R.colour], 1);
     }
-    static constexpr bool publishes_tiles = true;    /* later colours wait on the finished count */
 };
 
 /* ---------------------------------------------------------------- builders */
@@ -476,62 +470,42 @@ __device__ __forceinline__ long csr_at(const dws_smem &S, int c1, int c2)
     return S.rbase[c1] + (c2 / 27) * S.rsx[c1] + ((c2 / 9) % 3) * S.rsy[c1] + c2 % 9;
 }
 
-/* the warp's K tiles into the staging buffer, both triangles from the upper value
- * (Gamma goes to S.gam separately).  Every entry is written once: an off-diagonal tile
- * writes its entries and their mirrors; a diagonal tile writes its upper entries
- * (c1 <= c2) and the mirrors of those strictly above the diagonal. */
+/* the warp's K tiles plus Gamma on the diagonal component blocks, reduced into
+ * the CSR values; entry (c1, c2) and its mirror (c2, c1) receive the upper value */
 template <int W>
-__device__ __forceinline__ void warp_stage8(dws_smem &S, int lane, const cons_acc<W> &a)
+__device__ __forceinline__ void warp_scatter8(double *__restrict__ vals, const dws_smem &S, int lane,
+                                              const cons_acc<W> &a)
 {
     using WT = warp_tiles8<W>;
     const int r = lane >> 2, c = 2 * (lane & 3);
 #pragma unroll
     for (int t = 0; t < WT::NT; t++) {
         const int bi = WT::blk(WT::ti(t)), bj = WT::blk(WT::tj(t));
-        const int c1 = 8 * bi + r;
+        double v2[2] = {a.k[t][0], a.k[t][1]};
+        if (bi == bj) {
+            /* diagonal tile: entry (r, c + e) below the diagonal takes (c + e, r),
+             * held by lane 4 (c + e) + r / 2, element r & 1 */
+            const double x0 = __shfl_sync(0xffffffffu, a.k[t][0], 4 * c + (r >> 1));
+            const double y0 = __shfl_sync(0xffffffffu, a.k[t][1], 4 * c + (r >> 1));
+            const double x1 = __shfl_sync(0xffffffffu, a.k[t][0], 4 * (c + 1) + (r >> 1));
+            const double y1 = __shfl_sync(0xffffffffu, a.k[t][1], 4 * (c + 1) + (r >> 1));
+            if (r > c) v2[0] = (r & 1) ? y0 : x0;
+            if (r > c + 1) v2[1] = (r & 1) ? y1 : x1;
+        }
 #pragma unroll
         for (int e = 0; e < 2; e++) {
-            const int c2 = 8 * bj + c + e;
+            const int c1 = 8 * bi + r, c2 = 8 * bj + c + e;
             if (c1 < 81 && c2 < 81) {
-                const double v = a.k[t][e];
-                if (bi != bj || c1 <= c2) S.kst[c1 * 81 + c2] = v;
-                if (bi != bj || c1 < c2) S.kst[c2 * 81 + c1] = v;
+                const int a1 = c1 / 3, a2 = c2 / 3;
+                double v = v2[e];
+                if (c1 % 3 == c2 % 3) v += a1 <= a2 ? S.gam[a1 * 32 + a2] : S.gam[a2 * 32 + a1];
+                red_add(vals + csr_at(S, c1, c2), v);
+                if (bi != bj) red_add(vals + csr_at(S, c2, c1), v);
             }
         }
     }
 }
 
-#define KST_ROWS 27   /* rows c1 = 3 a1 + k1 per scatter thread */
-
-/* rows a1 in [a0, a1e) of the staged element's scatter.  Thread t < 243 owns element-
- * matrix column c2 = t mod 81 within component rows k1 = t / 81 and walks the rows c1 =
- * 3 a1 + k1: the column's CSR offset terms and its Gamma test are per-thread constants.
- * Each entry receives K (upper value) plus Gamma(min, max) on the diagonal component
- * blocks (k1 = c2 mod 3), reduced into the CSR values once. */
-__device__ __forceinline__ void kst_scatter_rows(double *__restrict__ vals, const dws_smem &S, int a0, int a1e,
-                                                 int tid)
-{
-    if (tid >= 243) return;
-    const int k1 = tid / 81, c2 = tid - 81 * k1, a2 = c2 / 3;
-    const int o2 = c2 / 27, p2 = (c2 / 9) % 3, z2 = c2 % 9;
-    const bool gam = k1 == c2 - 3 * a2;
-    for (int a1 = a0; a1 < a1e; a1++) {
-        const int c1 = 3 * a1 + k1;
-        double v = S.kst[c1 * 81 + c2];
-        if (gam) v += a1 <= a2 ? S.gam[a1 * 32 + a2] : S.gam[a2 * 32 + a1];
-        red_add(vals + S.rbase[c1] + o2 * S.rsx[c1] + p2 * S.rsy[c1] + z2, v);
-    }
-}
-
-/* The consumers.  Per element: the 16 batches of DMMA products with the accumulators in
- * registers; then (after a consumer barrier) the accumulators, Gamma and the element's
- * CSR row bases are staged in shared memory, and the element is reduced into the CSR
- * values during the next element's batches (two of its 27 basis-function rows after each
- * batch, one thread per (component, column)),
- * so the reductions overlap the DMMAs.  The barrier before staging also orders every
- * reduction of an element before any of the next one: per-entry order stays fixed.
- * The staged element is flushed at the end of the work, and at the end of every tile
- * when the work source publishes finished tiles (batched work lists). */
 template <int W, class Src>
 __device__ void dws_consumer(const Src &F, dws_smem &S)
 {
@@ -539,7 +513,6 @@ __device__ void dws_consumer(const Src &F, dws_smem &S)
     const int tid = threadIdx.x, lane = tid & 31;
     int gb = 0;   /* batches consumed so far */
     bool aborted = false;
-    double *pvals = nullptr;   /* CSR values of the staged element (nullptr: nothing staged) */
     for (int k = 0;; k++) {
         /* the first batch of tile k (or the end of the work) */
         if (!cons_acquire(S, gb)) {
@@ -559,7 +532,7 @@ __device__ void dws_consumer(const Src &F, dws_smem &S)
             for (int t = 0; t < (WT::NT > 0 ? WT::NT : 1); t++) a.k[t][0] = a.k[t][1] = 0.0;
 #pragma unroll
             for (int t = 0; t < (WT::NGT > 0 ? WT::NGT : 1); t++) a.g[t][0] = a.g[t][1] = 0.0;
-            for (int q0 = 0, bt = 0; q0 < IGAB_NQ3; q0 += DQ, bt++) {
+            for (int q0 = 0; q0 < IGAB_NQ3; q0 += DQ) {
                 if (!have && !cons_acquire(S, gb)) {
                     aborted = true;
                     break;
@@ -569,13 +542,9 @@ __device__ void dws_consumer(const Src &F, dws_smem &S)
                 warp_mma8<W>(S.X[b], S.sc[b], S.UT[b], S.VT[b], lane, a);
                 tc_mbar_arrive(&S.empty[b]);
                 gb++;
-                if (pvals && 2 * bt < KST_ROWS)
-                    kst_scatter_rows(pvals, S, 2 * bt, 2 * bt + 2 < KST_ROWS ? 2 * bt + 2 : KST_ROWS, tid);
             }
             if (aborted) break;
-            /* every reduction of the staged element is issued: stage this one */
-            tc_bar_sync(BAR_CONS, NCONS);
-            warp_stage8<W>(S, lane, a);
+            /* Gamma (upper tiles) and the CSR row bases of the element */
             if constexpr (WT::NGT > 0) {
                 const int r = lane >> 2, c = 2 * (lane & 3);
 #pragma unroll
@@ -588,20 +557,12 @@ __device__ void dws_consumer(const Src &F, dws_smem &S)
             if (tid < 81)
                 elem_row_base(R.g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez, tid, S.rbase[tid], S.rsx[tid],
                               S.rsy[tid]);
-            pvals = R.vals;
-            /* the next cons_acquire (a consumer barrier) publishes the stage before its use */
+            tc_bar_sync(BAR_CONS, NCONS);
+            warp_scatter8<W>(R.vals, S, lane, a);
+            tc_bar_sync(BAR_CONS, NCONS);
         }
         if (aborted) break;
-        if (Src::publishes_tiles && pvals) {
-            tc_bar_sync(BAR_CONS, NCONS);
-            kst_scatter_rows(pvals, S, 0, KST_ROWS, tid);
-            pvals = nullptr;
-        }
         F.done(R);
-    }
-    if (!aborted && pvals) {
-        tc_bar_sync(BAR_CONS, NCONS);
-        kst_scatter_rows(pvals, S, 0, KST_ROWS, tid);
     }
     if (aborted && tid == 0) {
         S.abort_flag = 1;

@@ -182,13 +182,14 @@ class Assembly:
                                          float(atol), int(maxit), ctypes.byref(info)))
         return info.iterations, bool(info.converged), info.residual_norm
 
-    def solve_mg_device(self, vals_ptr, b_ptr, x_ptr, prec="fp64", rtol=1e-5, atol=0.0, maxit=1000):
-        """x = K^-1 b by multigrid-preconditioned CG on the device (igab_solve_mg_device).
+    def solve_mg_device(self, vals_ptr, b_ptr, x_ptr, prec="fp64", rtol=1e-5, atol=0.0, maxit=1000, method="gmres"):
+        """x = K^-1 b by multigrid-preconditioned GMRES or CG on the device (igab_solve_mg_device).
         Returns (iterations, converged, residual norm, multigrid levels)."""
         info = native.IgabSolveInfo()
         check(self.lib, "igab_solve_mg_device",
-              self.lib.igab_solve_mg_device(self.h, vp(vals_ptr), PREC[prec], vp(b_ptr), vp(x_ptr), float(rtol),
-                                            float(atol), int(maxit), ctypes.byref(info)))
+              self.lib.igab_solve_mg_device(self.h, {"cg": 1, "gmres": 2}[method], vp(vals_ptr), PREC[prec],
+                                            vp(b_ptr), vp(x_ptr), float(rtol), float(atol), int(maxit),
+                                            ctypes.byref(info)))
         lev = ctypes.c_int()
         check(self.lib, "igab_solve_mg_levels", self.lib.igab_solve_mg_levels(self.h, ctypes.byref(lev)))
         return info.iterations, bool(info.converged), info.residual_norm, lev.value
@@ -205,7 +206,7 @@ class Assembly:
         o.ksp_maxit = int(ksp_maxit)
         o.abstol = float(abstol)
         o.max_subiter = int(max_subiter)
-        o.ksp = {"mg": 1, "bicgstab": 0}[ksp]
+        o.ksp = {"mg": 2, "mg-cg": 1, "bicgstab": 0}[ksp]
         o.verbose = 1 if verbose else 0
         info = native.IgabNewtonInfo()
         fh = np.zeros(history_cap)

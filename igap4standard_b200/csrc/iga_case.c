@@ -137,9 +137,13 @@ iga_case *iga_case_create(int phys_kind, const int nelem[3], const double *knots
     return c;
 }
 
+extern int snesiga_gpu_free(void *app_) __attribute__((weak));
+
 void iga_case_destroy(iga_case *c)
 {
     if (!c) return;
+    /* the GPU state is keyed by the IGA address, which a later case may reuse */
+    if (snesiga_gpu_free) snesiga_gpu_free(&c->app);
     VecDestroy(&c->sa.Residual_);
     VecDestroy(&c->sa.U);
     MatDestroy(&c->sa.Tangent_);

@@ -825,9 +825,10 @@ extern "C" int igab_solve_device(igab_ctx *ctx, const void *vals_dev, int prec, 
     return 0;
 }
 
-extern "C" int igab_solve_mg_device(igab_ctx *ctx, const void *vals_dev, int prec, const double *b_dev, double *x_dev,
-                                    double rtol, double atol, int maxit, igab_solve_info *info)
+extern "C" int igab_solve_mg_device(igab_ctx *ctx, int method, const void *vals_dev, int prec, const double *b_dev,
+                                    double *x_dev, double rtol, double atol, int maxit, igab_solve_info *info)
 {
+    ARG_CHECK(method == IGAB_KSP_MG_CG || method == IGAB_KSP_MG_GMRES, "igab_solve_mg_device: unknown method");
     ARG_CHECK(ctx && vals_dev && b_dev && x_dev, "igab_solve_mg_device: null argument");
     ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_solve_mg_device: bad precision");
     ARG_CHECK(maxit >= 1 && rtol >= 0.0 && atol >= 0.0, "igab_solve_mg_device: bad tolerances");
@@ -835,7 +836,7 @@ extern "C" int igab_solve_mg_device(igab_ctx *ctx, const void *vals_dev, int pre
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     int its = 0, conv = 0, brk = 0;
     double rn = 0.0, bn = 0.0;
-    int rc = igab_mg_solve(ctx, vals_dev, prec, b_dev, x_dev, rtol, atol, maxit, &its, &conv, &rn, &bn, &brk);
+    int rc = igab_mg_solve(ctx, method, vals_dev, prec, b_dev, x_dev, rtol, atol, maxit, &its, &conv, &rn, &bn, &brk);
     if (rc) return rc;
     if (info) {
         info->iterations = its;

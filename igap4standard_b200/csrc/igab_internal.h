@@ -166,9 +166,9 @@ int igab_krylov_solve(igab_ctx *c, const void *dvals, int prec, const double *db
                       double atol, int maxit, int *iterations, int *converged, double *rnorm, double *bnorm);
 void igab_krylov_release(igab_ctx *c);
 void igab_newton_release(igab_ctx *c);   /* igab_newton.cu */
-/* igab_mg.cu: multigrid-preconditioned CG on the context's tangent (breakdown: p.Kp <= 0) */
-int igab_mg_solve(igab_ctx *c, const void *vals, int prec, const double *b, double *x, double rtol, double atol,
-                  int maxit, int *iterations, int *converged, double *rnorm, double *bnorm, int *breakdown);
+/* igab_mg.cu: multigrid-preconditioned CG (breakdown: p.Kp <= 0) or GMRES on the context's tangent */
+int igab_mg_solve(igab_ctx *c, int method, const void *vals, int prec, const double *b, double *x, double rtol,
+                  double atol, int maxit, int *iterations, int *converged, double *rnorm, double *bnorm, int *breakdown);
 int igab_mg_levels(igab_ctx *c, int *levels);
 void igab_mg_release(igab_ctx *c);
 int igab_launch_tangent(igab_ctx *c, const double *dU, void *dvals, int prec);

@@ -247,9 +247,13 @@ struct igab_mg {
     std::vector<int> piv;
     double *h_vec = nullptr;        /* pinned nd doubles */
     double *part = nullptr, *dots = nullptr, *h_dots = nullptr;
-    double *zero = nullptr;         /* coarse zero state */
-    double *cg = nullptr;           /* CG vectors r, z, p, q of the caller's mesh */
-    long cg_n = 0;
+    double *zero = nullptr;         /* zero state (fine size) */
+    long zero_n = 0;
+    void *fine_vals = nullptr;      /* the caller's tangent at the zero state, FP32 */
+    double *kv = nullptr;           /* Krylov vectors of the caller's mesh */
+    long kv_n = 0;
+    double *mpart = nullptr;        /* multi-dot partial sums [GM_RESTART + 1][RD_BLOCKS] and results */
+    double *h_md = nullptr;         /* pinned results of a multi-dot */
     int launches = 0;
 };
 
@@ -277,7 +281,10 @@ void mg_free(igab_mg *m)
     for (int l = 0; l < m->nlev; l++) mg_free_level(m->L[l], l > 0);
     cudaFree(m->part);
     cudaFree(m->zero);
-    cudaFree(m->cg);
+    cudaFree(m->fine_vals);
+    cudaFree(m->kv);
+    cudaFree(m->mpart);
+    cudaFreeHost(m->h_md);
     cudaFreeHost(m->h_vec);
     cudaFreeHost(m->h_dots);
     delete m;
@@ -512,13 +519,34 @@ int mg_build(igab_ctx *c, igab_mg *m)
         int rc = mg_vectors(F);
         if (rc) return rc;
     }
+    /* the preconditioner's fine operator: the caller's tangent at the zero state (FP32),
+     * symmetric positive definite for a stable material whatever the current state is */
+    if (!m->zero || m->zero_n < F.n) {
+        cudaFree(m->zero);
+        m->zero = nullptr;
+        IGAB_CUDA_TRY(cudaMalloc((void **)&m->zero, (size_t)F.n * sizeof(double)));
+        IGAB_CUDA_TRY(cudaMemset(m->zero, 0, (size_t)F.n * sizeof(double)));
+        m->zero_n = F.n;
+    }
+    if (!m->fine_vals) IGAB_CUDA_TRY(cudaMalloc(&m->fine_vals, (size_t)c->nnz * sizeof(float)));
+    {
+        int rc = igab_launch_tangent(c, m->zero, m->fine_vals, IGAB_PREC_FP32);
+        if (rc) return rc;
+    }
+    F.vals = m->fine_vals;
+    F.prec = IGAB_PREC_FP32;
+    k_mg_diag_inv<<<(unsigned)((F.n + 255) / 256), 256, 0, c->stream>>>(c->geom(), F.vals, F.prec, F.dinv);
+    IGAB_CUDA_TRY(cudaGetLastError());
+    {
+        int rc = estimate_lmax(m, F);
+        if (rc) return rc;
+    }
     /* element log-scales of the caller's context (averaged per coarse element below) */
     std::vector<double> s_f;
     if (c->escale_on) {
         s_f.resize((size_t)c->nel);
         IGAB_CUDA_TRY(cudaMemcpy(s_f.data(), c->d_escale, (size_t)c->nel * sizeof(double), cudaMemcpyDeviceToHost));
     }
-    size_t zero_n = 0;
     while (m->nlev < MG_MAX_LEVELS) {
         igab_ctx *f = m->L[m->nlev - 1].ctx;
         if (f->ndof <= MG_COARSE_DOF) break;
@@ -587,14 +615,7 @@ int mg_build(igab_ctx *c, igab_mg *m)
             s_f.swap(sc);
             if ((rc = igab_set_element_log_scale(cc, gc.data(), 0))) return rc;
         }
-        /* the coarse tangent at the zero state */
-        if ((size_t)C.n > zero_n) {
-            cudaFree(m->zero);
-            m->zero = nullptr;
-            IGAB_CUDA_TRY(cudaMalloc((void **)&m->zero, (size_t)C.n * sizeof(double)));
-            IGAB_CUDA_TRY(cudaMemset(m->zero, 0, (size_t)C.n * sizeof(double)));
-            zero_n = (size_t)C.n;
-        }
+        /* the coarse tangent at the zero state (m->zero holds the fine level's zeros) */
         IGAB_CUDA_TRY(cudaMalloc((void **)&C.own_vals, (size_t)cc->nnz * sizeof(double)));
         if ((rc = igab_launch_tangent(cc, m->zero, C.own_vals, IGAB_PREC_FP64))) return rc;
         C.vals = C.own_vals;
@@ -644,88 +665,289 @@ int igab_mg_levels(igab_ctx *c, int *levels)
     return 0;
 }
 
-int igab_mg_solve(igab_ctx *c, const void *vals, int prec, const double *b, double *x, double rtol, double atol,
-                  int maxit, int *iterations, int *converged, double *rnorm, double *bnorm, int *breakdown)
+
+namespace {
+
+#define GM_RESTART 50          /* GMRES restart length */
+
+/* partial sums of V_i . w, i < k (V_i = V + i n), per block into part[i][RD_BLOCKS] */
+__global__ void __launch_bounds__(RD_THREADS) k_md_partial(long n, const double *__restrict__ V, int k,
+                                                           const double *__restrict__ w, double *part)
+{
+    __shared__ double red[RD_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = 0; i < k; i++) {
+        const double *v = V + (size_t)i * n;
+        double s0 = 0.0;
+        for (long t = blockIdx.x * (long)RD_THREADS + threadIdx.x; t < n; t += (long)RD_BLOCKS * RD_THREADS)
+            s0 += v[t] * w[t];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        if (lane == 0) red[warp] = s0;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (int q = 0; q < RD_THREADS / 32; q++) s += red[q];
+            part[(size_t)i * RD_BLOCKS + blockIdx.x] = s;
+        }
+        __syncthreads();
+    }
+}
+
+/* out[i] = sum of part[i][0..RD_BLOCKS) in a fixed order, one block per i */
+__global__ void __launch_bounds__(RD_THREADS) k_md_finish(const double *part, double *out)
+{
+    __shared__ double red[RD_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double s = 0.0;
+    for (int b = threadIdx.x; b < RD_BLOCKS; b += RD_THREADS) s += part[(size_t)blockIdx.x * RD_BLOCKS + b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int q = 0; q < RD_THREADS / 32; q++) t += red[q];
+        out[blockIdx.x] = t;
+    }
+}
+
+/* w -= sum_{i<k} h_i V_i  (h on the device) */
+__global__ void k_md_update(long n, const double *__restrict__ V, int k, const double *__restrict__ h, double *w)
+{
+    MG_LOOP(t, n)
+    {
+        double s = w[t];
+        for (int i = 0; i < k; i++) s -= h[i] * V[(size_t)i * n + t];
+        w[t] = s;
+    }
+}
+
+/* u = sum_{i<k} y_i V_i  (y on the device) */
+__global__ void k_md_combine(long n, const double *__restrict__ V, int k, const double *__restrict__ y, double *u)
+{
+    MG_LOOP(t, n)
+    {
+        double s = 0.0;
+        for (int i = 0; i < k; i++) s += y[i] * V[(size_t)i * n + t];
+        u[t] = s;
+    }
+}
+
+/* h = V[0..k)^T w on the host (and on the device at dev_h) */
+cudaError_t mdot(igab_mg *m, cudaStream_t st, long n, const double *V, int k, const double *w, double *h)
+{
+    double *dev_out = m->mpart + (size_t)(GM_RESTART + 1) * RD_BLOCKS;
+    k_md_partial<<<RD_BLOCKS, RD_THREADS, 0, st>>>(n, V, k, w, m->mpart);
+    k_md_finish<<<k, RD_THREADS, 0, st>>>(m->mpart, dev_out);
+    m->launches += 2;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->h_md, dev_out, (size_t)k * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) memcpy(h, m->h_md, (size_t)k * sizeof(double));
+    return e;
+}
+
+/* the V-cycle as the preconditioner: z = M r */
+int precond(igab_mg *m, const double *r, double *z)
+{
+    mg_level &F = m->L[0];
+    cudaStream_t st = F.ctx->stream;
+    k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(F.n, r, F.b);
+    int rc = vcycle(m, 0);
+    if (rc) return rc;
+    k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(F.n, F.x, z);
+    m->launches += 2;
+    return 0;
+}
+
+int dot1(igab_mg *m, cudaStream_t st, long n, const double *a, const double *b, double *out)
+{
+    double d2[2];
+    IGAB_CUDA_TRY(rd_dot2(st, n, a, b, nullptr, nullptr, m->part, m->dots, m->h_dots, d2));
+    *out = d2[0];
+    return 0;
+}
+
+/* preconditioned CG on K (vals, prec); breakdown when p.Kp <= 0 */
+int solve_cg(igab_mg *m, igab_ctx *c, const void *vals, int prec, const double *b, double *x, double tol, int maxit,
+             int *iterations, int *converged, double *rnorm, int *breakdown)
+{
+    cudaStream_t st = c->stream;
+    const long n = c->ndof;
+    double *r = m->kv, *z = r + n, *p = z + n, *q = p + n;
+    int rc = 0;
+    k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, b, r);
+    if ((rc = precond(m, r, z))) return rc;
+    k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, z, p);
+    double rz = 0.0;
+    if ((rc = dot1(m, st, n, r, z, &rz))) return rc;
+    for (int it = 1; it <= maxit; it++) {
+        if ((rc = igab_launch_spmv(c, vals, prec, p, q))) return rc;
+        double pq = 0.0, rr = 0.0;
+        if ((rc = dot1(m, st, n, p, q, &pq))) return rc;
+        if (!(pq > 0.0) || !(rz > 0.0)) {
+            *breakdown = 1;
+            return 0;
+        }
+        const double alpha = rz / pq;
+        k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, alpha, p, 1.0, x);
+        k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, -alpha, q, 1.0, r);
+        if ((rc = dot1(m, st, n, r, r, &rr))) return rc;
+        *iterations = it;
+        *rnorm = std::sqrt(rr);
+        if (*rnorm <= tol) {
+            *converged = 1;
+            return 0;
+        }
+        if ((rc = precond(m, r, z))) return rc;
+        double rz1 = 0.0;
+        if ((rc = dot1(m, st, n, r, z, &rz1))) return rc;
+        k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, 1.0, z, rz1 / rz, p);
+        rz = rz1;
+        m->launches += 4;
+    }
+    return 0;
+}
+
+/* right-preconditioned GMRES(GM_RESTART) on K with the V-cycle M: x = M u, u in the
+ * Krylov space of K M; classical Gram-Schmidt with one reorthogonalisation (CGS2), Givens
+ * rotations; the true residual is recomputed at every restart */
+int solve_gmres(igab_mg *m, igab_ctx *c, const void *vals, int prec, const double *b, double *x, double tol,
+                int maxit, int *iterations, int *converged, double *rnorm)
+{
+    cudaStream_t st = c->stream;
+    const long n = c->ndof;
+    const int mr = GM_RESTART;
+    double *V = m->kv, *t = V + (size_t)(mr + 1) * n, *w = t + n, *r = w + n;
+    double *dev_coef = m->mpart + (size_t)(GM_RESTART + 1) * RD_BLOCKS + (GM_RESTART + 1);
+    std::vector<double> H((size_t)(mr + 1) * mr), cs(mr), sn(mr), g(mr + 1), h(mr + 1), h2(mr + 1), y(mr);
+    int rc = 0, its = 0;
+    k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, b, r);
+    double beta = 0.0;
+    if ((rc = dot1(m, st, n, r, r, &beta))) return rc;
+    beta = std::sqrt(beta);
+    *rnorm = beta;
+    while (its < maxit) {
+        if (beta <= tol) {
+            *converged = 1;
+            break;
+        }
+        k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, 1.0 / beta, r, 0.0, V);
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int j = 0;
+        for (; j < mr && its < maxit; j++) {
+            if ((rc = precond(m, V + (size_t)j * n, t))) return rc;
+            if ((rc = igab_launch_spmv(c, vals, prec, t, w))) return rc;
+            /* CGS2: h = V^T w, w -= V h, twice */
+            IGAB_CUDA_TRY(mdot(m, st, n, V, j + 1, w, h.data()));
+            IGAB_CUDA_TRY(cudaMemcpyAsync(dev_coef, h.data(), (size_t)(j + 1) * sizeof(double), cudaMemcpyHostToDevice, st));
+            k_md_update<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, V, j + 1, dev_coef, w);
+            IGAB_CUDA_TRY(mdot(m, st, n, V, j + 1, w, h2.data()));
+            IGAB_CUDA_TRY(cudaMemcpyAsync(dev_coef, h2.data(), (size_t)(j + 1) * sizeof(double), cudaMemcpyHostToDevice, st));
+            k_md_update<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, V, j + 1, dev_coef, w);
+            for (int i = 0; i <= j; i++) h[i] += h2[i];
+            double hn = 0.0;
+            if ((rc = dot1(m, st, n, w, w, &hn))) return rc;
+            hn = std::sqrt(hn);
+            m->launches += 3;
+            its++;
+            /* apply the previous rotations, then a new one that zeroes hn */
+            for (int i = 0; i < j; i++) {
+                const double a = h[i], bb = h[i + 1];
+                h[i] = cs[i] * a + sn[i] * bb;
+                h[i + 1] = -sn[i] * a + cs[i] * bb;
+            }
+            const double den = std::sqrt(h[j] * h[j] + hn * hn);
+            if (den == 0.0) {
+                cs[j] = 1.0;
+                sn[j] = 0.0;
+            } else {
+                cs[j] = h[j] / den;
+                sn[j] = hn / den;
+            }
+            h[j] = den;
+            for (int i = 0; i <= j; i++) H[(size_t)i * mr + j] = h[i];
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            *rnorm = std::fabs(g[j + 1]);
+            if (*rnorm <= tol || hn == 0.0) {
+                j++;
+                break;
+            }
+            k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, 1.0 / hn, w, 0.0, V + (size_t)(j + 1) * n);
+        }
+        /* y = H^-1 g, x += M (V y) */
+        for (int i = j - 1; i >= 0; i--) {
+            double sacc = g[i];
+            for (int k = i + 1; k < j; k++) sacc -= H[(size_t)i * mr + k] * y[k];
+            y[i] = H[(size_t)i * mr + i] != 0.0 ? sacc / H[(size_t)i * mr + i] : 0.0;
+        }
+        IGAB_CUDA_TRY(cudaMemcpyAsync(dev_coef, y.data(), (size_t)j * sizeof(double), cudaMemcpyHostToDevice, st));
+        k_md_combine<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, V, j, dev_coef, w);
+        if ((rc = precond(m, w, t))) return rc;
+        k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, 1.0, t, 1.0, x);
+        /* true residual */
+        if ((rc = igab_launch_spmv(c, vals, prec, x, w))) return rc;
+        k_mg_sub<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, b, w, r);
+        m->launches += 4;
+        if ((rc = dot1(m, st, n, r, r, &beta))) return rc;
+        beta = std::sqrt(beta);
+        *rnorm = beta;
+    }
+    if (beta <= tol) *converged = 1;
+    *iterations = its;
+    IGAB_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+} /* namespace */
+
+int igab_mg_solve(igab_ctx *c, int method, const void *vals, int prec, const double *b, double *x, double rtol,
+                  double atol, int maxit, int *iterations, int *converged, double *rnorm, double *bnorm, int *breakdown)
 {
     if (!c->mg) {
         c->mg = new igab_mg();
         IGAB_CUDA_TRY(cudaMalloc((void **)&c->mg->part, (2 * RD_BLOCKS + 2) * sizeof(double)));
         c->mg->dots = c->mg->part + 2 * RD_BLOCKS;
         IGAB_CUDA_TRY(cudaMallocHost((void **)&c->mg->h_dots, 2 * sizeof(double)));
+        IGAB_CUDA_TRY(cudaMalloc((void **)&c->mg->mpart,
+                                 ((size_t)(GM_RESTART + 1) * RD_BLOCKS + 2 * (GM_RESTART + 1)) * sizeof(double)));
+        IGAB_CUDA_TRY(cudaMallocHost((void **)&c->mg->h_md, (GM_RESTART + 1) * sizeof(double)));
     }
     igab_mg *m = c->mg;
     m->launches = 0;
     int rc = 0;
     if (m->version != c->param_version || m->nlev == 0)
         if ((rc = mg_build(c, m))) return rc;
-    mg_level &F = m->L[0];
-    F.vals = vals;
-    F.prec = prec;
-    cudaStream_t st = c->stream;
-    const long n = F.n;
-    k_mg_diag_inv<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(c->geom(), vals, prec, F.dinv);
-    IGAB_CUDA_TRY(cudaGetLastError());
-    if ((rc = estimate_lmax(m, F))) return rc;
-    /* preconditioned CG: x = 0, r = b; the fine level's work vectors belong to the V-cycle,
-     * so CG keeps r, z, p, q in x's companions below */
-    if (m->cg_n != n) {
-        cudaFree(m->cg);
-        m->cg = nullptr;
-        m->cg_n = 0;
-        IGAB_CUDA_TRY(cudaMalloc((void **)&m->cg, (size_t)4 * n * sizeof(double)));
-        m->cg_n = n;
+    const long n = c->ndof;
+    const long need = (long)(GM_RESTART + 4) * n;
+    if (m->kv_n != need) {
+        cudaFree(m->kv);
+        m->kv = nullptr;
+        m->kv_n = 0;
+        IGAB_CUDA_TRY(cudaMalloc((void **)&m->kv, (size_t)need * sizeof(double)));
+        m->kv_n = need;
     }
-    double *r = m->cg, *z = r + n, *p = z + n, *q = p + n;
-    auto cleanup = [&]() {};
-    k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, b, r);
-    k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, 0.0, r, 0.0, x);
-    double d2[2];
-    cudaError_t e = rd_dot2(st, n, b, b, nullptr, nullptr, m->part, m->dots, m->h_dots, d2);
-    if (e != cudaSuccess) { cleanup(); IGAB_CUDA_TRY(e); }
-    const double bn = std::sqrt(d2[0]);
+    cudaStream_t st = c->stream;
+    IGAB_CUDA_TRY(cudaMemsetAsync(x, 0, (size_t)n * sizeof(double), st));
+    double bb = 0.0;
+    if ((rc = dot1(m, st, n, b, b, &bb))) return rc;
+    const double bn = std::sqrt(bb);
     const double tol = std::max(rtol * bn, atol);
     *bnorm = bn;
     *rnorm = bn;
     *iterations = 0;
     *converged = bn <= tol ? 1 : 0;
     *breakdown = 0;
-    if (*converged) { cleanup(); return 0; }
-    auto precond = [&](const double *rin, double *zout) -> int {
-        k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, rin, F.b);
-        int rc2 = vcycle(m, 0);
-        if (rc2) return rc2;
-        k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, F.x, zout);
-        m->launches += 2;
-        return 0;
-    };
-    if ((rc = precond(r, z))) { cleanup(); return rc; }
-    k_mg_copy<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, z, p);
-    e = rd_dot2(st, n, r, z, nullptr, nullptr, m->part, m->dots, m->h_dots, d2);
-    if (e != cudaSuccess) { cleanup(); IGAB_CUDA_TRY(e); }
-    double rz = d2[0];
-    for (int it = 1; it <= maxit; it++) {
-        if ((rc = igab_launch_spmv(c, vals, prec, p, q))) { cleanup(); return rc; }
-        e = rd_dot2(st, n, p, q, nullptr, nullptr, m->part, m->dots, m->h_dots, d2);
-        if (e != cudaSuccess) { cleanup(); IGAB_CUDA_TRY(e); }
-        const double pq = d2[0];
-        if (!(pq > 0.0) || !(rz > 0.0)) { *breakdown = 1; break; }
-        const double alpha = rz / pq;
-        k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, alpha, p, 1.0, x);
-        k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, -alpha, q, 1.0, r);
-        e = rd_dot2(st, n, r, r, nullptr, nullptr, m->part, m->dots, m->h_dots, d2);
-        if (e != cudaSuccess) { cleanup(); IGAB_CUDA_TRY(e); }
-        *iterations = it;
-        *rnorm = std::sqrt(d2[0]);
-        if (*rnorm <= tol) { *converged = 1; break; }
-        if ((rc = precond(r, z))) { cleanup(); return rc; }
-        e = rd_dot2(st, n, r, z, nullptr, nullptr, m->part, m->dots, m->h_dots, d2);
-        if (e != cudaSuccess) { cleanup(); IGAB_CUDA_TRY(e); }
-        const double beta = d2[0] / rz;
-        rz = d2[0];
-        k_mg_axpby<<<MG_BLOCKS, MG_THREADS, 0, st>>>(n, 1.0, z, beta, p);
-        m->launches += 10;
+    if (!*converged) {
+        if (method == IGAB_KSP_MG_CG)
+            rc = solve_cg(m, c, vals, prec, b, x, tol, maxit, iterations, converged, rnorm, breakdown);
+        else
+            rc = solve_gmres(m, c, vals, prec, b, x, tol, maxit, iterations, converged, rnorm);
+        if (rc) return rc;
     }
-    cleanup();
     IGAB_CUDA_TRY(cudaGetLastError());
     IGAB_CUDA_TRY(cudaStreamSynchronize(st));
     c->last_launches = m->launches;

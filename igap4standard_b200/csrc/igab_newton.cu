@@ -199,7 +199,7 @@ extern "C" void igab_newton_defaults(igab_newton_opts *o)
     o->max_subiter = 10000;
     o->ksp_rtol = 1e-5;
     o->ksp_maxit = 100000;
-    o->ksp = IGAB_KSP_MG_CG;
+    o->ksp = IGAB_KSP_MG_GMRES;
     o->verbose = 0;
 }
 
@@ -211,7 +211,7 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
         return IGAB_ERR_ARG;
     }
     if ((opts->prec != IGAB_PREC_FP64 && opts->prec != IGAB_PREC_FP32) || opts->max_subiter < 1 ||
-        (opts->ksp != IGAB_KSP_BICGSTAB && opts->ksp != IGAB_KSP_MG_CG) ||
+        (opts->ksp != IGAB_KSP_BICGSTAB && opts->ksp != IGAB_KSP_MG_CG && opts->ksp != IGAB_KSP_MG_GMRES) ||
         opts->ksp_maxit < 1 || !(opts->ksp_rtol >= 0.0) || !(opts->abstol >= 0.0)) {
         igab_set_error("igab_newton_solve: bad options");
         return IGAB_ERR_ARG;
@@ -282,9 +282,9 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
             t0 = clk::now();
             int conv = 0, brk = 1;
             double rn = 0.0, bn = 0.0;
-            if (opts->ksp == IGAB_KSP_MG_CG && ctx->phys == IGAB_PHYS_GE) {
-                rc = igab_mg_solve(ctx, w.vals, w.prec, w.F, w.Y, opts->ksp_rtol, 0.0, opts->ksp_maxit, &kits, &conv,
-                                   &rn, &bn, &brk);
+            if (opts->ksp != IGAB_KSP_BICGSTAB && ctx->phys == IGAB_PHYS_GE) {
+                rc = igab_mg_solve(ctx, opts->ksp, w.vals, w.prec, w.F, w.Y, opts->ksp_rtol, 0.0, opts->ksp_maxit, &kits,
+                                   &conv, &rn, &bn, &brk);
                 w.launches += ctx->last_launches;
                 if (rc) return rc;
             }

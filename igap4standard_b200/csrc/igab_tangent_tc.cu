@@ -83,10 +83,11 @@ struct tc_smem {
     double U[NCP * 3];
     double tab[3][TE][IGAB_TAB1D];
     double wh[3][TE][IGAB_NQ];
-    float tabf[3][TE][IGAB_TAB1D];
+    float4 tabf[3][TE][IGAB_NQ][3];     /* FP32 1-D tables [d][element][q][function], derivatives 0-2 in x, y, z */
     float pt[IGAB_NQ3][TP_N];
     unsigned short map[2][768];         /* bucket slot -> 12 q + v (positive, negative) */
-    float gk[2][TC_KC][3][9];           /* per chunk parity: r * d v'/d u_{k,m} of each slot (pre-pass) */
+    float4 gk[2][TC_KC][3][3];          /* per chunk parity: r * d v'/d u_{k,m} of each slot (pre-pass),
+                                           m = 0..8 in (x, y, z) of three float4 (w unused) */
     int qs[2][TC_KC];                   /* point of each slot, -1 for padding rows */
     int cnt[2];
     int vcnt[12][2][2];                 /* rows per (variable, point warp, sign) */
@@ -375,7 +376,7 @@ __device__ __forceinline__ void tc_prepass(tc_smem<TE> &S, int par, int bucket, 
     const int t = threadIdx.x;
     if (t >= 3 * TC_KC) return;
     const int j = t / 3, k = t % 3, slot = base + j;
-    float *gout = S.gk[par][j][k];
+    float *gout = reinterpret_cast<float *>(S.gk[par][j][k]);
     if (slot < cntb) {
         const int id = S.map[bucket][slot], q = id / 12, v = id % 12;
         const float *p = S.pt[q];
@@ -383,11 +384,11 @@ __device__ __forceinline__ void tc_prepass(tc_smem<TE> &S, int par, int bucket, 
         tc_grad_var(p, v, k, gv);
         const float r = fabsf(p[TP_RS + v]);
 #pragma unroll
-        for (int m = 0; m < 9; m++) gout[m] = r * gv[m];
+        for (int m = 0; m < 9; m++) gout[(m / 3) * 4 + m % 3] = r * gv[m];
         if (k == 0) S.qs[par][j] = q;
     } else {
 #pragma unroll
-        for (int m = 0; m < 9; m++) gout[m] = 0.f;
+        for (int m = 0; m < 9; m++) gout[(m / 3) * 4 + m % 3] = 0.f;
         if (k == 0) S.qs[par][j] = -1;
     }
 }
@@ -421,7 +422,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         int d = idx / (TE * IGAB_TAB1D), r = idx % (TE * IGAB_TAB1D), le = r / IGAB_TAB1D, o = r % IGAB_TAB1D;
         double t = le < Tl.nv[d] ? g.tab[d][(long)(Tl.e0[d] + le) * IGAB_TAB1D + o] : 0.0;
         S.tab[d][le][o] = t;
-        S.tabf[d][le][o] = (float)t;
+        reinterpret_cast<float *>(S.tabf[d][le])[(o / 3) * 4 + o % 3] = (float)t;
     }
     for (int idx = tid; idx < 3 * TE * IGAB_NQ; idx += TCN_BLD) {
         int d = idx / (TE * IGAB_NQ), r = idx % (TE * IGAB_NQ), le = r / IGAB_NQ, q = r % IGAB_NQ;
@@ -577,23 +578,28 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                 const int q = S.qs[par][j];
                 if (q >= 0) {
                     const int qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
-                    const float *gv = S.gk[par][j][k];
-                    const float *bxp = &S.tabf[0][lex][qx * 9 + ax * 3];
-                    const float bx0 = bxp[0], bx1 = bxp[1], bx2 = bxp[2];
+                    /* the row's coefficients m = 0..8 and the 1-D tables as float4 loads */
+                    const float4 ga = S.gk[par][j][k][0], gb = S.gk[par][j][k][1], gc = S.gk[par][j][k][2];
+                    const float4 bxv = S.tabf[0][lex][qx][ax];
+                    const float bx0 = bxv.x, bx1 = bxv.y, bx2 = bxv.z;
                     /* coefficients of By[ky] per kz: derivative m -> (kx, ky, kz) as eval_Bspline */
-                    const float t00 = gv[0] * bx1 + gv[3] * bx2, t01 = gv[1] * bx0 + gv[4] * bx1, t02 = gv[6] * bx0;
-                    const float t10 = gv[2] * bx0 + gv[5] * bx1, t11 = gv[7] * bx0;
-                    const float t20 = gv[8] * bx0;
-                    const float *bzq = &S.tabf[2][lez][qz * 9];
+                    const float t00 = ga.x * bx1 + gb.x * bx2, t01 = ga.y * bx0 + gb.y * bx1, t02 = gc.x * bx0;
+                    const float t10 = ga.z * bx0 + gb.z * bx1, t11 = gc.y * bx0;
+                    const float t20 = gc.z * bx0;
                     float bz[9];
 #pragma unroll
-                    for (int i = 0; i < 9; i++) bz[i] = bzq[i];
+                    for (int i = 0; i < 3; i++) {
+                        const float4 b4 = S.tabf[2][lez][qz][i];
+                        bz[3 * i] = b4.x;
+                        bz[3 * i + 1] = b4.y;
+                        bz[3 * i + 2] = b4.z;
+                    }
 #pragma unroll
                     for (int ay = 0; ay < 3; ay++) {
-                        const float *byp = &S.tabf[1][ley][qy * 9 + ay * 3];
-                        const float cy0 = t00 * byp[0] + t01 * byp[1] + t02 * byp[2];
-                        const float cy1 = t10 * byp[0] + t11 * byp[1];
-                        const float cy2 = t20 * byp[0];
+                        const float4 byv = S.tabf[1][ley][qy][ay];
+                        const float cy0 = t00 * byv.x + t01 * byv.y + t02 * byv.z;
+                        const float cy1 = t10 * byv.x + t11 * byv.y;
+                        const float cy2 = t20 * byv.x;
 #pragma unroll
                         for (int az = 0; az < 3; az++) {
                             const float y = cy0 * bz[3 * az] + cy1 * bz[3 * az + 1] + cy2 * bz[3 * az + 2];
@@ -616,18 +622,17 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                 const int srow = gch * TC_KC + j, q = srow / 6, i = srow % 6;
                 const int qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
                 const float *p = S.pt[q];
-                const float *bxp = &S.tabf[0][lex][qx * 9 + ax * 3];
-                const float *byp = &S.tabf[1][ley][qy * 9 + ay * 3];
-                const float bx0 = bxp[0], bx1 = bxp[1], bx2 = bxp[2];
-                const float by0 = byp[0], by1 = byp[1], by2 = byp[2];
+                const float4 bxv = S.tabf[0][lex][qx][ax], byv = S.tabf[1][ley][qy][ay];
+                const float bx0 = bxv.x, bx1 = bxv.y, bx2 = bxv.z;
+                const float by0 = byv.x, by1 = byv.y, by2 = byv.z;
                 const int I = i < 3 ? i : i - 3;
                 const float s00 = p[TP_S], s11 = p[TP_S + 1], s22 = p[TP_S + 2];
                 const float s01 = p[TP_S + 3], s02 = p[TP_S + 4], s12 = p[TP_S + 5];
                 const float tI0 = p[TP_T + 3 * I], tI1 = p[TP_T + 3 * I + 1], tI2 = p[TP_T + 3 * I + 2];
 #pragma unroll
                 for (int az = 0; az < 3; az++) {
-                    const float *bzp = &S.tabf[2][lez][qz * 9 + az * 3];
-                    const float bz0 = bzp[0], bz1 = bzp[1], bz2 = bzp[2];
+                    const float4 bzv = S.tabf[2][lez][qz][az];
+                    const float bz0 = bzv.x, bz1 = bzv.y, bz2 = bzv.z;
                     const float dx = bx1 * by0 * bz0, dy = bx0 * by1 * bz0, dz = bx0 * by0 * bz1;
                     /* second derivatives H[idx6(I, K)], K = 0..2 */
                     float h0, h1, h2;

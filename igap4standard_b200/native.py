@@ -108,8 +108,8 @@ IGAB_API = [
     ("igab_residual_noalloc", ctypes.c_int, [vp, vp, vp]),
     ("igab_staging_bytes", ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_size_t)]),
     ("igab_newton_defaults", None, [vp]),
-    ("igab_solve_mg_device", ctypes.c_int, [vp, vp, ctypes.c_int, vp, vp, ctypes.c_double, ctypes.c_double,
-                                            ctypes.c_int, vp]),
+    ("igab_solve_mg_device", ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int, vp, vp, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_int, vp]),
     ("igab_solve_mg_levels", ctypes.c_int, [vp, c_int_p]),
     ("igab_mg_prolongation_1d", ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int, vp]),
     ("igab_upload", ctypes.c_int, [vp, vp, vp, ctypes.c_long]),

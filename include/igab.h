@@ -263,23 +263,26 @@ int igab_spmv_device(igab_ctx *ctx, const void *vals_dev, int prec, const double
 int igab_solve_device(igab_ctx *ctx, const void *vals_dev, int prec, const double *b_dev, double *x_dev,
                       double rtol, double atol, int maxit, igab_solve_info *info);
 
-/* ---- multigrid-preconditioned conjugate gradients on the tangent (no reference counterpart;
+/* ---- multigrid-preconditioned Krylov solve on the tangent (no reference counterpart;
  * stands in for the PETSc KSP of src/snes_init.c:24-39).  The fourth-order phys/ge tangent
- * defeats Jacobi-preconditioned Krylov methods on fine meshes; this solve uses a geometric
- * multigrid V-cycle on nested spline spaces: every other interior knot removed per level
- * (elements per direction halved while even and >= 4, down to about 1,200 dofs), prolongation
- * by knot insertion, coarse tangents rediscretised at the zero state with the context's
- * material and (averaged) element scales, Chebyshev smoothing (degree 3 in D^-1 K), a dense
- * LU on the coarsest level.  The hierarchy is built on the first call and rebuilt after
- * igab_set_par_mat / igab_set_par_periodic / igab_set_element_log_scale.  x0 = 0, stop at
- * ||b - K x|| <= max(rtol ||b||, atol).  The tangent must be symmetric positive definite
- * (phys/ge near a stable state); a non-positive curvature p.Kp returns IGAB_ERR_UNSUPPORTED.
+ * defeats Jacobi-preconditioned Krylov methods on fine meshes; the preconditioner here is a
+ * geometric multigrid V-cycle on nested spline spaces: every other interior knot removed per
+ * level (elements per direction halved while even and >= 4, down to about 1,200 dofs),
+ * prolongation by knot insertion, all levels' operators the tangent at the zero state with
+ * the context's material and (averaged) element scales (symmetric positive definite for a
+ * stable material, so the V-cycle is an SPD preconditioner whatever the current state),
+ * Chebyshev smoothing (degree 3 in D^-1 K), a dense LU on the coarsest level.  The hierarchy
+ * is built on the first call and rebuilt after igab_set_par_mat / igab_set_par_periodic /
+ * igab_set_element_log_scale.  method: IGAB_KSP_MG_GMRES (right-preconditioned GMRES(50),
+ * any nonsingular tangent) or IGAB_KSP_MG_CG (CG, symmetric positive definite tangents; a
+ * non-positive curvature p.Kp returns IGAB_ERR_UNSUPPORTED).  x0 = 0, stop at
+ * ||b - K x|| <= max(rtol ||b||, atol).
  * igab_solve_mg_levels: levels of the current hierarchy (0 before the first solve).
  * igab_mg_prolongation_1d: the 1-D knot-insertion matrix P ((n+2+m) x (n+2), row-major) that
  * maps the spline coefficients on coarse_knots (n elements, open, p = 2) to those on the knot
  * vector with the m ascending interior knots `inserted` added. */
-int igab_solve_mg_device(igab_ctx *ctx, const void *vals_dev, int prec, const double *b_dev, double *x_dev,
-                         double rtol, double atol, int maxit, igab_solve_info *info);
+int igab_solve_mg_device(igab_ctx *ctx, int method, const void *vals_dev, int prec, const double *b_dev,
+                         double *x_dev, double rtol, double atol, int maxit, igab_solve_info *info);
 int igab_solve_mg_levels(igab_ctx *ctx, int *levels);
 int igab_mg_prolongation_1d(const double *coarse_knots, int n_coarse_elements, const double *inserted,
                             int n_inserted, double *P);
@@ -296,7 +299,7 @@ int igab_mg_prolongation_1d(const double *coarse_knots, int n_coarse_elements, c
  * Neumann values and history levels are used as set.  fnorm_history / krylov_history
  * (either may be NULL) receive ||F|| and the Krylov iteration count of the first
  * history_cap subiterations.  verbose = 1 prints the reference's line per subiteration. */
-enum igab_ksp_kind { IGAB_KSP_BICGSTAB = 0, IGAB_KSP_MG_CG = 1 };
+enum igab_ksp_kind { IGAB_KSP_BICGSTAB = 0, IGAB_KSP_MG_CG = 1, IGAB_KSP_MG_GMRES = 2 };
 enum igab_snes_reason {
     IGAB_SNES_CONVERGED_FNORM_ABS = 2, IGAB_SNES_CONVERGED_FNORM_RELATIVE = 3,
     IGAB_SNES_CONVERGED_SNORM_RELATIVE = 4, IGAB_SNES_DIVERGED_FNORM_NAN = -4,
@@ -311,8 +314,9 @@ typedef struct {
     int max_subiter;       /* 10000   src/snes_solve.c:24 */
     double ksp_rtol;       /* 1e-5    PETSc's default KSP relative tolerance */
     int ksp_maxit;         /* 100000  iterations per linear solve */
-    int ksp;               /* IGAB_KSP_MG_CG (default; phys/ge, falls back to BiCGStab on a CG breakdown)
-                              or IGAB_KSP_BICGSTAB (Jacobi BiCGStab; always for phys/getime) */
+    int ksp;               /* IGAB_KSP_MG_GMRES (default), IGAB_KSP_MG_CG (phys/ge; BiCGStab for a step whose
+                              CG meets non-positive curvature) or IGAB_KSP_BICGSTAB (Jacobi BiCGStab,
+                              always for phys/getime) */
     int verbose;           /* 0 */
 } igab_newton_opts;
 typedef struct {

@@ -1,11 +1,11 @@
-"""Multigrid-preconditioned CG on the assembled tangent (igab_solve_mg_device).
+"""Multigrid-preconditioned GMRES and CG on the assembled tangent (igab_solve_mg_device).
 
-  * 8^3 (two levels, dense coarsest): the solution equals scipy's sparse direct solve of
-    the same CSR system to 1e-9 relative;
+  * 8^3 (two levels, dense coarsest): both methods' solutions equal scipy's sparse direct
+    solve of the same CSR system to 1e-9 relative;
   * 16^3 and 32^3 of the config-1 workload (perturbed knots), at a nonzero state and with
     element scales exp(g), g ~ N(0, 0.3^2): the true residual ||b - K x|| (scipy's CSR
     product) meets the tolerance and the iteration count stays small where the Jacobi
-    BiCGStab of igab_solve_device needs thousands;
+    BiCGStab of igab_solve_device needs thousands; CG at the zero state likewise;
   * repeated solves are bitwise equal; a changed material rebuilds the hierarchy."""
 import numpy as np
 import pytest
@@ -17,7 +17,7 @@ from igap4standard_b200 import mesh
 pytestmark = pytest.mark.gpu
 
 
-def _problem(n, scales=False, seed=0):
+def _problem(n, scales=False, seed=0, amp=1e-3):
     import torch
     from igap4standard_b200 import Assembly
     nelem = (n, n, n)
@@ -28,25 +28,26 @@ def _problem(n, scales=False, seed=0):
     if scales:
         A.set_element_log_scale(np.random.default_rng(4).normal(0.0, 0.3, A.nelem_total))
     rng = np.random.default_rng(seed)
-    U = torch.as_tensor(rng.uniform(-1e-3, 1e-3, A.ndof)).cuda()
+    U = torch.as_tensor(rng.uniform(-amp, amp, A.ndof)).cuda()
     b = torch.as_tensor(rng.normal(size=A.ndof)).cuda()
     return A, st, U, b
 
 
-def _solve(A, st, U, b, prec="fp64", rtol=1e-8):
+def _solve(A, st, U, b, prec="fp64", rtol=1e-8, method="gmres"):
     import torch
     V = torch.empty(A.nnz, dtype=torch.float64 if prec == "fp64" else torch.float32, device="cuda")
     x = torch.zeros(A.ndof, dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
     A.tangent_device(U.data_ptr(), V.data_ptr(), prec)
     A.sync()
-    its, ok, rn, lev = A.solve_mg_device(V.data_ptr(), b.data_ptr(), x.data_ptr(), prec, rtol, 0.0, 500)
+    its, ok, rn, lev = A.solve_mg_device(V.data_ptr(), b.data_ptr(), x.data_ptr(), prec, rtol, 0.0, 500, method)
     return V.cpu().numpy().astype(np.float64), x.cpu().numpy(), its, ok, rn, lev
 
 
-def test_mg_matches_direct_solve_8cubed(built):
+@pytest.mark.parametrize("method", ["gmres", "cg"])
+def test_mg_matches_direct_solve_8cubed(built, method):
     A, st, U, b = _problem(8)
-    v, x, its, ok, rn, lev = _solve(A, st, U, b, rtol=1e-12)
+    v, x, its, ok, rn, lev = _solve(A, st, U, b, rtol=1e-12, method=method)
     rp, cols = A.pattern()
     K = sp.csr_matrix((v, cols, rp), shape=(A.ndof, A.ndof))
     x_ref = spla.spsolve(K.tocsc(), b.cpu().numpy())
@@ -68,6 +69,17 @@ def test_mg_converges_in_few_iterations(built, n, scales, prec):
     assert ok and true_res <= 2e-8
     assert its <= 100
     assert lev == {16: 3, 32: 4}[n]
+
+
+def test_mg_cg_at_zero_state_32cubed(built):
+    A, st, U, b = _problem(32, amp=0.0)
+    v, x, its, ok, rn, lev = _solve(A, st, U, b, rtol=1e-8, method="cg")
+    rp, cols = A.pattern()
+    K = sp.csr_matrix((v, cols, rp), shape=(A.ndof, A.ndof))
+    bh = b.cpu().numpy()
+    true_res = np.linalg.norm(bh - K @ x) / np.linalg.norm(bh)
+    print("32^3 CG at U = 0: levels %d, iterations %d, true relative residual %.2e" % (lev, its, true_res))
+    assert ok and true_res <= 2e-8 and its <= 60
 
 
 def test_mg_repeatable_and_rebuilt(built):

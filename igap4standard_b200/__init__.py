@@ -7,7 +7,7 @@ scatter into the AIJ pattern) as hand-written sm_100a kernels behind a C ABI
 """
 from .native import NativeLibraryMissing, IgabError, lib_cuda, lib_dropin
 from .mesh import (open_knot_vector, knots_for, par_mat_from_lame, bc_config0, bc_example,
-                   n_dof, nnz_of, PAR_MAT_DEFAULT)
+                   n_dof, nnz_of, affine_field, PAR_MAT_DEFAULT)
 from .assembly import Assembly
 from .batch import Batch
 from .case import Case, gpu_case

@@ -182,6 +182,19 @@ class Assembly:
                                          float(atol), int(maxit), ctypes.byref(info)))
         return info.iterations, bool(info.converged), info.residual_norm
 
+    def affine_start(self, knots, F0):
+        """A Newton start for static problems: the affine field u = F0 X at the control points'
+        Greville abscissae (mesh.affine_field), with every Dirichlet row set to its value
+        (R = U - g there, so g = U - R).  From U = 0 the reference's first step projects onto
+        the Dirichlet values and leaves a one-element boundary layer whose strain grows like
+        1/h; this start has none."""
+        from .mesh import affine_field
+        U = affine_field(self.nelem, knots, F0)
+        R = self.residual(U)
+        rows = self.dirichlet_rows()
+        U[rows] -= R[rows]
+        return U
+
     def solve_mg_device(self, vals_ptr, b_ptr, x_ptr, prec="fp64", rtol=1e-5, atol=0.0, maxit=1000, method="gmres"):
         """x = K^-1 b by multigrid-preconditioned GMRES or CG on the device (igab_solve_mg_device).
         Returns (iterations, converged, residual norm, multigrid levels)."""

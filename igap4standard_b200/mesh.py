@@ -91,6 +91,30 @@ def bc_example():
     return np.array(row * 6, dtype=np.int32), np.zeros(9)
 
 
+def greville(kv):
+    """Greville abscissae of a p = 2 knot vector: (k[j+1] + k[j+2]) / 2, one per basis
+    function.  Control values a + b x_j at these points reproduce the linear function
+    a + b x exactly (B-splines of degree >= 1)."""
+    kv = np.asarray(kv, dtype=np.float64)
+    return 0.5 * (kv[1:-2] + kv[2:-1])
+
+
+def affine_field(nelem, knots, F0):
+    """Control values (dof = 3 cp + i, cp = (x nb1 + y) nb2 + z) of u_i(X) = sum_j F0[i][j] X_j
+    on the mesh: the affine map the Dirichlet values reproduce (src/iga_dirichlet.c:10-12,
+    par_dirichlet = F0 row-major), so this field satisfies every Dirichlet row (values and
+    normal derivatives) of any bc_type table exactly."""
+    nelem = [int(n) for n in nelem]
+    kv, off = [], 0
+    for n in nelem:
+        kv.append(np.asarray(knots[off:off + n + 5], dtype=np.float64))
+        off += n + 5
+    gx, gy, gz = (greville(k) for k in kv)
+    X = np.stack(np.meshgrid(gx, gy, gz, indexing="ij"), axis=-1).reshape(-1, 3)
+    F = np.asarray(F0, dtype=np.float64).reshape(3, 3)
+    return (X @ F.T).reshape(-1)
+
+
 def n_dof(nelem):
     return 3 * int(np.prod(np.asarray(nelem) + P))
 

@@ -58,3 +58,4 @@ def test_prolongation_rejects_bad_knots(built):
     P = np.zeros((4 + 2) * 4)
     assert lib.igab_mg_prolongation_1d(coarse.ctypes.data_as(ctypes.c_void_p), 2, ins.ctypes.data_as(ctypes.c_void_p),
                                        2, P.ctypes.data_as(ctypes.c_void_p)) == 1
+

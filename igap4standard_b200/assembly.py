@@ -208,7 +208,7 @@ class Assembly:
         return info.iterations, bool(info.converged), info.residual_norm, lev.value
 
     def newton_solve_device(self, U_ptr, prec="fp64", ksp_rtol=1e-5, ksp_maxit=100000, abstol=1e-10,
-                            max_subiter=10000, verbose=False, history_cap=64, ksp="mg"):
+                            max_subiter=10000, verbose=False, history_cap=64, ksp="mg", fp64_polish=False):
         """Device Newton solve (igab_newton_solve) from the state at U_ptr (device, FP64,
         overwritten with the result).  Returns a dict of the solve info plus the ||F|| and
         Krylov-iteration history of each subiteration."""
@@ -221,6 +221,7 @@ class Assembly:
         o.max_subiter = int(max_subiter)
         o.ksp = {"mg": 2, "mg-cg": 1, "bicgstab": 0}[ksp]
         o.verbose = 1 if verbose else 0
+        o.fp64_polish = 1 if fp64_polish else 0
         info = native.IgabNewtonInfo()
         fh = np.zeros(history_cap)
         kh = np.zeros(history_cap, dtype=np.int32)

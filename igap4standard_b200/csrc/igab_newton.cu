@@ -91,7 +91,7 @@ double ms_since(clk::time_point t0)
 }
 
 struct nl_counters {
-    int nres = 0, ntan = 0;
+    int nres = 0, ntan = 0, ntan64 = 0;
     long kits = 0;
     double ms_res = 0.0, ms_tan = 0.0, ms_ksp = 0.0;
 };
@@ -201,6 +201,7 @@ extern "C" void igab_newton_defaults(igab_newton_opts *o)
     o->ksp_maxit = 100000;
     o->ksp = IGAB_KSP_MG_GMRES;
     o->verbose = 0;
+    o->fp64_polish = 0;
 }
 
 extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton_opts *opts, igab_newton_info *info,
@@ -230,12 +231,13 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
     const size_t es = opts->prec == IGAB_PREC_FP64 ? sizeof(double) : sizeof(float);
     if (!ctx->d_nl) IGAB_CUDA_TRY(cudaMalloc((void **)&ctx->d_nl, ((size_t)5 * n + 2 * NL_BLOCKS + 2) * sizeof(double)));
     if (!ctx->h_nl) IGAB_CUDA_TRY(cudaMallocHost((void **)&ctx->h_nl, 2 * sizeof(double)));
-    if (ctx->nl_vals_bytes < (size_t)ctx->nnz * es) {
+    const size_t es_max = opts->fp64_polish ? sizeof(double) : es;   /* the polish steps need FP64 values */
+    if (ctx->nl_vals_bytes < (size_t)ctx->nnz * es_max) {
         cudaFree(ctx->d_nl_vals);
         ctx->d_nl_vals = nullptr;
         ctx->nl_vals_bytes = 0;
-        IGAB_CUDA_TRY(cudaMalloc(&ctx->d_nl_vals, (size_t)ctx->nnz * es));
-        ctx->nl_vals_bytes = (size_t)ctx->nnz * es;
+        IGAB_CUDA_TRY(cudaMalloc(&ctx->d_nl_vals, (size_t)ctx->nnz * es_max));
+        ctx->nl_vals_bytes = (size_t)ctx->nnz * es_max;
     }
     nl_work w;
     w.c = ctx;
@@ -260,6 +262,7 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
         /* one SNESSolve with max_it = 1 */
         int kits = 0;
         if ((rc = eval_residual(w, X, w.F, &fnorm, k))) return rc;
+        const double fprev = fnorm;
         if (!std::isfinite(fnorm)) {
             reason = IGAB_SNES_DIVERGED_FNORM_NAN;
         } else if (fnorm < opts->abstol) {
@@ -278,6 +281,7 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
             }
             if (rc) return rc;
             k.ntan++;
+            if (w.prec == IGAB_PREC_FP64) k.ntan64++;
             k.ms_tan += ms_since(t0);
             t0 = clk::now();
             int conv = 0, brk = 1;
@@ -328,6 +332,10 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
                 reason = IGAB_SNES_CONVERGED_SNORM_RELATIVE;
             else
                 reason = IGAB_SNES_DIVERGED_MAX_IT;
+            /* FP32 tangent whose error now limits the step: polish in FP64 */
+            if (opts->fp64_polish && w.prec == IGAB_PREC_FP32 && reason == IGAB_SNES_DIVERGED_MAX_IT &&
+                fnorm > 0.1 * fprev)
+                w.prec = IGAB_PREC_FP64;
         }
         /* src/snes_solve.c:28-32: stagnation ends the loop */
         if (std::fabs(f_old - fnorm) / f_old < opts->stagnation) reason = IGAB_SNES_DIVERGED_LINE_SEARCH;
@@ -350,6 +358,7 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
     info->krylov_iterations = k.kits;
     info->n_residual = k.nres;
     info->n_tangent = k.ntan;
+    info->n_tangent_fp64 = k.ntan64;
     info->fnorm = fnorm;
     info->ms_residual = k.ms_res;
     info->ms_tangent = k.ms_tan;

@@ -46,13 +46,14 @@ class IgabNewtonOpts(ctypes.Structure):
     _fields_ = [("prec", ctypes.c_int), ("abstol", ctypes.c_double), ("rtol", ctypes.c_double),
                 ("stol", ctypes.c_double), ("stagnation", ctypes.c_double), ("max_subiter", ctypes.c_int),
                 ("ksp_rtol", ctypes.c_double), ("ksp_maxit", ctypes.c_int), ("ksp", ctypes.c_int),
-                ("verbose", ctypes.c_int)]
+                ("verbose", ctypes.c_int), ("fp64_polish", ctypes.c_int)]
 
 
 class IgabNewtonInfo(ctypes.Structure):
     """igab_newton_info of include/igab.h"""
     _fields_ = [("iterations", ctypes.c_int), ("reason", ctypes.c_int), ("converged", ctypes.c_int),
-                ("n_residual", ctypes.c_int), ("n_tangent", ctypes.c_int), ("krylov_iterations", ctypes.c_long),
+                ("n_residual", ctypes.c_int), ("n_tangent", ctypes.c_int), ("n_tangent_fp64", ctypes.c_int),
+                ("krylov_iterations", ctypes.c_long),
                 ("fnorm", ctypes.c_double), ("ms_residual", ctypes.c_double), ("ms_tangent", ctypes.c_double),
                 ("ms_krylov", ctypes.c_double), ("ms_total", ctypes.c_double), ("launches", ctypes.c_long)]
 

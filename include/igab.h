@@ -318,12 +318,15 @@ typedef struct {
                               CG meets non-positive curvature) or IGAB_KSP_BICGSTAB (Jacobi BiCGStab,
                               always for phys/getime) */
     int verbose;           /* 0 */
+    int fp64_polish;       /* 0; with prec FP32: once a step reduces ||F|| by less than 10x (the FP32
+                              tangent's error limits the step), the remaining steps use the FP64 tangent */
 } igab_newton_opts;
 typedef struct {
     int iterations;          /* Newton steps taken */
     int reason;              /* igab_snes_reason of the last subiteration */
     int converged;           /* reason > 0 */
     int n_residual, n_tangent;
+    int n_tangent_fp64;      /* tangents assembled in FP64 (all of them for prec FP64; the polish steps) */
     long krylov_iterations;  /* over all linear solves */
     double fnorm;            /* ||F||_2 at exit */
     double ms_residual, ms_tangent, ms_krylov, ms_total;   /* wall time by phase */

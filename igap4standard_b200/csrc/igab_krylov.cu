@@ -81,15 +81,29 @@ __global__ void __launch_bounds__(KV_THREADS) k_spmv(igab_geom g, const T *__res
     /* the three rows of the control point share the columns; row k starts k * total later */
     const T *v0 = vals + g.rowptr[3 * cp], *v1 = v0 + total, *v2 = v1 + total;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    for (int p0 = 0; p0 < total; p0 += 32) {
-        const int p = p0 + lane;
-        const int run = (int)(((unsigned)(p < total ? p : 0) * invL) >> 16);
-        const long base = __shfl_sync(0xffffffffu, base_own, run);
-        if (p < total) {
-            const double xv = x[base + (p - run * L)];
-            a0 += double(v0[p]) * xv;
-            a1 += double(v1[p]) * xv;
-            a2 += double(v2[p]) * xv;
+    /* four 32-entry chunks per pass: every load of the pass is issued before the first
+     * multiply, so a warp keeps 16 loads in flight; the additions keep the chunk order */
+    for (int p0 = 0; p0 < total; p0 += 128) {
+        double xv[4];
+        T w0[4], w1[4], w2[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int p = p0 + 32 * c + lane;
+            const bool in = p < total;
+            const int run = (int)(((unsigned)(in ? p : 0) * invL) >> 16);
+            const long base = __shfl_sync(0xffffffffu, base_own, run);
+            xv[c] = in ? x[base + (p - run * L)] : 0.0;
+            w0[c] = in ? v0[p] : T(0);
+            w1[c] = in ? v1[p] : T(0);
+            w2[c] = in ? v2[p] : T(0);
+        }
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            if (p0 + 32 * c + lane < total) {
+                a0 += double(w0[c]) * xv[c];
+                a1 += double(w1[c]) * xv[c];
+                a2 += double(w2[c]) * xv[c];
+            }
         }
     }
 #pragma unroll

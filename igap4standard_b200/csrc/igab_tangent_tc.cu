@@ -755,30 +755,30 @@ __global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32(igab_geom g, const doub
     tc_release<TE>(S, Q, status);
 }
 
-/* persistent FP32 tangent over the tiles of every instance of a batch: tensor
- * memory and barriers are set up once per CTA; after an abort the remaining
- * items are only published (their values are not computed) */
+/* FP32 tangent over the tiles of every instance of a batch: one CTA per work item.
+ * Each CTA takes the next item of the colour-major list from the batch counter when
+ * it starts (not by its block index), so every item it may wait for (an earlier colour
+ * of its instance) belongs to a CTA that started before it: the bounded waits always
+ * make progress.  Per CTA the code is the single-mesh kernel's (a persistent loop over
+ * items measured 1.8x slower per element: register spills across the item loop). */
 __global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32_batch(igab_batch_dev B, const double *__restrict__ U,
                                                                float *__restrict__ vals)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     tc_smem<2> &S = *reinterpret_cast<tc_smem<2> *>(smem_raw);
     __shared__ batch_slot sl;
+    if (!batch_next(B, sl)) return;   /* block-uniform, before any barrier of the tile */
     tc_state Q;
     tc_setup<2>(S, Q);
-    while (batch_next(B, sl)) {
-        if (!S.abort_flag) {
-            if (threadIdx.x < TCN_BLD) {
-                tile_t Tl;
-                decode_tile(sl.g, 2, sl.colour, sl.tile, Tl);
-                tc_tile<2>(sl.g, Tl, U + B.dof_off[sl.inst], vals + B.nnz_off[sl.inst], S, Q);
-            } else {
-                tc_issue<2>(S, Q);
-            }
-        }
-        batch_done(B, sl);
+    if (threadIdx.x < TCN_BLD) {
+        tile_t Tl;
+        decode_tile(sl.g, 2, sl.colour, sl.tile, Tl);
+        tc_tile<2>(sl.g, Tl, U + B.dof_off[sl.inst], vals + B.nnz_off[sl.inst], S, Q);
+    } else {
+        tc_issue<2>(S, Q);
     }
     tc_release<2>(S, Q, B.status);
+    batch_done(B, sl);
 }
 
 /* ---------------------------------------------------------------- self-test
@@ -965,10 +965,12 @@ int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv, int tx0, int 
 
 int igab_launch_tan_tc32_batch(const igab_batch_dev &B, int grid, cudaStream_t st, const double *dU, float *dv)
 {
+    (void)grid;   /* one CTA per work item; the hardware keeps at most two per SM (tensor memory) */
     const size_t sm = sizeof(tc_smem<2>);
     IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_tc32_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_tc32_batch, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    k_tan_tc32_batch<<<grid, TCN_THR, sm, st>>>(B, dU, dv);
+    if (B.nitems == 0) return 0;
+    k_tan_tc32_batch<<<B.nitems, TCN_THR, sm, st>>>(B, dU, dv);
     IGAB_CUDA_TRY(cudaGetLastError());
     return 0;
 }

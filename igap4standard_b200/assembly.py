@@ -15,6 +15,49 @@ def _ptr(a):
     return a.ctypes.data_as(vp)
 
 
+class TransientAdjoint:
+    """The checkpointed adjoint pass of igab_tadj_* on one Assembly (see transient_adjoint)."""
+
+    def __init__(self, A, opts, every, U_init_ptr, U_prev_ptr):
+        self.A, self.lib = A, A.lib
+        self.U_init_ptr, self.U_prev_ptr = U_init_ptr, U_prev_ptr
+        h = ctypes.c_void_p()
+        check(self.lib, "igab_tadj_create", self.lib.igab_tadj_create(A.h, ctypes.byref(opts), int(every),
+                                                                       ctypes.byref(h)))
+        self.h = h
+
+    def forward(self, U_final_ptr, U_init_ptr=None):
+        """The forward steps from U_init (device; the zero state when never given), U_N into U_final_ptr."""
+        u0 = U_init_ptr or self.U_init_ptr
+        if u0 is None:
+            import torch
+            self._zero = torch.zeros(self.A.ndof, dtype=torch.float64, device=torch.device("cuda", self.A.device))
+            u0 = self._zero.data_ptr()
+        check(self.lib, "igab_tadj_forward",
+              self.lib.igab_tadj_forward(self.h, vp(u0), vp(self.U_prev_ptr) if self.U_prev_ptr else None,
+                                         vp(U_final_ptr)))
+
+    def backward(self, dJdU_ptr, grad_ptr):
+        """dJ/dg (device, nel doubles) from dJ/dU_N (device)."""
+        check(self.lib, "igab_tadj_backward", self.lib.igab_tadj_backward(self.h, vp(dJdU_ptr), vp(grad_ptr)))
+
+    def info(self):
+        i = native.IgabTadjInfo()
+        check(self.lib, "igab_tadj_info", self.lib.igab_tadj_info(self.h, ctypes.byref(i)))
+        return {f: getattr(i, f) for f, _ in native.IgabTadjInfo._fields_}
+
+    def close(self):
+        if self.h:
+            self.lib.igab_tadj_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Assembly:
     """One single-rank mesh on one GPU: residual and tangent assembly.
 
@@ -208,7 +251,8 @@ class Assembly:
         return info.iterations, bool(info.converged), info.residual_norm, lev.value
 
     def newton_solve_device(self, U_ptr, prec="fp64", ksp_rtol=1e-5, ksp_maxit=100000, abstol=1e-10,
-                            max_subiter=10000, verbose=False, history_cap=64, ksp="mg", fp64_polish=False):
+                            max_subiter=10000, verbose=False, history_cap=64, ksp="mg", fp64_polish=False,
+                            use_graph=True):
         """Device Newton solve (igab_newton_solve) from the state at U_ptr (device, FP64,
         overwritten with the result).  Returns a dict of the solve info plus the ||F|| and
         Krylov-iteration history of each subiteration."""
@@ -222,6 +266,7 @@ class Assembly:
         o.ksp = {"mg": 2, "mg-cg": 1, "bicgstab": 0}[ksp]
         o.verbose = 1 if verbose else 0
         o.fp64_polish = 1 if fp64_polish else 0
+        o.use_graph = 1 if use_graph else 0
         info = native.IgabNewtonInfo()
         fh = np.zeros(history_cap)
         kh = np.zeros(history_cap, dtype=np.int32)
@@ -233,6 +278,45 @@ class Assembly:
         out["fnorms"] = fh[:m].tolist()
         out["krylov"] = kh[:m].tolist()
         return out
+
+    def transient_run(self, U_ptr, nsteps, prec="fp32", U_prev_ptr=None, dt=0.0, amplitude=0.01, face=1, order=0,
+                      dof=0, ksp_rtol=1e-5, ksp_maxit=100000, abstol=1e-10, use_graph=True, keep_steps=False):
+        """Time stepping of the transient physics on the device (igab_transient_run): nsteps
+        steps from U at t_0 (device, FP64, at U_ptr; overwritten with U at t_nsteps) and U at
+        t_-1 (U_prev_ptr; None = zero).  Returns (totals, per-step info dicts, the states
+        after every step as an (nsteps, ndof) array when keep_steps, else None)."""
+        o = self._transient_opts(nsteps, prec, dt, amplitude, face, order, dof, ksp_rtol, ksp_maxit, abstol,
+                                 use_graph)
+        steps = (native.IgabNewtonInfo * max(nsteps, 1))()
+        info = native.IgabTransientInfo()
+        hist = np.empty((nsteps, self.ndof)) if keep_steps else None
+        check(self.lib, "igab_transient_run",
+              self.lib.igab_transient_run(self.h, ctypes.byref(o), vp(U_ptr), vp(U_prev_ptr) if U_prev_ptr else None,
+                                          _ptr(hist) if keep_steps else None, steps, ctypes.byref(info)))
+        per_step = [{f: getattr(steps[i], f) for f, _ in native.IgabNewtonInfo._fields_} for i in range(nsteps)]
+        return {f: getattr(info, f) for f, _ in native.IgabTransientInfo._fields_}, per_step, hist
+
+    def _transient_opts(self, nsteps, prec, dt, amplitude, face, order, dof, ksp_rtol, ksp_maxit, abstol, use_graph):
+        o = native.IgabTransientOpts()
+        self.lib.igab_transient_defaults(ctypes.byref(o))
+        o.nsteps = int(nsteps)
+        o.dt = float(dt)
+        o.amplitude = float(amplitude)
+        o.face, o.order, o.dof = int(face), int(order), int(dof)
+        o.newton.prec = PREC[prec]
+        o.newton.ksp_rtol = float(ksp_rtol)
+        o.newton.ksp_maxit = int(ksp_maxit)
+        o.newton.abstol = float(abstol)
+        o.newton.use_graph = 1 if use_graph else 0
+        return o
+
+    def transient_adjoint(self, nsteps, every=10, U_init_ptr=None, U_prev_ptr=None, dt=0.0, amplitude=0.01, face=1,
+                          order=0, dof=0, ksp_rtol=1e-12, ksp_maxit=100000, abstol=1e-13, use_graph=True):
+        """A checkpointed discrete adjoint of nsteps time steps (igab_tadj_*), FP64 tangents.
+        Returns a TransientAdjoint: forward(U_final_ptr), then backward(dJdU_ptr, grad_ptr)."""
+        o = self._transient_opts(nsteps, "fp64", dt, amplitude, face, order, dof, ksp_rtol, ksp_maxit, abstol,
+                                 use_graph)
+        return TransientAdjoint(self, o, every, U_init_ptr, U_prev_ptr)
 
     def ndensity(self):
         n = ctypes.c_int()

@@ -108,6 +108,7 @@ extern "C" int igab_autotune(igab_ctx *ctx, const double *U_dev, int what, int r
         tms = best;
     }
     ctx->profiling = prof;
+    ctx->sched_version++;
     IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return rc;
 }

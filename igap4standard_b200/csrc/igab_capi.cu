@@ -518,7 +518,10 @@ extern "C" long igab_csr_offset(const igab_ctx *ctx, long row, long col)
 extern "C" int igab_set_par_mat(igab_ctx *ctx, const double par_mat[9])
 {
     ARG_CHECK(ctx && par_mat, "igab_set_par_mat: null argument");
-    if (memcmp(ctx->par_mat, par_mat, sizeof(ctx->par_mat)) != 0) ctx->param_version++;
+    if (memcmp(ctx->par_mat, par_mat, sizeof(ctx->par_mat)) != 0) {
+        ctx->param_version++;
+        ctx->sched_version++;
+    }
     memcpy(ctx->par_mat, par_mat, sizeof(ctx->par_mat));
     return 0;
 }
@@ -528,6 +531,7 @@ extern "C" int igab_set_par_dirichlet(igab_ctx *ctx, const double par_dirichlet[
     ARG_CHECK(ctx && par_dirichlet, "igab_set_par_dirichlet: null argument");
     if (memcmp(ctx->par_dirichlet, par_dirichlet, sizeof(ctx->par_dirichlet)) != 0) {
         memcpy(ctx->par_dirichlet, par_dirichlet, sizeof(ctx->par_dirichlet));
+        ctx->sched_version++;
         IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
         IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         return build_dirichlet(ctx);
@@ -538,7 +542,10 @@ extern "C" int igab_set_par_dirichlet(igab_ctx *ctx, const double par_dirichlet[
 extern "C" int igab_set_par_periodic(igab_ctx *ctx, const double par_periodic[9])
 {
     ARG_CHECK(ctx && par_periodic, "igab_set_par_periodic: null argument");
-    if (memcmp(ctx->par_periodic, par_periodic, sizeof(ctx->par_periodic)) != 0) ctx->param_version++;
+    if (memcmp(ctx->par_periodic, par_periodic, sizeof(ctx->par_periodic)) != 0) {
+        ctx->param_version++;
+        ctx->sched_version++;
+    }
     memcpy(ctx->par_periodic, par_periodic, sizeof(ctx->par_periodic));
     return 0;
 }
@@ -584,7 +591,7 @@ extern "C" int igab_set_neumann_values(igab_ctx *ctx, const double *values)
         if (values[i] != 0.0) { nz = true; break; }
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     /* zeros are copied too while a captured graph (which always runs the Neumann kernel) exists */
-    if (nz || ctx->graph_exec)
+    if (nz || ctx->graph_exec || ctx->nlg)
         IGAB_CUDA_TRY(cudaMemcpyAsync(ctx->d_hval, values, (size_t)ctx->n_neu_points * sizeof(double),
                                       cudaMemcpyHostToDevice, ctx->stream));
     IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -602,7 +609,6 @@ extern "C" int igab_set_history(igab_ctx *ctx, int level, const double *U, int o
     return 0;
 }
 
-static int check_status(igab_ctx *ctx);
 
 static int ensure_buffers(igab_ctx *ctx, int prec)
 {
@@ -725,7 +731,7 @@ extern "C" int igab_tangent(igab_ctx *ctx, const double *U_host, void *vals_host
     if (rc) return rc;
     IGAB_CUDA_TRY(ce);
     IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    rc = check_status(ctx);
+    rc = igab_check_status(ctx);
     if (rc) return rc;
     if (!fin) { igab_set_error("igab_tangent: non-finite entry"); return IGAB_ERR_NONFINITE; }
     return 0;
@@ -871,7 +877,7 @@ extern "C" int igab_set_stream(igab_ctx *ctx, void *cuda_stream)
 }
 
 /* after a stream synchronisation: report (and clear) a kernel's bounded-wait failure */
-static int check_status(igab_ctx *ctx)
+int igab_check_status(igab_ctx *ctx)
 {
     int st = 0;
     IGAB_CUDA_TRY(cudaMemcpy(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
@@ -888,7 +894,7 @@ extern "C" int igab_sync(igab_ctx *ctx)
     ARG_CHECK(ctx, "igab_sync: null context");
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return check_status(ctx);
+    return igab_check_status(ctx);
 }
 
 extern "C" int igab_check_finite(igab_ctx *ctx, const void *dev, long n, int prec, int *all_finite)
@@ -905,6 +911,7 @@ extern "C" int igab_set_tile(igab_ctx *ctx, int residual_tile, int tangent_tile)
     ARG_CHECK(tangent_tile == 0 || tangent_tile == 2, "igab_set_tile: tangent tile must be 2");
     ctx->tile_res = residual_tile ? residual_tile : 2;
     ctx->tile_tan = tangent_tile ? tangent_tile : 2;
+    ctx->sched_version++;
     return 0;
 }
 
@@ -960,10 +967,12 @@ extern "C" int igab_set_option(igab_ctx *ctx, int option, int value)
     case IGAB_OPT_TANGENT_FP64_KERNEL:
         ARG_CHECK(value == 0 || value == 1, "igab_set_option: tangent kernel must be 0 or 1");
         ctx->tan_kernel = value;
+        ctx->sched_version++;
         return 0;
     case IGAB_OPT_TANGENT_FP32_KERNEL:
         ARG_CHECK(value == 0 || value == 1, "igab_set_option: tangent kernel must be 0 or 1");
         ctx->tan32_kernel = value;
+        ctx->sched_version++;
         return 0;
     default:
         igab_set_error("igab_set_option: unknown option %d", option);
@@ -1060,6 +1069,7 @@ extern "C" int igab_set_element_log_scale(igab_ctx *ctx, const double *g, int on
     ARG_CHECK(ctx, "igab_set_element_log_scale: null context");
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     ctx->param_version++;
+    ctx->sched_version++;
     if (!g) {
         ctx->escale_on = false;
         return 0;
@@ -1094,6 +1104,8 @@ extern "C" int igab_adjoint_forward(igab_ctx *ctx, const double *g_dev, const do
         if (!rc) rc = igab_launch_exp_scale(ctx, g_dev);
         if (rc) return rc;
         ctx->escale_on = true;
+        ctx->param_version++;
+        ctx->sched_version++;
     }
     if (R_dev) rc = igab_launch_residual(ctx, U_dev, R_dev);
     if (!rc && vals_dev) rc = igab_launch_tangent(ctx, U_dev, vals_dev, prec);

@@ -149,6 +149,12 @@ struct igab_ctx {
     struct igab_mg *mg = nullptr;
     long param_version = 0;            /* bumped by every change of par_mat, par_periodic, element scales */
 
+    /* assembly graphs of the device Newton solve (igab_newton.cu), re-captured when
+     * sched_version changes */
+    struct igab_nl_graphs *nlg = nullptr;
+    long sched_version = 0;            /* bumped by every change of a kernel parameter (par_mat, par_periodic,
+                                          Dirichlet rows, element scales) or of the schedule (tiles, kernels) */
+
     /* captured assembly graph */
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -166,6 +172,7 @@ int igab_krylov_solve(igab_ctx *c, const void *dvals, int prec, const double *db
                       double atol, int maxit, int *iterations, int *converged, double *rnorm, double *bnorm);
 void igab_krylov_release(igab_ctx *c);
 void igab_newton_release(igab_ctx *c);   /* igab_newton.cu */
+int igab_check_status(igab_ctx *c);      /* after a synchronisation: a bounded wait that gave up -> error */
 /* igab_mg.cu: multigrid-preconditioned CG (breakdown: p.Kp <= 0) or GMRES on the context's tangent */
 int igab_mg_solve(igab_ctx *c, int method, const void *vals, int prec, const double *b, double *x, double rtol,
                   double atol, int maxit, int *iterations, int *converged, double *rnorm, double *bnorm, int *breakdown);

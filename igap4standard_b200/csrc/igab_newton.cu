@@ -24,6 +24,12 @@
  * two-pass reduction (per-block partial sums over a fixed grid, then one block),
  * so a solve is bitwise repeatable.  The host holds only the scalars of the
  * line search and the convergence tests.
+ *
+ * With opts.use_graph each assembly (the residual at the iterate, the residual at
+ * the line-search point, the tangent at the iterate) is replayed from a CUDA graph
+ * kept on the context: captured on first use (that call runs eagerly once, then is
+ * captured), replayed while its pointers, kind and the context's schedule version
+ * are unchanged, so a sequence of solves (time steps) captures each once.
  */
 #include <chrono>
 #include <cmath>
@@ -53,8 +59,26 @@ __global__ void k_nl_scale(long n, double *__restrict__ Y, double s)
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) Y[i] *= s;
 }
 
+/* one captured assembly of the Newton loop */
+struct nl_graph {
+    cudaGraphExec_t exec = nullptr;
+    const void *in = nullptr, *out = nullptr;
+    int kind = 0;           /* -1 residual, else the tangent precision */
+    long version = -1;      /* igab_ctx::sched_version at capture */
+    int launches = 0;       /* kernels in the graph */
+};
+
+} /* namespace */
+
+struct igab_nl_graphs {
+    nl_graph slot[3];       /* residual at the iterate, residual at the trial point, tangent at the iterate */
+};
+
+namespace {
+
 struct nl_work {
     igab_ctx *c;
+    bool use_graph;
     long n;
     double *F, *G, *Y, *JY, *W;   /* residual at X, at the trial point, step, J Y, trial point */
     double *part, *dots;          /* reduction scratch (device) */
@@ -96,12 +120,72 @@ struct nl_counters {
     double ms_res = 0.0, ms_tan = 0.0, ms_ksp = 0.0;
 };
 
-/* F = R(X) and ||F|| */
-int eval_residual(nl_work &w, const double *X, double *F, double *fnorm, nl_counters &k)
+int launch_assembly(igab_ctx *c, int kind, const double *in, void *out)
+{
+    return kind < 0 ? igab_launch_residual(c, in, (double *)out) : igab_launch_tangent(c, in, out, kind);
+}
+
+/* one assembly (kind -1: the residual, else the tangent in that precision) of `in` into
+ * `out`: replayed from the graph of `slot` when that was captured for the same pointers,
+ * kind and schedule version, else run eagerly (this call's result; it also sets the
+ * kernel attributes outside the capture) and captured for the next calls */
+int nl_assemble(nl_work &w, int slot, int kind, const double *in, void *out)
+{
+    igab_ctx *c = w.c;
+    if (!w.use_graph) {
+        const int rc = launch_assembly(c, kind, in, out);
+        w.launches += c->last_launches;
+        return rc;
+    }
+    if (!c->nlg) c->nlg = new igab_nl_graphs();
+    nl_graph &G = c->nlg->slot[slot];
+    if (G.exec && G.in == in && G.out == out && G.kind == kind && G.version == c->sched_version) {
+        IGAB_CUDA_TRY(cudaGraphLaunch(G.exec, c->stream));
+        w.launches += G.launches;
+        return 0;
+    }
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    G = nl_graph();
+    /* a graph always runs the Neumann kernel: zero values that the last upload skipped */
+    if (!c->neumann_nonzero && c->d_hval)
+        IGAB_CUDA_TRY(cudaMemsetAsync(c->d_hval, 0, (size_t)c->n_neu_points * sizeof(double), c->stream));
+    const bool prof = c->profiling;
+    c->profiling = false;
+    c->force_neumann = true;
+    int rc = launch_assembly(c, kind, in, out);
+    w.launches += c->last_launches;
+    if (!rc) {
+        cudaGraph_t gr = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            rc = launch_assembly(c, kind, in, out);
+            const int n = c->last_launches;
+            e = cudaStreamEndCapture(c->stream, &gr);
+            if (!rc && e == cudaSuccess) e = cudaGraphInstantiate(&G.exec, gr, 0);
+            if (gr) cudaGraphDestroy(gr);
+            if (!rc && e == cudaSuccess) {
+                G.in = in;
+                G.out = out;
+                G.kind = kind;
+                G.version = c->sched_version;
+                G.launches = n;
+            }
+        }
+        if (!rc && e != cudaSuccess) {
+            igab_set_error("igab_newton_solve: assembly graph: %s", cudaGetErrorString(e));
+            rc = IGAB_ERR_CUDA;
+        }
+    }
+    c->profiling = prof;
+    c->force_neumann = false;
+    return rc;
+}
+
+/* F = R(X) and ||F|| (slot 0: F at the iterate, 1: G at the trial point) */
+int eval_residual(nl_work &w, int slot, const double *X, double *F, double *fnorm, nl_counters &k)
 {
     const auto t0 = clk::now();
-    int rc = igab_launch_residual(w.c, X, F);
-    w.launches += w.c->last_launches;
+    int rc = nl_assemble(w, slot, -1, X, F);
     if (!rc) rc = w.norm(F, fnorm);
     k.nres++;
     k.ms_res += ms_since(t0);
@@ -131,7 +215,7 @@ int line_search(nl_work &w, const double *X, double fnorm, double &gnorm, double
     auto accept = [&](double gn, double l) { return std::isfinite(gn) && 0.5 * gn * gn <= 0.5 * f2 + l * alpha * initslope; };
     lam = 1.0;
     w.step(X, lam, w.W);
-    if ((rc = eval_residual(w, w.W, w.G, &gnorm, k))) return rc;
+    if ((rc = eval_residual(w, 1, w.W, w.G, &gnorm, k))) return rc;
     if (!std::isfinite(gnorm)) {
         ok = false;
         return 0;
@@ -146,7 +230,7 @@ int line_search(nl_work &w, const double *X, double fnorm, double &gnorm, double
     lam = lamtemp <= 0.1 * lam ? 0.1 * lam : lamtemp;
     w.step(X, lam, w.W);
     double gprev = gnorm, lamprev = 1.0;
-    if ((rc = eval_residual(w, w.W, w.G, &gnorm, k))) return rc;
+    if ((rc = eval_residual(w, 1, w.W, w.G, &gnorm, k))) return rc;
     if (accept(gnorm, lam)) {
         ok = true;
         return 0;
@@ -165,7 +249,7 @@ int line_search(nl_work &w, const double *X, double fnorm, double &gnorm, double
         lamtemp = std::min(lamtemp, 0.5 * lam);
         lam = lamtemp <= 0.1 * lam ? 0.1 * lam : lamtemp;
         w.step(X, lam, w.W);
-        if ((rc = eval_residual(w, w.W, w.G, &gnorm, k))) return rc;
+        if ((rc = eval_residual(w, 1, w.W, w.G, &gnorm, k))) return rc;
         if (accept(gnorm, lam)) {
             ok = true;
             return 0;
@@ -179,6 +263,12 @@ int line_search(nl_work &w, const double *X, double fnorm, double &gnorm, double
 
 void igab_newton_release(igab_ctx *c)
 {
+    if (c->nlg) {
+        for (nl_graph &G : c->nlg->slot)
+            if (G.exec) cudaGraphExecDestroy(G.exec);
+        delete c->nlg;
+        c->nlg = nullptr;
+    }
     cudaFree(c->d_nl);
     cudaFree(c->d_nl_vals);
     cudaFreeHost(c->h_nl);
@@ -202,6 +292,7 @@ extern "C" void igab_newton_defaults(igab_newton_opts *o)
     o->ksp = IGAB_KSP_MG_GMRES;
     o->verbose = 0;
     o->fp64_polish = 0;
+    o->use_graph = 1;
 }
 
 extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton_opts *opts, igab_newton_info *info,
@@ -241,6 +332,7 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
     }
     nl_work w;
     w.c = ctx;
+    w.use_graph = opts->use_graph != 0;
     w.n = n;
     w.F = ctx->d_nl;
     w.G = w.F + n;
@@ -261,7 +353,7 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
     for (int sub = 0; sub < opts->max_subiter; sub++) {
         /* one SNESSolve with max_it = 1 */
         int kits = 0;
-        if ((rc = eval_residual(w, X, w.F, &fnorm, k))) return rc;
+        if ((rc = eval_residual(w, 0, X, w.F, &fnorm, k))) return rc;
         const double fprev = fnorm;
         if (!std::isfinite(fnorm)) {
             reason = IGAB_SNES_DIVERGED_FNORM_NAN;
@@ -270,14 +362,14 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
         } else {
             const double ttol = fnorm * opts->rtol;
             auto t0 = clk::now();
-            rc = igab_launch_tangent(ctx, X, w.vals, w.prec);
-            w.launches += ctx->last_launches;
+            rc = nl_assemble(w, 2, w.prec, X, w.vals);
             if (!rc) {
                 cudaError_t e = cudaStreamSynchronize(ctx->stream);
                 if (e != cudaSuccess) {
                     igab_set_error("igab_newton_solve: tangent: %s", cudaGetErrorString(e));
                     return IGAB_ERR_CUDA;
                 }
+                rc = igab_check_status(ctx);
             }
             if (rc) return rc;
             k.ntan++;
@@ -312,9 +404,6 @@ extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton
             if ((rc = line_search(w, X, fnorm, gnorm, lam, ok, k))) return rc;
             /* the accepted (or last tried) point becomes the iterate, as in SNESNEWTONLS */
             IGAB_CUDA_TRY(cudaMemcpyAsync(X, w.W, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-            double *t = w.F;
-            w.F = w.G;
-            w.G = t;
             fnorm = gnorm;
             its++;
             double yn = 0.0;

@@ -46,7 +46,7 @@ class IgabNewtonOpts(ctypes.Structure):
     _fields_ = [("prec", ctypes.c_int), ("abstol", ctypes.c_double), ("rtol", ctypes.c_double),
                 ("stol", ctypes.c_double), ("stagnation", ctypes.c_double), ("max_subiter", ctypes.c_int),
                 ("ksp_rtol", ctypes.c_double), ("ksp_maxit", ctypes.c_int), ("ksp", ctypes.c_int),
-                ("verbose", ctypes.c_int), ("fp64_polish", ctypes.c_int)]
+                ("verbose", ctypes.c_int), ("fp64_polish", ctypes.c_int), ("use_graph", ctypes.c_int)]
 
 
 class IgabNewtonInfo(ctypes.Structure):
@@ -56,6 +56,28 @@ class IgabNewtonInfo(ctypes.Structure):
                 ("krylov_iterations", ctypes.c_long),
                 ("fnorm", ctypes.c_double), ("ms_residual", ctypes.c_double), ("ms_tangent", ctypes.c_double),
                 ("ms_krylov", ctypes.c_double), ("ms_total", ctypes.c_double), ("launches", ctypes.c_long)]
+
+
+class IgabTransientOpts(ctypes.Structure):
+    """igab_transient_opts of include/igab.h"""
+    _fields_ = [("nsteps", ctypes.c_int), ("dt", ctypes.c_double), ("amplitude", ctypes.c_double),
+                ("face", ctypes.c_int), ("order", ctypes.c_int), ("dof", ctypes.c_int),
+                ("newton", IgabNewtonOpts)]
+
+
+class IgabTransientInfo(ctypes.Structure):
+    """igab_transient_info of include/igab.h"""
+    _fields_ = [("steps", ctypes.c_int), ("steps_converged", ctypes.c_int), ("newton_iterations", ctypes.c_long),
+                ("krylov_iterations", ctypes.c_long), ("n_residual", ctypes.c_long), ("n_tangent", ctypes.c_long),
+                ("ms_total", ctypes.c_double), ("launches", ctypes.c_long)]
+
+
+class IgabTadjInfo(ctypes.Structure):
+    """igab_tadj_info_t of include/igab.h"""
+    _fields_ = [("forward_steps", ctypes.c_int), ("recomputed_steps", ctypes.c_int), ("checkpoints", ctypes.c_int),
+                ("forward_converged", ctypes.c_int), ("krylov_iterations_backward", ctypes.c_long),
+                ("adjoint_solves_converged", ctypes.c_int), ("adjoint_solves", ctypes.c_int),
+                ("ms_forward", ctypes.c_double), ("ms_backward", ctypes.c_double)]
 
 
 class IgabBatchTuneResult(ctypes.Structure):
@@ -116,6 +138,13 @@ IGAB_API = [
     ("igab_upload", ctypes.c_int, [vp, vp, vp, ctypes.c_long]),
     ("igab_download", ctypes.c_int, [vp, vp, vp, ctypes.c_long]),
     ("igab_newton_solve", ctypes.c_int, [vp, vp, vp, vp, vp, vp, ctypes.c_int]),
+    ("igab_transient_defaults", None, [vp]),
+    ("igab_transient_run", ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp]),
+    ("igab_tadj_create", ctypes.c_int, [vp, vp, ctypes.c_int, vp]),
+    ("igab_tadj_forward", ctypes.c_int, [vp, vp, vp, vp]),
+    ("igab_tadj_backward", ctypes.c_int, [vp, vp, vp]),
+    ("igab_tadj_info", ctypes.c_int, [vp, vp]),
+    ("igab_tadj_destroy", None, [vp]),
     ("igab_set_option", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
     ("igab_graph_capture", ctypes.c_int, [vp, vp, vp, vp, ctypes.c_int, ctypes.c_int]),
     ("igab_graph_launch", ctypes.c_int, [vp]),

@@ -74,6 +74,9 @@ long igab_csr_offset(const igab_ctx *ctx, long row, long col);
 int igab_set_par_mat(igab_ctx *ctx, const double par_mat[9]);
 int igab_set_par_dirichlet(igab_ctx *ctx, const double par_dirichlet[9]);
 int igab_set_par_periodic(igab_ctx *ctx, const double par_periodic[9]);
+/* the Dirichlet rows (dofs whose residual row is U - g, src/iga_dirichlet.c), ascending:
+ * n receives the count, rows (NULL or n ints) the dofs */
+int igab_dirichlet_rows(igab_ctx *ctx, long *n, int *rows);
 
 /* ---- Neumann data: the caller evaluates its traction at the surface Gauss
  * points and hands the values over.  n_points = total point count; xyz
@@ -294,8 +297,11 @@ int igab_mg_prolongation_1d(const double *coarse_knots, int n_coarse_elements, c
  * iterations", or until ||F|| stagnates (|F_old - F_new| / F_old < stagnation, F_old =
  * 999 at the start; reported as DIVERGED_LINE_SEARCH, as the reference does).  The linear
  * solve of each step (stand-in for PETSc's GMRES + ASM) runs to ksp_rtol on the tangent
- * assembled in opts.prec: opts.ksp selects multigrid CG (igab_solve_mg_device) or the
- * Jacobi BiCGStab of igab_solve_device; no residual or tangent leaves the GPU.  U_dev holds the initial guess and receives the solution; the context's
+ * assembled in opts.prec: opts.ksp selects multigrid GMRES or CG (igab_solve_mg_device) or
+ * the Jacobi BiCGStab of igab_solve_device; no residual or tangent leaves the GPU.  With
+ * opts.use_graph each assembly is replayed from a CUDA graph held by the context (captured
+ * on first use, re-captured when a pointer, the precision or a parameter or schedule
+ * setting changes).  U_dev holds the initial guess and receives the solution; the context's
  * Neumann values and history levels are used as set.  fnorm_history / krylov_history
  * (either may be NULL) receive ||F|| and the Krylov iteration count of the first
  * history_cap subiterations.  verbose = 1 prints the reference's line per subiteration. */
@@ -320,6 +326,7 @@ typedef struct {
     int verbose;           /* 0 */
     int fp64_polish;       /* 0; with prec FP32: once a step reduces ||F|| by less than 10x (the FP32
                               tangent's error limits the step), the remaining steps use the FP64 tangent */
+    int use_graph;         /* 1: residual and tangent assemblies replayed from CUDA graphs */
 } igab_newton_opts;
 typedef struct {
     int iterations;          /* Newton steps taken */
@@ -335,6 +342,67 @@ typedef struct {
 void igab_newton_defaults(igab_newton_opts *opts);
 int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton_opts *opts, igab_newton_info *info,
                       double *fnorm_history, int *krylov_history, int history_cap);
+
+/* ---- time stepping of the transient physics on the device (replaces the application's
+ * step of example/ex1/main.c:48-56 -- initial guess U = U_hist[1], snes_solve, history
+ * shift U_hist[2] <- U_hist[1] <- U -- repeated nsteps times).  Step n (0-based) solves at
+ * t = (n + 1) dt, with the traction amplitude * sin(2 pi t) on the Neumann points of the
+ * (face, order, dof) combination given and zero on the other combinations of the BC table,
+ * by igab_newton_solve with opts.newton.  U_dev: U at t_0 on entry (history level 1), U at
+ * t_nsteps on return; U_prev_dev: U at t_-1 (history level 2; NULL = zero).  dt = 0 takes
+ * the physics' own time step (par_mat[7]).  The history shifts after every step; a step
+ * whose Newton solve ends without convergence is counted in info (steps_converged).  On
+ * return the context's history levels hold U at t_nsteps - 1 and t_nsteps - 2.  Optional
+ * outputs: U_steps_host (nsteps x ndof: the state after every step) and step_info
+ * (nsteps entries). */
+typedef struct {
+    int nsteps;
+    double dt;
+    double amplitude;      /* 0.01 */
+    int face, order, dof;  /* 1, 0, 0: x-traction on x = 1 */
+    igab_newton_opts newton;
+} igab_transient_opts;
+typedef struct {
+    int steps;               /* steps run */
+    int steps_converged;
+    long newton_iterations, krylov_iterations;
+    long n_residual, n_tangent;
+    double ms_total;         /* wall time of the whole run */
+    long launches;
+} igab_transient_info;
+void igab_transient_defaults(igab_transient_opts *opts);
+int igab_transient_run(igab_ctx *ctx, const igab_transient_opts *opts, double *U_dev, const double *U_prev_dev,
+                       double *U_steps_host, igab_newton_info *step_info, igab_transient_info *info);
+
+/* ---- discrete adjoint of the time stepping (no reference counterpart), for the element
+ * log-scales g of igab_set_element_log_scale (set by the caller; the scales in force are
+ * used).  Steps n = 0 .. N-1 solve R_n(U_{n+1}; U_n, U_{n-1}, g) = 0 as igab_transient_run
+ * does.  For an objective J(U_N):
+ *   K_n^T lam_n = b_n,  b_n = dJ/dU_{n+1} - J1_{n+1}^T lam_{n+1} - J0_{n+2}^T lam_{n+2},
+ *   dJ/dg = - sum_n lam_n . dR_n/dg,
+ * K_n the FP64 tangent at U_{n+1}, J1 / J0 the history Jacobians (levels 1 and 2), b and
+ * lam zero on the Dirichlet rows, each K^T lam = b (K symmetric) solved by the Jacobi
+ * BiCGStab to opts.newton.ksp_rtol.  The forward pass keeps the states at checkpoints
+ * every `every` steps (two states each); the backward pass recomputes each segment from
+ * its checkpoint (the same solves, so the same states bit for bit) before sweeping it:
+ * device memory O(N / every + every) states plus two FP64 value arrays.
+ * igab_tadj_create: the pass's buffers.  igab_tadj_forward: the N steps from U_init_dev
+ * (U at t_0) and U_prev_dev (U at t_-1; NULL = zero), U_N into U_final_dev.
+ * igab_tadj_backward: dJ/dg into grad_dev (nel doubles, device) from dJ/dU_N (device),
+ * after a forward pass.  igab_tadj_info: counts of the last passes. */
+typedef struct igab_tadj igab_tadj;
+typedef struct {
+    int forward_steps, recomputed_steps, checkpoints;
+    int forward_converged;            /* forward steps whose Newton solve converged */
+    long krylov_iterations_backward;  /* over the adjoint solves */
+    int adjoint_solves_converged, adjoint_solves;
+    double ms_forward, ms_backward;
+} igab_tadj_info_t;
+int igab_tadj_create(igab_ctx *ctx, const igab_transient_opts *opts, int every, igab_tadj **out);
+int igab_tadj_forward(igab_tadj *t, const double *U_init_dev, const double *U_prev_dev, double *U_final_dev);
+int igab_tadj_backward(igab_tadj *t, const double *dJdU_dev, double *grad_dev);
+int igab_tadj_info(const igab_tadj *t, igab_tadj_info_t *info);
+void igab_tadj_destroy(igab_tadj *t);
 
 /* ---- mesh refinement and solution files (mesh/nurbs/nurbs_knotinsert.c:7, src/ioutil.c:89, :126).
  * igab_knot_insert: refine the p = 2 control points of a field, in place in host memory

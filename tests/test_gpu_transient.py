@@ -1,7 +1,7 @@
-"""Transient driver (phys/getime, CUDA-graph replay per Newton iteration) against
-the reference's own transient callbacks driven by the same solver semantics on
-the CPU (direct solve): per-step displacements, Newton iteration counts and the
-mixed-precision variant."""
+"""Transient driver (igab_transient_run: phys/getime on the device, CUDA-graph replay of
+every assembly) against the reference's own transient callbacks driven by the same solver
+semantics on the CPU (direct solve): per-step displacements, Newton iteration counts and
+the mixed-precision variant."""
 import numpy as np
 import pytest
 
@@ -59,9 +59,11 @@ def test_transient_fp64_matches_reference(transient_case):
     from igap4standard_b200 import transient
     c, dt, ref_hist, ref_its = transient_case
     A = _assembly(c)
-    hist, res, P = transient.run(A, NSTEPS, dt, prec="fp64", use_graph=True, rtol_lin=1e-13)
+    hist, res, tot = transient.run(A, NSTEPS, dt, prec="fp64", use_graph=True, rtol_lin=1e-13)
     its = [r.iterations for r in res]
-    print("reference iterations", ref_its, "gpu", its, "krylov", P.krylov_its)
+    print("reference iterations", ref_its, "gpu", its, "krylov", tot["krylov_per_step"])
+    assert tot["steps"] == NSTEPS and tot["steps_converged"] == NSTEPS
+    assert np.array_equal(tot["U_final"], hist[-1])
     assert all(r.converged for r in res)
     assert its == ref_its
     assert np.abs(ref_hist[-1]).max() > 0.0        # the traction moved the body

@@ -92,22 +92,22 @@ def test_transient_adjoint_matches_central_differences(built):
     Ustar = np.random.default_rng(21).uniform(-1e-3, 1e-3, n)
     g0 = np.random.default_rng(5).normal(0.0, 0.3, ne)
 
-    def traction(A_, t):
-        return transient.traction_values(A_, t, amplitude=AMP)
-
     def J(U):
         return 0.5 * np.sum(mask * (U - Ustar) ** 2)
 
     out = transient.adjoint(A, NSTEPS, DT, g0, lambda U: mask * (U - Ustar), every=EVERY, rtol_lin=1e-13,
-                            traction=traction, abs_tol=1e-14, objective=J)
+                            amplitude=AMP, abs_tol=1e-14, objective=J)
     assert out["checkpoints"] == [0, 2, 4] and out["recomputed_steps"] == NSTEPS
+    info = out["info"]
+    assert info["forward_converged"] == NSTEPS and info["adjoint_solves"] == NSTEPS
+    assert info["adjoint_solves_converged"] == NSTEPS
     assert np.abs(out["U_N"]).max() > 1e-4            # the traction moved the body
     grad = out["grad"]
 
     def J_of(g):
         A.set_element_log_scale(g)
         hist, res, _ = transient.run(A, NSTEPS, DT, prec="fp64", use_graph=False, rtol_lin=1e-13,
-                                     traction=traction, abs_tol=1e-14)
+                                     amplitude=AMP, abs_tol=1e-14)
         A.set_element_log_scale(None)
         return J(hist[-1])
 

@@ -14,9 +14,23 @@ BiCGStab of igab_solve_device as the stand-in for PETSc's GMRES + ASM
 The traction of the transient workload is amplitude * sin(2 pi t) on face x = 1 in the x
 direction (face 1, standard order, dof 0), evaluated at t_{n+1}.
 """
+from dataclasses import dataclass, field
+
 import numpy as np
 
-from . import newton
+ABS_TOL = 1e-10   # SNESSetTolerances abstol, src/snes_init.c:18
+
+
+@dataclass
+class StepResult:
+    """The Newton solve of one time step (igab_newton_info of the step)."""
+    U: object
+    converged: bool
+    reason: int
+    iterations: int
+    fnorms: list = field(default_factory=list)   # ||F|| at the end of the step's solve
+    n_residual: int = 0
+    n_tangent: int = 0
 
 
 def _device_vector(A, x):
@@ -28,11 +42,11 @@ def _device_vector(A, x):
 
 
 def run(A, nsteps, dt, prec="fp32", use_graph=True, rtol_lin=1e-5, amplitude=0.01, U_init=None, U_prev=None,
-        abs_tol=newton.ABS_TOL, keep_steps=True):
+        abs_tol=ABS_TOL, keep_steps=True):
     """Time-step A (an Assembly with phys="getime") nsteps times from the history (U_init
     at t_0, U_prev at t_{-1}; zeros by default) with the time step dt.  Returns (the state
     after every step as host arrays (empty when keep_steps is False), per-step
-    NewtonResults, the run's totals)."""
+    StepResults, the run's totals)."""
     import torch
     U = _device_vector(A, U_init)
     Up = _device_vector(A, U_prev) if U_prev is not None else None
@@ -41,9 +55,9 @@ def run(A, nsteps, dt, prec="fp32", use_graph=True, rtol_lin=1e-5, amplitude=0.0
                                        dt=dt, amplitude=amplitude, ksp_rtol=rtol_lin, abstol=abs_tol,
                                        use_graph=use_graph, keep_steps=keep_steps)
     states = list(hist) if keep_steps else []
-    results = [newton.NewtonResult(U=states[i] if keep_steps else None, converged=bool(s["converged"]),
-                                   reason=int(s["reason"]), iterations=int(s["iterations"]), fnorms=[s["fnorm"]],
-                                   n_residual=int(s["n_residual"]), n_tangent=int(s["n_tangent"]))
+    results = [StepResult(U=states[i] if keep_steps else None, converged=bool(s["converged"]), reason=int(s["reason"]),
+                          iterations=int(s["iterations"]), fnorms=[s["fnorm"]], n_residual=int(s["n_residual"]),
+                          n_tangent=int(s["n_tangent"]))
                for i, s in enumerate(steps)]
     tot["krylov_per_step"] = [int(s["krylov_iterations"]) for s in steps]
     tot["U_final"] = U.cpu().numpy()

@@ -1,4 +1,6 @@
-"""Newton driver with the reference application's solver semantics.
+"""Newton driver with the reference application's solver semantics -- test
+infrastructure: the parity tests run the reference's CPU assembly and the GPU
+assembly through this same host loop; nothing in the product imports it.
 
 IGAP4STANDARD solves R(U) = 0 with PETSc SNES configured in src/snes_init.c:
 NEWTONLS (:19), backtracking line search of cubic order (:21-22), absolute

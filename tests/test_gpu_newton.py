@@ -30,7 +30,7 @@ def _assembly(c):
 
 
 def _ref_problem(checker, c):
-    from igap4standard_b200 import newton
+    from oracle import newton_loop as newton
     case = checker("ge", c["nelem"], c["knots"], c["par_mat"], c["bc_type"], c["par_periodic"],
                    c["par_dirichlet"], c["par_neumann"])
     return newton.case_problem(case), case.ndof
@@ -38,7 +38,7 @@ def _ref_problem(checker, c):
 
 @pytest.mark.parametrize("name", ["perturbed_lame", "ragged_config0", "newton_backtrack", "config0_8"])
 def test_newton_parity(built, checker, name):
-    from igap4standard_b200 import newton
+    from oracle import newton_loop as newton
     c = make_case(name)
     (r_ref, j_ref), n = _ref_problem(checker, c)
     ref = newton.solve(r_ref, j_ref, np.zeros(n))
@@ -55,7 +55,7 @@ def test_newton_parity(built, checker, name):
 
 @pytest.mark.parametrize("name", ["perturbed_lame", "config0_8", "newton_backtrack"])
 def test_mixed_precision_newton(built, name):
-    from igap4standard_b200 import newton
+    from oracle import newton_loop as newton
     c = make_case(name)
     A = _assembly(c)
     n = A.ndof

@@ -19,7 +19,7 @@ def _pn(t):
 
 
 def _reference_run(oracle_lib, c, dt, nsteps):
-    from igap4standard_b200 import newton
+    from oracle import newton_loop as newton
     args = ("getime", c["nelem"], c["knots"], c["par_mat"], c["bc_type"], c["par_periodic"], c["par_dirichlet"],
             _pn(dt))
     ref = oracle_lib.case(*args)

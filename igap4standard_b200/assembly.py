@@ -9,6 +9,7 @@ PHYS = {"ge": 0, "getime": 1}
 PREC = {"fp64": 0, "fp32": 1}
 OPT_TANGENT_FP64_KERNEL = 1
 OPT_TANGENT_FP32_KERNEL = 2
+OPT_COLOUR_ORDER = 3
 
 
 def _ptr(a):
@@ -163,7 +164,8 @@ class Assembly:
     def autotune(self, U_ptr=None, what=7, reps=3, cache=None):
         """Time every candidate schedule (igab_autotune) and keep the fastest; with a
         cache file, a schedule stored for this GPU and mesh is applied without timing.
-        Returns dict(residual_tile, tangent_fp64_kernel, tangent_fp32_kernel, *_ms, cached)."""
+        what: bit 0 residual tile, bit 1 / 2 FP64 / FP32 tangent kernel, bit 3 colour order.
+        Returns dict(residual_tile, tangent_fp64_kernel, tangent_fp32_kernel, *_ms, colour_order, cached)."""
         from . import tuning
         key = tuning.mesh_key(self.device, self.nelem, self.phys, what) if cache else None
         hit = tuning.load(cache).get(key) if cache else None
@@ -171,6 +173,7 @@ class Assembly:
             self.set_tile(hit["residual_tile"], 0)
             self.set_option(OPT_TANGENT_FP64_KERNEL, hit["tangent_fp64_kernel"])
             self.set_option(OPT_TANGENT_FP32_KERNEL, hit["tangent_fp32_kernel"])
+            self.set_option(OPT_COLOUR_ORDER, hit.get("colour_order", 0))
             return dict(hit, cached=True)
         r = native.IgabTuneResult()
         check(self.lib, "igab_autotune",
@@ -424,6 +427,14 @@ def tc_peak_tflops(n_cols=256, device=0):
     lib = native.lib_cuda()
     t = ctypes.c_double()
     check(lib, "igab_tc_peak", lib.igab_tc_peak(int(device), int(n_cols), ctypes.byref(t)))
+    return t.value
+
+
+def dmma_peak_tflops(device=0):
+    """FP64 tensor-pipe (mma.sync m8n8k4 f64) throughput of the device, TFLOP/s."""
+    lib = native.lib_cuda()
+    t = ctypes.c_double()
+    check(lib, "igab_dmma_peak", lib.igab_dmma_peak(int(device), ctypes.byref(t)))
     return t.value
 
 

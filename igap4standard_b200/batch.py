@@ -80,6 +80,14 @@ class Batch:
         check(self.lib, "igab_batch_get_schedule", self.lib.igab_batch_get_schedule(self.h, *[ctypes.byref(x) for x in v]))
         return tuple(x.value for x in v)
 
+    def set_colour_order(self, order):
+        check(self.lib, "igab_batch_set_colour_order", self.lib.igab_batch_set_colour_order(self.h, int(order)))
+
+    def get_colour_order(self):
+        v = ctypes.c_int()
+        check(self.lib, "igab_batch_get_colour_order", self.lib.igab_batch_get_colour_order(self.h, ctypes.byref(v)))
+        return v.value
+
     def autotune(self, U_ptr=None, what=7, reps=2, cache=None):
         """Time the candidate batch schedules (igab_batch_autotune) and keep the fastest;
         with a cache file, a schedule stored for this GPU and batch shape is applied."""
@@ -88,6 +96,7 @@ class Batch:
         hit = tuning.load(cache).get(key) if cache else None
         if hit:
             self.set_schedule(hit["ctas_res"], hit["ctas_tan64"], hit["ctas_tan32"], hit["order"])
+            self.set_colour_order(hit.get("colour_order", 0))
             return dict(hit, cached=True)
         r = native.IgabBatchTuneResult()
         check(self.lib, "igab_batch_autotune",

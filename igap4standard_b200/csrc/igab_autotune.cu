@@ -5,14 +5,18 @@
  * kept and left applied.
  *
  * Single mesh (igab_autotune):
- *   residual       elements per tile edge of the 8-colour schedule: 2 or 4
+ *   residual       elements per block: tile edge 2 or 4 of the 8-colour schedule
  *   FP64 tangent   FP64 tensor path (mma f64) or FP64 FMA pipe
  *   FP32 tangent   tcgen05 tensor cores (TF32 hi/lo) or FP32 FMA pipe
+ *   colour order   natural, mirrored or Gray (igab_colour_at), on the sum of the
+ *                  kernels chosen above
  * Batch (igab_batch_autotune):
- *   CTAs per SM of each persistent kernel (1 or as many as fit) and the
- *   instance order of the colour-major work list (natural or largest first).
- * All candidates give the same result up to the kernel's own arithmetic (tile
- * size and instance order do not change any per-entry summation order).
+ *   CTAs per SM of the persistent residual and FP64 tangent kernels (1 or as many
+ *   as fit; the FP32 kernel runs one CTA per work item), the instance
+ *   order of the colour-major work list (natural or largest first) and the
+ *   colour order.
+ * Tile size, CTA count and instance order leave every per-entry summation order
+ * as it is; the kernel variant and the colour order change results by rounding.
  */
 #include <algorithm>
 #include <vector>
@@ -58,7 +62,7 @@ struct dev_buf {
 
 extern "C" int igab_autotune(igab_ctx *ctx, const double *U_dev, int what, int reps, igab_tune_result *out)
 {
-    if (!ctx || !out || reps < 1 || (what & ~7)) {
+    if (!ctx || !out || reps < 1 || (what & ~15)) {
         igab_set_error("igab_autotune: bad argument");
         return IGAB_ERR_ARG;
     }
@@ -70,13 +74,14 @@ extern "C" int igab_autotune(igab_ctx *ctx, const double *U_dev, int what, int r
         U_dev = (const double *)U0.p;
     }
     IGAB_CUDA_TRY(cudaMalloc(&R.p, (size_t)ctx->ndof * sizeof(double)));
-    if (what & 6) IGAB_CUDA_TRY(cudaMalloc(&V.p, (size_t)ctx->nnz * sizeof(double)));
+    if (what & 14) IGAB_CUDA_TRY(cudaMalloc(&V.p, (size_t)ctx->nnz * sizeof(double)));
     const bool prof = ctx->profiling;
     ctx->profiling = false;
     int rc = 0;
     out->residual_tile = ctx->tile_res;
     out->tangent_fp64_kernel = ctx->tan_kernel;
     out->tangent_fp32_kernel = ctx->tan32_kernel;
+    out->colour_order = ctx->colour_order;
     out->residual_ms = out->tangent_fp64_ms = out->tangent_fp32_ms = -1.0;
     if (what & 1) {
         double best = 1e300;
@@ -107,6 +112,29 @@ extern "C" int igab_autotune(igab_ctx *ctx, const double *U_dev, int what, int r
         knob = pick;
         tms = best;
     }
+    if ((what & 8) && !rc) {
+        /* colour order: the kernels chosen above (all three when none was tuned), summed */
+        const int kern = (what & 7) ? (what & 7) : 7;
+        double best = 1e300;
+        for (int order = 0; order < 3 && !rc; order++) {
+            ctx->colour_order = order;
+            double total = 0.0;
+            for (int k = 0; k < 3 && !rc; k++) {
+                if (!(kern & (1 << k))) continue;
+                double t = 0.0;
+                if (k == 0)
+                    rc = time_ms(ctx->stream, reps, [&] { return igab_launch_residual(ctx, U_dev, (double *)R.p); }, &t);
+                else
+                    rc = time_ms(ctx->stream, reps, [&] { return igab_launch_tangent(ctx, U_dev, V.p, k - 1); }, &t);
+                total += t;
+            }
+            if (!rc && total < best) {
+                best = total;
+                out->colour_order = order;
+            }
+        }
+        ctx->colour_order = out->colour_order;
+    }
     ctx->profiling = prof;
     ctx->sched_version++;
     IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -117,7 +145,7 @@ extern "C" int igab_autotune(igab_ctx *ctx, const double *U_dev, int what, int r
 
 extern "C" int igab_batch_autotune(igab_batch *b, const double *U_dev, int what, int reps, igab_batch_tune_result *out)
 {
-    if (!b || !out || reps < 1 || (what & ~7)) {
+    if (!b || !out || reps < 1 || (what & ~15)) {
         igab_set_error("igab_batch_autotune: bad argument");
         return IGAB_ERR_ARG;
     }
@@ -134,7 +162,7 @@ extern "C" int igab_batch_autotune(igab_batch *b, const double *U_dev, int what,
         U_dev = (const double *)U0.p;
     }
     IGAB_CUDA_TRY(cudaMalloc(&R.p, (size_t)ndof * sizeof(double)));
-    if (what & 6) IGAB_CUDA_TRY(cudaMalloc(&V.p, (size_t)nnz * sizeof(double)));
+    if (what & 14) IGAB_CUDA_TRY(cudaMalloc(&V.p, (size_t)nnz * sizeof(double)));
     int occ[3] = {0, 0, 0};
     if ((rc = igab_batch_occupancy_res(&occ[0])) || (rc = igab_batch_occupancy_dmma(&occ[1])) ||
         (rc = igab_batch_occupancy_tc32(&occ[2])))
@@ -151,7 +179,8 @@ extern "C" int igab_batch_autotune(igab_batch *b, const double *U_dev, int what,
         for (int k = 0; k < 3 && !rc; k++) {
             if (!(what & (1 << k))) continue;
             std::vector<int> cands = {0};
-            for (int c = 1; c < occ[k]; c++) cands.push_back(c);
+            if (k != 2)   /* the FP32 batch kernel runs one CTA per work item: no CTA count to choose */
+                for (int c = 1; c < occ[k]; c++) cands.push_back(c);
             double bk = 1e300;
             for (int cand : cands) {
                 int sch[3] = {pick[0], pick[1], pick[2]};
@@ -178,6 +207,37 @@ extern "C" int igab_batch_autotune(igab_batch *b, const double *U_dev, int what,
     int rc2 = igab_batch_set_schedule(b, best[0], best[1], best[2], best[3]);
     if (rc) return rc;
     if (rc2) return rc2;
+    int corder = 0;
+    if ((rc = igab_batch_get_colour_order(b, &corder))) return rc;
+    if (what & 8) {
+        /* colour order on the chosen schedule: the selected kernels (all three when none), summed */
+        const int kern = (what & 7) ? (what & 7) : 7;
+        double best_total_c = 1e300;
+        int pick = corder;
+        for (int co = 0; co < 3 && !rc; co++) {
+            if ((rc = igab_batch_set_colour_order(b, co))) break;
+            double total = 0.0;
+            for (int k = 0; k < 3 && !rc; k++) {
+                if (!(kern & (1 << k))) continue;
+                double t = 0.0;
+                auto run = [&]() -> int {
+                    if (k == 0) return igab_batch_residual_device(b, U_dev, (double *)R.p);
+                    return igab_batch_tangent_device(b, U_dev, V.p, k == 1 ? IGAB_PREC_FP64 : IGAB_PREC_FP32);
+                };
+                rc = time_ms(s, reps, run, &t);
+                total += t;
+            }
+            if (!rc && total < best_total_c) {
+                best_total_c = total;
+                pick = co;
+            }
+        }
+        rc2 = igab_batch_set_colour_order(b, pick);
+        if (rc) return rc;
+        if (rc2) return rc2;
+        corder = pick;
+    }
+    out->colour_order = corder;
     out->ctas_res = best[0];
     out->ctas_tan64 = best[1];
     out->ctas_tan32 = best[2];

@@ -48,6 +48,7 @@ struct igab_batch {
     /* schedule: CTAs per SM of the persistent kernels (0 = as many as fit), instance order */
     int ctas[3] = {0, 0, 0};
     int order = 0;
+    int colour_order = 0;   /* igab_colour_order of the work list */
     /* colour-dependency wait: poll limit, and the test switch that makes it run out */
     long spin_limit = IGAB_BATCH_SPIN;
     int hold = 0;
@@ -70,7 +71,7 @@ void free_batch(igab_batch *b)
     delete b;
 }
 
-/* work list in the current order; need[8 i + c] = tiles of colour c of instance i */
+/* work list in the current orders; need[8 i + p] = tiles of instance i at sweep position p */
 int build_items(igab_batch *b)
 {
     std::vector<int> ord(b->n);
@@ -79,13 +80,15 @@ int build_items(igab_batch *b)
         std::stable_sort(ord.begin(), ord.end(), [b](int x, int y) { return b->inst[x]->nel > b->inst[y]->nel; });
     std::vector<int4> items;
     std::vector<int> need(8 * (size_t)b->n, 0);
-    for (int c = 0; c < 8; c++)
+    for (int p = 0; p < 8; p++) {
+        const int c = igab_colour_at(b->colour_order, p);
         for (int i : ord) {
             const igab_geom g = b->inst[i]->geom();
             const long nt = tiles_of_colour(g, 2, c);
-            need[8 * (size_t)i + c] = (int)nt;
-            for (long t = 0; t < nt; t++) items.push_back(make_int4(i, c, (int)t, 0));
+            need[8 * (size_t)i + p] = (int)nt;
+            for (long t = 0; t < nt; t++) items.push_back(make_int4(i, p, (int)t, c));
         }
+    }
     if (b->d_items && (int)items.size() != b->nitems) {
         igab_set_error("internal: batch work list changed size");
         return IGAB_ERR_ARG;
@@ -367,6 +370,26 @@ extern "C" int igab_batch_set_schedule(igab_batch *b, int ctas_res, int ctas_tan
         b->order = order;
         return build_items(b);
     }
+    return 0;
+}
+
+extern "C" int igab_batch_set_colour_order(igab_batch *b, int colour_order)
+{
+    BATCH_CHECK(b, "igab_batch_set_colour_order: null batch");
+    BATCH_CHECK(colour_order >= 0 && colour_order <= 2, "igab_batch_set_colour_order: order must be 0, 1 or 2");
+    IGAB_CUDA_TRY(cudaSetDevice(b->device));
+    IGAB_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    if (colour_order != b->colour_order) {
+        b->colour_order = colour_order;
+        return build_items(b);
+    }
+    return 0;
+}
+
+extern "C" int igab_batch_get_colour_order(const igab_batch *b, int *colour_order)
+{
+    BATCH_CHECK(b && colour_order, "igab_batch_get_colour_order: null argument");
+    *colour_order = b->colour_order;
     return 0;
 }
 

@@ -960,6 +960,13 @@ extern "C" int igab_fma_peak(int device, int prec, double *tflops)
     return igab_launch_fma_peak(prec, tflops);
 }
 
+extern "C" int igab_dmma_peak(int device, double *tflops)
+{
+    ARG_CHECK(tflops, "igab_dmma_peak: null argument");
+    IGAB_CUDA_TRY(cudaSetDevice(device));
+    return igab_launch_dmma_peak(tflops);
+}
+
 extern "C" int igab_set_option(igab_ctx *ctx, int option, int value)
 {
     ARG_CHECK(ctx, "igab_set_option: null context");
@@ -974,6 +981,11 @@ extern "C" int igab_set_option(igab_ctx *ctx, int option, int value)
         ctx->tan32_kernel = value;
         ctx->sched_version++;
         return 0;
+    case IGAB_OPT_COLOUR_ORDER:
+        ARG_CHECK(value >= 0 && value <= 2, "igab_set_option: colour order must be 0, 1 or 2");
+        ctx->colour_order = value;
+        ctx->sched_version++;
+        return 0;
     default:
         igab_set_error("igab_set_option: unknown option %d", option);
         return IGAB_ERR_ARG;
@@ -986,6 +998,7 @@ extern "C" int igab_get_option(const igab_ctx *ctx, int option, int *value)
     switch (option) {
     case IGAB_OPT_TANGENT_FP64_KERNEL: *value = ctx->tan_kernel; return 0;
     case IGAB_OPT_TANGENT_FP32_KERNEL: *value = ctx->tan32_kernel; return 0;
+    case IGAB_OPT_COLOUR_ORDER: *value = ctx->colour_order; return 0;
     default:
         igab_set_error("igab_get_option: unknown option %d", option);
         return IGAB_ERR_ARG;

@@ -109,8 +109,8 @@ __device__ __forceinline__ double elem_scale(const igab_geom &g, int ex, int ey,
 /* ---- persistent batched launches: one work item (a tile of one instance) at a time */
 #define IGAB_BATCH_SPIN (1L << 22)   /* polls (with a 128 ns sleep) before a dependency wait gives up */
 
-/* one thread: wait until every colour before `colour` of instance `inst` is
- * complete.  Each wait polls at most B.spin_limit times (128 ns sleep between
+/* one thread: wait until every sweep position before `colour` (a position in the
+ * batch's colour order) of instance `inst` is complete.  Each wait polls at most B.spin_limit times (128 ns sleep between
  * polls), then sets bit 2 of the status word and moves on; B.hold raises the
  * count that colour 0 of instance 0 must reach, so that the waits on it cannot
  * finish (a host-set test switch that exercises the give-up path). */
@@ -134,6 +134,7 @@ __device__ __forceinline__ void batch_wait_colours(const igab_batch_dev &B, int 
 struct batch_slot {
     igab_geom g;      /* geometry of the current item's instance */
     int item, inst, colour, tile;
+    int pos;          /* position of the colour in the batch's colour order */
 };
 
 /* all threads: fetch the next item, wait until every earlier colour of its
@@ -147,8 +148,9 @@ __device__ __forceinline__ bool batch_next(const igab_batch_dev &B, batch_slot &
         if (it < B.nitems) {
             const int4 w = B.items[it];
             sl.inst = w.x;
-            sl.colour = w.y;
+            sl.pos = w.y;
             sl.tile = w.z;
+            sl.colour = w.w;
             batch_wait_colours(B, w.x, w.y);
             __threadfence();
         }
@@ -167,7 +169,7 @@ __device__ __forceinline__ void batch_done(const igab_batch_dev &B, const batch_
 {
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(&B.done[8 * sl.inst + sl.colour], 1);
+    if (threadIdx.x == 0) atomicAdd(&B.done[8 * sl.inst + sl.pos], 1);
 }
 
 long tiles_of_colour(const igab_geom &g, int TE, int colour)

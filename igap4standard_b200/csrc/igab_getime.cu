@@ -487,7 +487,8 @@ int launch_t(igab_ctx *c, const double *dU, T *dv, int level)
     }
     size_t sm = sizeof(gt_smem<2>);
     IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_getime<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    for (int colour = 0; colour < 8; colour++) {
+    for (int k = 0; k < 8; k++) {
+        const int colour = igab_colour_at(c->colour_order, k);
         long nblk = tiles_of_colour(g, 2, colour);
         if (nblk == 0) continue;
         k_tan_getime<T, 2><<<(unsigned)nblk, 256, sm, c->stream>>>(g, dU, dv, colour);

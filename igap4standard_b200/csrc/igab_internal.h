@@ -42,11 +42,12 @@ struct igab_geom {
 };
 
 /* Batched assembly: the work list of a persistent launch over many meshes.
- * item = (instance, colour, tile, 0), ordered colour-major; done[8 i + c]
- * counts the finished tiles of colour c of instance i, need[8 i + c] how many
- * there are.  A tile of colour c starts once every earlier colour of its
- * instance is complete (bounded wait), so tiles of one instance never overlap
- * in time unless they are of one colour. */
+ * item = (instance, sweep position p, tile, colour), ordered colour-major in the
+ * batch's colour order (colour = igab_colour_at(order, p)); done[8 i + p] counts the
+ * finished tiles of position p of instance i, need[8 i + p] how many there are.  A
+ * tile of position p starts once every earlier position of its instance is complete
+ * (bounded wait), so tiles of one instance never overlap in time unless they are of
+ * one colour. */
 struct igab_batch_dev {
     const igab_geom *geoms;
     const int4 *items;
@@ -116,6 +117,7 @@ struct igab_ctx {
     int tile_res = 2, tile_tan = 2;
     int tan_kernel = 1;   /* FP64 tangent: 1 tensor-core (mma f64), 0 SIMT */
     int tan32_kernel = 1; /* FP32 tangent: 1 tcgen05 tensor cores (TF32 hi/lo), 0 SIMT */
+    int colour_order = 0; /* igab_colour_order */
     int *d_status = nullptr;   /* device status word: nonzero after a bounded wait gave up */
     int last_launches = 0;
 
@@ -163,6 +165,15 @@ struct igab_ctx {
     igab_geom geom() const;
 };
 
+/* the k-th colour swept under colour order `order` (igab_colour_order); every order sweeps
+ * the even-x colours (0-3) first */
+__host__ __device__ inline int igab_colour_at(int order, int k)
+{
+    if (order == 1) return (k & 4) | (3 - (k & 3));   /* 3,2,1,0,7,6,5,4 */
+    if (order == 2) return k ^ (k >> 1);              /* 0,1,3,2,6,7,5,4 */
+    return k;
+}
+
 /* kernels / launchers (igab_kernels.cu) */
 int igab_launch_residual(igab_ctx *c, const double *dU, double *dR);
 int igab_launch_density(igab_ctx *c, const double *dU, double *dHH);   /* igab_density.cu */
@@ -186,6 +197,7 @@ int igab_launch_csr_cols(igab_ctx *c, int *dcols);
 int igab_launch_check_finite(igab_ctx *c, const void *dev, long n, int prec, int *all_finite);
 int igab_launch_basis_tables(igab_ctx *c, int d, const double *dkv, const double *dgx, const double *dgw);
 int igab_launch_fma_peak(int prec, double *tflops);
+int igab_launch_dmma_peak(double *tflops);   /* igab_tangent_dmma.cu */
 /* tangent volume kernels over the tiles with x tile coordinate in [tx0, tx1) (tiles of 2 elements) */
 int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv, int tx0, int tx1);
 int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv, int tx0, int tx1);

@@ -837,7 +837,8 @@ int launch_res_volume_t(igab_ctx *c, const igab_geom &g, const double *dU, doubl
 {
     size_t sm = sizeof(res_smem<TE, GT ? 3 : 1>);
     IGAB_CUDA_TRY(cudaFuncSetAttribute(k_res_volume<TE, GT, VJP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    for (int colour = 0; colour < 8; colour++) {
+    for (int k = 0; k < 8; k++) {
+        const int colour = igab_colour_at(c->colour_order, k);
         long nblk = tiles_of_colour(g, TE, colour);
         if (nblk == 0) continue;
         k_res_volume<TE, GT, VJP><<<(unsigned)nblk, 256, sm, c->stream>>>(g, dU, dR, colour, dlam, dgrad);
@@ -852,7 +853,8 @@ int launch_tan_volume(igab_ctx *c, const igab_geom &g, const double *dU, T *dv)
 {
     size_t sm = sizeof(tan_smem<T, TE>);
     IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_volume<T, TE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    for (int colour = 0; colour < 8; colour++) {
+    for (int k = 0; k < 8; k++) {
+        const int colour = igab_colour_at(c->colour_order, k);
         long nblk = tiles_of_colour(g, TE, colour);
         if (nblk == 0) continue;
         k_tan_volume<T, TE><<<(unsigned)nblk, 256, sm, c->stream>>>(g, dU, dv, colour);

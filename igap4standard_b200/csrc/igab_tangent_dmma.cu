@@ -75,7 +75,7 @@ struct dws_tile {
     igab_geom g;
     const double *U;
     double *vals;
-    int tile, colour, inst, pad;   /* tile < 0: no more work */
+    int tile, colour, inst, pos;   /* tile < 0: no more work; pos: sweep position of a batch item */
 };
 
 struct dws_smem {
@@ -149,8 +149,8 @@ struct src_colour {
     __device__ void done(const dws_tile &) const {}
 };
 
-/* the batched work list: items (instance, colour, tile) in colour-major order;
- * an item starts once every earlier colour of its instance is complete */
+/* the batched work list: items (instance, sweep position, tile, colour) in colour-major
+ * order; an item starts once every earlier position of its instance is complete */
 struct src_batch {
     igab_batch_dev B;
     const double *U;
@@ -170,7 +170,8 @@ struct src_batch {
         R.U = U + B.dof_off[w.x];
         R.vals = vals + B.nnz_off[w.x];
         R.tile = w.z;
-        R.colour = w.y;
+        R.colour = w.w;
+        R.pos = w.y;
         R.inst = w.x;
     }
     /* consumers, after the tile's last reduction: publish the finished tile */
@@ -178,7 +179,7 @@ struct src_batch {
     {
         __threadfence();
         tc_bar_sync(BAR_CONS, NCONS);
-        if (threadIdx.x == 0) atomicAdd(&B.done[8 * R.inst + R.colour], 1);
+        if (threadIdx.x == 0) atomicAdd(&B.done[8 * R.inst + R.pos], 1);
     }
 };
 
@@ -657,13 +658,70 @@ int igab_batch_occupancy_dmma(int *per_sm)
     return 0;
 }
 
+/* FP64 tensor-pipe issue rate: every warp issues back-to-back mma.sync m8n8k4 f64 on
+ * eight independent accumulator pairs (512 flops per warp instruction) */
+__global__ void __launch_bounds__(256) k_dmma_peak(int reps, double *sink)
+{
+    double c[8][2];
+#pragma unroll
+    for (int i = 0; i < 8; i++) c[i][0] = c[i][1] = 0.0;
+    const double a = 1.0 + 1e-9 * threadIdx.x, b = 0.999;
+    for (int r = 0; r < reps; r++) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) dmma(c[i][0], c[i][1], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) s += c[i][0] + c[i][1];
+    if (s == -12345.0) sink[0] = s;   /* keeps the chains live */
+}
+
+int igab_launch_dmma_peak(double *tflops)
+{
+    int dev = 0, nsm = 0;
+    IGAB_CUDA_TRY(cudaGetDevice(&dev));
+    IGAB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    double *sink = nullptr;
+    IGAB_CUDA_TRY(cudaMalloc((void **)&sink, sizeof(double)));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t err = cudaEventCreate(&e0);
+    if (err == cudaSuccess) err = cudaEventCreate(&e1);
+    const int reps = 1 << 13;
+    const unsigned nblk = (unsigned)nsm * 4u;   /* 32 warps per SM */
+    float best = 1e30f;
+    if (err == cudaSuccess) {
+        k_dmma_peak<<<nblk, 256>>>(reps, sink);   /* warm-up */
+        for (int rep = 0; rep < 3 && err == cudaSuccess; rep++) {
+            cudaEventRecord(e0);
+            k_dmma_peak<<<nblk, 256>>>(reps, sink);
+            cudaEventRecord(e1);
+            err = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+            if (err == cudaSuccess && ms < best) best = ms;
+        }
+        if (err == cudaSuccess) err = cudaGetLastError();
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (err != cudaSuccess) {
+        igab_set_error("igab_dmma_peak: %s", cudaGetErrorString(err));
+        return IGAB_ERR_CUDA;
+    }
+    const double flops = 512.0 * 8.0 * reps * (double)nblk * 8.0;   /* per warp instruction x chains x warps */
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return 0;
+}
+
 int igab_launch_tan_dmma(igab_ctx *c, const double *dU, double *dv, int tx0, int tx1)
 {
     igab_geom g = c->geom();
     const size_t sm = sizeof(dws_smem);
     IGAB_CUDA_TRY(cudaFuncSetAttribute(k_tan_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const int nsm = sm_count();
-    for (int colour = 0; colour < 8; colour++) {
+    for (int k = 0; k < 8; k++) {
+        const int colour = igab_colour_at(c->colour_order, k);
         long first = 0;
         const long nt = tiles_of_colour_in(g, TE, colour, tx0, tx1, &first);
         if (nt == 0) continue;

@@ -952,7 +952,8 @@ int igab_launch_tan_tc32(igab_ctx *c, const double *dU, float *dv, int tx0, int 
         igab_set_error("k_tan_tc32: %d CTAs per SM (needs 1 or 2 for its tensor memory)", per_sm);
         return IGAB_ERR_UNSUPPORTED;
     }
-    for (int colour = 0; colour < 8; colour++) {
+    for (int k = 0; k < 8; k++) {
+        const int colour = igab_colour_at(c->colour_order, k);
         long first = 0;
         const long nblk = tiles_of_colour_in(g, 2, colour, tx0, tx1, &first);
         if (nblk == 0) continue;

@@ -32,7 +32,8 @@ class IgabTuneResult(ctypes.Structure):
     """igab_tune_result of include/igab.h"""
     _fields_ = [("residual_tile", ctypes.c_int), ("tangent_fp64_kernel", ctypes.c_int),
                 ("tangent_fp32_kernel", ctypes.c_int), ("residual_ms", ctypes.c_double),
-                ("tangent_fp64_ms", ctypes.c_double), ("tangent_fp32_ms", ctypes.c_double)]
+                ("tangent_fp64_ms", ctypes.c_double), ("tangent_fp32_ms", ctypes.c_double),
+                ("colour_order", ctypes.c_int)]
 
 
 class IgabSolveInfo(ctypes.Structure):
@@ -84,7 +85,7 @@ class IgabBatchTuneResult(ctypes.Structure):
     """igab_batch_tune_result of include/igab.h"""
     _fields_ = [("ctas_res", ctypes.c_int), ("ctas_tan64", ctypes.c_int), ("ctas_tan32", ctypes.c_int),
                 ("order", ctypes.c_int), ("residual_ms", ctypes.c_double), ("tangent_fp64_ms", ctypes.c_double),
-                ("tangent_fp32_ms", ctypes.c_double)]
+                ("tangent_fp32_ms", ctypes.c_double), ("colour_order", ctypes.c_int)]
 
 
 class IgabMeshDesc(ctypes.Structure):
@@ -128,6 +129,7 @@ IGAB_API = [
     ("igab_set_profiling", ctypes.c_int, [vp, ctypes.c_int]),
     ("igab_last_kernel_ms", ctypes.c_int, [vp, c_double_p]),
     ("igab_fma_peak", ctypes.c_int, [ctypes.c_int, ctypes.c_int, c_double_p]),
+    ("igab_dmma_peak", ctypes.c_int, [ctypes.c_int, c_double_p]),
     ("igab_residual_noalloc", ctypes.c_int, [vp, vp, vp]),
     ("igab_staging_bytes", ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_size_t)]),
     ("igab_newton_defaults", None, [vp]),
@@ -175,6 +177,8 @@ IGAB_API = [
     ("igab_batch_set_stream", ctypes.c_int, [vp, vp]),
     ("igab_batch_set_schedule", ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("igab_batch_get_schedule", ctypes.c_int, [vp, c_int_p, c_int_p, c_int_p, c_int_p]),
+    ("igab_batch_set_colour_order", ctypes.c_int, [vp, ctypes.c_int]),
+    ("igab_batch_get_colour_order", ctypes.c_int, [vp, c_int_p]),
     ("igab_batch_residual_device", ctypes.c_int, [vp, vp, vp]),
     ("igab_batch_tangent_device", ctypes.c_int, [vp, vp, vp, ctypes.c_int]),
     ("igab_batch_sync", ctypes.c_int, [vp]),

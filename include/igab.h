@@ -115,8 +115,15 @@ int igab_check_finite(igab_ctx *ctx, const void *dev, long n, int prec, int *all
 int igab_set_tile(igab_ctx *ctx, int residual_tile, int tangent_tile);
 /* kernel choices: IGAB_OPT_TANGENT_FP64_KERNEL 1 = FP64 tensor path (mma f64), 0 = FP64 FMA pipe;
  * IGAB_OPT_TANGENT_FP32_KERNEL 1 = tcgen05 tensor cores (TF32 hi/lo split, FP32 accumulation in
- * tensor memory), 0 = FP32 FMA pipe */
-enum igab_option { IGAB_OPT_TANGENT_FP64_KERNEL = 1, IGAB_OPT_TANGENT_FP32_KERNEL = 2 };
+ * tensor memory), 0 = FP32 FMA pipe.  IGAB_OPT_COLOUR_ORDER: the order in which the 8 colours
+ * of the element schedule are swept (colour = 4 x-parity + 2 y-parity + z-parity):
+ * IGAB_COLOURS_NATURAL 0..7, IGAB_COLOURS_MIRRORED 3,2,1,0,7,6,5,4, IGAB_COLOURS_GRAY
+ * 0,1,3,2,6,7,5,4.  Each order fixes the order in which every CSR entry receives its
+ * additions (results are bitwise repeatable per order; orders differ by rounding); all three
+ * sweep the even-x colours first, which keeps the x-slab tangent of the host entry points
+ * equal to the whole-mesh one. */
+enum igab_option { IGAB_OPT_TANGENT_FP64_KERNEL = 1, IGAB_OPT_TANGENT_FP32_KERNEL = 2, IGAB_OPT_COLOUR_ORDER = 3 };
+enum igab_colour_order { IGAB_COLOURS_NATURAL = 0, IGAB_COLOURS_MIRRORED = 1, IGAB_COLOURS_GRAY = 2 };
 int igab_set_option(igab_ctx *ctx, int option, int value);
 int igab_get_option(const igab_ctx *ctx, int option, int *value);
 /* launches issued by the last assembly call (kernel count) */
@@ -132,6 +139,9 @@ int igab_set_profiling(igab_ctx *ctx, int on);
 int igab_last_kernel_ms(igab_ctx *ctx, double ms[6]);
 /* FMA throughput probe of the device (TFLOP/s, 2 flops per FMA), prec = igab_prec */
 int igab_fma_peak(int device, int prec, double *tflops);
+/* FP64 tensor-pipe throughput probe (TFLOP/s): back-to-back mma.sync m8n8k4 f64 on
+ * independent accumulators, 32 warps per SM (the pipe of the FP64 tangent's products) */
+int igab_dmma_peak(int device, double *tflops);
 /* Check of the tcgen05 operand layout and descriptors used by the FP32 tensor-core tangent
  * (no reference counterpart): one CTA computes A B^T for fixed small-integer A (128 x 32) and
  * B (96 x 32) with the M 128 / N 96 and M 128 / N 32 instruction shapes; out (128 x 160 floats,
@@ -172,11 +182,14 @@ int igab_adjoint_backward(igab_ctx *ctx, const double *U_dev, const void *vals_d
 /* ---- autotuner (no reference counterpart): times every candidate schedule on this
  * mesh and state (U_dev; NULL = zero state) with CUDA events on the context stream,
  * reps timed runs after one warm-up, and leaves the fastest applied.  what: bit 0
- * residual (tile edge 2 or 4), bit 1 FP64 tangent (tensor path or FMA pipe), bit 2
- * FP32 tangent (tcgen05 or FMA pipe).  Times of the chosen candidates in ms. */
+ * residual (elements per block: tile edge 2 or 4), bit 1 FP64 tangent (tensor path or FMA
+ * pipe), bit 2 FP32 tangent (tcgen05 or FMA pipe), bit 3 colour order (the three orders of
+ * IGAB_OPT_COLOUR_ORDER, timed on the sum of the kernels bits 0-2 select, all three when
+ * none).  Times of the chosen candidates in ms. */
 typedef struct {
     int residual_tile, tangent_fp64_kernel, tangent_fp32_kernel;
     double residual_ms, tangent_fp64_ms, tangent_fp32_ms;
+    int colour_order;
 } igab_tune_result;
 int igab_autotune(igab_ctx *ctx, const double *U_dev, int what, int reps, igab_tune_result *out);
 
@@ -201,6 +214,9 @@ int igab_batch_refresh(igab_batch *b);
 int igab_batch_set_stream(igab_batch *b, void *cuda_stream);
 int igab_batch_set_schedule(igab_batch *b, int ctas_res, int ctas_tan64, int ctas_tan32, int order);
 int igab_batch_get_schedule(const igab_batch *b, int *ctas_res, int *ctas_tan64, int *ctas_tan32, int *order);
+/* colour order of the batch's work list (igab_colour_order; natural by default) */
+int igab_batch_set_colour_order(igab_batch *b, int colour_order);
+int igab_batch_get_colour_order(const igab_batch *b, int *colour_order);
 /* The launches below return once enqueued.  A tile of colour c waits (bounded) for the
  * earlier colours of its instance; a wait that gives up sets a status word and the
  * launch still ends, with that instance's R or values incomplete.  igab_batch_sync
@@ -219,11 +235,13 @@ int igab_batch_last_launch_count(const igab_batch *b, int *n);
 int igab_batch_graph_capture(igab_batch *b, const double *U_dev, double *R_dev, void *vals_dev, int prec);
 int igab_batch_graph_launch(igab_batch *b);
 /* autotuner of the batch schedule: CTAs per SM of each persistent kernel and the
- * instance order (what: bit 0 residual, bit 1 FP64 tangent, bit 2 FP32 tangent);
+ * instance order (what: bit 0 residual, bit 1 FP64 tangent, bit 2 FP32 tangent), and with
+ * bit 3 the colour order (on the sum of the selected kernels, all three when none);
  * the fastest schedule is left applied. */
 typedef struct {
     int ctas_res, ctas_tan64, ctas_tan32, order;
     double residual_ms, tangent_fp64_ms, tangent_fp32_ms;
+    int colour_order;
 } igab_batch_tune_result;
 int igab_batch_autotune(igab_batch *b, const double *U_dev, int what, int reps, igab_batch_tune_result *out);
 

@@ -86,3 +86,11 @@ def test_fp32_tensor_core_tangent_deterministic(built):
     v1 = A.tangent(c["U"], "fp32")
     v2 = A.tangent(c["U"], "fp32")
     assert np.array_equal(v1, v2)
+
+
+def test_fp64_tensor_pipe_probe(built):
+    """igab_dmma_peak: back-to-back mma.sync m8n8k4 f64 gives a plausible B200 rate (TFLOP/s)."""
+    from igap4standard_b200.assembly import dmma_peak_tflops
+    t = dmma_peak_tflops(0)
+    print("FP64 tensor pipe: %.2f TFLOP/s" % t)
+    assert 5.0 < t < 200.0

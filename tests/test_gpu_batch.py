@@ -30,9 +30,10 @@ def _instances(seed=11):
     return out
 
 
-def _single(c, U, prec):
+def _single(c, U, prec, colour_order=0):
     from igap4standard_b200 import Assembly
     A = Assembly(c["nelem"], c["knots"], c["par_mat"], c["bc_type"], c["par_dirichlet"], c["par_periodic"])
+    A.set_option(3, colour_order)
     R = A.residual(U)
     V = A.tangent(U, prec)
     A.close()
@@ -60,6 +61,23 @@ def test_batch_equals_single_mesh(batch_case, prec):
         R1, V1 = _single(c, U[d0:d1], prec)
         assert np.array_equal(R[d0:d1], R1), "instance %d residual" % i
         assert np.array_equal(V[z0:z1], V1), "instance %d tangent (%s)" % (i, prec)
+
+
+@pytest.mark.parametrize("colour_order", [1, 2])
+def test_batch_colour_orders_equal_single_mesh(batch_case, colour_order):
+    """Under each colour order the batch (waits by sweep position) equals the single-mesh
+    assembly swept in the same order, bit for bit."""
+    inst, B, U = batch_case
+    B.set_colour_order(colour_order)
+    assert B.get_colour_order() == colour_order
+    R, V, W = B.residual(U), B.tangent(U, "fp64"), B.tangent(U, "fp32")
+    B.set_colour_order(0)
+    for i, c in enumerate(inst):
+        d0, d1 = B.dof_offsets[i], B.dof_offsets[i + 1]
+        z0, z1 = B.nnz_offsets[i], B.nnz_offsets[i + 1]
+        R1, V1 = _single(c, U[d0:d1], "fp64", colour_order)
+        _, W1 = _single(c, U[d0:d1], "fp32", colour_order)
+        assert np.array_equal(R[d0:d1], R1) and np.array_equal(V[z0:z1], V1) and np.array_equal(W[z0:z1], W1), i
 
 
 @pytest.mark.parametrize("sched", [(1, 1, 1, 0), (0, 0, 0, 1), (1, 1, 1, 1)])

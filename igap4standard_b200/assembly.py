@@ -67,7 +67,7 @@ class Assembly:
     src/snesiga_Tangent.c:13), with plain arrays instead of PETSc objects."""
 
     def __init__(self, nelem, knots, par_mat, bc_type, par_dirichlet=None, par_periodic=None,
-                 phys="ge", device=0):
+                 phys="ge", device=0, bc_periodic=(0, 0, 0)):
         self.lib = native.lib_cuda()
         d = IgabMeshDesc()
         d.phys = PHYS[phys]
@@ -83,6 +83,8 @@ class Assembly:
             d.par_periodic[i] = float(par_periodic[i]) if par_periodic is not None else 0.0
         for i in range(36):
             d.bc_type[i] = int(bc_type[i])
+        for i in range(3):
+            d.bc_periodic[i] = int(bc_periodic[i])
         h = vp()
         check(self.lib, "igab_create", self.lib.igab_create(ctypes.byref(d), int(device), ctypes.byref(h)))
         self.h = h

@@ -26,7 +26,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
 
 CUDA_SOURCES = ["igab_kernels.cu", "igab_tangent_dmma.cu", "igab_tangent_tc.cu", "igab_getime.cu", "igab_capi.cu",
                 "igab_batch.cu", "igab_autotune.cu", "igab_noalloc.cu", "igab_density.cu", "igab_krylov.cu",
-                "igab_refine.cu", "igab_newton.cu", "igab_mg.cu", "igab_transient.cu"]
+                "igab_refine.cu", "igab_newton.cu", "igab_mg.cu", "igab_transient.cu", "igab_periodic.cu"]
 CUDA_HEADERS = ["igab_internal.h", "igab_math.cuh", "igab_device.cuh", "igab_warp_tiles8.inc", "igab_tc.cuh",
                 "igab_reduce.cuh"]
 

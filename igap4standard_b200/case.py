@@ -18,7 +18,7 @@ def _p(a):
 
 class Case:
     def __init__(self, lib, phys, nelem, knots, par_mat, bc_type, par_periodic=None, par_dirichlet=None,
-                 par_neumann=None):
+                 par_neumann=None, bc_periodic=(0, 0, 0)):
         self.lib = lib
         self._nel = np.ascontiguousarray(nelem, dtype=np.int32)
         self._kn = np.ascontiguousarray(knots, dtype=np.float64)
@@ -28,8 +28,9 @@ class Case:
         self._pd = np.ascontiguousarray(par_dirichlet if par_dirichlet is not None else np.zeros(9), dtype=np.float64)
         pn = np.ascontiguousarray(par_neumann if par_neumann is not None else np.zeros(39), dtype=np.float64)
         self._pn = pn
-        h = lib.iga_case_create(KIND[phys], _p(self._nel), _p(self._kn), _p(self._pm), _p(self._bc),
-                                _p(self._pp), _p(self._pd), _p(pn), int(pn.size))
+        self._per = np.ascontiguousarray(bc_periodic, dtype=np.int32)
+        h = lib.iga_case_create_periodic(KIND[phys], _p(self._nel), _p(self._kn), _p(self._pm), _p(self._bc),
+                                         _p(self._pp), _p(self._pd), _p(pn), int(pn.size), _p(self._per))
         if not h:
             raise RuntimeError("iga_case_create failed")
         self.h = h
@@ -67,6 +68,14 @@ class Case:
         vals = np.empty(nnz)
         self.lib.iga_case_tangent_csr(self.h, _p(rowptr), _p(cols), _p(vals))
         return rowptr, cols, vals
+
+    def index_maps(self):
+        """(selfIdx, sendIdx, recvIdx, globalIdx) as the linked snesiga_init left them."""
+        n = np.zeros(3, dtype=np.int32)
+        self.lib.iga_case_index_maps(self.h, _p(n), None, None, None, None)
+        a = [np.empty(int(k), dtype=np.int32) for k in (n[0], n[1], n[2], n[0] + n[2])]
+        self.lib.iga_case_index_maps(self.h, _p(n), *[_p(x) for x in a])
+        return tuple(a)
 
     def set_history(self, level, U):
         U = np.ascontiguousarray(U, dtype=np.float64)

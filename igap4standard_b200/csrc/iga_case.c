@@ -1,10 +1,12 @@
 /*
  * Single-rank case builder (see include/iga_case.h).
  *
- * One rank, non-periodic, p = 2: every control point is owned, there are no
- * halo parts, the six faces are all boundaries (mesh/nurbs/nurbs_init.c:78-88
- * with npart = {1,1,1}), and the universal index of a control point is its
- * local index (mesh/nurbs/nurbs_init.c:93-97).
+ * One rank, p = 2 (mesh/nurbs/nurbs_init.c with npart = {1,1,1}, ipart = 0): the
+ * faces of the non-periodic directions are the boundaries (:24-27), the rank owns
+ * nelem + 2 points along a non-periodic direction and nelem along a periodic one
+ * (:36-39), and along every periodic direction it is its own neighbour: the halo
+ * parts of set_mpi_part (:156-199) are all rank 0, so the ghost layers arrive as
+ * messages to self.  The universal index of an owned point follows :42-47.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -65,9 +67,36 @@ iga_case *iga_case_create(int phys_kind, const int nelem[3], const double *knots
                           const double par_periodic[9], const double par_dirichlet[9],
                           const double *par_neumann, int n_par_neumann)
 {
+    const int none[3] = {0, 0, 0};
+    return iga_case_create_periodic(phys_kind, nelem, knots, par_mat, bc_type, par_periodic, par_dirichlet,
+                                    par_neumann, n_par_neumann, none);
+}
+
+/* the halo parts of one rank that is its own neighbour along the periodic directions:
+ * blocks 0-6 = z, y, x, yz, xz, xy, xyz in set_mpi_part's order (nurbs_init.c:162-169) */
+static int self_blocks(const int per[3], int *block)
+{
+    const int c0 = per[0], c1 = per[1], c2 = per[2];
+    const int on[7] = {c2, c1, c0, c1 && c2, c0 && c2, c0 && c1, c0 && c1 && c2};
+    int n = 0;
+    for (int b = 0; b < 7; b++)
+        if (on[b]) {
+            if (block) block[n] = b;
+            n++;
+        }
+    return n;
+}
+
+iga_case *iga_case_create_periodic(int phys_kind, const int nelem[3], const double *knots,
+                                   const double par_mat[9], const int bc_type[36],
+                                   const double par_periodic[9], const double par_dirichlet[9],
+                                   const double *par_neumann, int n_par_neumann, const int bc_periodic[3])
+{
     const int p = 2;
     if (phys_kind != IGA_CASE_GE && phys_kind != IGA_CASE_GETIME) return NULL;
     for (int d = 0; d < 3; d++) if (nelem[d] < 1) return NULL;
+    for (int d = 0; d < 3; d++)
+        if ((bc_periodic[d] != 0 && bc_periodic[d] != 1) || (bc_periodic[d] && nelem[d] < 3)) return NULL;
     iga_case *c = (iga_case *)calloc(1, sizeof(iga_case));
     if (!c) return NULL;
     c->kind = phys_kind;
@@ -96,24 +125,34 @@ iga_case *iga_case_create(int phys_kind, const int nelem[3], const double *knots
     size_t off = 0;
     for (int d = 0; d < 3; d++) {
         nb->nelem[d] = nelem[d];
-        nb->nbasis[d] = nelem[d] + p;
+        nb->nbasis[d] = bc_periodic[d] ? nelem[d] : nelem[d] + p;
         nb->nknot[d] = nelem[d] + 1 + 2 * p;
         nb->knotVector[d] = (double *)xmalloc((size_t)nb->nknot[d] * sizeof(double));
         memcpy(nb->knotVector[d], knots + off, (size_t)nb->nknot[d] * sizeof(double));
         off += (size_t)nb->nknot[d];
     }
-    nb->nboun = 6;
+    nb->nboun = 0;
     nb->boun = (int *)xmalloc(6 * sizeof(int));
-    for (int f = 0; f < 6; f++) nb->boun[f] = f;
-    nb->nsendPart = 0;
-    nb->sendPart = (int *)xmalloc(0);
-    nb->nrecvPart = 0;
-    nb->recvPart = (int *)xmalloc(0);
-    nb->sendBlock = (int *)xmalloc(0);
-    nb->recvBlock = (int *)xmalloc(0);
+    for (int f = 0; f < 6; f++)
+        if (!bc_periodic[f / 2]) nb->boun[nb->nboun++] = f;
+    const int npart = self_blocks(bc_periodic, NULL);
+    nb->nsendPart = npart;
+    nb->sendPart = (int *)calloc((size_t)(npart > 0 ? npart : 1), sizeof(int));   /* rank 0: itself */
+    nb->nrecvPart = npart;
+    nb->recvPart = (int *)calloc((size_t)(npart > 0 ? npart : 1), sizeof(int));
+    nb->sendBlock = (int *)xmalloc((size_t)npart * sizeof(int));
+    nb->recvBlock = (int *)xmalloc((size_t)npart * sizeof(int));
+    self_blocks(bc_periodic, nb->sendBlock);
+    self_blocks(bc_periodic, nb->recvBlock);
     int ncp = nb->nbasis[0] * nb->nbasis[1] * nb->nbasis[2];
     nb->universalIdx_temp = (int *)xmalloc((size_t)ncp * sizeof(int));
-    for (int i = 0; i < ncp; i++) nb->universalIdx_temp[i] = i;
+    {
+        const int gy = nelem[1] + (bc_periodic[1] ? 0 : p), gz = nelem[2] + (bc_periodic[2] ? 0 : p);
+        int ia = 0;
+        for (int x = 0; x < nb->nbasis[0]; x++)
+            for (int y = 0; y < nb->nbasis[1]; y++)
+                for (int z = 0; z < nb->nbasis[2]; z++) nb->universalIdx_temp[ia++] = gy * gz * x + gz * y + z;
+    }
     nb->bc_periodic = NULL;
     nb->nelem_global = NULL;
     nb->knotVector_global = NULL;
@@ -160,6 +199,20 @@ void iga_case_destroy(iga_case *c)
 }
 
 int iga_case_ndof(const iga_case *c) { return c->ndof; }
+
+int iga_case_index_maps(const iga_case *c, int n[3], int *selfIdx, int *sendIdx, int *recvIdx, int *globalIdx)
+{
+    if (!c || !n) return -1;
+    const IGA *a = &c->app;
+    n[0] = a->nselfIdx;
+    n[1] = a->nsendIdx;
+    n[2] = a->nrecvIdx;
+    if (selfIdx) memcpy(selfIdx, a->selfIdx, (size_t)a->nselfIdx * sizeof(int));
+    if (sendIdx) memcpy(sendIdx, a->sendIdx, (size_t)a->nsendIdx * sizeof(int));
+    if (recvIdx) memcpy(recvIdx, a->recvIdx, (size_t)a->nrecvIdx * sizeof(int));
+    if (globalIdx) memcpy(globalIdx, a->globalIdx, (size_t)(a->nselfIdx + a->nrecvIdx) * sizeof(int));
+    return 0;
+}
 
 int iga_case_set_history(iga_case *c, int level, const double *U)
 {

@@ -252,6 +252,11 @@ extern "C" int igab_batch_create(const igab_mesh_desc *descs, int n, int device,
             igab_set_error("igab_batch_create: instance %d: batched assembly is built for phys/ge only", i);
             return IGAB_ERR_UNSUPPORTED;
         }
+    for (int i = 0; i < n; i++)
+        if (descs[i].bc_periodic[0] || descs[i].bc_periodic[1] || descs[i].bc_periodic[2]) {
+            igab_set_error("igab_batch_create: instance %d: batched assembly takes non-periodic meshes", i);
+            return IGAB_ERR_UNSUPPORTED;
+        }
     IGAB_CUDA_TRY(cudaSetDevice(device));
     igab_batch *b = new igab_batch;
     b->device = device;

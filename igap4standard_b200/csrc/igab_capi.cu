@@ -191,20 +191,31 @@ static void dirichlet_values(const igab_ctx *c, int face, int order, int idof, s
  * (src/snesiga_Residual.c:331-409 loop order) */
 static int build_dirichlet(igab_ctx *c)
 {
-    std::vector<double> g(c->ndof, 0.0);
-    std::vector<char> is(c->ndof, 0);
+    /* with periodic directions the rows are owned dofs: the faces of periodic directions are
+     * no boundaries, and along a periodic tangential direction the face has its owned points
+     * only (nbasis = nelem, mesh/nurbs/nurbs_init.c:24-39) */
+    long nbo[3];
+    for (int d = 0; d < 3; d++) nbo[d] = c->periodic[d] ? c->ne[d] : c->nb[d];
+    const long nown = 3 * nbo[0] * nbo[1] * nbo[2];
+    std::vector<double> g(nown, 0.0);
+    std::vector<char> is(nown, 0);
     std::vector<double> vals;
     for (int face = 0; face < 6; face++) {
         int d0, d1, dn;
         face_dirs(face, d0, d1, dn);
+        if (c->periodic[dn]) continue;
         for (int order = 0; order < 2; order++)
             for (int idof = 0; idof < 3; idof++) {
                 if (c->bc_type[6 * face + 3 * order + idof] != 0) continue;
                 dirichlet_values(c, face, order, idof, vals);
                 int layer = layer_of(c, face, order);
-                for (int i = 0; i < c->nb[d0]; i++)
-                    for (int j = 0; j < c->nb[d1]; j++) {
-                        long r = 3 * cp_of(c, face, i, j, layer) + idof;
+                for (int i = 0; i < nbo[d0]; i++)
+                    for (int j = 0; j < nbo[d1]; j++) {
+                        int xyz[3];
+                        xyz[d0] = i;
+                        xyz[d1] = j;
+                        xyz[dn] = layer;
+                        long r = 3 * (((long)xyz[0] * nbo[1] + xyz[1]) * nbo[2] + xyz[2]) + idof;
                         g[r] = vals[(size_t)c->nb[d1] * i + j];
                         is[r] = 1;
                     }
@@ -212,8 +223,13 @@ static int build_dirichlet(igab_ctx *c)
     }
     std::vector<int> rows;
     std::vector<double> gv;
-    for (long r = 0; r < c->ndof; r++)
+    for (long r = 0; r < nown; r++)
         if (is[r]) { rows.push_back((int)r); gv.push_back(g[r]); }
+    if (c->per) {
+        c->nd = 0;   /* the local-grid kernels apply none; the owned system does */
+        c->dirichlet_dirty = false;
+        return igab_periodic_set_dirichlet(c, rows, gv);
+    }
     /* the Dirichlet row set depends only on bc_type; values change with par_dirichlet.
      * Existing buffers are refilled in place so captured graphs stay valid. */
     if ((long)rows.size() != c->nd || !c->d_drow) {
@@ -241,6 +257,7 @@ static int build_neumann(igab_ctx *c)
     for (int face = 0; face < 6; face++) {
         int d0, d1, dn;
         face_dirs(face, d0, d1, dn);
+        if (c->periodic[dn]) continue;   /* no boundary (mesh/nurbs/nurbs_init.c:24-27) */
         for (int order = 0; order < 2; order++)
             for (int idof = 0; idof < 3; idof++) {
                 if (c->bc_type[6 * face + 3 * order + idof] != 1) continue;
@@ -331,6 +348,7 @@ static void free_ctx(igab_ctx *c)
     cudaFree(c->d_U); cudaFree(c->d_R); cudaFree(c->d_vals);
     cudaFree(c->d_escale); cudaFree(c->d_lam); cudaFree(c->d_status);
     cudaFree(c->d_dens_part); cudaFree(c->d_HH);
+    igab_periodic_release(c);
     igab_krylov_release(c);
     igab_newton_release(c);
     igab_mg_release(c);
@@ -355,6 +373,10 @@ extern "C" int igab_create(const igab_mesh_desc *desc, int device, igab_ctx **ou
     /* the reference reads bc_type as 0 (Dirichlet) or 1 (Neumann) only (include/bc.h:6) */
     for (int i = 0; i < 36; i++)
         ARG_CHECK(desc->bc_type[i] == 0 || desc->bc_type[i] == 1, "igab_create: bc_type entries must be 0 or 1");
+    for (int d = 0; d < 3; d++) {
+        ARG_CHECK(desc->bc_periodic[d] == 0 || desc->bc_periodic[d] == 1, "igab_create: bc_periodic entries must be 0 or 1");
+        ARG_CHECK(!desc->bc_periodic[d] || desc->nelem[d] >= 3, "igab_create: a periodic direction needs nelem >= 3");
+    }
     long ncp = 1;
     for (int d = 0; d < 3; d++) ncp *= desc->nelem[d] + 2;
     ARG_CHECK(3 * ncp < 2147483647L, "igab_create: dof count exceeds int32");
@@ -394,6 +416,7 @@ extern "C" int igab_create(const igab_mesh_desc *desc, int device, igab_ctx **ou
     memcpy(c->par_dirichlet, desc->par_dirichlet, sizeof(c->par_dirichlet));
     memcpy(c->par_periodic, desc->par_periodic, sizeof(c->par_periodic));
     memcpy(c->bc_type, desc->bc_type, sizeof(c->bc_type));
+    for (int d = 0; d < 3; d++) c->periodic[d] = desc->bc_periodic[d];
 
     int rc = 0;
     cudaError_t ce = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
@@ -456,7 +479,8 @@ extern "C" int igab_create(const igab_mesh_desc *desc, int device, igab_ctx **ou
         TRY(cudaMemset(c->d_hist, 0, (size_t)c->torder * c->ndof * sizeof(double)));
     }
 #undef TRY
-    rc = build_dirichlet(c);
+    if (c->periodic[0] || c->periodic[1] || c->periodic[2]) rc = igab_periodic_build(c);
+    if (!rc) rc = build_dirichlet(c);
     if (!rc) rc = build_neumann(c);
     if (rc) { free_ctx(c); return rc; }
     *out = c;
@@ -475,8 +499,8 @@ extern "C" int igab_destroy(igab_ctx *ctx)
 extern "C" int igab_sizes(const igab_ctx *ctx, long *ndof, long *nnz, long *nelem_total)
 {
     ARG_CHECK(ctx, "igab_sizes: null context");
-    if (ndof) *ndof = ctx->ndof;
-    if (nnz) *nnz = ctx->nnz;
+    if (ndof) *ndof = igab_periodic_ndof(ctx);
+    if (nnz) *nnz = igab_periodic_nnz(ctx);
     if (nelem_total) *nelem_total = ctx->nel;
     return 0;
 }
@@ -484,6 +508,12 @@ extern "C" int igab_sizes(const igab_ctx *ctx, long *ndof, long *nnz, long *nele
 extern "C" int igab_csr_pattern(igab_ctx *ctx, int *rowptr, int *cols)
 {
     ARG_CHECK(ctx, "igab_csr_pattern: null context");
+    if (ctx->per) {
+        const std::vector<int> &rp = igab_periodic_rowptr(ctx), &cl = igab_periodic_cols(ctx);
+        if (rowptr) memcpy(rowptr, rp.data(), rp.size() * sizeof(int));
+        if (cols) memcpy(cols, cl.data(), cl.size() * sizeof(int));
+        return 0;
+    }
     if (rowptr) memcpy(rowptr, ctx->rowptr_h.data(), ctx->rowptr_h.size() * sizeof(int));
     if (cols) {
         IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
@@ -503,6 +533,14 @@ extern "C" int igab_csr_pattern(igab_ctx *ctx, int *rowptr, int *cols)
 
 extern "C" long igab_csr_offset(const igab_ctx *ctx, long row, long col)
 {
+    if (ctx && ctx->per) {
+        const long n = igab_periodic_ndof(ctx);
+        if (row < 0 || col < 0 || row >= n || col >= n) return -1;
+        const std::vector<int> &rp = igab_periodic_rowptr(ctx), &cl = igab_periodic_cols(ctx);
+        const int *b = cl.data() + rp[(size_t)row], *e = cl.data() + rp[(size_t)row + 1];
+        const int *it = std::lower_bound(b, e, (int)col);
+        return it != e && *it == col ? (long)(it - cl.data()) : -1;
+    }
     if (!ctx || row < 0 || col < 0 || row >= ctx->ndof || col >= ctx->ndof) return -1;
     long cp = row / 3, cq = col / 3;
     int z = (int)(cp % ctx->nb[2]), y = (int)((cp / ctx->nb[2]) % ctx->nb[1]), x = (int)(cp / ((long)ctx->nb[2] * ctx->nb[1]));
@@ -604,7 +642,22 @@ extern "C" int igab_set_history(igab_ctx *ctx, int level, const double *U, int o
     ARG_CHECK(ctx && U, "igab_set_history: null argument");
     ARG_CHECK(level >= 1 && level <= ctx->torder, "igab_set_history: level outside 1..torder");
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
-    IGAB_CUDA_TRY(cudaMemcpyAsync(ctx->d_hist + (size_t)(level - 1) * ctx->ndof, U, (size_t)ctx->ndof * sizeof(double),
+    double *dst = ctx->d_hist + (size_t)(level - 1) * ctx->ndof;
+    if (ctx->per) {   /* owned level -> local grid (ghosts from their owners) */
+        const long n = igab_periodic_ndof(ctx);
+        const double *src = U;
+        double *tmp = nullptr;
+        if (!on_device) {
+            IGAB_CUDA_TRY(cudaMallocAsync((void **)&tmp, (size_t)n * sizeof(double), ctx->stream));
+            IGAB_CUDA_TRY(cudaMemcpyAsync(tmp, U, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            src = tmp;
+        }
+        int rc = igab_periodic_gather(ctx, src, dst);
+        if (tmp) IGAB_CUDA_TRY(cudaFreeAsync(tmp, ctx->stream));
+        if (!on_device) IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        return rc;
+    }
+    IGAB_CUDA_TRY(cudaMemcpyAsync(dst, U, (size_t)ctx->ndof * sizeof(double),
                                   on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
     return 0;
 }
@@ -672,6 +725,7 @@ extern "C" int igab_residual_device(igab_ctx *ctx, const double *U_dev, double *
 {
     ARG_CHECK(ctx && U_dev && R_dev, "igab_residual_device: null argument");
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (ctx->per) return igab_periodic_residual(ctx, U_dev, R_dev);
     return igab_launch_residual(ctx, U_dev, R_dev);
 }
 
@@ -681,12 +735,13 @@ extern "C" int igab_residual(igab_ctx *ctx, const double *U_host, double *R_host
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     int rc = ensure_buffers(ctx, -1);
     if (rc) return rc;
-    IGAB_CUDA_TRY(cudaMemcpyAsync(ctx->d_U, U_host, (size_t)ctx->ndof * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    const long n = igab_periodic_ndof(ctx);   /* the owned dofs (all of them without periodic directions) */
+    IGAB_CUDA_TRY(cudaMemcpyAsync(ctx->d_U, U_host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     rc = igab_residual_device(ctx, ctx->d_U, ctx->d_R);
     if (rc) return rc;
-    IGAB_CUDA_TRY(cudaMemcpyAsync(R_host, ctx->d_R, (size_t)ctx->ndof * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    IGAB_CUDA_TRY(cudaMemcpyAsync(R_host, ctx->d_R, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    for (long i = 0; i < ctx->ndof; i++)
+    for (long i = 0; i < n; i++)
         if (!isfinite(R_host[i])) { igab_set_error("igab_residual: non-finite entry at %ld", i); return IGAB_ERR_NONFINITE; }
     return 0;
 }
@@ -696,6 +751,7 @@ extern "C" int igab_tangent_device(igab_ctx *ctx, const double *U_dev, void *val
     ARG_CHECK(ctx && U_dev && vals_dev, "igab_tangent_device: null argument");
     ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_tangent_device: bad precision");
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (ctx->per) return igab_periodic_tangent(ctx, U_dev, vals_dev, prec);
     return igab_launch_tangent(ctx, U_dev, vals_dev, prec);
 }
 
@@ -706,6 +762,19 @@ extern "C" int igab_tangent(igab_ctx *ctx, const double *U_host, void *vals_host
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     int rc = ensure_buffers(ctx, prec);
     if (rc) return rc;
+    if (ctx->per) {   /* owned system: one pass, one download */
+        const long n = igab_periodic_ndof(ctx), nnz = igab_periodic_nnz(ctx);
+        const size_t es = prec == IGAB_PREC_FP64 ? sizeof(double) : sizeof(float);
+        IGAB_CUDA_TRY(cudaMemcpyAsync(ctx->d_U, U_host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = igab_periodic_tangent(ctx, ctx->d_U, ctx->d_vals, prec))) return rc;
+        int fin = 1;
+        if ((rc = igab_launch_check_finite(ctx, ctx->d_vals, nnz, prec, &fin))) return rc;
+        IGAB_CUDA_TRY(cudaMemcpyAsync(vals_host, ctx->d_vals, (size_t)nnz * es, cudaMemcpyDeviceToHost, ctx->stream));
+        IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if ((rc = igab_check_status(ctx))) return rc;
+        if (!fin) { igab_set_error("igab_tangent: non-finite entry"); return IGAB_ERR_NONFINITE; }
+        return 0;
+    }
     if (!ctx->copy_stream) IGAB_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
     IGAB_CUDA_TRY(cudaMemcpyAsync(ctx->d_U, U_host, (size_t)ctx->ndof * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     /* x-slab by x-slab: the rows a slab finishes are downloaded on the copy stream while
@@ -745,6 +814,7 @@ extern "C" int igab_dirichlet_rows(igab_ctx *ctx, long *n, int *rows)
         int rc = build_dirichlet(ctx);
         if (rc) return rc;
     }
+    if (ctx->per) return igab_periodic_dirichlet_rows(ctx, n, rows);
     *n = ctx->nd;
     if (rows && ctx->nd > 0) {
         IGAB_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -755,6 +825,7 @@ extern "C" int igab_dirichlet_rows(igab_ctx *ctx, long *n, int *rows)
 
 extern "C" int igab_history_jacobian_device(igab_ctx *ctx, const double *U_dev, void *vals_dev, int prec, int level)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_history_jacobian_device");
     ARG_CHECK(ctx && U_dev && vals_dev, "igab_history_jacobian_device: null argument");
     ARG_CHECK(ctx->phys == IGAB_PHYS_GETIME, "igab_history_jacobian_device: needs the transient physics");
     ARG_CHECK(level == 1 || level == 2, "igab_history_jacobian_device: level must be 1 or 2");
@@ -777,6 +848,7 @@ extern "C" int igab_ndensity(const igab_ctx *ctx, int *n)
 
 extern "C" int igab_intdensity_device(igab_ctx *ctx, const double *U_dev, double *HH_dev)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_intdensity_device");
     ARG_CHECK(ctx && U_dev && HH_dev, "igab_intdensity_device: null argument");
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     return igab_launch_density(ctx, U_dev, HH_dev);
@@ -784,6 +856,7 @@ extern "C" int igab_intdensity_device(igab_ctx *ctx, const double *U_dev, double
 
 extern "C" int igab_intdensity(igab_ctx *ctx, const double *U_host, double *HH_host)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_intdensity");
     ARG_CHECK(ctx && U_host && HH_host, "igab_intdensity: null argument");
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
     int rc = ensure_buffers(ctx, -1);
@@ -803,6 +876,7 @@ extern "C" int igab_intdensity(igab_ctx *ctx, const double *U_host, double *HH_h
 
 extern "C" int igab_spmv_device(igab_ctx *ctx, const void *vals_dev, int prec, const double *x_dev, double *y_dev)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_spmv_device");
     ARG_CHECK(ctx && vals_dev && x_dev && y_dev, "igab_spmv_device: null argument");
     ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_spmv_device: bad precision");
     IGAB_CUDA_TRY(cudaSetDevice(ctx->device));
@@ -813,6 +887,7 @@ extern "C" int igab_spmv_device(igab_ctx *ctx, const void *vals_dev, int prec, c
 extern "C" int igab_solve_device(igab_ctx *ctx, const void *vals_dev, int prec, const double *b_dev, double *x_dev,
                                  double rtol, double atol, int maxit, igab_solve_info *info)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_solve_device");
     ARG_CHECK(ctx && vals_dev && b_dev && x_dev, "igab_solve_device: null argument");
     ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_solve_device: bad precision");
     ARG_CHECK(maxit >= 1 && rtol >= 0.0 && atol >= 0.0, "igab_solve_device: bad tolerances");
@@ -834,6 +909,7 @@ extern "C" int igab_solve_device(igab_ctx *ctx, const void *vals_dev, int prec, 
 extern "C" int igab_solve_mg_device(igab_ctx *ctx, int method, const void *vals_dev, int prec, const double *b_dev,
                                     double *x_dev, double rtol, double atol, int maxit, igab_solve_info *info)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_solve_mg_device");
     ARG_CHECK(method == IGAB_KSP_MG_CG || method == IGAB_KSP_MG_GMRES, "igab_solve_mg_device: unknown method");
     ARG_CHECK(ctx && vals_dev && b_dev && x_dev, "igab_solve_mg_device: null argument");
     ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_solve_mg_device: bad precision");
@@ -1016,6 +1092,7 @@ extern "C" int igab_graph_destroy(igab_ctx *ctx)
 
 extern "C" int igab_graph_capture(igab_ctx *ctx, const double *U_dev, double *R_dev, void *vals_dev, int prec, int what)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_graph_capture");
     ARG_CHECK(ctx && U_dev, "igab_graph_capture: null argument");
     ARG_CHECK(what >= 1 && what <= 3, "igab_graph_capture: what must be 1, 2 or 3");
     ARG_CHECK(!(what & 1) || R_dev, "igab_graph_capture: residual output missing");
@@ -1107,6 +1184,7 @@ extern "C" int igab_set_element_log_scale(igab_ctx *ctx, const double *g, int on
 extern "C" int igab_adjoint_forward(igab_ctx *ctx, const double *g_dev, const double *U_dev, double *R_dev,
                                     void *vals_dev, int prec)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_adjoint_forward");
     ARG_CHECK(ctx && U_dev, "igab_adjoint_forward: null argument");
     ARG_CHECK(R_dev || vals_dev, "igab_adjoint_forward: nothing to compute");
     ARG_CHECK(prec == IGAB_PREC_FP64 || prec == IGAB_PREC_FP32, "igab_adjoint_forward: bad precision");
@@ -1128,6 +1206,7 @@ extern "C" int igab_adjoint_forward(igab_ctx *ctx, const double *g_dev, const do
 extern "C" int igab_adjoint_backward(igab_ctx *ctx, const double *U_dev, const void *vals_dev, int prec,
                                      const double *lam_dev, double *KTlam_dev, double *grad_dev)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_adjoint_backward");
     ARG_CHECK(ctx && lam_dev, "igab_adjoint_backward: null argument");
     ARG_CHECK(KTlam_dev || grad_dev, "igab_adjoint_backward: nothing to compute");
     ARG_CHECK(!KTlam_dev || vals_dev, "igab_adjoint_backward: K^T lam needs the tangent values");

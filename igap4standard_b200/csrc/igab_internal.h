@@ -157,6 +157,11 @@ struct igab_ctx {
     long sched_version = 0;            /* bumped by every change of a kernel parameter (par_mat, par_periodic,
                                           Dirichlet rows, element scales) or of the schedule (tiles, kernels) */
 
+    /* periodic directions: the kernels run on the local grid (nb), the owned system
+     * (igab_periodic.cu) gathers, folds and applies the Dirichlet rows */
+    int periodic[3] = {0, 0, 0};
+    struct igab_periodic *per = nullptr;
+
     /* captured assembly graph */
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -184,6 +189,26 @@ int igab_krylov_solve(igab_ctx *c, const void *dvals, int prec, const double *db
 void igab_krylov_release(igab_ctx *c);
 void igab_newton_release(igab_ctx *c);   /* igab_newton.cu */
 int igab_check_status(igab_ctx *c);      /* after a synchronisation: a bounded wait that gave up -> error */
+/* entry points without a periodic form return IGAB_ERR_UNSUPPORTED for such a mesh */
+#define IGAB_NO_PERIODIC(ctx, name)                                                                   \
+    do {                                                                                              \
+        if ((ctx) && (ctx)->per) {                                                                    \
+            igab_set_error("%s: not available for a mesh with periodic directions", name);           \
+            return IGAB_ERR_UNSUPPORTED;                                                              \
+        }                                                                                             \
+    } while (0)
+/* igab_periodic.cu: the owned system of a mesh with periodic directions */
+int igab_periodic_build(igab_ctx *c);
+int igab_periodic_set_dirichlet(igab_ctx *c, const std::vector<int> &rows, const std::vector<double> &g);
+int igab_periodic_residual(igab_ctx *c, const double *U_own, double *R_own);
+int igab_periodic_tangent(igab_ctx *c, const double *U_own, void *V_own, int prec);
+int igab_periodic_gather(igab_ctx *c, const double *U_own, double *U_loc);
+int igab_periodic_dirichlet_rows(igab_ctx *c, long *n, int *rows);
+void igab_periodic_release(igab_ctx *c);
+long igab_periodic_ndof(const igab_ctx *c);
+long igab_periodic_nnz(const igab_ctx *c);
+const std::vector<int> &igab_periodic_rowptr(const igab_ctx *c);
+const std::vector<int> &igab_periodic_cols(const igab_ctx *c);
 /* igab_mg.cu: multigrid-preconditioned CG (breakdown: p.Kp <= 0) or GMRES on the context's tangent */
 int igab_mg_solve(igab_ctx *c, int method, const void *vals, int prec, const double *b, double *x, double rtol,
                   double atol, int maxit, int *iterations, int *converged, double *rnorm, double *bnorm, int *breakdown);

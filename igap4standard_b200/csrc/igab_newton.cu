@@ -298,6 +298,7 @@ extern "C" void igab_newton_defaults(igab_newton_opts *o)
 extern "C" int igab_newton_solve(igab_ctx *ctx, double *U_dev, const igab_newton_opts *opts, igab_newton_info *info,
                                  double *fnorm_history, int *krylov_history, int history_cap)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_newton_solve");
     if (!ctx || !U_dev || !opts || !info) {
         igab_set_error("igab_newton_solve: null argument");
         return IGAB_ERR_ARG;

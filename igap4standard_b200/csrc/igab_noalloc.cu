@@ -46,6 +46,7 @@ static int stage_address(double **out)
 
 extern "C" int igab_residual_noalloc(igab_ctx *ctx, const double *U_host, double *R_host)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_residual_noalloc");
     if (!ctx || !U_host || !R_host) {
         igab_set_error("igab_residual_noalloc: null argument");
         return IGAB_ERR_ARG;

@@ -142,6 +142,7 @@ extern "C" void igab_transient_defaults(igab_transient_opts *o)
 extern "C" int igab_transient_run(igab_ctx *ctx, const igab_transient_opts *o, double *U_dev, const double *U_prev_dev,
                                   double *U_steps_host, igab_newton_info *step_info, igab_transient_info *info)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_transient_run");
     int rc = check_opts(ctx, o, "igab_transient_run");
     if (rc) return rc;
     if (!U_dev || !info) {
@@ -234,6 +235,7 @@ struct igab_tadj {
 
 extern "C" int igab_tadj_create(igab_ctx *ctx, const igab_transient_opts *o, int every, igab_tadj **out)
 {
+    IGAB_NO_PERIODIC(ctx, "igab_tadj_create");
     int rc = check_opts(ctx, o, "igab_tadj_create");
     if (rc) return rc;
     if (!out || every < 1 || o->nsteps < 1) {

@@ -111,8 +111,11 @@ static int create_state(IGA *app, int device, gpu_state **out)
     BC *bc = app->bc;
     int nproc = 1;
     MPI_Comm_size(MPI_COMM_WORLD, &nproc);
-    if (nproc != 1 || nurbs->nsendPart != 0 || nurbs->nrecvPart != 0) {
-        fprintf(stderr, "snesiga_b200: only single-rank, non-periodic meshes are supported\n");
+    int self_only = nproc == 1;
+    for (int i = 0; i < nurbs->nsendPart; i++) self_only = self_only && nurbs->sendPart[i] == 0;
+    for (int i = 0; i < nurbs->nrecvPart; i++) self_only = self_only && nurbs->recvPart[i] == 0;
+    if (!self_only) {
+        fprintf(stderr, "snesiga_b200: only single-rank meshes are supported (periodic directions included)\n");
         return PETSC_ERR_SUP;
     }
     if (phys->ndim != 3 || phys->ndof != 3 || nurbs->porder != 2 || (phys->torder != 0 && phys->torder != 2)) {
@@ -137,6 +140,9 @@ static int create_state(IGA *app, int device, gpu_state **out)
     memcpy(d.bc_type, bc->bc_type, 36 * sizeof(int));
     memcpy(d.par_periodic, bc->par_periodic, 9 * sizeof(double));
     memcpy(d.par_dirichlet, bc->par_dirichlet, 9 * sizeof(double));
+    /* one rank: a direction whose owned points number its elements is periodic
+     * (mesh/nurbs/nurbs_init.c:39) */
+    for (int i = 0; i < 3; i++) d.bc_periodic[i] = nurbs->nbasis[i] == nurbs->nelem[i];
     gpu_state *s = (gpu_state *)calloc(1, sizeof(gpu_state));
     if (!s) { free(knots); return PETSC_ERR_MEM; }
     int rc = igab_create(&d, device, &s->ctx);
@@ -493,10 +499,37 @@ PetscErrorCode snesiga_Tangent(SNES snes, Vec U_, Mat Tangent_, Mat Pmat_, void 
     return snesiga_b200_Tangent(snes, U_, Tangent_, Pmat_, app_);
 }
 
-/* Single-rank snesiga_init (src/snesiga_init.c:12-132 with nproc = 1 and
- * no halo parts): identity index maps, universal = local ordering, one
- * sequential AIJ matrix preallocated with the per-row count of
- * src/snesiga_init.c:341-359, callbacks installed. */
+/* the points of halo block b (0-6 = z, y, x, yz, xz, xy, xyz) on the local grid of
+ * nelem + p points per direction: along the block's directions the first p owned layers
+ * (send) or the p ghost layers after the owned ones (recv), all owned points along the
+ * others; dof indices in x, y, z, dof order (src/snesiga_init.c:186-330) */
+static int halo_block(const int nb[3], const int nel[3], int p, int ndof, int b, int recv, int *out)
+{
+    static const int dims[7] = {1, 2, 4, 3, 5, 6, 7};   /* bit 2: x, bit 1: y, bit 0: z */
+    int lo[3], hi[3];
+    for (int d = 0; d < 3; d++) {
+        const int in = (dims[b] >> (2 - d)) & 1;
+        lo[d] = in && recv ? nb[d] : 0;
+        hi[d] = in ? lo[d] + p : nb[d];
+    }
+    const int ny = nel[1] + p, nz = nel[2] + p;
+    int n = 0;
+    for (int x = lo[0]; x < hi[0]; x++)
+        for (int y = lo[1]; y < hi[1]; y++)
+            for (int z = lo[2]; z < hi[2]; z++)
+                for (int k = 0; k < ndof; k++) {
+                    if (out) out[n] = ndof * ((ny * nz) * x + nz * y + z) + k;
+                    n++;
+                }
+    return n;
+}
+
+/* Single-rank snesiga_init (src/snesiga_init.c:12-132 with nproc = 1): the rank's
+ * index maps (src/snesiga_init.c:134-330; along a periodic direction the halo
+ * blocks are messages to itself, so a ghost's global index is its owner's), universal
+ * = local ordering, one sequential AIJ matrix preallocated with the row lengths of
+ * the owned pattern (src/snesiga_init.c:341-359 plus the wrapped neighbours of a
+ * periodic direction), callbacks installed. */
 void snesiga_init(void *app_, void *phys_, void *nurbs_, void *bc_, void *snesassmbl_, void *iocomm_)
 {
     IGA *app = (IGA *)app_;
@@ -511,18 +544,37 @@ void snesiga_init(void *app_, void *phys_, void *nurbs_, void *bc_, void *snesas
     app->bc = (BC *)bc_;
     int nproc = 1;
     MPI_Comm_size(MPI_COMM_WORLD, &nproc);
-    if (nproc != 1 || nurbs->nsendPart != 0 || nurbs->nrecvPart != 0)
-        fprintf(stderr, "snesiga_b200: snesiga_init supports one rank without halo parts; callbacks will fail\n");
+    int self_only = nproc == 1;
+    for (int i = 0; i < nurbs->nsendPart; i++) self_only = self_only && nurbs->sendPart[i] == 0;
+    for (int i = 0; i < nurbs->nrecvPart; i++) self_only = self_only && nurbs->recvPart[i] == 0;
+    if (!self_only)
+        fprintf(stderr, "snesiga_b200: snesiga_init supports one rank (periodic directions as its own halo); "
+                        "callbacks will fail\n");
     int n = ndof * nb[0] * nb[1] * nb[2];
     app->nselfIdx = n;
     app->selfIdx = (int *)malloc((size_t)n * sizeof(int));
-    for (int i = 0; i < n; i++) app->selfIdx[i] = i;
-    app->nsendIdx = 0;
-    app->sendIdx = (int *)malloc(sizeof(int));
-    app->sendPtr = (int *)calloc(1, sizeof(int));
-    app->nrecvIdx = 0;
-    app->recvIdx = (int *)malloc(sizeof(int));
-    app->recvPtr = (int *)calloc(1, sizeof(int));
+    {
+        const int *nel = nurbs->nelem, ny = nel[1] + p, nz = nel[2] + p;
+        int ia = 0;
+        for (int x = 0; x < nb[0]; x++)
+            for (int y = 0; y < nb[1]; y++)
+                for (int z = 0; z < nb[2]; z++)
+                    for (int k = 0; k < ndof; k++) app->selfIdx[ia++] = ndof * ((ny * nz) * x + nz * y + z) + k;
+    }
+    app->sendPtr = (int *)calloc((size_t)nurbs->nsendPart + 1, sizeof(int));
+    app->recvPtr = (int *)calloc((size_t)nurbs->nrecvPart + 1, sizeof(int));
+    for (int i = 0; i < nurbs->nsendPart; i++)
+        app->sendPtr[i + 1] = app->sendPtr[i] + halo_block(nb, nurbs->nelem, p, ndof, nurbs->sendBlock[i], 0, NULL);
+    for (int i = 0; i < nurbs->nrecvPart; i++)
+        app->recvPtr[i + 1] = app->recvPtr[i] + halo_block(nb, nurbs->nelem, p, ndof, nurbs->recvBlock[i], 1, NULL);
+    app->nsendIdx = app->sendPtr[nurbs->nsendPart];
+    app->nrecvIdx = app->recvPtr[nurbs->nrecvPart];
+    app->sendIdx = (int *)malloc((size_t)(app->nsendIdx > 0 ? app->nsendIdx : 1) * sizeof(int));
+    app->recvIdx = (int *)malloc((size_t)(app->nrecvIdx > 0 ? app->nrecvIdx : 1) * sizeof(int));
+    for (int i = 0; i < nurbs->nsendPart; i++)
+        halo_block(nb, nurbs->nelem, p, ndof, nurbs->sendBlock[i], 0, app->sendIdx + app->sendPtr[i]);
+    for (int i = 0; i < nurbs->nrecvPart; i++)
+        halo_block(nb, nurbs->nelem, p, ndof, nurbs->recvBlock[i], 1, app->recvIdx + app->recvPtr[i]);
     io->nDof = n;
     io->nDof_array = (int *)malloc(sizeof(int));
     io->nDof_array[0] = n;
@@ -536,18 +588,23 @@ void snesiga_init(void *app_, void *phys_, void *nurbs_, void *bc_, void *snesas
     free(nurbs->universalIdx_temp);
     nurbs->universalIdx_temp = NULL;
     app->U_hist = (double *)malloc((size_t)(phys->torder + 1) * (size_t)n * sizeof(double));
-    app->globalIdx = (int *)malloc((size_t)n * sizeof(int));
-    for (int i = 0; i < n; i++) app->globalIdx[i] = i;
+    app->globalIdx = (int *)malloc((size_t)(n + app->nrecvIdx) * sizeof(int));
+    for (int i = 0; i < n; i++) app->globalIdx[app->selfIdx[i]] = i;
+    /* the blocks sent to itself come back in order: a ghost takes its owner's global index */
+    if (self_only && app->nsendIdx == app->nrecvIdx)
+        for (int i = 0; i < app->nrecvIdx; i++) app->globalIdx[app->recvIdx[i]] = app->globalIdx[app->sendIdx[i]];
     VecCreateMPI(MPI_COMM_WORLD, n, n, &sa->Residual_);
     VecDuplicate(sa->Residual_, &sa->U);
     int *d_nz = (int *)malloc((size_t)n * sizeof(int));
     int ia = 0;
+    int per[3];
+    for (int d = 0; d < 3; d++) per[d] = nb[d] == nurbs->nelem[d];   /* owned = elements: periodic */
     for (int x = 0; x < nb[0]; x++)
         for (int y = 0; y < nb[1]; y++)
             for (int z = 0; z < nb[2]; z++) {
-                int cx = (x < p ? x : p) + 1 + (x > nb[0] - 1 - p ? nb[0] - 1 - x : p);
-                int cy = (y < p ? y : p) + 1 + (y > nb[1] - 1 - p ? nb[1] - 1 - y : p);
-                int cz = (z < p ? z : p) + 1 + (z > nb[2] - 1 - p ? nb[2] - 1 - z : p);
+                int cx = per[0] ? (nb[0] < 5 ? nb[0] : 5) : (x < p ? x : p) + 1 + (x > nb[0] - 1 - p ? nb[0] - 1 - x : p);
+                int cy = per[1] ? (nb[1] < 5 ? nb[1] : 5) : (y < p ? y : p) + 1 + (y > nb[1] - 1 - p ? nb[1] - 1 - y : p);
+                int cz = per[2] ? (nb[2] < 5 ? nb[2] : 5) : (z < p ? z : p) + 1 + (z > nb[2] - 1 - p ? nb[2] - 1 - z : p);
                 for (int d = 0; d < ndof; d++) d_nz[ia++] = ndof * cx * cy * cz;
             }
     MatCreateAIJ(MPI_COMM_WORLD, n, n, n, n, 0, d_nz, 0, NULL, &sa->Tangent_);

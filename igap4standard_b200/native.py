@@ -98,6 +98,7 @@ class IgabMeshDesc(ctypes.Structure):
         ("bc_type", ctypes.c_int * 36),
         ("par_periodic", ctypes.c_double * 9),
         ("par_dirichlet", ctypes.c_double * 9),
+        ("bc_periodic", ctypes.c_int * 3),
     ]
 
 
@@ -217,6 +218,8 @@ DROPIN_API = [
 
 CASE_API = [
     ("iga_case_create", vp, [ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int]),
+    ("iga_case_create_periodic", vp, [ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int, vp]),
+    ("iga_case_index_maps", ctypes.c_int, [vp, vp, vp, vp, vp, vp]),
     ("iga_case_destroy", None, [vp]),
     ("iga_case_ndof", ctypes.c_int, [vp]),
     ("iga_case_set_history", ctypes.c_int, [vp, ctypes.c_int, vp]),

@@ -32,6 +32,18 @@ iga_case *iga_case_create(int phys_kind, const int nelem[3], const double *knots
                           const double par_mat[9], const int bc_type[36],
                           const double par_periodic[9], const double par_dirichlet[9],
                           const double *par_neumann, int n_par_neumann);
+/* the same with periodic directions (bc_periodic[d] = 1): the knot vector of such a
+ * direction is the uniform extension of mesh/nurbs/nurbs_genuniform.c:40-43 (nelem[d]+5
+ * values), the rank owns nelem[d] points along it and exchanges the two ghost layers
+ * with itself (mesh/nurbs/nurbs_init.c:24-39, :156-199 with npart = 1). */
+iga_case *iga_case_create_periodic(int phys_kind, const int nelem[3], const double *knots,
+                                   const double par_mat[9], const int bc_type[36],
+                                   const double par_periodic[9], const double par_dirichlet[9],
+                                   const double *par_neumann, int n_par_neumann, const int bc_periodic[3]);
+/* the rank's index maps as snesiga_init left them (src/snesiga_init.c:42-50, :84-110):
+ * counts into n[3] = {nselfIdx, nsendIdx, nrecvIdx}; arrays (either may be NULL) of
+ * nselfIdx, nsendIdx, nrecvIdx and nselfIdx + nrecvIdx ints */
+int  iga_case_index_maps(const iga_case *c, int n[3], int *selfIdx, int *sendIdx, int *recvIdx, int *globalIdx);
 void iga_case_destroy(iga_case *c);
 
 int  iga_case_ndof(const iga_case *c);

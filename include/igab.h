@@ -50,12 +50,27 @@ enum igab_prec { IGAB_PREC_FP64 = 0, IGAB_PREC_FP32 = 1 };
 typedef struct {
     int phys;                 /* igab_phys */
     int nelem[3];             /* elements per direction */
-    const double *knots;      /* 3 open knot vectors back to back, nelem[d]+5 values each */
+    const double *knots;      /* 3 knot vectors back to back, nelem[d]+5 values each (open, or the
+                                 uniform extension of mesh/nurbs/nurbs_genuniform.c:40-43 along a
+                                 periodic direction) */
     double par_mat[9];        /* {r, curv, e0, e345, le, rho, cii, dt, t} (phys/ge/init.c:17-18) */
     int bc_type[36];          /* [face][order][dof], 0 Dirichlet, 1 Neumann (include/bc.h:6) */
     double par_periodic[9];   /* affine F0 added at Gauss points (src/snesiga_Residual.c:140-144) */
     double par_dirichlet[9];  /* affine map of the Dirichlet values (src/iga_dirichlet.c:10-12) */
+    int bc_periodic[3];       /* 1: the direction is periodic (nelem[d] >= 3 control points owned, no
+                                 boundary faces; mesh/nurbs/nurbs_init.c:24-39 on one rank) */
 } igab_mesh_desc;
+
+/* Periodic directions (one rank).  The mesh owns nelem[d] control points along a periodic
+ * direction (nelem[d] + 2 otherwise); dofs, the residual, the AIJ pattern (rows and columns
+ * of every pair of owned points that share an element, ascending) and the tangent values
+ * are in that owned numbering.  The kernels assemble on the local grid of nelem[d] + 2
+ * points per direction, whose last two along a periodic direction are the ghosts of owned
+ * points 0 and 1 (the halo the reference exchanges with itself, src/snesiga_Residual.c:54-74);
+ * the ghost rows and columns are then added into their owners in a fixed order, and the
+ * Dirichlet rows of the non-periodic faces applied on the owned system.  A periodic mesh
+ * takes igab_residual[_device], igab_tangent[_device], igab_set_history, the pattern and
+ * parameter calls; the other entry points return IGAB_ERR_UNSUPPORTED for it. */
 
 /* ---- lifetime */
 int igab_create(const igab_mesh_desc *desc, int device, igab_ctx **out);

@@ -1,8 +1,8 @@
 /*
- * Geometric multigrid on nested spline spaces, as the preconditioner of a conjugate
- * gradient solve with the assembled tangent (no reference counterpart: it stands in
- * for the PETSc KSP of the reference application, src/snes_init.c:24-39, which is
- * outside the assembly path).
+ * Geometric multigrid on nested spline spaces, as the preconditioner of a GMRES or
+ * conjugate gradient solve with the assembled tangent (no reference counterpart: it
+ * stands in for the PETSc KSP of the reference application, src/snes_init.c:24-39,
+ * which is outside the assembly path).
  *
  * Why: the phys/ge tangent is a fourth-order operator (the strain-gradient term
  * le^2 |grad grad u|^2), so its condition number grows like h^-4; Jacobi-preconditioned
@@ -26,10 +26,20 @@
  * estimated by power iteration; the same polynomial before and after the coarse
  * correction, so the V-cycle is a symmetric preconditioner and CG applies.
  *
- * The coarse levels are rebuilt when the material, the boundary tables' values or
- * the element scales change (the context's parameter version); the fine level's
- * diagonal and lmax are recomputed at every solve (the tangent changes per Newton step).
- * Every dot product is a fixed-order reduction: solves are bitwise repeatable.
+ * Coarsest level: its tangent (symmetric positive definite: the zero-state tangent with
+ * unit Dirichlet rows and columns) is inverted on the device by Gauss-Jordan elimination
+ * without pivoting, one launch per pivot, and each V-cycle applies the inverse as a dense
+ * product with a fixed summation order (no host round trip).  A pivot that is not
+ * positive and finite (an unstable material) falls back to a dense LU with partial
+ * pivoting on the host.
+ *
+ * Operators: every level's is the tangent at the zero state (the fine one in FP32, the
+ * coarse ones in FP64), symmetric positive definite for a stable material, so the V-cycle
+ * does not depend on the Newton iterate.  The hierarchy is rebuilt when the material, the
+ * boundary tables' values or the element scales change (the context's parameter
+ * version).  Every dot product is a fixed-order reduction: solves are bitwise repeatable.
+ * Measured and rejected: the smoothing operators stored in half precision (64^3: 4.58 ->
+ * 4.36 ms per GMRES iteration, but one more iteration per solve; no gain per Newton step).
  */
 #include <algorithm>
 #include <cmath>
@@ -241,11 +251,15 @@ struct igab_mg {
     int nlev = 0;
     mg_level L[MG_MAX_LEVELS];
     long version = -1;
-    bool direct = false;            /* coarsest level solved by dense LU */
+    bool direct = false;            /* coarsest level solved directly */
+    bool dev_inv = false;           /* by the device inverse (else by the host LU) */
     int nd = 0;                     /* its size */
     std::vector<double> lu;
     std::vector<int> piv;
     double *h_vec = nullptr;        /* pinned nd doubles */
+    double *inv = nullptr;          /* nd x nd inverse of the coarsest tangent (row-major) */
+    double *gj = nullptr;           /* Gauss-Jordan pivot row and column buffers, 2 x 2 x nd */
+    int *gj_flag = nullptr;         /* set by a pivot that is not positive and finite */
     double *part = nullptr, *dots = nullptr, *h_dots = nullptr;
     double *zero = nullptr;         /* zero state (fine size) */
     long zero_n = 0;
@@ -286,6 +300,9 @@ void mg_free(igab_mg *m)
     cudaFree(m->mpart);
     cudaFreeHost(m->h_md);
     cudaFreeHost(m->h_vec);
+    cudaFree(m->inv);
+    cudaFree(m->gj);
+    cudaFree(m->gj_flag);
     cudaFreeHost(m->h_dots);
     delete m;
 }
@@ -462,13 +479,68 @@ void zero_dirichlet(igab_mg *m, mg_level &L, double *v)
     }
 }
 
+/* A (row-major n x n) from the structured CSR of the coarsest level: one thread per row */
+__global__ void k_mg_dense(int n, const int *__restrict__ rowptr, const int *__restrict__ cols,
+                           const double *__restrict__ vals, double *__restrict__ A)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    for (int k = rowptr[r]; k < rowptr[r + 1]; k++) A[(size_t)r * n + cols[k]] = vals[k];
+}
+
+/* pivot row and column 0 into the step buffers */
+__global__ void k_mg_gj_init(int n, const double *__restrict__ A, double *__restrict__ row, double *__restrict__ col)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    row[i] = A[i];
+    col[i] = A[(size_t)i * n];
+}
+
+/* Gauss-Jordan step k in place (row-major A), from the old pivot row / column (row, col);
+ * writes row / column k + 1 of the result into (nrow, ncol) for the next step.  Each
+ * entry is computed by one thread from the old values only. */
+__global__ void k_mg_gj_step(int n, int k, double *__restrict__ A, const double *__restrict__ row,
+                             const double *__restrict__ col, double *__restrict__ nrow, double *__restrict__ ncol,
+                             int *__restrict__ flag)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= n || j >= n) return;
+    const double p = col[k];
+    if (i == k && j == k && !(p > 0.0 && isfinite(p))) *flag = 1;
+    const double ip = 1.0 / p;
+    double v;
+    if (i == k) v = j == k ? ip : row[j] * ip;
+    else if (j == k) v = -col[i] * ip;
+    else v = A[(size_t)i * n + j] - col[i] * (row[j] * ip);
+    A[(size_t)i * n + j] = v;
+    if (i == k + 1) nrow[j] = v;
+    if (j == k + 1) ncol[i] = v;
+}
+
+/* x = Ainv b: one warp per row, lane-strided partial sums then a fixed shuffle tree */
+__global__ void k_mg_gemv(long n, const double *__restrict__ Ai, const double *__restrict__ b, double *__restrict__ x)
+{
+    const long r = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= n) return;
+    double s = 0.0;
+    for (long j = lane; j < n; j += 32) s += Ai[r * n + j] * b[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) x[r] = s;
+}
+
 /* x_l = V-cycle approximation of K_l^-1 b_l (b in L.b, result in L.x) */
 int vcycle(igab_mg *m, int l)
 {
     mg_level &L = m->L[l];
     cudaStream_t st = L.ctx->stream;
     if (l == m->nlev - 1) {
-        if (m->direct) {
+        if (m->direct && m->dev_inv) {
+            k_mg_gemv<<<(unsigned)((L.n + 7) / 8), 256, 0, st>>>(L.n, m->inv, L.b, L.x);
+            m->launches++;
+        } else if (m->direct) {
             IGAB_CUDA_TRY(cudaMemcpyAsync(m->h_vec, L.b, (size_t)L.n * sizeof(double), cudaMemcpyDeviceToHost, st));
             IGAB_CUDA_TRY(cudaStreamSynchronize(st));
             lu_solve(m->nd, m->lu, m->piv, m->h_vec);
@@ -623,9 +695,53 @@ int mg_build(igab_ctx *c, igab_mg *m)
         IGAB_CUDA_TRY(cudaGetLastError());
         if ((rc = estimate_lmax(m, C))) return rc;
     }
-    /* the coarsest level directly, when small */
+    /* the coarsest level directly, when small: the device inverse */
     mg_level &B = m->L[m->nlev - 1];
+    m->dev_inv = false;
     if (m->nlev > 1 && B.n <= MG_COARSE_DOF) {
+        igab_ctx *cc = B.ctx;
+        const int n = (int)B.n;
+        cudaFree(m->inv);
+        cudaFree(m->gj);
+        m->inv = nullptr;
+        m->gj = nullptr;
+        IGAB_CUDA_TRY(cudaMalloc((void **)&m->inv, (size_t)n * n * sizeof(double)));
+        IGAB_CUDA_TRY(cudaMalloc((void **)&m->gj, (size_t)4 * n * sizeof(double)));
+        if (!m->gj_flag) IGAB_CUDA_TRY(cudaMalloc((void **)&m->gj_flag, sizeof(int)));
+        int *dcols = nullptr;
+        IGAB_CUDA_TRY(cudaMalloc((void **)&dcols, (size_t)cc->nnz * sizeof(int)));
+        int rc = igab_launch_csr_cols(cc, dcols);
+        if (!rc) {
+            cudaStream_t st = c->stream;
+            cudaError_t e = cudaMemsetAsync(m->inv, 0, (size_t)n * n * sizeof(double), st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(m->gj_flag, 0, sizeof(int), st);
+            if (e == cudaSuccess) {
+                k_mg_dense<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, cc->d_rowptr, dcols, B.own_vals, m->inv);
+                k_mg_gj_init<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, m->inv, m->gj, m->gj + n);
+                const dim3 grid((unsigned)((n + 15) / 16), (unsigned)((n + 15) / 16)), blk(16, 16);
+                for (int k = 0; k < n; k++) {
+                    double *rk = m->gj + (size_t)(k & 1) * 2 * n, *nx = m->gj + (size_t)((k + 1) & 1) * 2 * n;
+                    k_mg_gj_step<<<grid, blk, 0, st>>>(n, k, m->inv, rk, rk + n, nx, nx + n, m->gj_flag);
+                }
+                e = cudaGetLastError();
+            }
+            int flag = 1;
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, m->gj_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) {
+                igab_set_error("multigrid coarse inverse: %s", cudaGetErrorString(e));
+                rc = IGAB_ERR_CUDA;
+            } else if (!flag) {
+                m->dev_inv = true;
+            }
+        }
+        cudaFree(dcols);
+        if (rc) return rc;
+    }
+    if (m->nlev > 1 && B.n <= MG_COARSE_DOF && m->dev_inv) {
+        m->direct = true;
+        m->nd = (int)B.n;
+    } else if (m->nlev > 1 && B.n <= MG_COARSE_DOF) {   /* not positive definite: host LU */
         igab_ctx *cc = B.ctx;
         const int n = (int)B.n;
         std::vector<int> cols((size_t)cc->nnz);

@@ -307,7 +307,7 @@ int igab_solve_device(igab_ctx *ctx, const void *vals_dev, int prec, const doubl
  * prolongation by knot insertion, all levels' operators the tangent at the zero state with
  * the context's material and (averaged) element scales (symmetric positive definite for a
  * stable material, so the V-cycle is an SPD preconditioner whatever the current state),
- * Chebyshev smoothing (degree 3 in D^-1 K), a dense LU on the coarsest level.  The hierarchy
+ * Chebyshev smoothing (degree 3 in D^-1 K), the coarsest level by its inverse (Gauss-Jordan on the device).  The hierarchy
  * is built on the first call and rebuilt after igab_set_par_mat / igab_set_par_periodic /
  * igab_set_element_log_scale.  method: IGAB_KSP_MG_GMRES (right-preconditioned GMRES(50),
  * any nonsingular tangent) or IGAB_KSP_MG_CG (CG, symmetric positive definite tangents; a

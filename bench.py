@@ -455,15 +455,15 @@ def bench_newton_config1(args, device):
     return out
 
 
-def bench_adjoint_static(args, device):
-    """Config 4 (static) end to end at 32^3: per-element stiffness scales s_e = exp(g_e),
-    g ~ N(0, 0.3^2) (32,768 parameters, seed 4); J = 1/2 sum over the control points of face
-    x = 1 of |U - U*|^2 with U* the solution at g* (seed 5).  One gradient = the forward
-    Newton solve at g (device), the tangent at the solution, the adjoint solve K^T lam =
-    dJ/dU (device multigrid GMRES; K is symmetric), then dJ/dg = -lam . dR/dg (igab_adjoint_backward)."""
+def bench_adjoint_static(args, device, n=32):
+    """Config 4 (static) end to end at n^3 (32^3 in the config; 64^3 for the metric's mesh):
+    per-element stiffness scales s_e = exp(g_e), g ~ N(0, 0.3^2) (seed 4); J = 1/2 sum over
+    the control points of face x = 1 of |U - U*|^2 with U* the solution at g* (seed 5).  One
+    gradient = the forward Newton solve at g (device), the tangent at the solution, the
+    adjoint solve K^T lam = dJ/dU (device multigrid GMRES; K is symmetric), then
+    dJ/dg = -lam . dR/dg (igab_adjoint_backward)."""
     import torch
     from igap4standard_b200 import Assembly, mesh
-    n = 32
     nelem = (n, n, n)
     kn = mesh.knots_for(nelem, perturb=0.1, seed=1)
     pm = mesh.par_mat_from_lame(1.0, 1.0, 0.1)
@@ -507,7 +507,7 @@ def bench_adjoint_static(args, device):
         gradient(g)                       # warm-up (graph captures, workspaces)
         grad, J, fwd, its, ok, tf, tb = gradient(g)
     A.set_element_log_scale(None)
-    out = {"parameters": ne, "grads_per_s": round(1.0 / (tf + tb), 4), "forward_s": round(tf, 3),
+    out = {"mesh": [n, n, n], "parameters": ne, "grads_per_s": round(1.0 / (tf + tb), 4), "forward_s": round(tf, 3),
            "adjoint_s": round(tb, 3), "forward_newton_iterations": fwd["iterations"],
            "forward_krylov_iterations": fwd["krylov_iterations"], "forward_fnorm": fwd["fnorm"],
            "adjoint_krylov_iterations": its, "adjoint_converged": bool(ok), "J": J,
@@ -768,6 +768,7 @@ def run_ours(args):
     trans_adj = bench_transient_adjoint(args, local) if args.transient_adjoint > 0 else None
     newton1 = None if args.no_newton else bench_newton_config1(args, local)
     adj_static = None if args.no_adjoint_static else bench_adjoint_static(args, local)
+    adj_static64 = None if args.no_adjoint_static else bench_adjoint_static(args, local, n=64)
 
     # ---- roofline of the dominant kernel (tangent volume, 8 colour launches per step)
     tan_ms = k64[2]
@@ -824,6 +825,7 @@ def run_ours(args):
             "intdensity": dens, "knot_insert": knot,
             "schedule": schedule, "batch_config3": batch, "transient_config2": trans,
             "transient_adjoint_config4": trans_adj, "newton_config1": newton1, "adjoint_config4_e2e": adj_static,
+            "adjoint_64cubed_e2e": adj_static64,
             "clocks": clk, "gpu_launches": int(launches64), "roofline": roofline,
             "roofline_mixed": roofline_mixed,
             "peaks_measured": {"fp64_tflops": round(peak64_fma, 2), "fp64_dmma_tflops": round(peak64_dmma, 2), "fp32_tflops": round(peak32, 2),

@@ -14,12 +14,13 @@
  *   E = Y_hi^T Y_hi + Y_hi^T (2 Y_lo),   Y^T Y = (E + E^T)/2 + O(2^-22),
  * so the symmetric part taken at read-out recovers the cross term Y_lo^T Y_hi.
  * The geometric block, identical for the three displacement components, is
- *   Gamma(a,b) = sum_q sum_m,n N_a^m (w geo_q)[m][n] N_b^n = sum_q sum_i U_qi[a] V_qi[b]
- * with six rows per point (geo = [[S, T], [T^T, 0]], S the 3x3 first-derivative
- * block, T the 3x6 coupling to second derivatives):
- *   U_i = d_i N_a,  V_i = (S grad N_a)_i + (T H_a)_i        (i < 3)
- *   U_i = (T H_a)_I, V_i = d_I N_a                          (i = 3 + I)
- * and three MMAs per k-step (hi hi, hi lo, lo hi).
+ *   Gamma(a,b) = sum_q [grad N_a^T S grad N_b + grad N_a . (T H_b) + (T H_a) . grad N_b]
+ * (geo = [[S, T], [T^T, 0]], S the 3x3 first-derivative block, T the coupling to the
+ * second derivatives H): 27 x 27 entries, computed on the FP32 FMA pipe by sum
+ * factorisation, three contractions (z, y, x) of its 15 derivative-pair terms with the
+ * 1-D tables, intermediates in the free operand stages at the element's start.  (Built
+ * as six U / V operand rows per point it took twelve tcgen05 chunks per element whose
+ * construction cost more than the whole contraction does here: 64^3 59.7 -> 55.1 ms.)
  *
  * Work per CTA: a 2x2x2 tile of elements of one of the 8 colours (the scatter
  * is conflict-free within a colour).  Warps 0-8 build, warp 9 issues MMAs.
@@ -31,13 +32,11 @@
  * builder thread's 9 outputs are 1024 bytes apart) and hand each to the issuer
  * through an mbarrier.  The issuer
  * runs 4 k-steps x 2 MMAs (M 128, N 96; negate-A for negative-curvature rows)
- * or x 3 (M 128, N 32, Gamma rows) per chunk and commits to the stage's
- * mbarrier, which frees the stage for the chunk after next.  An element
- * accumulates in two tensor-memory accumulators per class, by chunk parity:
- * about 96 accumulating MMAs each, 5e-6 rowwise agreement with the FP64
- * reference (one accumulator for all 192 gave 1e-5).  Tensor memory: 256
- * columns per CTA (element matrix 2 x 96, Gamma 2 x 32); at most two CTAs per
- * SM.  Rows 81-127 of the M side and columns 81-95 of the N side read whatever
+ * per chunk and commits to the stage's mbarrier, which frees the stage for the
+ * chunk after next.  An element accumulates in two tensor-memory accumulators,
+ * by chunk parity: about 96 accumulating MMAs each, 5e-6 rowwise agreement with
+ * the FP64 reference (one accumulator for all 192 gave 1e-5).  Tensor memory:
+ * 256 columns per CTA (element matrix 2 x 96); at most two CTAs per SM.  Rows 81-127 of the M side and columns 81-95 of the N side read whatever
  * lies behind the operand in the stage; they only feed accumulator rows and
  * columns that are never read.  At the end of an element the builders sum the
  * accumulators into shared memory, release them to the issuer, take the
@@ -55,13 +54,8 @@ namespace {
 #define TC_BAR_BLD 1           /* named barrier of the builder warps */
 #define TC_STAGE 24576         /* bytes per operand stage */
 #define TC_MAIN_LO 11264       /* 2 Y_lo after Y_hi (11 groups of 8 rows) */
-#define TC_G_ULO 4096          /* Gamma chunk: U_hi 0, U_lo, V_hi, V_lo (4 groups each) */
-#define TC_G_VHI 8192
-#define TC_G_VLO 12288
 #define TC_TMEM_COLS 256u
 #define TC_COL_MAIN 0u         /* two 96-column element-matrix accumulators */
-#define TC_COL_GAM 192u        /* two 32-column Gamma accumulators */
-#define TC_NGCHUNK 12          /* 64 points x 6 Gamma rows / 32 */
 
 /* float point data per Gauss point */
 #define TP_F 0      /* F[k][J], 9 */
@@ -77,7 +71,8 @@ template <int TE>
 struct tc_smem {
     static constexpr int TC = TE + 2;
     static constexpr int NCP = TC * TC * TC;
-    unsigned char stage[2][TC_STAGE];   /* operand stages; E and Gamma staging at read-out */
+    unsigned char stage[2][TC_STAGE];   /* operand stages; the geometric block's intermediates at an
+                                           element's start, E staging at read-out */
     double A[972];                      /* interpolation temporaries */
     double C[864];
     double U[NCP * 3];
@@ -97,11 +92,39 @@ struct tc_smem {
     unsigned long long done[2];         /* MMAs of the chunk in stage / accumulator b completed (commit) */
     unsigned long long freed;           /* the element's accumulators read out (288 builder arrivals) */
     unsigned long long drain;           /* issuer: every MMA it issued has completed */
-    int ckind[2];                       /* chunk in stage b: 0 positive rows, 1 negative rows, 2 Gamma,
+    float gam[27 * 27];                 /* the element's geometric block (sum-factorised, FP32) */
+    int ckind[2];                       /* chunk in stage b: 0 positive rows, 1 negative rows,
                                            3 end of tile; + 4 on an element's first chunk */
     unsigned int tmem_base;
     int abort_flag;
 };
+
+/* the 15 terms of the geometric block Gamma = sym(P),
+ *   P(a,b) = sum_q [ sum_{I<=J} c_IJ d_I N_a d_J N_b + 2 sum_{I,K} T_IK d_I N_a d_I d_K N_b ],
+ * c_II = S_II, c_IJ = 2 S_IJ (I < J): term t's derivative order along axis d on the a side
+ * (side 0) and the b side (side 1), and its coefficient at a point */
+__device__ __forceinline__ int g_ord(int t, int side, int d)
+{
+    if (t < 3) return d == t;
+    if (t < 6) {
+        const int p = t - 3, i0 = p < 2 ? 0 : 1, j0 = p == 0 ? 1 : 2;
+        return side == 0 ? d == i0 : d == j0;
+    }
+    const int I = (t - 6) / 3, K = (t - 6) % 3;
+    return side == 0 ? d == I : (d == I) + (d == K);
+}
+
+__device__ __forceinline__ float g_coef(const float *p, int t)
+{
+    if (t < 3) return p[TP_S + t];
+    if (t < 6) return 2.f * p[TP_S + t];   /* S01, S02, S12 */
+    return 2.f * p[TP_T + (t - 6)];        /* T[I][K] */
+}
+
+__device__ __forceinline__ float g_sel(float4 v, int ord)
+{
+    return ord == 0 ? v.x : (ord == 1 ? v.y : v.z);
+}
 
 /* eigen-rotation of [[a, b], [b, c]]: [[a,b],[b,c]] = l1 e1 e1^T + l2 e2 e2^T,
  * e1 = (cs, -sn), e2 = (sn, cs) (same convention as the FP64 tensor kernel) */
@@ -236,7 +259,7 @@ __device__ __forceinline__ void tc_release(tc_smem<TE> &S, tc_state &Q, int *sta
 
 /* the issuer warp for one tile: wait for each built chunk and issue its MMAs.
  * An element's chunks accumulate in two tensor-memory accumulators by chunk
- * parity (element matrix: 96 columns each, Gamma: 32 each); negative-curvature
+ * parity (96 columns each); negative-curvature
  * chunks use the negate-A form.  Before the first MMA of an element the issuer
  * waits until the builders have read the previous element's accumulators.  Ends
  * at the builders' end-of-tile chunk; before returning it waits (bounded) until
@@ -247,7 +270,7 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
     const int lane = threadIdx.x & 31;
     const volatile int *abort = &S.abort_flag;
     bool ok = !*abort;
-    bool started[2][2] = {{false, false}, {false, false}};   /* [element matrix / Gamma][accumulator] */
+    bool started[2] = {false, false};   /* accumulator b holds this element's sums */
     while (ok) {
         const int b = Q.gc & 1;
         if (lane == 0) ok = tc_mbar_wait_abortable(&S.full[b], Q.ph_full[b], abort);
@@ -267,37 +290,22 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
                 if (!ok) break;
             }
             Q.nelem++;
-            started[0][0] = started[0][1] = started[1][0] = started[1][1] = false;
+            started[0] = started[1] = false;
         }
         const int kind = ck & 3;
-        const int cls = kind == 2 ? 1 : 0;
-        const uint32_t acc0 = started[cls][b] ? 1u : 0u;
-        started[cls][b] = true;
+        const uint32_t acc0 = started[b] ? 1u : 0u;
+        started[b] = true;
         if (lane == 0) {
             tc_fence_after_sync();
             const uint32_t sb = tc_smem_u32(S.stage[b]);
-            if (kind < 2) {
-                const uint32_t idm = kind == 0 ? tc_idesc_tf32(128, 96) : tc_idesc_tf32(128, 96, true);
-                const uint32_t d = Q.tmem + TC_COL_MAIN + (uint32_t)b * 96u;
+            const uint32_t idm = kind == 0 ? tc_idesc_tf32(128, 96) : tc_idesc_tf32(128, 96, true);
+            const uint32_t d = Q.tmem + TC_COL_MAIN + (uint32_t)b * 96u;
 #pragma unroll
-                for (int kk = 0; kk < 4; kk++) {
-                    const uint64_t ah = tc_sdesc(sb + kk * TC_KSTEP_BYTES);
-                    const uint64_t bl = tc_sdesc(sb + TC_MAIN_LO + kk * TC_KSTEP_BYTES);
-                    tc_mma_tf32(d, ah, ah, idm, kk == 0 ? acc0 : 1u);
-                    tc_mma_tf32(d, ah, bl, idm, 1u);
-                }
-            } else {
-                constexpr uint32_t idg = tc_idesc_tf32(128, 32);
-                const uint32_t d = Q.tmem + TC_COL_GAM + (uint32_t)b * 32u;
-#pragma unroll
-                for (int kk = 0; kk < 4; kk++) {
-                    const uint32_t o = kk * TC_KSTEP_BYTES;
-                    const uint64_t uh = tc_sdesc(sb + o), ul = tc_sdesc(sb + TC_G_ULO + o);
-                    const uint64_t vh = tc_sdesc(sb + TC_G_VHI + o), vl = tc_sdesc(sb + TC_G_VLO + o);
-                    tc_mma_tf32(d, uh, vh, idg, kk == 0 ? acc0 : 1u);
-                    tc_mma_tf32(d, uh, vl, idg, 1u);
-                    tc_mma_tf32(d, ul, vh, idg, 1u);
-                }
+            for (int kk = 0; kk < 4; kk++) {
+                const uint64_t ah = tc_sdesc(sb + kk * TC_KSTEP_BYTES);
+                const uint64_t bl = tc_sdesc(sb + TC_MAIN_LO + kk * TC_KSTEP_BYTES);
+                tc_mma_tf32(d, ah, ah, idm, kk == 0 ? acc0 : 1u);
+                tc_mma_tf32(d, ah, bl, idm, 1u);
             }
             tc_commit(&S.done[b]);
         }
@@ -316,10 +324,8 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
 
 /* Sum the element's accumulators into shared memory (FP32, round to nearest):
  * element-matrix rows by warps 0-2 / 4-6 (TMEM lanes = rows 0-95, columns
- * 0-47 / 48-95), Gamma rows by warp 8 (lanes 0-31, 32 columns).  used[c][b]:
- * accumulator b of class c (element matrix, Gamma) holds this element's sums. */
-__device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2][2], int warp, int lane, float *E,
-                                           float *Gm)
+ * 0-47 / 48-95).  used[b]: accumulator b holds this element's sums (none: zeros). */
+__device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2], int warp, int lane, float *E)
 {
     if (warp < 8) {
         if (warp == 3 || warp == 7) return;   /* lanes 96-127: rows beyond 80 */
@@ -332,7 +338,7 @@ __device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2][
             for (int i = 0; i < 16; i++) s[i] = 0.f;
 #pragma unroll
             for (int b = 0; b < 2; b++) {
-                if (!used[0][b]) continue;   /* warp-uniform */
+                if (!used[b]) continue;   /* warp-uniform */
                 float v[16];
                 tc_ld16(tmem + ((uint32_t)lb << 16) + TC_COL_MAIN + (uint32_t)b * 96u + (uint32_t)c0, v);
 #pragma unroll
@@ -342,25 +348,6 @@ __device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2][
 #pragma unroll
                 for (int i = 0; i < 16; i++)
                     if (c0 + i < 81) E[row * 81 + c0 + i] = s[i];
-        }
-    } else {
-#pragma unroll 1
-        for (int part = 0; part < 2; part++) {
-            float s[16];
-#pragma unroll
-            for (int i = 0; i < 16; i++) s[i] = 0.f;
-#pragma unroll
-            for (int b = 0; b < 2; b++) {
-                if (!used[1][b]) continue;
-                float v[16];
-                tc_ld16(tmem + TC_COL_GAM + (uint32_t)b * 32u + 16u * part, v);
-#pragma unroll
-                for (int i = 0; i < 16; i++) s[i] += v[i];
-            }
-            if (lane < 27)
-#pragma unroll
-                for (int i = 0; i < 16; i++)
-                    if (16 * part + i < 27) Gm[lane * 27 + 16 * part + i] = s[i];
         }
     }
 }
@@ -544,7 +531,55 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         tc_bar_sync(TC_BAR_BLD, TCN_BLD);
         const int npos = S.cnt[0], nneg = S.cnt[1];
         const int cpos = (npos + TC_KC - 1) / TC_KC, cneg = (nneg + TC_KC - 1) / TC_KC;
-        const int nch = cpos + cneg + TC_NGCHUNK;
+        const int nch = cpos + cneg;
+
+        /* ---- geometric block by sum factorisation (FP32 FMA pipe): z, y, x contractions of
+         * the 15 terms, intermediates in the (free) operand stages */
+        {
+            float *Zs = reinterpret_cast<float *>(S.stage[0]);   /* [15][16 (qx,qy)][9 (az,bz)] */
+            float *Ys = Zs + 2160;                               /* [15][4 qx][81 (ay,by,az,bz)] */
+            for (int o = tid; o < 2160; o += TCN_BLD) {
+                const int t = o / 144, rem = o % 144, qxy = rem / 9, azbz = rem % 9;
+                const int qx = qxy & 3, qy = qxy >> 2, az = azbz / 3, bz = azbz % 3;
+                const int oa = g_ord(t, 0, 2), ob = g_ord(t, 1, 2);
+                float s = 0.f;
+#pragma unroll
+                for (int qz = 0; qz < 4; qz++) {
+                    const int q = 16 * qz + 4 * qy + qx;
+                    s += g_coef(S.pt[q], t) * g_sel(S.tabf[2][lez][qz][az], oa) * g_sel(S.tabf[2][lez][qz][bz], ob);
+                }
+                Zs[o] = s;
+            }
+            tc_bar_sync(TC_BAR_BLD, TCN_BLD);
+            for (int o = tid; o < 4860; o += TCN_BLD) {
+                const int t = o / 324, rem = o % 324, qx = rem / 81, r2 = rem % 81, ayby = r2 / 9, azbz = r2 % 9;
+                const int ay = ayby / 3, by = ayby % 3;
+                const int oa = g_ord(t, 0, 1), ob = g_ord(t, 1, 1);
+                float s = 0.f;
+#pragma unroll
+                for (int qy = 0; qy < 4; qy++)
+                    s += g_sel(S.tabf[1][ley][qy][ay], oa) * g_sel(S.tabf[1][ley][qy][by], ob) *
+                         Zs[t * 144 + (4 * qy + qx) * 9 + azbz];
+                Ys[o] = s;
+            }
+            tc_bar_sync(TC_BAR_BLD, TCN_BLD);
+            for (int o = tid; o < 729; o += TCN_BLD) {
+                const int a = o / 27, b = o % 27;
+                const int ax = a / 9, ay = (a / 3) % 3, az = a % 3, bx = b / 9, by = (b / 3) % 3, bz = b % 3;
+                const int yo = (3 * ay + by) * 9 + 3 * az + bz;
+                float s = 0.f;
+#pragma unroll
+                for (int t = 0; t < 15; t++) {
+                    const int oa = g_ord(t, 0, 0), ob = g_ord(t, 1, 0);
+#pragma unroll
+                    for (int qx = 0; qx < 4; qx++)
+                        s += g_sel(S.tabf[0][lex][qx][ax], oa) * g_sel(S.tabf[0][lex][qx][bx], ob) *
+                             Ys[t * 324 + qx * 81 + yo];
+                }
+                S.gam[o] = s;
+            }
+            tc_bar_sync(TC_BAR_BLD, TCN_BLD);
+        }
 
         /* ---- chunk loop: chunk ch is built into stage gc & 1 while the tensor core
          * works on the previous chunks; the element accumulates in tensor memory */
@@ -615,46 +650,6 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                         *reinterpret_cast<float *>(lo + off) = 0.f;
                     }
                 }
-            } else {
-                /* Gamma rows: task (slot j, ax, ay) -> 3 outputs (az) of U and V */
-                const int gch = ch - cpos - cneg;
-                const int j = tid / 9, ax = (tid / 3) % 3, ay = tid % 3;
-                const int srow = gch * TC_KC + j, q = srow / 6, i = srow % 6;
-                const int qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
-                const float *p = S.pt[q];
-                const float4 bxv = S.tabf[0][lex][qx][ax], byv = S.tabf[1][ley][qy][ay];
-                const float bx0 = bxv.x, bx1 = bxv.y, bx2 = bxv.z;
-                const float by0 = byv.x, by1 = byv.y, by2 = byv.z;
-                const int I = i < 3 ? i : i - 3;
-                const float s00 = p[TP_S], s11 = p[TP_S + 1], s22 = p[TP_S + 2];
-                const float s01 = p[TP_S + 3], s02 = p[TP_S + 4], s12 = p[TP_S + 5];
-                const float tI0 = p[TP_T + 3 * I], tI1 = p[TP_T + 3 * I + 1], tI2 = p[TP_T + 3 * I + 2];
-#pragma unroll
-                for (int az = 0; az < 3; az++) {
-                    const float4 bzv = S.tabf[2][lez][qz][az];
-                    const float bz0 = bzv.x, bz1 = bzv.y, bz2 = bzv.z;
-                    const float dx = bx1 * by0 * bz0, dy = bx0 * by1 * bz0, dz = bx0 * by0 * bz1;
-                    /* second derivatives H[idx6(I, K)], K = 0..2 */
-                    float h0, h1, h2;
-                    if (I == 0) { h0 = bx2 * by0 * bz0; h1 = bx1 * by1 * bz0; h2 = bx1 * by0 * bz1; }
-                    else if (I == 1) { h0 = bx1 * by1 * bz0; h1 = bx0 * by2 * bz0; h2 = bx0 * by1 * bz1; }
-                    else { h0 = bx1 * by0 * bz1; h1 = bx0 * by1 * bz1; h2 = bx0 * by0 * bz2; }
-                    const float th = tI0 * h0 + tI1 * h1 + tI2 * h2;   /* (T H_a)_I */
-                    const float dI = I == 0 ? dx : (I == 1 ? dy : dz);
-                    float uval, vval;
-                    if (i < 3) {
-                        const float sg = I == 0 ? s00 * dx + s01 * dy + s02 * dz
-                                       : (I == 1 ? s01 * dx + s11 * dy + s12 * dz : s02 * dx + s12 * dy + s22 * dz);
-                        uval = dI;
-                        vval = sg + th;
-                    } else {
-                        uval = th;
-                        vval = dI;
-                    }
-                    const uint32_t off = tc_off(9 * ax + 3 * ay + az, j);
-                    st_pair(st, st + TC_G_ULO, off, uval, 1.f);
-                    st_pair(st + TC_G_VHI, st + TC_G_VLO, off, vval, 1.f);
-                }
             }
             /* coefficients of the next element-matrix chunk (read after the next barrier) */
             if (ch + 1 < cmain) {
@@ -662,7 +657,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                 tc_prepass<TE>(S, (ch + 1) & 1, nb, (nb ? ch + 1 - cpos : ch + 1) * TC_KC, nb ? nneg : npos);
             }
             /* hand the chunk to the issuer */
-            const int ck = (ch < cpos ? 0 : (ch < cpos + cneg ? 1 : 2)) | (ch == 0 ? 4 : 0);
+            const int ck = (ch < cpos ? 0 : 1) | (ch == 0 ? 4 : 0);
             if (tid == 0) S.ckind[b] = ck;
             tc_fence_proxy_async();
             tc_mbar_arrive(&S.full[b]);
@@ -682,17 +677,14 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         }
         if (aborted) break;
         const int g0 = gc - nch;   /* the element's first chunk */
-        bool used[2][2];
-        used[0][g0 & 1] = cmain > 0;
-        used[0][(g0 + 1) & 1] = cmain > 1;
-        used[1][(g0 + cmain) & 1] = true;                 /* TC_NGCHUNK >= 2 Gamma chunks */
-        used[1][(g0 + cmain + 1) & 1] = TC_NGCHUNK > 1;
+        bool used[2];
+        used[g0 & 1] = cmain > 0;
+        used[(g0 + 1) & 1] = cmain > 1;
         float *E = reinterpret_cast<float *>(&S.stage[0][0]);   /* [81][81] */
-        float *Gm = E + 81 * 81;                                  /* [27][27] */
         tc_fence_after_sync();
-        tc_readout(tmem, used, warp, lane, E, Gm);
+        tc_readout(tmem, used, warp, lane, E);
         tc_fence_before_sync();
-        tc_mbar_arrive(&S.freed);
+        if (cmain > 0) tc_mbar_arrive(&S.freed);   /* the issuer saw this element only through its chunks */
         if (tid >= 192 && tid < 192 + 81)
             elem_row_base(g, Tl.e0[0] + lex, Tl.e0[1] + ley, Tl.e0[2] + lez, tid - 192, S.rbase[tid - 192],
                           S.rsx[tid - 192], S.rsy[tid - 192]);
@@ -717,7 +709,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                 for (int g1 = 0; g1 < 9; g1++) {
                     const int a1 = 9 * ax1 + g1, c1 = 3 * a1 + k1, q1 = pb + ps * g1;
                     float v = 0.5f * (E[q1 * 81 + q2] + E[q2 * 81 + q1]);
-                    if (gam) v += 0.5f * (Gm[a1 * 27 + a2] + Gm[a2 * 27 + a1]);
+                    if (gam) v += 0.5f * (S.gam[a1 * 27 + a2] + S.gam[a2 * 27 + a1]);
                     atomicAdd(&vals[S.rbase[c1] + o2 * S.rsx[c1] + p2 * S.rsy[c1] + z2], v);
                 }
             }
@@ -784,7 +776,7 @@ __global__ void __launch_bounds__(TCN_THR, 2) k_tan_tc32_batch(igab_batch_dev B,
 /* ---------------------------------------------------------------- self-test
  * One CTA: A (128 x 32) and B (96 x 32) of small exact values in the operand
  * layout, D = A B^T with M 128 / N 96 (4 k-steps) into columns 0-95 and, for
- * the Gamma shape, A B[0:32]^T with M 128 / N 32 into columns 96-127 (first
+ * a narrow shape, A B[0:32]^T with M 128 / N 32 into columns 96-127 (first
  * k-step overwrite, then accumulate), and with negate-A on k-steps 2-3 into
  * columns 128-159.  out[128][160] receives columns 0-159. */
 __global__ void __launch_bounds__(128) k_tc_selftest(float *out, int *status)

@@ -17,10 +17,13 @@
  *   Gamma(a,b) = sum_q [grad N_a^T S grad N_b + grad N_a . (T H_b) + (T H_a) . grad N_b]
  * (geo = [[S, T], [T^T, 0]], S the 3x3 first-derivative block, T the coupling to the
  * second derivatives H): 27 x 27 entries, computed on the FP32 FMA pipe by sum
- * factorisation, three contractions (z, y, x) of its 15 derivative-pair terms with the
- * 1-D tables, intermediates in the free operand stages at the element's start.  (Built
- * as six U / V operand rows per point it took twelve tcgen05 chunks per element whose
- * construction cost more than the whole contraction does here: 64^3 59.7 -> 55.1 ms.)
+ * factorisation, three contractions (z, y, x) with the 1-D tables, intermediates in the
+ * free operand stage at the element's start.  Its 15 derivative-pair terms share their
+ * (x, y) derivative orders in 12 classes and their x orders in 5, so the z contraction
+ * yields 12 partial sums per (qx, qy, az, bz), the y contraction 5 per (qx, ay, by, az, bz)
+ * and the x contraction reads 5 per point (64^3: 55.3 -> 46.9 ms against one contraction
+ * chain per term; built as six U / V operand rows per point it took twelve tcgen05 chunks
+ * per element whose construction cost more than the whole contraction does: 59.7 ms).
  *
  * Work per CTA: a 2x2x2 tile of elements of one of the 8 colours (the scatter
  * is conflict-free within a colour).  Warps 0-8 build, warp 9 issues MMAs.
@@ -63,8 +66,8 @@ namespace {
 #define TP_CS 27    /* rotation of the (va, vb) block */
 #define TP_SN 28
 #define TP_RS 29    /* sign(s) sqrt|s|, 12 */
-#define TP_S 41     /* w * (sig0, sig1, sig2, d1[3]/2, d1[4]/2, d1[5]/2) */
-#define TP_T 47     /* w * tau[I][K], 9 */
+#define TP_C 41     /* the geometric block's 15 term coefficients: w sig_I (3), w d1[3 + I] (3),
+                       2 w tau[I][K] (9) */
 #define TP_N 57
 
 template <int TE>
@@ -98,33 +101,6 @@ struct tc_smem {
     unsigned int tmem_base;
     int abort_flag;
 };
-
-/* the 15 terms of the geometric block Gamma = sym(P),
- *   P(a,b) = sum_q [ sum_{I<=J} c_IJ d_I N_a d_J N_b + 2 sum_{I,K} T_IK d_I N_a d_I d_K N_b ],
- * c_II = S_II, c_IJ = 2 S_IJ (I < J): term t's derivative order along axis d on the a side
- * (side 0) and the b side (side 1), and its coefficient at a point */
-__device__ __forceinline__ int g_ord(int t, int side, int d)
-{
-    if (t < 3) return d == t;
-    if (t < 6) {
-        const int p = t - 3, i0 = p < 2 ? 0 : 1, j0 = p == 0 ? 1 : 2;
-        return side == 0 ? d == i0 : d == j0;
-    }
-    const int I = (t - 6) / 3, K = (t - 6) % 3;
-    return side == 0 ? d == I : (d == I) + (d == K);
-}
-
-__device__ __forceinline__ float g_coef(const float *p, int t)
-{
-    if (t < 3) return p[TP_S + t];
-    if (t < 6) return 2.f * p[TP_S + t];   /* S01, S02, S12 */
-    return 2.f * p[TP_T + (t - 6)];        /* T[I][K] */
-}
-
-__device__ __forceinline__ float g_sel(float4 v, int ord)
-{
-    return ord == 0 ? v.x : (ord == 1 ? v.y : v.z);
-}
 
 /* eigen-rotation of [[a, b], [b, c]]: [[a,b],[b,c]] = l1 e1 e1^T + l2 e2 e2^T,
  * e1 = (cs, -sn), e2 = (sn, cs) (same convention as the FP64 tensor kernel) */
@@ -485,13 +461,13 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                 if (s < 0.0) nmask |= 1u << v;
             }
 #pragma unroll
-            for (int I = 0; I < 3; I++) pt[TP_S + I] = (float)(w * P.sig[I]);
+            for (int I = 0; I < 3; I++) pt[TP_C + I] = (float)(w * P.sig[I]);
 #pragma unroll
-            for (int I = 0; I < 3; I++) pt[TP_S + 3 + I] = (float)(w * 0.5 * P.d1[3 + I]);
+            for (int I = 0; I < 3; I++) pt[TP_C + 3 + I] = (float)(w * P.d1[3 + I]);
 #pragma unroll
             for (int I = 0; I < 3; I++)
 #pragma unroll
-                for (int K = 0; K < 3; K++) pt[TP_T + 3 * I + K] = (float)(w * P.tau[I][K]);
+                for (int K = 0; K < 3; K++) pt[TP_C + 6 + 3 * I + K] = (float)(2.0 * w * P.tau[I][K]);
         }
         /* ---- sign buckets in variable-major order: the slot of row (q, v) counts the
          * bucket's rows of smaller variables, then the points before q with the same
@@ -533,48 +509,71 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         const int cpos = (npos + TC_KC - 1) / TC_KC, cneg = (nneg + TC_KC - 1) / TC_KC;
         const int nch = cpos + cneg;
 
-        /* ---- geometric block by sum factorisation (FP32 FMA pipe): z, y, x contractions of
-         * the 15 terms, intermediates in the (free) operand stages */
+        /* ---- geometric block by sum factorisation (FP32 FMA pipe).  The 15 terms fall
+         * into 12 classes h of equal (x, y) derivative orders, and those into 5 classes G of
+         * equal x orders: the z contraction sums each class h (Zs), the y contraction each
+         * class G (Ys), the x contraction the 5 G.  Intermediates in the free operand stage. */
         {
-            float *Zs = reinterpret_cast<float *>(S.stage[0]);   /* [15][16 (qx,qy)][9 (az,bz)] */
-            float *Ys = Zs + 2160;                               /* [15][4 qx][81 (ay,by,az,bz)] */
-            for (int o = tid; o < 2160; o += TCN_BLD) {
-                const int t = o / 144, rem = o % 144, qxy = rem / 9, azbz = rem % 9;
-                const int qx = qxy & 3, qy = qxy >> 2, az = azbz / 3, bz = azbz % 3;
-                const int oa = g_ord(t, 0, 2), ob = g_ord(t, 1, 2);
-                float s = 0.f;
+            float *Zs = reinterpret_cast<float *>(S.stage[0]);   /* [12 h][16 (qx, qy)][9 (az, bz)] */
+            float *Ys = Zs + 12 * 144;                           /* [5 G][4 qx][81 (ay, by, az, bz)] */
+            if (tid < 144) {
+                const int qxy = tid / 9, az = (tid % 9) / 3, bz = tid % 3;
+                float z[12];
+#pragma unroll
+                for (int h = 0; h < 12; h++) z[h] = 0.f;
 #pragma unroll
                 for (int qz = 0; qz < 4; qz++) {
-                    const int q = 16 * qz + 4 * qy + qx;
-                    s += g_coef(S.pt[q], t) * g_sel(S.tabf[2][lez][qz][az], oa) * g_sel(S.tabf[2][lez][qz][bz], ob);
+                    const float4 na = S.tabf[2][lez][qz][az], nb = S.tabf[2][lez][qz][bz];
+                    const float *c = S.pt[16 * qz + qxy] + TP_C;
+                    const float z00 = na.x * nb.x, z11 = na.y * nb.y, z01 = na.x * nb.y, z12 = na.y * nb.z;
+                    z[0] += c[0] * z00 + c[8] * z01;     /* t 0, 8 */
+                    z[1] += c[1] * z00 + c[11] * z01;    /* t 1, 11 */
+                    z[2] += c[2] * z11 + c[14] * z12;    /* t 2, 14 */
+                    z[3] += c[3] * z00;
+                    z[4] += c[4] * z01;
+                    z[5] += c[5] * z01;
+                    z[6] += c[6] * z00;
+                    z[7] += c[7] * z00;
+                    z[8] += c[9] * z00;
+                    z[9] += c[10] * z00;
+                    z[10] += c[12] * z11;
+                    z[11] += c[13] * z11;
                 }
-                Zs[o] = s;
+#pragma unroll
+                for (int h = 0; h < 12; h++) Zs[h * 144 + tid] = z[h];
             }
             tc_bar_sync(TC_BAR_BLD, TCN_BLD);
-            for (int o = tid; o < 4860; o += TCN_BLD) {
-                const int t = o / 324, rem = o % 324, qx = rem / 81, r2 = rem % 81, ayby = r2 / 9, azbz = r2 % 9;
-                const int ay = ayby / 3, by = ayby % 3;
-                const int oa = g_ord(t, 0, 1), ob = g_ord(t, 1, 1);
-                float s = 0.f;
+            for (int o = tid; o < 324; o += TCN_BLD) {
+                const int qx = o / 81, ay = (o / 27) % 3, by = (o / 9) % 3, azbz = o % 9;
+                float G[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-                for (int qy = 0; qy < 4; qy++)
-                    s += g_sel(S.tabf[1][ley][qy][ay], oa) * g_sel(S.tabf[1][ley][qy][by], ob) *
-                         Zs[t * 144 + (4 * qy + qx) * 9 + azbz];
-                Ys[o] = s;
+                for (int qy = 0; qy < 4; qy++) {
+                    const float4 na = S.tabf[1][ley][qy][ay], nb = S.tabf[1][ley][qy][by];
+                    const float *zs = Zs + (4 * qy + qx) * 9 + azbz;
+                    const float y00 = na.x * nb.x, y11 = na.y * nb.y, y01 = na.x * nb.y, y10 = na.y * nb.x,
+                                y12 = na.y * nb.z;
+                    G[0] += y00 * zs[0 * 144] + y01 * zs[7 * 144];
+                    G[1] += y11 * zs[1 * 144] + y00 * zs[2 * 144] + y10 * zs[5 * 144] + y12 * zs[9 * 144] +
+                            y01 * zs[11 * 144];
+                    G[2] += y01 * zs[3 * 144] + y00 * zs[4 * 144];
+                    G[3] += y00 * zs[6 * 144];
+                    G[4] += y11 * zs[8 * 144] + y00 * zs[10 * 144];
+                }
+#pragma unroll
+                for (int c = 0; c < 5; c++) Ys[c * 324 + o] = G[c];
             }
             tc_bar_sync(TC_BAR_BLD, TCN_BLD);
             for (int o = tid; o < 729; o += TCN_BLD) {
                 const int a = o / 27, b = o % 27;
-                const int ax = a / 9, ay = (a / 3) % 3, az = a % 3, bx = b / 9, by = (b / 3) % 3, bz = b % 3;
-                const int yo = (3 * ay + by) * 9 + 3 * az + bz;
+                const int ax = a / 9, bx = b / 9;
+                const int yo = (3 * ((a / 3) % 3) + (b / 3) % 3) * 9 + 3 * (a % 3) + b % 3;
                 float s = 0.f;
 #pragma unroll
-                for (int t = 0; t < 15; t++) {
-                    const int oa = g_ord(t, 0, 0), ob = g_ord(t, 1, 0);
-#pragma unroll
-                    for (int qx = 0; qx < 4; qx++)
-                        s += g_sel(S.tabf[0][lex][qx][ax], oa) * g_sel(S.tabf[0][lex][qx][bx], ob) *
-                             Ys[t * 324 + qx * 81 + yo];
+                for (int qx = 0; qx < 4; qx++) {
+                    const float4 na = S.tabf[0][lex][qx][ax], nb = S.tabf[0][lex][qx][bx];
+                    const float *ys = Ys + qx * 81 + yo;
+                    s += na.y * nb.y * ys[0] + na.x * nb.x * ys[324] + na.y * nb.x * ys[2 * 324] +
+                         na.y * nb.z * ys[3 * 324] + na.x * nb.y * ys[4 * 324];
                 }
                 S.gam[o] = s;
             }

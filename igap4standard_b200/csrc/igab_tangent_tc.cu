@@ -29,20 +29,25 @@
  * is conflict-free within a colour).  Warps 0-8 build, warp 9 issues MMAs.
  * Per element the builders compute the sum-factorised field at the 64 Gauss
  * points (FP64), the point integrand (FP64, 64 threads) and sign buckets of
- * the 768 (point, variable) rows, then build chunks of 32 rows into a double-
- * buffered shared-memory stage (TF32 hi/lo in the K-major layout of
+ * the 768 (point, variable) rows, then build chunks of 32 rows into one of three
+ * shared-memory stages (TF32 hi/lo in the K-major layout of
  * igab_tc.cuh; element-matrix column c sits at operand row tc_pos(c), so that a
- * builder thread's 9 outputs are 1024 bytes apart) and hand each to the issuer
- * through an mbarrier.  The issuer
- * runs 4 k-steps x 2 MMAs (M 128, N 96; negate-A for negative-curvature rows)
- * per chunk and commits to the stage's mbarrier, which frees the stage for the
- * chunk after next.  An element accumulates in two tensor-memory accumulators,
- * by chunk parity: about 96 accumulating MMAs each, 5e-6 rowwise agreement with
- * the FP64 reference (one accumulator for all 192 gave 1e-5).  Tensor memory:
- * 256 columns per CTA (element matrix 2 x 96); at most two CTAs per SM.  Rows 81-127 of the M side and columns 81-95 of the N side read whatever
- * lies behind the operand in the stage; they only feed accumulator rows and
- * columns that are never read.  At the end of an element the builders sum the
- * accumulators into shared memory, release them to the issuer, take the
+ * builder thread's 9 outputs are 1024 bytes apart; each thread evaluates its row's
+ * coefficients itself, which took 46.7 -> 43.3 ms at 64^3 against a pre-pass by 96
+ * threads that the other builders waited for) and hand each to the issuer through
+ * an mbarrier, on which the issuer spins (no suspension: 43.3 -> 43.1 ms).  The issuer
+ * runs 4 k-steps of one MMA each per chunk (M 128 rows of Y_hi, N 192 rows of Y_hi and
+ * 2 Y_lo, so that A is read once: 42.8 -> 41.5 ms against two N 96 MMAs; negate-A for
+ * negative-curvature rows) and commits to the stage's mbarrier, which frees the stage
+ * for the chunk three later (three stages rather than two: 43.1 -> 42.8 ms).  An
+ * element accumulates Y_hi^T Y_hi in tensor-memory columns 0-95 and Y_hi^T 2 Y_lo in
+ * 96-191: about 100 accumulating MMAs per column, as with two 96-column accumulators
+ * by chunk parity before (5e-6 rowwise agreement with the FP64 reference; one
+ * 96-column accumulator for all 200 MMAs gave 1e-5).  Tensor memory: 256 columns per
+ * CTA; at most two CTAs per SM.  Rows 81-127 of the M side and rows 81-95 / 177-191
+ * of the N side read whatever lies behind the operand in the stage; they only feed
+ * accumulator rows and columns that are never read.  At the end of an element the
+ * builders sum the two halves into shared memory, release them to the issuer, take the
  * symmetric part, add Gamma on the k1 = k2 blocks and read-modify-write the
  * 81 x 81 values into the FP32 CSR values.
  */
@@ -56,9 +61,11 @@ namespace {
 #define TCN_THR 320            /* + warp 9: the MMA issuer */
 #define TC_BAR_BLD 1           /* named barrier of the builder warps */
 #define TC_STAGE 24576         /* bytes per operand stage */
-#define TC_MAIN_LO 11264       /* 2 Y_lo after Y_hi (11 groups of 8 rows) */
+#define TC_NS 3                /* operand stages */
+#define TC_MAIN_LO 12288       /* 2 Y_lo: B operand rows 96-191 (Y_hi rows 0-80 in groups 0-10) */
 #define TC_TMEM_COLS 256u
-#define TC_COL_MAIN 0u         /* two 96-column element-matrix accumulators */
+#define TC_COL_MAIN 0u         /* the element-matrix accumulator: Y_hi^T Y_hi in columns 0-95,
+                                  Y_hi^T 2 Y_lo in 96-191 */
 
 /* float point data per Gauss point */
 #define TP_F 0      /* F[k][J], 9 */
@@ -74,33 +81,50 @@ template <int TE>
 struct tc_smem {
     static constexpr int TC = TE + 2;
     static constexpr int NCP = TC * TC * TC;
-    unsigned char stage[2][TC_STAGE];   /* operand stages; the geometric block's intermediates at an
-                                           element's start, E staging at read-out */
-    double A[972];                      /* interpolation temporaries */
-    double C[864];
+    unsigned char stage[TC_NS][TC_STAGE];   /* operand stages; at an element's start the interpolation
+                                               temporaries (stage 1) and the geometric block's
+                                               intermediates (stage 0), E staging at read-out */
     double U[NCP * 3];
     double tab[3][TE][IGAB_TAB1D];
     double wh[3][TE][IGAB_NQ];
     float4 tabf[3][TE][IGAB_NQ][3];     /* FP32 1-D tables [d][element][q][function], derivatives 0-2 in x, y, z */
     float pt[IGAB_NQ3][TP_N];
     unsigned short map[2][768];         /* bucket slot -> 12 q + v (positive, negative) */
-    float4 gk[2][TC_KC][3][3];          /* per chunk parity: r * d v'/d u_{k,m} of each slot (pre-pass),
-                                           m = 0..8 in (x, y, z) of three float4 (w unused) */
-    int qs[2][TC_KC];                   /* point of each slot, -1 for padding rows */
     int cnt[2];
     int vcnt[12][2][2];                 /* rows per (variable, point warp, sign) */
     long rbase[81];                     /* CSR row bases of the element matrix (elem_row_base) */
     int rsx[81], rsy[81];
-    unsigned long long full[2];         /* stage b written (288 builder arrivals) */
-    unsigned long long done[2];         /* MMAs of the chunk in stage / accumulator b completed (commit) */
+    unsigned long long full[TC_NS];         /* stage b written (288 builder arrivals) */
+    unsigned long long done[TC_NS];         /* MMAs of the chunk in stage / accumulator b completed (commit) */
     unsigned long long freed;           /* the element's accumulators read out (288 builder arrivals) */
     unsigned long long drain;           /* issuer: every MMA it issued has completed */
     float gam[27 * 27];                 /* the element's geometric block (sum-factorised, FP32) */
-    int ckind[2];                       /* chunk in stage b: 0 positive rows, 1 negative rows,
+    int ckind[TC_NS];                       /* chunk in stage b: 0 positive rows, 1 negative rows,
                                            3 end of tile; + 4 on an element's first chunk */
     unsigned int tmem_base;
     int abort_flag;
 };
+
+
+/* spin (no suspension) until the phase with the given parity completes; bounded, abortable */
+__device__ __forceinline__ bool tc_mbar_spin_abortable(unsigned long long *bar, uint32_t parity,
+                                                       const volatile int *abort)
+{
+    const uint32_t a = tc_smem_u32(bar);
+    for (long i = 0; i < 64 * TC_WAIT_POLLS; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if ((i & 1023) == 1023 && *abort) return false;
+    }
+    return false;
+}
 
 /* eigen-rotation of [[a, b], [b, c]]: [[a,b],[b,c]] = l1 e1 e1^T + l2 e2 e2^T,
  * e1 = (cs, -sn), e2 = (sn, cs) (same convention as the FP64 tensor kernel) */
@@ -180,9 +204,9 @@ __device__ __forceinline__ void st_pair(unsigned char *hi_base, unsigned char *l
 /* pipeline state of a thread, carried across the tiles its CTA processes: the
  * builders track the commits they wait for, the issuer the arrivals it waits for */
 struct tc_state {
-    uint32_t ph_done[2];   /* builders: parity of the next wait on done[b] */
-    bool pend[2];          /* builders: a chunk in stage b whose completion is not yet waited for */
-    uint32_t ph_full[2];   /* issuer: parity of the next wait on full[b] */
+    uint32_t ph_done[TC_NS];   /* builders: parity of the next wait on done[b] */
+    bool pend[TC_NS];          /* builders: a chunk in stage b whose completion is not yet waited for */
+    uint32_t ph_full[TC_NS];   /* issuer: parity of the next wait on full[b] */
     uint32_t ph_free;      /* issuer: parity of the next wait on freed */
     uint32_t ph_drain;
     int gc;                /* chunks (with MMAs) so far */
@@ -197,7 +221,7 @@ __device__ __forceinline__ void tc_setup(tc_smem<TE> &S, tc_state &Q)
 {
     const int tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0) {
-        for (int b = 0; b < 2; b++) {
+        for (int b = 0; b < TC_NS; b++) {
             tc_mbar_init(&S.full[b], TCN_BLD);
             tc_mbar_init(&S.done[b], 1);
         }
@@ -211,8 +235,10 @@ __device__ __forceinline__ void tc_setup(tc_smem<TE> &S, tc_state &Q)
     __syncthreads();
     tc_fence_after_sync();
     Q.tmem = S.tmem_base;
-    Q.ph_done[0] = Q.ph_done[1] = Q.ph_full[0] = Q.ph_full[1] = 0u;
-    Q.pend[0] = Q.pend[1] = false;
+    for (int b = 0; b < TC_NS; b++) {
+        Q.ph_done[b] = Q.ph_full[b] = 0u;
+        Q.pend[b] = false;
+    }
     Q.ph_free = Q.ph_drain = 0u;
     Q.gc = 0;
     Q.nelem = 0;
@@ -234,9 +260,8 @@ __device__ __forceinline__ void tc_release(tc_smem<TE> &S, tc_state &Q, int *sta
 }
 
 /* the issuer warp for one tile: wait for each built chunk and issue its MMAs.
- * An element's chunks accumulate in two tensor-memory accumulators by chunk
- * parity (96 columns each); negative-curvature
- * chunks use the negate-A form.  Before the first MMA of an element the issuer
+ * An element's chunks accumulate in one tensor-memory accumulator of 192 columns
+ * (Y_hi^T Y_hi | Y_hi^T 2 Y_lo); negative-curvature chunks use the negate-A form.  Before the first MMA of an element the issuer
  * waits until the builders have read the previous element's accumulators.  Ends
  * at the builders' end-of-tile chunk; before returning it waits (bounded) until
  * every MMA it issued has completed. */
@@ -246,10 +271,10 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
     const int lane = threadIdx.x & 31;
     const volatile int *abort = &S.abort_flag;
     bool ok = !*abort;
-    bool started[2] = {false, false};   /* accumulator b holds this element's sums */
+    bool started = false;   /* the accumulator holds this element's sums */
     while (ok) {
-        const int b = Q.gc & 1;
-        if (lane == 0) ok = tc_mbar_wait_abortable(&S.full[b], Q.ph_full[b], abort);
+        const int b = Q.gc % TC_NS;
+        if (lane == 0) ok = tc_mbar_spin_abortable(&S.full[b], Q.ph_full[b], abort);
         ok = __shfl_sync(0xffffffffu, ok, 0);
         Q.ph_full[b] ^= 1u;
         if (!ok) break;
@@ -266,22 +291,21 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
                 if (!ok) break;
             }
             Q.nelem++;
-            started[0] = started[1] = false;
+            started = false;
         }
         const int kind = ck & 3;
-        const uint32_t acc0 = started[b] ? 1u : 0u;
-        started[b] = true;
+        const uint32_t acc0 = started ? 1u : 0u;
+        started = true;
         if (lane == 0) {
             tc_fence_after_sync();
             const uint32_t sb = tc_smem_u32(S.stage[b]);
-            const uint32_t idm = kind == 0 ? tc_idesc_tf32(128, 96) : tc_idesc_tf32(128, 96, true);
-            const uint32_t d = Q.tmem + TC_COL_MAIN + (uint32_t)b * 96u;
+            const uint32_t idm = kind == 0 ? tc_idesc_tf32(128, 192) : tc_idesc_tf32(128, 192, true);
+            const uint32_t d = Q.tmem + TC_COL_MAIN;
 #pragma unroll
             for (int kk = 0; kk < 4; kk++) {
+                /* A: Y_hi (rows 0-127); B: Y_hi and 2 Y_lo (rows 0-191) of the same stage */
                 const uint64_t ah = tc_sdesc(sb + kk * TC_KSTEP_BYTES);
-                const uint64_t bl = tc_sdesc(sb + TC_MAIN_LO + kk * TC_KSTEP_BYTES);
                 tc_mma_tf32(d, ah, ah, idm, kk == 0 ? acc0 : 1u);
-                tc_mma_tf32(d, ah, bl, idm, 1u);
             }
             tc_commit(&S.done[b]);
         }
@@ -298,10 +322,11 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
     __syncwarp();
 }
 
-/* Sum the element's accumulators into shared memory (FP32, round to nearest):
- * element-matrix rows by warps 0-2 / 4-6 (TMEM lanes = rows 0-95, columns
- * 0-47 / 48-95).  used[b]: accumulator b holds this element's sums (none: zeros). */
-__device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2], int warp, int lane, float *E)
+/* The element matrix E = Y_hi^T Y_hi + Y_hi^T 2 Y_lo (accumulator columns c and 96 + c)
+ * into shared memory (FP32, round to nearest): rows by warps 0-2 / 4-6 (TMEM lanes =
+ * rows 0-95, columns 0-47 / 48-95).  used: the accumulator holds this element's sums
+ * (none: zeros). */
+__device__ __forceinline__ void tc_readout(uint32_t tmem, bool used, int warp, int lane, float *E)
 {
     if (warp < 8) {
         if (warp == 3 || warp == 7) return;   /* lanes 96-127: rows beyond 80 */
@@ -313,8 +338,8 @@ __device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2],
 #pragma unroll
             for (int i = 0; i < 16; i++) s[i] = 0.f;
 #pragma unroll
-            for (int b = 0; b < 2; b++) {
-                if (!used[b]) continue;   /* warp-uniform */
+            for (int b = 0; b < 2; b++) {   /* Y_hi^T Y_hi, then Y_hi^T 2 Y_lo */
+                if (!used) continue;   /* warp-uniform */
                 float v[16];
                 tc_ld16(tmem + ((uint32_t)lb << 16) + TC_COL_MAIN + (uint32_t)b * 96u + (uint32_t)c0, v);
 #pragma unroll
@@ -328,34 +353,6 @@ __device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2],
     }
 }
 
-/* Pre-pass of an element-matrix chunk (builder threads 0-95, one (slot, component)
- * each): the row's coefficients r * d v'/d u_{k,m} (m = 0..8) and its point, so that
- * the 288 build tasks read them instead of each evaluating the variable gradient
- * (which branches on the variable; the variable-major slot order makes the branch
- * mostly uniform across a warp). */
-template <int TE>
-__device__ __forceinline__ void tc_prepass(tc_smem<TE> &S, int par, int bucket, int base, int cntb)
-{
-    const int t = threadIdx.x;
-    if (t >= 3 * TC_KC) return;
-    const int j = t / 3, k = t % 3, slot = base + j;
-    float *gout = reinterpret_cast<float *>(S.gk[par][j][k]);
-    if (slot < cntb) {
-        const int id = S.map[bucket][slot], q = id / 12, v = id % 12;
-        const float *p = S.pt[q];
-        float gv[9];
-        tc_grad_var(p, v, k, gv);
-        const float r = fabsf(p[TP_RS + v]);
-#pragma unroll
-        for (int m = 0; m < 9; m++) gout[(m / 3) * 4 + m % 3] = r * gv[m];
-        if (k == 0) S.qs[par][j] = q;
-    } else {
-#pragma unroll
-        for (int m = 0; m < 9; m++) gout[(m / 3) * 4 + m % 3] = 0.f;
-        if (k == 0) S.qs[par][j] = -1;
-    }
-}
-
 /* the builder warps (threads 0..287) for one tile of up to TE^3 elements */
 template <int TE>
 __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, const double *__restrict__ U,
@@ -366,8 +363,15 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
     constexpr int NEL = TE * TE * TE;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     /* local copies of the pipeline state (registers), written back at the end */
-    uint32_t ph[2] = {Q.ph_done[0], Q.ph_done[1]};
-    bool pend[2] = {Q.pend[0], Q.pend[1]};
+    uint32_t ph[TC_NS];
+    bool pend[TC_NS];
+#pragma unroll
+    for (int b = 0; b < TC_NS; b++) {
+        ph[b] = Q.ph_done[b];
+        pend[b] = Q.pend[b];
+    }
+    double *SA = reinterpret_cast<double *>(S.stage[1]);   /* interpolation temporaries */
+    double *SC = SA + 972;
     int gc = Q.gc;
     bool aborted = Q.aborted;
     const uint32_t tmem = Q.tmem;
@@ -403,14 +407,14 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         for (int o = tid; o < 972; o += TCN_BLD) {
             int i = o % 3, kz = (o / 3) % 3, ay = (o / 9) % 3, ax = (o / 27) % 3, q = o / 81;
             const double *u0 = &S.U[(((lex + ax) * TC + (ley + ay)) * TC + lez) * 3 + i];
-            S.A[o] = Bz[q * 9 + kz] * u0[0] + Bz[q * 9 + 3 + kz] * u0[3] + Bz[q * 9 + 6 + kz] * u0[6];
+            SA[o] = Bz[q * 9 + kz] * u0[0] + Bz[q * 9 + 3 + kz] * u0[3] + Bz[q * 9 + 6 + kz] * u0[6];
         }
         tc_bar_sync(TC_BAR_BLD, TCN_BLD);
         for (int o = tid; o < 864; o += TCN_BLD) {
             int i = o % 3, kk = (o / 3) % 6, ax = (o / 18) % 3, qq = o / 54;
             int qyy = qq & 3, qzz = qq >> 2;
-            const double *a0 = &S.A[((qzz * 3 + ax) * 3) * 9 + kk_kz(kk) * 3 + i];
-            S.C[o] = By[qyy * 9 + kk_ky(kk)] * a0[0] + By[qyy * 9 + 3 + kk_ky(kk)] * a0[9] +
+            const double *a0 = &SA[((qzz * 3 + ax) * 3) * 9 + kk_kz(kk) * 3 + i];
+            SC[o] = By[qyy * 9 + kk_ky(kk)] * a0[0] + By[qyy * 9 + 3 + kk_ky(kk)] * a0[9] +
                      By[qyy * 9 + 6 + kk_ky(kk)] * a0[18];
         }
         tc_bar_sync(TC_BAR_BLD, TCN_BLD);
@@ -426,7 +430,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                     double s = 0.0;
 #pragma unroll
                     for (int ax = 0; ax < 3; ax++)
-                        s += Bx[qx * 9 + ax * 3 + a_kx(a)] * S.C[((qq * 3 + ax) * 6 + a_kk(a)) * 3 + i];
+                        s += Bx[qx * 9 + ax * 3 + a_kx(a)] * SC[((qq * 3 + ax) * 6 + a_kk(a)) * 3 + i];
                     u[10 * i + a] = s;
                 }
             if (g.periodic) {
@@ -455,8 +459,8 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
 #pragma unroll
             for (int v = 0; v < 12; v++) {
                 const double s = w * (v == 1 ? l1 : (v == 2 ? l2 : P.d2[v]));
-                const double r = sqrt(fabs(s));
-                pt[TP_RS + v] = (float)(s < 0.0 ? -r : r);
+                const float r = sqrtf(fabsf((float)s));   /* FP32: the operand rows are FP32 */
+                pt[TP_RS + v] = s < 0.0 ? -r : r;
                 if (s > 0.0) pmask |= 1u << v;
                 if (s < 0.0) nmask |= 1u << v;
             }
@@ -472,7 +476,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         /* ---- sign buckets in variable-major order: the slot of row (q, v) counts the
          * bucket's rows of smaller variables, then the points before q with the same
          * sign for v (ballot ranks over the two point warps).  Consecutive slots then
-         * share their variable, so the pre-pass branches alike across a warp. */
+         * share their variable, so the coefficient evaluation branches alike across a warp. */
         if (tid < IGAB_NQ3) {
 #pragma unroll 1
             for (int v = 0; v < 12; v++) {
@@ -580,16 +584,15 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
             tc_bar_sync(TC_BAR_BLD, TCN_BLD);
         }
 
-        /* ---- chunk loop: chunk ch is built into stage gc & 1 while the tensor core
+        /* ---- chunk loop: chunk ch is built into stage gc % 3 while the tensor core
          * works on the previous chunks; the element accumulates in tensor memory */
         const int cmain = cpos + cneg;
-        if (cmain > 0) tc_prepass<TE>(S, 0, 0 < cpos ? 0 : 1, 0, 0 < cpos ? npos : nneg);
         for (int ch = 0; ch < nch; ch++) {
-            const int b = gc & 1;
+            const int b = gc % TC_NS;
             unsigned char *st = S.stage[b];
-            /* stage b holds chunk gc-2: one thread waits for its MMAs (their operand reads
+            /* stage b holds chunk gc-3: one thread waits for its MMAs (their operand reads
              * are complete once the commit arrives); the barrier passes that on to the
-             * other builders and also publishes the pre-pass */
+             * other builders */
             bool ok = true;
             if (pend[b]) {
                 if (tid == 0) ok = tc_mbar_wait_abortable(&S.done[b], ph[b], abort);
@@ -602,24 +605,29 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                  * c = 3 (9 ax + 3 ay + az) + k at operand row tc_pos(c): row 8 g + 3 k + ax
                  * for g = 3 ay + az, or 72 + g for k = ax = 2, so the 9 stores sit at
                  * off0 + g * step (+ adj at g = 8) */
-                const int par = ch & 1;
+                const int bucket = ch < cpos ? 0 : 1;
+                const int slot = (bucket ? ch - cpos : ch) * TC_KC + tid / 9;
                 const int j = tid / 9, k = (tid / 3) % 3, ax = tid % 3, cb = 3 * k + ax;
                 const uint32_t off0 = (uint32_t)((j >> 2) * TC_LBO + (j & 3) * 4) +
                                       (cb < 8 ? (uint32_t)cb * 16u : 9u * TC_SBO);
                 const uint32_t step = cb < 8 ? (uint32_t)TC_SBO : 16u;
                 const uint32_t adj8 = cb < 8 ? 0u : (uint32_t)(TC_SBO - 128);
                 unsigned char *hi = st, *lo = st + TC_MAIN_LO;
-                const int q = S.qs[par][j];
-                if (q >= 0) {
+                if (slot < (bucket ? nneg : npos)) {
+                    const int id = S.map[bucket][slot], q = id / 12, v = id - 12 * q;
                     const int qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
-                    /* the row's coefficients m = 0..8 and the 1-D tables as float4 loads */
-                    const float4 ga = S.gk[par][j][k][0], gb = S.gk[par][j][k][1], gc = S.gk[par][j][k][2];
+                    /* the row's coefficients r d v'/d u_{k,m}, m = 0..8 (variable-major slots: v is
+                     * nearly uniform across a warp) and the 1-D tables as float4 loads */
+                    const float *p = S.pt[q];
+                    float gv[9];
+                    tc_grad_var(p, v, k, gv);
+                    const float r = fabsf(p[TP_RS + v]);
                     const float4 bxv = S.tabf[0][lex][qx][ax];
-                    const float bx0 = bxv.x, bx1 = bxv.y, bx2 = bxv.z;
+                    const float bx0 = r * bxv.x, bx1 = r * bxv.y, bx2 = r * bxv.z;
                     /* coefficients of By[ky] per kz: derivative m -> (kx, ky, kz) as eval_Bspline */
-                    const float t00 = ga.x * bx1 + gb.x * bx2, t01 = ga.y * bx0 + gb.y * bx1, t02 = gc.x * bx0;
-                    const float t10 = ga.z * bx0 + gb.z * bx1, t11 = gc.y * bx0;
-                    const float t20 = gc.z * bx0;
+                    const float t00 = gv[0] * bx1 + gv[3] * bx2, t01 = gv[1] * bx0 + gv[4] * bx1, t02 = gv[6] * bx0;
+                    const float t10 = gv[2] * bx0 + gv[5] * bx1, t11 = gv[7] * bx0;
+                    const float t20 = gv[8] * bx0;
                     float bz[9];
 #pragma unroll
                     for (int i = 0; i < 3; i++) {
@@ -650,11 +658,6 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                     }
                 }
             }
-            /* coefficients of the next element-matrix chunk (read after the next barrier) */
-            if (ch + 1 < cmain) {
-                const int nb = ch + 1 < cpos ? 0 : 1;
-                tc_prepass<TE>(S, (ch + 1) & 1, nb, (nb ? ch + 1 - cpos : ch + 1) * TC_KC, nb ? nneg : npos);
-            }
             /* hand the chunk to the issuer */
             const int ck = (ch < cpos ? 0 : 1) | (ch == 0 ? 4 : 0);
             if (tid == 0) S.ckind[b] = ck;
@@ -666,8 +669,8 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         if (aborted) break;
 
         /* ---- all chunks of the element done (older stage first), accumulators -> shared memory */
-        for (int k = 0; k < 2 && !aborted; k++) {
-            const int b = (gc + k) & 1;   /* chunk gc-2, then gc-1 */
+        for (int k = 0; k < TC_NS && !aborted; k++) {
+            const int b = (gc + k) % TC_NS;   /* chunk gc-3, gc-2, gc-1 */
             if (!pend[b]) continue;
             const bool ok = tid == 0 ? tc_mbar_wait_abortable(&S.done[b], ph[b], abort) : true;
             ph[b] ^= 1u;
@@ -675,10 +678,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
             if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) aborted = true;
         }
         if (aborted) break;
-        const int g0 = gc - nch;   /* the element's first chunk */
-        bool used[2];
-        used[g0 & 1] = cmain > 0;
-        used[(g0 + 1) & 1] = cmain > 1;
+        const bool used = cmain > 0;
         float *E = reinterpret_cast<float *>(&S.stage[0][0]);   /* [81][81] */
         tc_fence_after_sync();
         tc_readout(tmem, used, warp, lane, E);
@@ -718,14 +718,15 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
     /* end of tile for the issuer (also after an abort: it stops at the flag) */
     if (aborted && tid == 0) S.abort_flag = 1;
     if (!aborted) {
-        const int b = gc & 1;
+        const int b = gc % TC_NS;
         if (tid == 0) S.ckind[b] = 3;
         tc_mbar_arrive(&S.full[b]);
     }
-    Q.ph_done[0] = ph[0];
-    Q.ph_done[1] = ph[1];
-    Q.pend[0] = pend[0];
-    Q.pend[1] = pend[1];
+#pragma unroll
+    for (int b = 0; b < TC_NS; b++) {
+        Q.ph_done[b] = ph[b];
+        Q.pend[b] = pend[b];
+    }
     Q.gc = gc;
     Q.aborted = aborted;
 }

@@ -10,9 +10,12 @@
  * per-point rotation that diagonalises Phi'' (its one 2x2 block), and
  * s_qv = w_q lambda_v(q).  With y = sqrt|s| x and the rows split by the sign
  * of s,  K_main = Y_+^T Y_+ - Y_-^T Y_-.  A Gram product Y^T Y needs only two
- * TF32 MMAs per k-step for FP32 accuracy: with y = y_hi + y_lo (both TF32),
- *   E = Y_hi^T Y_hi + Y_hi^T (2 Y_lo),   Y^T Y = (E + E^T)/2 + O(2^-22),
+ * TF32 MMAs per k-step for FP32 accuracy: with y = y_hi + y_lo (y_hi TF32, y_lo the
+ * FP32 remainder, which the MMA reads truncated to TF32: an error of 2^-21 |y|),
+ *   E = Y_hi^T Y_hi + 2 Y_hi^T Y_lo,   Y^T Y = (E + E^T)/2 + O(2^-21),
  * so the symmetric part taken at read-out recovers the cross term Y_lo^T Y_hi.
+ * (Storing y_lo unrounded and unscaled, the factor 2 applied at read-out, saved two
+ * instructions per operand value: 64^3 41.5 -> 39.8 ms.)
  * The geometric block, identical for the three displacement components, is
  *   Gamma(a,b) = sum_q [grad N_a^T S grad N_b + grad N_a . (T H_b) + (T H_a) . grad N_b]
  * (geo = [[S, T], [T^T, 0]], S the 3x3 first-derivative block, T the coupling to the
@@ -37,10 +40,10 @@
  * threads that the other builders waited for) and hand each to the issuer through
  * an mbarrier, on which the issuer spins (no suspension: 43.3 -> 43.1 ms).  The issuer
  * runs 4 k-steps of one MMA each per chunk (M 128 rows of Y_hi, N 192 rows of Y_hi and
- * 2 Y_lo, so that A is read once: 42.8 -> 41.5 ms against two N 96 MMAs; negate-A for
+ * Y_lo, so that A is read once: 42.8 -> 41.5 ms against two N 96 MMAs; negate-A for
  * negative-curvature rows) and commits to the stage's mbarrier, which frees the stage
  * for the chunk three later (three stages rather than two: 43.1 -> 42.8 ms).  An
- * element accumulates Y_hi^T Y_hi in tensor-memory columns 0-95 and Y_hi^T 2 Y_lo in
+ * element accumulates Y_hi^T Y_hi in tensor-memory columns 0-95 and Y_hi^T Y_lo in
  * 96-191: about 100 accumulating MMAs per column, as with two 96-column accumulators
  * by chunk parity before (5e-6 rowwise agreement with the FP64 reference; one
  * 96-column accumulator for all 200 MMAs gave 1e-5).  Tensor memory: 256 columns per
@@ -62,10 +65,10 @@ namespace {
 #define TC_BAR_BLD 1           /* named barrier of the builder warps */
 #define TC_STAGE 24576         /* bytes per operand stage */
 #define TC_NS 3                /* operand stages */
-#define TC_MAIN_LO 12288       /* 2 Y_lo: B operand rows 96-191 (Y_hi rows 0-80 in groups 0-10) */
+#define TC_MAIN_LO 12288       /* Y_lo: B operand rows 96-191 (Y_hi rows 0-80 in groups 0-10) */
 #define TC_TMEM_COLS 256u
 #define TC_COL_MAIN 0u         /* the element-matrix accumulator: Y_hi^T Y_hi in columns 0-95,
-                                  Y_hi^T 2 Y_lo in 96-191 */
+                                  Y_hi^T Y_lo in 96-191 */
 
 /* float point data per Gauss point */
 #define TP_F 0      /* F[k][J], 9 */
@@ -192,13 +195,13 @@ __device__ __forceinline__ int tc_pos(int c)
     return cb < 8 ? 8 * g + cb : 72 + g;
 }
 
-__device__ __forceinline__ void st_pair(unsigned char *hi_base, unsigned char *lo_base, uint32_t off, float y,
-                                        float lo_scale)
+/* y = hi + lo: hi rounded to TF32 (exact in the MMA), lo = y - hi stored as FP32 (exact);
+ * the MMA reads lo truncated to TF32, an error of at most 2^-21 |y| */
+__device__ __forceinline__ void st_pair(unsigned char *hi_base, unsigned char *lo_base, uint32_t off, float y)
 {
-    float h, l;
-    tc_split(y, h, l);
+    const float h = tc_tf32(y);
     *reinterpret_cast<float *>(hi_base + off) = h;
-    *reinterpret_cast<float *>(lo_base + off) = lo_scale * l;
+    *reinterpret_cast<float *>(lo_base + off) = y - h;
 }
 
 /* pipeline state of a thread, carried across the tiles its CTA processes: the
@@ -261,8 +264,9 @@ __device__ __forceinline__ void tc_release(tc_smem<TE> &S, tc_state &Q, int *sta
 
 /* the issuer warp for one tile: wait for each built chunk and issue its MMAs.
  * An element's chunks accumulate in one tensor-memory accumulator of 192 columns
- * (Y_hi^T Y_hi | Y_hi^T 2 Y_lo); negative-curvature chunks use the negate-A form.  Before the first MMA of an element the issuer
- * waits until the builders have read the previous element's accumulators.  Ends
+ * (Y_hi^T Y_hi | Y_hi^T Y_lo); negative-curvature chunks use the negate-A form.
+ * Before the first MMA of an element the issuer waits until the builders have
+ * read the previous element's accumulator.  Ends
  * at the builders' end-of-tile chunk; before returning it waits (bounded) until
  * every MMA it issued has completed. */
 template <int TE>
@@ -303,7 +307,7 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
             const uint32_t d = Q.tmem + TC_COL_MAIN;
 #pragma unroll
             for (int kk = 0; kk < 4; kk++) {
-                /* A: Y_hi (rows 0-127); B: Y_hi and 2 Y_lo (rows 0-191) of the same stage */
+                /* A: Y_hi (rows 0-127); B: Y_hi and Y_lo (rows 0-191) of the same stage */
                 const uint64_t ah = tc_sdesc(sb + kk * TC_KSTEP_BYTES);
                 tc_mma_tf32(d, ah, ah, idm, kk == 0 ? acc0 : 1u);
             }
@@ -322,7 +326,7 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
     __syncwarp();
 }
 
-/* The element matrix E = Y_hi^T Y_hi + Y_hi^T 2 Y_lo (accumulator columns c and 96 + c)
+/* The element matrix E = Y_hi^T Y_hi + 2 Y_hi^T Y_lo (accumulator columns c and 96 + c)
  * into shared memory (FP32, round to nearest): rows by warps 0-2 / 4-6 (TMEM lanes =
  * rows 0-95, columns 0-47 / 48-95).  used: the accumulator holds this element's sums
  * (none: zeros). */
@@ -338,12 +342,12 @@ __device__ __forceinline__ void tc_readout(uint32_t tmem, bool used, int warp, i
 #pragma unroll
             for (int i = 0; i < 16; i++) s[i] = 0.f;
 #pragma unroll
-            for (int b = 0; b < 2; b++) {   /* Y_hi^T Y_hi, then Y_hi^T 2 Y_lo */
+            for (int b = 0; b < 2; b++) {   /* Y_hi^T Y_hi, then 2 Y_hi^T Y_lo */
                 if (!used) continue;   /* warp-uniform */
                 float v[16];
                 tc_ld16(tmem + ((uint32_t)lb << 16) + TC_COL_MAIN + (uint32_t)b * 96u + (uint32_t)c0, v);
 #pragma unroll
-                for (int i = 0; i < 16; i++) s[i] += v[i];
+                for (int i = 0; i < 16; i++) s[i] += b ? 2.f * v[i] : v[i];
             }
             if (row < 81)
 #pragma unroll
@@ -646,7 +650,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                         for (int az = 0; az < 3; az++) {
                             const float y = cy0 * bz[3 * az] + cy1 * bz[3 * az + 1] + cy2 * bz[3 * az + 2];
                             const int gg = 3 * ay + az;
-                            st_pair(hi, lo, off0 + (uint32_t)gg * step + (gg == 8 ? adj8 : 0u), y, 2.f);
+                            st_pair(hi, lo, off0 + (uint32_t)gg * step + (gg == 8 ? adj8 : 0u), y);
                         }
                     }
                 } else {

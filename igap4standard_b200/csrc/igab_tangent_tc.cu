@@ -44,10 +44,13 @@
  * negative-curvature rows) and commits to the stage's mbarrier, which frees the stage
  * for the chunk three later (three stages rather than two: 43.1 -> 42.8 ms).  An
  * element accumulates Y_hi^T Y_hi in tensor-memory columns 0-95 and Y_hi^T Y_lo in
- * 96-191: about 100 accumulating MMAs per column, as with two 96-column accumulators
- * by chunk parity before (5e-6 rowwise agreement with the FP64 reference; one
- * 96-column accumulator for all 200 MMAs gave 1e-5).  Tensor memory: 256 columns per
- * CTA; at most two CTAs per SM.  Rows 81-127 of the M side and rows 81-95 / 177-191
+ * 96-191: about 100 accumulating MMAs per column, whose FP32 accumulation sets the
+ * rowwise agreement with the FP64 reference (6.9e-6 / 4.9e-6 / 8.6e-6 on three parity
+ * cases, against 5.4e-6 / 4.8e-6 / 6.2e-6 with two 96-column accumulators by chunk
+ * parity and 1e-5 with one 96-column accumulator for all 200 MMAs).  Positive and
+ * negative chunks alternate while both last, so that the running sums stay near the
+ * final values (6.4e-6 against 7.0e-6 on a case with negative rows).  Tensor memory:
+ * 256 columns per CTA; at most two CTAs per SM.  Rows 81-127 of the M side and rows 81-95 / 177-191
  * of the N side read whatever lies behind the operand in the stage; they only feed
  * accumulator rows and columns that are never read.  At the end of an element the
  * builders sum the two halves into shared memory, release them to the issuer, take the
@@ -97,12 +100,12 @@ struct tc_smem {
     int vcnt[12][2][2];                 /* rows per (variable, point warp, sign) */
     long rbase[81];                     /* CSR row bases of the element matrix (elem_row_base) */
     int rsx[81], rsy[81];
-    unsigned long long full[TC_NS];         /* stage b written (288 builder arrivals) */
-    unsigned long long done[TC_NS];         /* MMAs of the chunk in stage / accumulator b completed (commit) */
-    unsigned long long freed;           /* the element's accumulators read out (288 builder arrivals) */
+    unsigned long long full[TC_NS];     /* stage b written (288 builder arrivals) */
+    unsigned long long done[TC_NS];     /* MMAs of the chunk in stage b completed (commit) */
+    unsigned long long freed;           /* the element's accumulator read out (288 builder arrivals) */
     unsigned long long drain;           /* issuer: every MMA it issued has completed */
     float gam[27 * 27];                 /* the element's geometric block (sum-factorised, FP32) */
-    int ckind[TC_NS];                       /* chunk in stage b: 0 positive rows, 1 negative rows,
+    int ckind[TC_NS];                   /* chunk in stage b: 0 positive rows, 1 negative rows,
                                            3 end of tile; + 4 on an element's first chunk */
     unsigned int tmem_base;
     int abort_flag;
@@ -591,8 +594,13 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
         /* ---- chunk loop: chunk ch is built into stage gc % 3 while the tensor core
          * works on the previous chunks; the element accumulates in tensor memory */
         const int cmain = cpos + cneg;
+        const int cmin = min(cpos, cneg);
         for (int ch = 0; ch < nch; ch++) {
             const int b = gc % TC_NS;
+            /* positive and negative chunks alternate while both last, so that the running
+             * sum in the accumulator stays near the final value */
+            const int cbk = ch < 2 * cmin ? (ch & 1) : (cpos > cneg ? 0 : 1);
+            const int cix = ch < 2 * cmin ? (ch >> 1) : cmin + (ch - 2 * cmin);
             unsigned char *st = S.stage[b];
             /* stage b holds chunk gc-3: one thread waits for its MMAs (their operand reads
              * are complete once the commit arrives); the barrier passes that on to the
@@ -609,8 +617,8 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                  * c = 3 (9 ax + 3 ay + az) + k at operand row tc_pos(c): row 8 g + 3 k + ax
                  * for g = 3 ay + az, or 72 + g for k = ax = 2, so the 9 stores sit at
                  * off0 + g * step (+ adj at g = 8) */
-                const int bucket = ch < cpos ? 0 : 1;
-                const int slot = (bucket ? ch - cpos : ch) * TC_KC + tid / 9;
+                const int bucket = cbk;
+                const int slot = cix * TC_KC + tid / 9;
                 const int j = tid / 9, k = (tid / 3) % 3, ax = tid % 3, cb = 3 * k + ax;
                 const uint32_t off0 = (uint32_t)((j >> 2) * TC_LBO + (j & 3) * 4) +
                                       (cb < 8 ? (uint32_t)cb * 16u : 9u * TC_SBO);
@@ -663,7 +671,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                 }
             }
             /* hand the chunk to the issuer */
-            const int ck = (ch < cpos ? 0 : 1) | (ch == 0 ? 4 : 0);
+            const int ck = cbk | (ch == 0 ? 4 : 0);
             if (tid == 0) S.ckind[b] = ck;
             tc_fence_proxy_async();
             tc_mbar_arrive(&S.full[b]);

@@ -10,12 +10,11 @@
  * per-point rotation that diagonalises Phi'' (its one 2x2 block), and
  * s_qv = w_q lambda_v(q).  With y = sqrt|s| x and the rows split by the sign
  * of s,  K_main = Y_+^T Y_+ - Y_-^T Y_-.  A Gram product Y^T Y needs only two
- * TF32 MMAs per k-step for FP32 accuracy: with y = y_hi + y_lo (y_hi TF32, y_lo the
+ * TF32 MMAs per k-step for FP32 accuracy: with y = y_hi + y_lo (y_hi TF32, 2 y_lo the
  * FP32 remainder, which the MMA reads truncated to TF32: an error of 2^-21 |y|),
- *   E = Y_hi^T Y_hi + 2 Y_hi^T Y_lo,   Y^T Y = (E + E^T)/2 + O(2^-21),
+ *   E = Y_hi^T Y_hi + Y_hi^T (2 Y_lo),   Y^T Y = (E + E^T)/2 + O(2^-21),
  * so the symmetric part taken at read-out recovers the cross term Y_lo^T Y_hi.
- * (Storing y_lo unrounded and unscaled, the factor 2 applied at read-out, saved two
- * instructions per operand value: 64^3 41.5 -> 39.8 ms.)
+ * (2 y_lo stored unrounded saves one conversion per operand value.)
  * The geometric block, identical for the three displacement components, is
  *   Gamma(a,b) = sum_q [grad N_a^T S grad N_b + grad N_a . (T H_b) + (T H_a) . grad N_b]
  * (geo = [[S, T], [T^T, 0]], S the 3x3 first-derivative block, T the coupling to the
@@ -39,21 +38,22 @@
  * coefficients itself, which took 46.7 -> 43.3 ms at 64^3 against a pre-pass by 96
  * threads that the other builders waited for) and hand each to the issuer through
  * an mbarrier, on which the issuer spins (no suspension: 43.3 -> 43.1 ms).  The issuer
- * runs 4 k-steps of one MMA each per chunk (M 128 rows of Y_hi, N 192 rows of Y_hi and
- * Y_lo, so that A is read once: 42.8 -> 41.5 ms against two N 96 MMAs; negate-A for
- * negative-curvature rows) and commits to the stage's mbarrier, which frees the stage
- * for the chunk three later (three stages rather than two: 43.1 -> 42.8 ms).  An
- * element accumulates Y_hi^T Y_hi in tensor-memory columns 0-95 and Y_hi^T Y_lo in
- * 96-191: about 100 accumulating MMAs per column, whose FP32 accumulation sets the
- * rowwise agreement with the FP64 reference (6.9e-6 / 4.9e-6 / 8.6e-6 on three parity
- * cases, against 5.4e-6 / 4.8e-6 / 6.2e-6 with two 96-column accumulators by chunk
- * parity and 1e-5 with one 96-column accumulator for all 200 MMAs).  Positive and
- * negative chunks alternate while both last, so that the running sums stay near the
- * final values (6.4e-6 against 7.0e-6 on a case with negative rows).  Tensor memory:
- * 256 columns per CTA; at most two CTAs per SM.  Rows 81-127 of the M side and rows 81-95 / 177-191
- * of the N side read whatever lies behind the operand in the stage; they only feed
- * accumulator rows and columns that are never read.  At the end of an element the
- * builders sum the two halves into shared memory, release them to the issuer, take the
+ * runs 4 k-steps x 2 MMAs per chunk (M 128, N 96: Y_hi^T Y_hi and Y_hi^T 2 Y_lo; negate-A
+ * for negative-curvature rows) and commits to the stage's mbarrier, which frees the
+ * stage for the chunk three later (three stages rather than two: 43.1 -> 42.8 ms).  An
+ * element accumulates in two 96-column tensor-memory accumulators by chunk parity,
+ * about 100 accumulating MMAs each, whose FP32 accumulation sets the rowwise agreement
+ * with the FP64 reference (4.5e-6 / 3.1e-6 / 6.0e-6 on three parity cases).  One M 128
+ * x N 192 MMA per k-step (Y_hi against Y_hi | Y_lo, A read once) into one 192-column
+ * accumulator measured 39.6 against 41.7 ms but 6.9e-6 / 4.9e-6 / 8.6e-6, and the 64^3
+ * Newton solve with FP32 tangents then took 14 steps instead of 7 (6 instead of 5 with
+ * the FP64 polish): tensor memory holds only one such accumulator per CTA at two CTAs
+ * per SM.  Positive and negative chunks alternate while both last, so that the running
+ * sums stay near the final values.  Tensor memory: 256 columns per CTA; at most two CTAs
+ * per SM.  Rows 81-127 of the M side and columns 81-95 of the N side read whatever
+ * lies behind the operand in the stage; they only feed accumulator rows and columns
+ * that are never read.  At the end of an element the builders sum the two
+ * accumulators into shared memory, release them to the issuer, take the
  * symmetric part, add Gamma on the k1 = k2 blocks and read-modify-write the
  * 81 x 81 values into the FP32 CSR values.
  */
@@ -68,10 +68,9 @@ namespace {
 #define TC_BAR_BLD 1           /* named barrier of the builder warps */
 #define TC_STAGE 24576         /* bytes per operand stage */
 #define TC_NS 3                /* operand stages */
-#define TC_MAIN_LO 12288       /* Y_lo: B operand rows 96-191 (Y_hi rows 0-80 in groups 0-10) */
+#define TC_MAIN_LO 12288       /* 2 Y_lo after Y_hi (groups 0-10, 81 rows) and a free group */
 #define TC_TMEM_COLS 256u
-#define TC_COL_MAIN 0u         /* the element-matrix accumulator: Y_hi^T Y_hi in columns 0-95,
-                                  Y_hi^T Y_lo in 96-191 */
+#define TC_COL_MAIN 0u         /* two 96-column element-matrix accumulators */
 
 /* float point data per Gauss point */
 #define TP_F 0      /* F[k][J], 9 */
@@ -198,13 +197,13 @@ __device__ __forceinline__ int tc_pos(int c)
     return cb < 8 ? 8 * g + cb : 72 + g;
 }
 
-/* y = hi + lo: hi rounded to TF32 (exact in the MMA), lo = y - hi stored as FP32 (exact);
- * the MMA reads lo truncated to TF32, an error of at most 2^-21 |y| */
+/* y = hi + lo: hi rounded to TF32 (exact in the MMA), 2 lo = 2 (y - hi) stored as FP32
+ * (exact); the MMA reads it truncated to TF32, an error of at most 2^-21 |y| */
 __device__ __forceinline__ void st_pair(unsigned char *hi_base, unsigned char *lo_base, uint32_t off, float y)
 {
     const float h = tc_tf32(y);
     *reinterpret_cast<float *>(hi_base + off) = h;
-    *reinterpret_cast<float *>(lo_base + off) = y - h;
+    *reinterpret_cast<float *>(lo_base + off) = 2.f * (y - h);
 }
 
 /* pipeline state of a thread, carried across the tiles its CTA processes: the
@@ -266,8 +265,8 @@ __device__ __forceinline__ void tc_release(tc_smem<TE> &S, tc_state &Q, int *sta
 }
 
 /* the issuer warp for one tile: wait for each built chunk and issue its MMAs.
- * An element's chunks accumulate in one tensor-memory accumulator of 192 columns
- * (Y_hi^T Y_hi | Y_hi^T Y_lo); negative-curvature chunks use the negate-A form.
+ * An element's chunks accumulate in two tensor-memory accumulators by chunk parity
+ * (96 columns each); negative-curvature chunks use the negate-A form.
  * Before the first MMA of an element the issuer waits until the builders have
  * read the previous element's accumulator.  Ends
  * at the builders' end-of-tile chunk; before returning it waits (bounded) until
@@ -278,7 +277,7 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
     const int lane = threadIdx.x & 31;
     const volatile int *abort = &S.abort_flag;
     bool ok = !*abort;
-    bool started = false;   /* the accumulator holds this element's sums */
+    bool started[2] = {false, false};   /* accumulator b holds this element's sums */
     while (ok) {
         const int b = Q.gc % TC_NS;
         if (lane == 0) ok = tc_mbar_spin_abortable(&S.full[b], Q.ph_full[b], abort);
@@ -298,21 +297,23 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
                 if (!ok) break;
             }
             Q.nelem++;
-            started = false;
+            started[0] = started[1] = false;
         }
         const int kind = ck & 3;
-        const uint32_t acc0 = started ? 1u : 0u;
-        started = true;
+        const int acc = Q.gc & 1;   /* accumulator by chunk parity */
+        const uint32_t acc0 = started[acc] ? 1u : 0u;
+        started[acc] = true;
         if (lane == 0) {
             tc_fence_after_sync();
             const uint32_t sb = tc_smem_u32(S.stage[b]);
-            const uint32_t idm = kind == 0 ? tc_idesc_tf32(128, 192) : tc_idesc_tf32(128, 192, true);
-            const uint32_t d = Q.tmem + TC_COL_MAIN;
+            const uint32_t idm = kind == 0 ? tc_idesc_tf32(128, 96) : tc_idesc_tf32(128, 96, true);
+            const uint32_t d = Q.tmem + TC_COL_MAIN + (uint32_t)acc * 96u;
 #pragma unroll
             for (int kk = 0; kk < 4; kk++) {
-                /* A: Y_hi (rows 0-127); B: Y_hi and Y_lo (rows 0-191) of the same stage */
                 const uint64_t ah = tc_sdesc(sb + kk * TC_KSTEP_BYTES);
-                tc_mma_tf32(d, ah, ah, idm, kk == 0 ? acc0 : 1u);
+                const uint64_t bl = tc_sdesc(sb + TC_MAIN_LO + kk * TC_KSTEP_BYTES);
+                tc_mma_tf32(d, ah, ah, idm, kk == 0 ? acc0 : 1u);   /* Y_hi^T Y_hi */
+                tc_mma_tf32(d, ah, bl, idm, 1u);                    /* Y_hi^T 2 Y_lo */
             }
             tc_commit(&S.done[b]);
         }
@@ -329,11 +330,10 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
     __syncwarp();
 }
 
-/* The element matrix E = Y_hi^T Y_hi + 2 Y_hi^T Y_lo (accumulator columns c and 96 + c)
- * into shared memory (FP32, round to nearest): rows by warps 0-2 / 4-6 (TMEM lanes =
- * rows 0-95, columns 0-47 / 48-95).  used: the accumulator holds this element's sums
- * (none: zeros). */
-__device__ __forceinline__ void tc_readout(uint32_t tmem, bool used, int warp, int lane, float *E)
+/* Sum the element's two accumulators into shared memory (FP32, round to nearest):
+ * element-matrix rows by warps 0-2 / 4-6 (TMEM lanes = rows 0-95, columns 0-47 /
+ * 48-95).  used[b]: accumulator b holds this element's sums (none: zeros). */
+__device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2], int warp, int lane, float *E)
 {
     if (warp < 8) {
         if (warp == 3 || warp == 7) return;   /* lanes 96-127: rows beyond 80 */
@@ -345,12 +345,12 @@ __device__ __forceinline__ void tc_readout(uint32_t tmem, bool used, int warp, i
 #pragma unroll
             for (int i = 0; i < 16; i++) s[i] = 0.f;
 #pragma unroll
-            for (int b = 0; b < 2; b++) {   /* Y_hi^T Y_hi, then 2 Y_hi^T Y_lo */
-                if (!used) continue;   /* warp-uniform */
+            for (int b = 0; b < 2; b++) {
+                if (!used[b]) continue;   /* warp-uniform */
                 float v[16];
                 tc_ld16(tmem + ((uint32_t)lb << 16) + TC_COL_MAIN + (uint32_t)b * 96u + (uint32_t)c0, v);
 #pragma unroll
-                for (int i = 0; i < 16; i++) s[i] += b ? 2.f * v[i] : v[i];
+                for (int i = 0; i < 16; i++) s[i] += v[i];
             }
             if (row < 81)
 #pragma unroll
@@ -690,7 +690,10 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
             if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) aborted = true;
         }
         if (aborted) break;
-        const bool used = cmain > 0;
+        const int g0 = gc - nch;   /* the element's first chunk */
+        bool used[2];
+        used[g0 & 1] = cmain > 0;
+        used[(g0 + 1) & 1] = cmain > 1;
         float *E = reinterpret_cast<float *>(&S.stage[0][0]);   /* [81][81] */
         tc_fence_after_sync();
         tc_readout(tmem, used, warp, lane, E);

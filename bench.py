@@ -796,8 +796,8 @@ def run_ours(args):
                                "MEASURED_PEAKS.json has no FP64 figure"}
     res_tf = nel * RES_ALG_FLOPS / (k64[0] * 1e-3) / 1e12 if k64[0] > 0 else None
     # FP32 (mixed) tangent on tcgen05: per element 768 curvature rows in chunks of 32 (about 25 chunks,
-    # 8 MMAs M128 x N96 x K8 each) plus 12 geometric chunks of 12 MMAs M128 x N32 x K8
-    tc_exec_per_el = 25 * 8 * 2 * 128 * 96 * 8 + 12 * 12 * 2 * 128 * 32 * 8
+    # 8 MMAs M128 x N96 x K8 each); the geometric block runs on the FP32 FMA pipe
+    tc_exec_per_el = 25 * 8 * 2 * 128 * 96 * 8
     tan32_ms = k32[2]
     nl32 = max(k32[5], 1)
     roofline_mixed = {"bound": "tensor", "pipe": "TF32 tcgen05 (hi/lo split, FP32 accumulation)",

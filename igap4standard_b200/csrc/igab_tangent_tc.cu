@@ -10,7 +10,7 @@
  * per-point rotation that diagonalises Phi'' (its one 2x2 block), and
  * s_qv = w_q lambda_v(q).  With y = sqrt|s| x and the rows split by the sign
  * of s,  K_main = Y_+^T Y_+ - Y_-^T Y_-.  A Gram product Y^T Y needs only two
- * TF32 MMAs per k-step for FP32 accuracy: with y = y_hi + y_lo (y_hi TF32, 2 y_lo the
+ * TF32 products per k-step for FP32 accuracy: with y = y_hi + y_lo (y_hi TF32, 2 y_lo the
  * FP32 remainder, which the MMA reads truncated to TF32: an error of 2^-21 |y|),
  *   E = Y_hi^T Y_hi + Y_hi^T (2 Y_lo),   Y^T Y = (E + E^T)/2 + O(2^-21),
  * so the symmetric part taken at read-out recovers the cross term Y_lo^T Y_hi.
@@ -38,22 +38,25 @@
  * coefficients itself, which took 46.7 -> 43.3 ms at 64^3 against a pre-pass by 96
  * threads that the other builders waited for) and hand each to the issuer through
  * an mbarrier, on which the issuer spins (no suspension: 43.3 -> 43.1 ms).  The issuer
- * runs 4 k-steps x 2 MMAs per chunk (M 128, N 96: Y_hi^T Y_hi and Y_hi^T 2 Y_lo; negate-A
- * for negative-curvature rows) and commits to the stage's mbarrier, which frees the
- * stage for the chunk three later (three stages rather than two: 43.1 -> 42.8 ms).  An
- * element accumulates in two 96-column tensor-memory accumulators by chunk parity,
- * about 100 accumulating MMAs each, whose FP32 accumulation sets the rowwise agreement
- * with the FP64 reference (4.5e-6 / 3.1e-6 / 6.0e-6 on three parity cases).  One M 128
- * x N 192 MMA per k-step (Y_hi against Y_hi | Y_lo, A read once) into one 192-column
- * accumulator measured 39.6 against 41.7 ms but 6.9e-6 / 4.9e-6 / 8.6e-6, and the 64^3
- * Newton solve with FP32 tangents then took 14 steps instead of 7 (6 instead of 5 with
- * the FP64 polish): tensor memory holds only one such accumulator per CTA at two CTAs
- * per SM.  Positive and negative chunks alternate while both last, so that the running
- * sums stay near the final values.  Tensor memory: 256 columns per CTA; at most two CTAs
- * per SM.  Rows 81-127 of the M side and columns 81-95 of the N side read whatever
- * lies behind the operand in the stage; they only feed accumulator rows and columns
- * that are never read.  At the end of an element the builders sum the two
- * accumulators into shared memory, release them to the issuer, take the
+ * runs 4 k-steps of one MMA each per chunk (M 128: Y_hi; N 192: the whole stage) and
+ * commits to the stage's mbarrier, which frees the stage for the chunk three later
+ * (three stages rather than two: 43.1 -> 42.8 ms); negative-curvature rows use the
+ * negate-A form.  Even chunks hold Y_hi then 2 Y_lo, odd chunks 2 Y_lo then Y_hi, so the
+ * 192 accumulator columns take Y_hi^T Y_hi and Y_hi^T 2 Y_lo alternately: each half
+ * sums half of each product (about 100 accumulating MMAs, half the magnitude), and the
+ * read-out adds the halves.  The FP32 accumulation sets the rowwise agreement with the
+ * FP64 reference: 4.4e-6 / 3.0e-6 / 5.9e-6 on three parity cases (41.2 ms at 64^3).
+ * Two N 96 MMAs per k-step into two accumulators by chunk parity gave 4.5e-6 / 3.1e-6 /
+ * 6.0e-6 at 41.7 ms; one N 192 MMA with Y_hi^T Y_hi always in columns 0-95 gave 39.6 ms
+ * but 6.9e-6 / 4.9e-6 / 8.6e-6 (each column one FP32 sum over the whole element), and
+ * the 64^3 Newton solve with FP32 tangents then took 14 steps instead of 7 (6 instead
+ * of 5 with the FP64 polish).  Positive and negative chunks alternate while both last,
+ * so that the running sums stay near the final values.  Tensor memory: 256 columns per
+ * CTA; at most two CTAs per SM.  Rows 81-127 of the M side (for odd chunks rows 96-127
+ * lie in the next stage or behind the stages) and columns 81-95 / 177-191 of the N side
+ * read data that only feed accumulator rows and columns that are never read.  At the
+ * end of an element the builders sum the two halves into shared memory, release the
+ * accumulator to the issuer, take the
  * symmetric part, add Gamma on the k1 = k2 blocks and read-modify-write the
  * 81 x 81 values into the FP32 CSR values.
  */
@@ -68,9 +71,10 @@ namespace {
 #define TC_BAR_BLD 1           /* named barrier of the builder warps */
 #define TC_STAGE 24576         /* bytes per operand stage */
 #define TC_NS 3                /* operand stages */
-#define TC_MAIN_LO 12288       /* 2 Y_lo after Y_hi (groups 0-10, 81 rows) and a free group */
+#define TC_MAIN_LO 12288       /* the second operand half (B rows 96-191): 2 Y_lo in even chunks,
+                                  Y_hi in odd ones; each half 81 rows and 15 free */
 #define TC_TMEM_COLS 256u
-#define TC_COL_MAIN 0u         /* two 96-column element-matrix accumulators */
+#define TC_COL_MAIN 0u         /* the 192-column element-matrix accumulator */
 
 /* float point data per Gauss point */
 #define TP_F 0      /* F[k][J], 9 */
@@ -265,8 +269,9 @@ __device__ __forceinline__ void tc_release(tc_smem<TE> &S, tc_state &Q, int *sta
 }
 
 /* the issuer warp for one tile: wait for each built chunk and issue its MMAs.
- * An element's chunks accumulate in two tensor-memory accumulators by chunk parity
- * (96 columns each); negative-curvature chunks use the negate-A form.
+ * An element's chunks accumulate in one tensor-memory accumulator of 192 columns
+ * (A = the chunk's Y_hi half, B = the whole stage); negative-curvature chunks use the
+ * negate-A form.
  * Before the first MMA of an element the issuer waits until the builders have
  * read the previous element's accumulator.  Ends
  * at the builders' end-of-tile chunk; before returning it waits (bounded) until
@@ -277,7 +282,7 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
     const int lane = threadIdx.x & 31;
     const volatile int *abort = &S.abort_flag;
     bool ok = !*abort;
-    bool started[2] = {false, false};   /* accumulator b holds this element's sums */
+    bool started = false;   /* the accumulator holds this element's sums */
     while (ok) {
         const int b = Q.gc % TC_NS;
         if (lane == 0) ok = tc_mbar_spin_abortable(&S.full[b], Q.ph_full[b], abort);
@@ -297,23 +302,23 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
                 if (!ok) break;
             }
             Q.nelem++;
-            started[0] = started[1] = false;
+            started = false;
         }
         const int kind = ck & 3;
-        const int acc = Q.gc & 1;   /* accumulator by chunk parity */
-        const uint32_t acc0 = started[acc] ? 1u : 0u;
-        started[acc] = true;
+        const int odd = Q.gc & 1;   /* odd chunks: 2 Y_lo first, then Y_hi, in the stage */
+        const uint32_t acc0 = started ? 1u : 0u;
+        started = true;
         if (lane == 0) {
             tc_fence_after_sync();
             const uint32_t sb = tc_smem_u32(S.stage[b]);
-            const uint32_t idm = kind == 0 ? tc_idesc_tf32(128, 96) : tc_idesc_tf32(128, 96, true);
-            const uint32_t d = Q.tmem + TC_COL_MAIN + (uint32_t)acc * 96u;
+            const uint32_t idm = kind == 0 ? tc_idesc_tf32(128, 192) : tc_idesc_tf32(128, 192, true);
+            const uint32_t d = Q.tmem + TC_COL_MAIN;
+            const uint32_t sa = sb + (odd ? (uint32_t)TC_MAIN_LO : 0u);
 #pragma unroll
             for (int kk = 0; kk < 4; kk++) {
-                const uint64_t ah = tc_sdesc(sb + kk * TC_KSTEP_BYTES);
-                const uint64_t bl = tc_sdesc(sb + TC_MAIN_LO + kk * TC_KSTEP_BYTES);
-                tc_mma_tf32(d, ah, ah, idm, kk == 0 ? acc0 : 1u);   /* Y_hi^T Y_hi */
-                tc_mma_tf32(d, ah, bl, idm, 1u);                    /* Y_hi^T 2 Y_lo */
+                /* A: Y_hi; B: the whole stage, 192 rows (Y_hi | 2 Y_lo, or 2 Y_lo | Y_hi) */
+                tc_mma_tf32(d, tc_sdesc(sa + kk * TC_KSTEP_BYTES), tc_sdesc(sb + kk * TC_KSTEP_BYTES), idm,
+                            kk == 0 ? acc0 : 1u);
             }
             tc_commit(&S.done[b]);
         }
@@ -330,10 +335,11 @@ __device__ __forceinline__ void tc_issue(tc_smem<TE> &S, tc_state &Q)
     __syncwarp();
 }
 
-/* Sum the element's two accumulators into shared memory (FP32, round to nearest):
- * element-matrix rows by warps 0-2 / 4-6 (TMEM lanes = rows 0-95, columns 0-47 /
- * 48-95).  used[b]: accumulator b holds this element's sums (none: zeros). */
-__device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2], int warp, int lane, float *E)
+/* Sum the two 96-column halves of the element's accumulator into shared memory
+ * (FP32, round to nearest): element-matrix rows by warps 0-2 / 4-6 (TMEM lanes = rows
+ * 0-95, columns 0-47 / 48-95).  used: the accumulator holds this element's sums (none:
+ * zeros). */
+__device__ __forceinline__ void tc_readout(uint32_t tmem, bool used, int warp, int lane, float *E)
 {
     if (warp < 8) {
         if (warp == 3 || warp == 7) return;   /* lanes 96-127: rows beyond 80 */
@@ -346,7 +352,7 @@ __device__ __forceinline__ void tc_readout(uint32_t tmem, const bool (&used)[2],
             for (int i = 0; i < 16; i++) s[i] = 0.f;
 #pragma unroll
             for (int b = 0; b < 2; b++) {
-                if (!used[b]) continue;   /* warp-uniform */
+                if (!used) continue;   /* warp-uniform */
                 float v[16];
                 tc_ld16(tmem + ((uint32_t)lb << 16) + TC_COL_MAIN + (uint32_t)b * 96u + (uint32_t)c0, v);
 #pragma unroll
@@ -624,7 +630,9 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
                                       (cb < 8 ? (uint32_t)cb * 16u : 9u * TC_SBO);
                 const uint32_t step = cb < 8 ? (uint32_t)TC_SBO : 16u;
                 const uint32_t adj8 = cb < 8 ? 0u : (uint32_t)(TC_SBO - 128);
-                unsigned char *hi = st, *lo = st + TC_MAIN_LO;
+                /* odd chunks put 2 Y_lo first: the MMA's 192 columns then take Y_hi^T Y_hi and
+                 * Y_hi^T 2 Y_lo alternately, so each half of the accumulator sums half of each */
+                unsigned char *hi = st + ((gc & 1) ? TC_MAIN_LO : 0), *lo = st + ((gc & 1) ? 0 : TC_MAIN_LO);
                 if (slot < (bucket ? nneg : npos)) {
                     const int id = S.map[bucket][slot], q = id / 12, v = id - 12 * q;
                     const int qx = q & 3, qy = (q >> 2) & 3, qz = q >> 4;
@@ -690,10 +698,7 @@ __device__ __forceinline__ void tc_tile(const igab_geom &g, const tile_t &Tl, co
             if (!tc_bar_and(TC_BAR_BLD, TCN_BLD, ok)) aborted = true;
         }
         if (aborted) break;
-        const int g0 = gc - nch;   /* the element's first chunk */
-        bool used[2];
-        used[g0 & 1] = cmain > 0;
-        used[(g0 + 1) & 1] = cmain > 1;
+        const bool used = cmain > 0;
         float *E = reinterpret_cast<float *>(&S.stage[0][0]);   /* [81][81] */
         tc_fence_after_sync();
         tc_readout(tmem, used, warp, lane, E);
